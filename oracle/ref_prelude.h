@@ -1,0 +1,13 @@
+/* Host-C++ prelude that lets the reference's CUDA sources compile as plain C++ so that they
+ * can be run on the CPU as a parity oracle (test infrastructure only).  A CUDA "launch" is
+ * emulated by ref_launch.cpp, which walks blockIdx/threadIdx one thread at a time. */
+#pragma once
+#include <cmath>
+#include <algorithm>
+using std::fmax; using std::fmin; using std::sqrt; using std::acos;
+#define __global__
+#define __device__
+#define __forceinline__ inline
+#define __restrict__
+struct hb_dim3 { long long x, y, z; };
+extern hb_dim3 blockIdx, threadIdx, blockDim, gridDim;

@@ -1,0 +1,324 @@
+"""FP64 CPU oracle for the HEALPix SHT hot path (Python half).
+
+TEST INFRASTRUCTURE ONLY: the arbiter the CUDA path is checked against.  Only tests/,
+__graft_entry__.smoke() and bench.py's cpu_baseline leg may import this module; the
+product package (hellblast_b200) never does.
+
+The Legendre work is done by the C half (oracle/sht_oracle.c -> oracle/liborc.so, OpenMP).
+This file restates the per-ring FFT step of the reference with numpy's pocketfft:
+
+* ``sht_raw.py:38-43`` / ``sht_fallback.py:51-55``: ``F_r = fft(f_r) / nphi_r``, then the
+  contraction weights ``weights_dz`` (``sht_raw.py:50-53``) and the 2*pi factor
+  (``sht_fallback.py:63``).  Here the per-pixel quadrature weight is ``2*pi*w_r/nphi_r``.
+* corrected relative to the reference (each correction can be switched off by ``ref_compat``):
+  the per-ring phase ``exp(-i m phi0_r)`` and the m-aliasing fold ``m -> m mod nphi_r``
+  (the reference reads bin m for m < nphi and uses 0 for m >= nphi, ``sht_raw.py:51``).
+* ``isht.py:15-25`` (synthesis) corrected the same way: ``f(phi_j) = Re sum_m c_m G(m)
+  exp(i m phi_j)`` with ``c_0 = 1, c_m = 2``, folded onto the ring's nphi bins.
+
+alm layout: healpy m-major, ``idx(l, m) = m*(2*lmax+1-m)//2 + l``.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+
+
+def _lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(_HERE, "liborc.so")
+        if not os.path.exists(path):
+            build()
+        lib = ctypes.CDLL(path)
+        D = ctypes.POINTER(ctypes.c_double)
+        I32 = ctypes.POINTER(ctypes.c_int32)
+        I64 = ctypes.POINTER(ctypes.c_int64)
+        lib.orc_ring_tables.argtypes = [ctypes.c_int64, ctypes.c_int, D, D, I32, D, I64, D]
+        lib.orc_lambda_lm.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int64, D, D, D]
+        lib.orc_legendre_analysis.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int64, D, D, D, D]
+        lib.orc_legendre_synthesis.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int64, D, D, D, D]
+        lib.orc_spin2_lambda.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int64, D, D, D, D]
+        lib.orc_spin2_analysis.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int64, D, D, D, D, D, D]
+        lib.orc_spin2_synthesis.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int64, D, D, D, D, D, D]
+        lib.orc_alm2cl.argtypes = [ctypes.c_int, ctypes.c_int, D, D, D]
+        for f in (lib.orc_ring_tables, lib.orc_lambda_lm, lib.orc_legendre_analysis,
+                  lib.orc_legendre_synthesis, lib.orc_spin2_lambda, lib.orc_spin2_analysis,
+                  lib.orc_spin2_synthesis, lib.orc_alm2cl):
+            f.restype = None
+        _LIB = lib
+    return _LIB
+
+
+def build() -> None:
+    """Compile oracle/liborc.so (gcc, OpenMP)."""
+    import subprocess
+    subprocess.run(["make", "-s", "-C", _HERE, "liborc.so"], check=True)
+
+
+def _p(a, ct=ctypes.c_double):
+    return a.ctypes.data_as(ctypes.POINTER(ct))
+
+
+# ----------------------------------------------------------------------------- layout
+def alm_size(lmax: int, mmax: int | None = None) -> int:
+    mmax = lmax if mmax is None else mmax
+    return mmax * (2 * lmax + 1 - mmax) // 2 + lmax + 1
+
+
+def alm_index(lmax: int, l, m):
+    return m * (2 * lmax + 1 - m) // 2 + l
+
+
+def healpy_to_ref(alm: np.ndarray, lmax: int, mmax: int | None = None) -> np.ndarray:
+    """healpy m-major -> the reference's l(l+1)+m layout (alm_ops.py:4-5), length (lmax+1)^2."""
+    mmax = lmax if mmax is None else mmax
+    out = np.zeros((lmax + 1) ** 2, dtype=np.complex128)
+    for m in range(mmax + 1):
+        l = np.arange(m, lmax + 1)
+        out[l * (l + 1) + m] = alm[alm_index(lmax, l, m)]
+    return out
+
+
+def ref_to_healpy(alm_ref: np.ndarray, lmax: int, mmax: int | None = None) -> np.ndarray:
+    mmax = lmax if mmax is None else mmax
+    out = np.zeros(alm_size(lmax, mmax), dtype=np.complex128)
+    for m in range(mmax + 1):
+        l = np.arange(m, lmax + 1)
+        out[alm_index(lmax, l, m)] = alm_ref[l * (l + 1) + m]
+    return out
+
+
+# ----------------------------------------------------------------------------- geometry
+def ring_tables(nside: int, phi0: str = "healpix") -> dict:
+    """HEALPix RING geometry (ring_tables_healpix.cu:14-51, ring_tables.py:39-40)."""
+    nr = 4 * nside - 1
+    z = np.empty(nr); th = np.empty(nr); ph = np.empty(nr); ze = np.empty(nr + 1)
+    nphi = np.empty(nr, dtype=np.int32); rs = np.empty(nr + 1, dtype=np.int64)
+    _lib().orc_ring_tables(nside, 1 if phi0 == "healpix" else 0, _p(z), _p(th), _p(nphi, ctypes.c_int32),
+                           _p(ph), _p(rs, ctypes.c_int64), _p(ze))
+    i = np.arange(1, nr + 1, dtype=np.float64)
+    ip = np.minimum(i, 4 * nside - i)
+    polar = ip < nside
+    t = ip * ip / (3.0 * nside * nside)           # 1-|z| exactly on the polar caps
+    sin_theta = np.where(polar, np.sqrt(t * (2.0 - t)), np.sqrt((1.0 - z) * (1.0 + z)))
+    return dict(nside=nside, nr=nr, npix=int(rs[-1]), z=z, theta=th, nphi=nphi, phi0=ph,
+                ring_start=rs, z_edges=ze, weights_dz=ze[:-1] - ze[1:], x=z.copy(),
+                sin_theta=sin_theta)
+
+
+def generic_geometry(theta, nphi, phi0=None, weights=None) -> dict:
+    theta = np.asarray(theta, dtype=np.float64)
+    nphi = np.asarray(nphi, dtype=np.int32)
+    nr = theta.size
+    rs = np.zeros(nr + 1, dtype=np.int64)
+    rs[1:] = np.cumsum(nphi)
+    return dict(nr=nr, npix=int(rs[-1]), theta=theta, nphi=nphi,
+                phi0=np.zeros(nr) if phi0 is None else np.asarray(phi0, dtype=np.float64),
+                ring_start=rs, weights_dz=None if weights is None else np.asarray(weights, dtype=np.float64),
+                x=np.cos(theta), sin_theta=np.sin(theta))
+
+
+def uniform_weights(geom: dict) -> np.ndarray:
+    """Per-ring w such that 2*pi*w_r/nphi_r = 4*pi/npix (healpy's default quadrature)."""
+    return 2.0 * geom["nphi"].astype(np.float64) / geom["npix"]
+
+
+# ----------------------------------------------------------------------------- ring FFTs
+def ring_analysis(maps: np.ndarray, geom: dict, mmax: int, weights=None, phase=True, fold=True,
+                  scale: float = 2.0 * math.pi, mdouble: bool = False) -> np.ndarray:
+    """F[m, r] = scale * w_r / nphi_r * exp(-i m phi0_r) * DFT_r[m mod nphi_r].
+
+    With ``fold=False`` bins m >= nphi_r are zero (reference behaviour, sht_raw.py:51).
+    ``weights=None`` means unit per-pixel weights (scale/nphi factor dropped); used by adjoints.
+    ``mdouble`` multiplies m>0 by 2 (adjoint of the real-field synthesis).
+    """
+    nr = geom["nr"]
+    F = np.zeros((mmax + 1, nr), dtype=np.complex128)
+    m = np.arange(mmax + 1)
+    for r in range(nr):
+        n = int(geom["nphi"][r]); s = int(geom["ring_start"][r])
+        R = np.fft.rfft(np.asarray(maps[s:s + n], dtype=np.float64))
+        k = m % n
+        D = np.where(k <= n // 2, R[np.minimum(k, n // 2)], np.conj(R[np.minimum(n - k, n // 2)]))
+        if not fold:
+            D = np.where(m < n, D, 0.0)
+        if phase:
+            D = D * np.exp(-1j * m * geom["phi0"][r])
+        if weights is not None:
+            D = D * (scale * weights[r] / n)
+        if mdouble:
+            D = D * np.where(m > 0, 2.0, 1.0)
+        F[:, r] = D
+    return F
+
+
+def ring_synthesis(G: np.ndarray, geom: dict, weights=None, phase=True, mdouble=True,
+                   scale: float = 2.0 * math.pi) -> np.ndarray:
+    """f_r(phi_j) = Re sum_m c_m G[m, r] exp(i m phi_j), folded onto nphi_r bins.
+
+    ``mdouble=True`` uses c_0 = 1, c_m = 2 (real field); False uses c_m = 1 (adjoint of the
+    weighted analysis).  ``weights`` multiplies the result by scale*w_r/nphi_r (adjoint only).
+    """
+    mmax = G.shape[0] - 1
+    out = np.zeros(int(geom["npix"]))
+    m = np.arange(mmax + 1)
+    c = np.where(m > 0, 2.0, 1.0) if mdouble else np.ones(mmax + 1)
+    for r in range(geom["nr"]):
+        n = int(geom["nphi"][r]); s = int(geom["ring_start"][r])
+        T = c * G[:, r]
+        if phase:
+            T = T * np.exp(1j * m * geom["phi0"][r])
+        k = m % n
+        X = np.zeros(n // 2 + 1, dtype=np.complex128)
+        edge = (k == 0) | (k * 2 == n)
+        np.add.at(X, k[edge], T[edge].real)
+        lo = (~edge) & (2 * k < n)
+        np.add.at(X, k[lo], 0.5 * T[lo])
+        hi = (~edge) & (2 * k > n)
+        np.add.at(X, n - k[hi], 0.5 * np.conj(T[hi]))
+        f = np.fft.irfft(X, n) * n
+        if weights is not None:
+            f = f * (scale * weights[r] / n)
+        out[s:s + n] = f
+    return out
+
+
+# ----------------------------------------------------------------------------- transforms
+def _c(a):
+    return np.ascontiguousarray(a)
+
+
+def legendre_analysis(F: np.ndarray, geom: dict, lmax: int) -> np.ndarray:
+    mmax = F.shape[0] - 1
+    Fi = _c(F.astype(np.complex128)).view(np.float64)
+    alm = np.zeros(alm_size(lmax, mmax), dtype=np.complex128)
+    _lib().orc_legendre_analysis(lmax, mmax, geom["nr"], _p(_c(geom["x"])), _p(_c(geom["sin_theta"])),
+                                 _p(Fi), _p(alm.view(np.float64)))
+    return alm
+
+
+def legendre_synthesis(alm: np.ndarray, geom: dict, lmax: int, mmax: int) -> np.ndarray:
+    G = np.zeros((mmax + 1, geom["nr"]), dtype=np.complex128)
+    a = _c(np.asarray(alm, dtype=np.complex128))
+    _lib().orc_legendre_synthesis(lmax, mmax, geom["nr"], _p(_c(geom["x"])), _p(_c(geom["sin_theta"])),
+                                  _p(a.view(np.float64)), _p(G.view(np.float64)))
+    return G
+
+
+def map2alm(maps, geom: dict, lmax: int, mmax: int | None = None, weights=None, phase=True,
+            fold=True, scale=2.0 * math.pi) -> np.ndarray:
+    """a_lm = sum_pixels (scale*w_r/nphi_r) f lambda_lm e^{-i m phi} (healpy layout)."""
+    mmax = lmax if mmax is None else mmax
+    w = geom["weights_dz"] if weights is None else weights
+    F = ring_analysis(maps, geom, mmax, weights=w, phase=phase, fold=fold, scale=scale)
+    return legendre_analysis(F, geom, lmax)
+
+
+def alm2map(alm, geom: dict, lmax: int, mmax: int | None = None, phase=True) -> np.ndarray:
+    mmax = lmax if mmax is None else mmax
+    G = legendre_synthesis(alm, geom, lmax, mmax)
+    return ring_synthesis(G, geom, phase=phase)
+
+
+def map2alm_ref_compat(maps, geom: dict, lmax: int, mmax: int | None = None, flavour: str = "fallback"):
+    """The reference's own conventions (sht_raw.py:30-57 / sht_fallback.py:36-65): no phi0 phase,
+    no alias fold, 2*pi only in the fallback flavour, and sht_raw's m <= 2*nside cut (its
+    ``mmax_eff``, sht_raw.py:43).  Returned in healpy layout."""
+    mmax = lmax if mmax is None else mmax
+    scale = 2.0 * math.pi if flavour == "fallback" else 1.0
+    alm = map2alm(maps, geom, lmax, mmax, phase=False, fold=False, scale=scale)
+    if flavour == "raw":
+        mcut = min(mmax, int(np.max(geom["nphi"])) // 2)
+        for m in range(mcut + 1, mmax + 1):
+            alm[alm_index(lmax, np.arange(m, lmax + 1), m)] = 0.0
+    return alm
+
+
+def map2alm_adjoint(galm, geom: dict, lmax: int, mmax: int | None = None, weights=None, phase=True):
+    """Exact transpose of map2alm (real map -> complex alm, Re/Im as independent outputs)."""
+    mmax = lmax if mmax is None else mmax
+    w = geom["weights_dz"] if weights is None else weights
+    G = legendre_synthesis(galm, geom, lmax, mmax)
+    return ring_synthesis(G, geom, weights=w, phase=phase, mdouble=False)
+
+
+def alm2map_adjoint(gmap, geom: dict, lmax: int, mmax: int | None = None, phase=True):
+    """Exact transpose of alm2map (includes the m>0 real-field doubling)."""
+    mmax = lmax if mmax is None else mmax
+    F = ring_analysis(gmap, geom, mmax, weights=None, phase=phase, mdouble=True)
+    return legendre_analysis(F, geom, lmax)
+
+
+def map2alm_spin2(Q, U, geom: dict, lmax: int, mmax: int | None = None, weights=None, phase=True):
+    mmax = lmax if mmax is None else mmax
+    w = geom["weights_dz"] if weights is None else weights
+    Qf = _c(ring_analysis(Q, geom, mmax, weights=w, phase=phase))
+    Uf = _c(ring_analysis(U, geom, mmax, weights=w, phase=phase))
+    n = alm_size(lmax, mmax)
+    E = np.zeros(n, dtype=np.complex128); B = np.zeros(n, dtype=np.complex128)
+    _lib().orc_spin2_analysis(lmax, mmax, geom["nr"], _p(_c(geom["x"])), _p(_c(geom["theta"])),
+                              _p(Qf.view(np.float64)), _p(Uf.view(np.float64)),
+                              _p(E.view(np.float64)), _p(B.view(np.float64)))
+    return E, B
+
+
+def alm2map_spin2(E, B, geom: dict, lmax: int, mmax: int | None = None, phase=True):
+    mmax = lmax if mmax is None else mmax
+    Qg = np.zeros((mmax + 1, geom["nr"]), dtype=np.complex128)
+    Ug = np.zeros_like(Qg)
+    E = _c(np.asarray(E, dtype=np.complex128)); B = _c(np.asarray(B, dtype=np.complex128))
+    _lib().orc_spin2_synthesis(lmax, mmax, geom["nr"], _p(_c(geom["x"])), _p(_c(geom["theta"])),
+                               _p(E.view(np.float64)), _p(B.view(np.float64)),
+                               _p(Qg.view(np.float64)), _p(Ug.view(np.float64)))
+    return ring_synthesis(Qg, geom, phase=phase), ring_synthesis(Ug, geom, phase=phase)
+
+
+def lambda_lm(lmax: int, m: int, x, sin_theta) -> np.ndarray:
+    x = _c(np.asarray(x, dtype=np.float64)); s = _c(np.asarray(sin_theta, dtype=np.float64))
+    out = np.zeros((x.size, lmax + 1))
+    _lib().orc_lambda_lm(lmax, m, x.size, _p(x), _p(s), _p(out))
+    return out
+
+
+def spin2_lambda(lmax: int, m: int, theta):
+    th = _c(np.asarray(theta, dtype=np.float64)); x = np.cos(th)
+    p2 = np.zeros((th.size, lmax + 1)); m2 = np.zeros_like(p2)
+    _lib().orc_spin2_lambda(lmax, m, th.size, _p(x), _p(th), _p(p2), _p(m2))
+    return p2, m2
+
+
+def alm2cl(alm1, lmax: int, mmax: int | None = None, alm2=None) -> np.ndarray:
+    mmax = lmax if mmax is None else mmax
+    a1 = _c(np.asarray(alm1, dtype=np.complex128))
+    a2 = None if alm2 is None else _c(np.asarray(alm2, dtype=np.complex128))
+    cl = np.zeros(lmax + 1)
+    _lib().orc_alm2cl(lmax, mmax, _p(a1.view(np.float64)),
+                      None if a2 is None else _p(a2.view(np.float64)), _p(cl))
+    return cl
+
+
+def synalm(cl, lmax: int | None = None, seed: int = 0) -> np.ndarray:
+    """Gaussian alm in healpy layout drawn like alm_ops.py:34-54 (l ascending; m=0 real
+    N(0,C_l); m>0 Re, Im ~ N(0, C_l/2); nothing drawn when C_l <= 0), numpy default_rng."""
+    cl = np.asarray(cl, dtype=np.float64)
+    lmax = cl.size - 1 if lmax is None else lmax
+    rng = np.random.default_rng(seed)
+    alm = np.zeros(alm_size(lmax), dtype=np.complex128)
+    for l in range(lmax + 1):
+        C = float(cl[l])
+        if C <= 0.0:
+            continue
+        alm[alm_index(lmax, l, 0)] = rng.normal(0.0, math.sqrt(C))
+        if l > 0:
+            sd = math.sqrt(C / 2.0)
+            re = rng.normal(0.0, sd, size=l); im = rng.normal(0.0, sd, size=l)
+            ms = np.arange(1, l + 1)
+            alm[alm_index(lmax, l, ms)] = re + 1j * im
+    return alm
