@@ -1,0 +1,304 @@
+"""Benchmark: map2alm+alm2map pairs/s at nside 2048, lmax 4095 on B200.
+
+One step = one alm2map + map2alm pair for each map of the batch (synthetic Gaussian alm,
+C_l = (l+10)^-2, float32 maps of 50,331,648 pixels: every input is larger than the 126 MB L2).
+N GPUs: independent maps per rank (weak scaling, no data-path collective), timed on the device
+with CUDA events, max over ranks.  Prints one JSON line on rank 0.
+
+  python bench.py [--gpus N --steps K --warmup W --mode plain|batched --nmaps B]
+  python bench.py --impl reference   # the CPU restatement of the reference path (oracle port)
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "map2alm+alm2map/s, nside 2048 lmax 4095: batched vs plain, rel err ≤1e-5 vs FP64"
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--mode", default="plain", choices=["plain"])
+    p.add_argument("--nside", type=int, default=2048)
+    p.add_argument("--lmax", type=int, default=None)
+    p.add_argument("--nmaps", type=int, default=1)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--cpu-sample-m", type=int, default=12)
+    return p.parse_args()
+
+
+def n_lm(lmax, mmax=None):
+    mmax = lmax if mmax is None else mmax
+    return mmax * (2 * lmax + 1 - mmax) // 2 + lmax + 1
+
+
+class Clocks:
+    """Samples nvidia-smi SM clocks and throttle reasons while the timed region runs."""
+    Q = ("clocks.sm,clocks.max.sm,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def _run(self):
+        while not self._stop.is_set():
+            try:
+                out = subprocess.run(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                      "--format=csv,noheader,nounits"], capture_output=True, text=True, timeout=5)
+                self.samples.append([x.strip() for x in out.stdout.strip().split(",")])
+            except Exception:
+                pass
+            self._stop.wait(0.2)
+
+    def __enter__(self):
+        self._t = threading.Thread(target=self._run, daemon=True)
+        self._t.start()
+        return self
+
+    def __exit__(self, *a):
+        self._stop.set()
+        self._t.join(timeout=10)
+
+    def summary(self):
+        sm = [float(s[0]) for s in self.samples if len(s) >= 7 and s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if len(s) >= 7 and s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples if len(s) >= 7 for i in range(4) if s[3 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+# ----------------------------------------------------------------------------- CPU side
+def cpu_baseline(nside, lmax, sample_m):
+    """The FP64 oracle (C restatement of the reference path, OpenMP on all host cores) on a
+    bounded sample: ring FFTs of the whole map, Legendre work for m = 0..sample_m-1, scaled
+    to all m by the Legendre work ratio.  Returns pairs/s and a description."""
+    from oracle import sht_oracle as O
+    g = O.ring_tables(nside)
+    cl = 1.0 / (np.arange(lmax + 1) + 10.0) ** 2
+    ms = sample_m - 1
+    rng = np.random.default_rng(1)
+    alm = (rng.standard_normal(n_lm(lmax, ms)) + 1j * rng.standard_normal(n_lm(lmax, ms))) * math.sqrt(cl[0])
+    t0 = time.perf_counter()
+    G = O.legendre_synthesis(alm, g, lmax, ms)
+    t1 = time.perf_counter()
+    mp = O.ring_synthesis(G, g)
+    t2 = time.perf_counter()
+    F = O.ring_analysis(mp, g, ms, weights=g["weights_dz"])
+    t3 = time.perf_counter()
+    O.legendre_analysis(F, g, lmax)
+    t4 = time.perf_counter()
+    leg_sample = (t1 - t0) + (t4 - t3)
+    fft = (t2 - t1) + (t3 - t2)
+    ratio = n_lm(lmax) / n_lm(lmax, ms)
+    per_pair = leg_sample * ratio + fft
+    cores = os.cpu_count()
+    return 1.0 / per_pair, {
+        "cores": cores, "kind": "port",
+        "sample": (f"FP64 oracle (oracle/sht_oracle.c, OpenMP {cores} threads + numpy FFT) at nside {nside}, "
+                   f"lmax {lmax}: ring FFTs of the full map ({fft:.1f} s) + Legendre for m<{sample_m} "
+                   f"({leg_sample:.1f} s) scaled x{ratio:.0f} to all m"),
+        "seconds": t4 - t0}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    lmax = 2 * args.nside - 1 if args.lmax is None else args.lmax
+    vals = []
+    info = None
+    for _ in range(max(1, args.steps)):
+        v, info = cpu_baseline(args.nside, lmax, args.cpu_sample_m)
+        vals.append(v)
+    v = float(np.median(vals))
+    print(json.dumps({
+        "impl": "reference", "metric": METRIC, "value": v, "unit": "pairs/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": 0, "ms_per_step": 1000.0 / v, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"scalar map2alm+alm2map pair, nside {args.nside}, lmax {lmax}, float64, CPU",
+                   "nside": args.nside, "lmax": lmax},
+        "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": info["cores"], "kind": "port",
+                         "sample": info["sample"]},
+        "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }), flush=True)
+
+
+# ----------------------------------------------------------------------------- GPU side
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    import torch
+    import torch.distributed as dist
+    import hellblast_b200 as hb
+    from hellblast_b200 import _lib as L
+    from hellblast_b200 import geometry as G
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        import datetime
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+
+    nside = args.nside
+    lmax = 2 * nside - 1 if args.lmax is None else args.lmax
+    mmax = lmax
+    B = args.nmaps
+    nalm = n_lm(lmax)
+    npix = 12 * nside * nside
+    P = 2 * nside
+    g = G.healpix(nside)
+    st = torch.cuda.current_stream(dev)
+    sp = st.cuda_stream
+
+    # synthetic Gaussian alm, C_l = (l+10)^-2, seeded per rank (independent maps)
+    cl = 1.0 / (np.arange(lmax + 1) + 10.0) ** 2
+    alm_h = hb.synalm(cl, lmax=lmax, seed=1 + rank, device="cpu", dtype=torch.complex64)
+    alm = alm_h.to(dev).reshape(1, -1).repeat(B, 1).contiguous()
+    maps = torch.empty(B, npix, dtype=torch.float32, device=dev)
+    alm_out = torch.empty_like(alm)
+    ws = torch.empty(g.workspace_bytes(lmax, mmax, 32, B), dtype=torch.uint8, device=dev)
+
+    def stage_events():
+        return [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+
+    def step(ev=None):
+        if ev: ev[0].record(st)
+        L.call("hb_legendre_synthesis", g.handle, 32, lmax, mmax, B, alm.data_ptr(), ws.data_ptr(), sp)
+        if ev: ev[1].record(st)
+        L.call("hb_ring_synthesis", g.handle, 32, mmax, B, ws.data_ptr(), maps.data_ptr(), 0, sp)
+        if ev: ev[2].record(st)
+        L.call("hb_ring_analysis", g.handle, 32, mmax, B, maps.data_ptr(), None, ws.data_ptr(), 0, sp)
+        if ev: ev[3].record(st)
+        L.call("hb_legendre_analysis", g.handle, 32, lmax, mmax, B, ws.data_ptr(), alm_out.data_ptr(), sp)
+        if ev: ev[4].record(st)
+
+    # FP32-pipe peak measured on this GPU (FFMA probe)
+    probe_out = torch.empty(148 * 8 * 256, dtype=torch.float32, device=dev)
+    iters = 20000
+    L.call("hb_probe_fp32", 148 * 8, 256, 2000, probe_out.data_ptr(), sp)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    L.call("hb_probe_fp32", 148 * 8, 256, iters, probe_out.data_ptr(), sp)
+    e1.record(st)
+    torch.cuda.synchronize(dev)
+    fp32_peak = 148 * 8 * 256 * iters * 8 * 2 / (e0.elapsed_time(e1) * 1e-3) / 1e12
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    evs = [stage_events() for _ in range(args.steps)]
+    with Clocks(local) as clk:
+        torch.cuda.synchronize(dev)
+        t0 = torch.cuda.Event(enable_timing=True); t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(st)
+        for k in range(args.steps):
+            step(evs[k])
+        t1.record(st)
+        torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    ms = t0.elapsed_time(t1)
+    stage = np.array([[ev[i].elapsed_time(ev[i + 1]) for i in range(4)] for ev in evs]).mean(0)  # ms
+    if world > 1:
+        tt = torch.tensor([ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    value = world * args.steps * B / (ms * 1e-3)
+
+    # accuracy of the FP32 pair vs the FP64 GPU path on the same input (this step's alm_out)
+    a64 = alm_h.to(dev, torch.complex128)
+    m64 = hb.hp_compat.alm2map(a64, nside, lmax=lmax)
+    b64 = hb.hp_compat.map2alm(m64, lmax=lmax)
+    relerr = float(torch.linalg.norm(alm_out[0].to(torch.complex128) - b64) / torch.linalg.norm(b64))
+
+    # end to end through the public API: pinned host alm in, host alm out, copies timed
+    alm_pin = alm_h.reshape(1, -1).repeat(B, 1).contiguous().pin_memory()
+    out_pin = torch.empty_like(alm_pin).pin_memory()
+
+    def e2e_step():
+        a = alm_pin.to(dev, non_blocking=True)
+        m = hb.hp_compat.alm2map(a, nside, lmax=lmax)
+        b = hb.hp_compat.map2alm(m, lmax=lmax)
+        out_pin.copy_(b, non_blocking=True)
+
+    for _ in range(max(1, args.warmup)):
+        e2e_step()
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    t2 = torch.cuda.Event(enable_timing=True); t3 = torch.cuda.Event(enable_timing=True)
+    t2.record(st)
+    for _ in range(args.steps):
+        e2e_step()
+    t3.record(st)
+    torch.cuda.synchronize(dev)
+    ms_e2e = t2.elapsed_time(t3)
+    if world > 1:
+        tt = torch.tensor([ms_e2e], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms_e2e = float(tt.item())
+    e2e = world * args.steps * B / (ms_e2e * 1e-3)
+
+    # roofline of the dominant kernels: the two Legendre launches of a step
+    flop = 8.0 * nalm * P * B  # per Legendre launch (one direction), FMA = 2
+    t_leg = (stage[0] + stage[3]) * 1e-3
+    achieved = 2 * flop / t_leg / 1e12
+    out = {
+        "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (Gaussian alm, C_l=(l+10)^-2)",
+        "config": {"workload": f"scalar map2alm+alm2map pair, nside {nside}, lmax {lmax}, float32, plain per-map "
+                               f"FP32 path, {B} map(s) per GPU", "nside": nside, "lmax": lmax, "maps_per_gpu": B,
+                   "mode": args.mode, "l2": "inputs larger than L2 (map 201 MB, alm 67 MB)",
+                   "parallelism": f"replicas x{world}"},
+        "rel_err_vs_fp64": relerr,
+        "stages_ms": {"legendre_synthesis": stage[0], "ring_synthesis": stage[1], "ring_analysis": stage[2],
+                      "legendre_analysis": stage[3]},
+        "roofline": {"bound": "fp32", "kernel": "leg_synthesis + leg_analysis", "achieved": achieved,
+                     "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
+                     "peak_source": "FFMA probe (hb_probe_fp32) on this GPU, this run",
+                     "flop_per_launch": flop},
+        "e2e": {"value": e2e, "unit": "pairs/s", "h2d_bytes_per_step": int(alm_pin.numel() * 8),
+                "d2h_bytes_per_step": int(out_pin.numel() * 8)},
+        "gpu_launches": args.steps * 4,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        v, info = cpu_baseline(nside, lmax, args.cpu_sample_m)
+        out["cpu_baseline"] = {"value": v, "unit": "pairs/s", "cores": info["cores"], "kind": info["kind"],
+                               "sample": info["sample"]}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,103 @@
+"""Loader for the C-ABI library ``hellblast_b200/_lib/libhbsht.so`` (include/hbsht.h).
+
+There is no fallback: if the library is missing or fails to load, every transform raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import threading
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libhbsht.so")
+
+HB_OK = 0
+HB_ERR_INVALID = -1
+HB_ERR_UNSUPPORTED = -2
+HB_ERR_CUDA = -3
+HB_ERR_WORKSPACE = -4
+HB_ERR_ALLOC = -5
+
+HB_PHI0_HEALPIX = 0
+HB_PHI0_REFERENCE = 1
+HB_WEIGHTS_DZ = 0
+HB_WEIGHTS_UNIFORM = 1
+HB_F_NOPHASE = 1
+HB_F_NOFOLD = 2
+HB_F_NO2PI = 4
+
+_lock = threading.Lock()
+_lib = None
+
+vp = ctypes.c_void_p
+i32 = ctypes.c_int
+i64 = ctypes.c_int64
+sz = ctypes.c_size_t
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "hb_last_error_string": (ctypes.c_char_p, []),
+    "hb_version": (ctypes.c_char_p, []),
+    "hb_alm_size": (i64, [i32, i32]),
+    "hb_ring_tables": (i32, [i64, i32, vp, vp, vp, vp, vp, vp, vp, vp]),
+    "hb_geom_create_healpix": (i32, [i64, i32, i32, ctypes.POINTER(vp)]),
+    "hb_geom_create": (i32, [i64, vp, vp, vp, vp, ctypes.POINTER(vp)]),
+    "hb_geom_destroy": (i32, [vp]),
+    "hb_geom_info": (i32, [vp, ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.POINTER(i64)]),
+    "hb_sht_workspace_size": (sz, [vp, i32, i32, i32, i32]),
+    "hb_spin2_workspace_size": (sz, [vp, i32, i32, i32, i32]),
+    "hb_alm2cl_f32": (i32, [i32, i32, i32, vp, vp, vp, vp]),
+    "hb_ring_analysis": (i32, [vp, i32, i32, i32, vp, vp, vp, i32, vp]),
+    "hb_ring_synthesis": (i32, [vp, i32, i32, i32, vp, vp, i32, vp]),
+    "hb_legendre_analysis": (i32, [vp, i32, i32, i32, i32, vp, vp, vp]),
+    "hb_legendre_synthesis": (i32, [vp, i32, i32, i32, i32, vp, vp, vp]),
+    "hb_probe_fp32": (i32, [i32, i32, i32, vp, vp]),
+    "hb_alm2cl_f64": (i32, [i32, i32, i32, vp, vp, vp, vp]),
+}
+for _p in ("f32", "f64"):
+    SIGNATURES[f"hb_map2alm_{_p}"] = (i32, [vp, i32, i32, i32, vp, vp, vp, vp, sz, i32, vp])
+    SIGNATURES[f"hb_alm2map_{_p}"] = (i32, [vp, i32, i32, i32, vp, vp, vp, sz, i32, vp])
+    SIGNATURES[f"hb_alm2map_adjoint_{_p}"] = (i32, [vp, i32, i32, i32, vp, vp, vp, sz, i32, vp])
+    SIGNATURES[f"hb_map2alm_adjoint_{_p}"] = (i32, [vp, i32, i32, i32, vp, vp, vp, vp, sz, i32, vp])
+    SIGNATURES[f"hb_map2alm_spin2_{_p}"] = (i32, [vp, i32, i32, i32, vp, vp, vp, vp, vp, vp, sz, i32, vp])
+    SIGNATURES[f"hb_alm2map_spin2_{_p}"] = (i32, [vp, i32, i32, i32, vp, vp, vp, vp, vp, sz, i32, vp])
+    SIGNATURES[f"hb_alm2map_spin2_adjoint_{_p}"] = (i32, [vp, i32, i32, i32, vp, vp, vp, vp, vp, sz, i32, vp])
+    SIGNATURES[f"hb_map2alm_spin2_adjoint_{_p}"] = (i32, [vp, i32, i32, i32, vp, vp, vp, vp, vp, vp, sz, i32, vp])
+
+
+class HBError(RuntimeError):
+    """A C-ABI call returned an error status."""
+
+
+def lib():
+    """Load libhbsht.so once; raise if it is absent (no CPU fallback exists)."""
+    global _lib
+    if _lib is None:
+        with _lock:
+            if _lib is None:
+                if not os.path.exists(LIB_PATH):
+                    raise ImportError(
+                        f"hellblast_b200: CUDA library {LIB_PATH} is missing; build it with "
+                        "`python -c 'import __graft_entry__ as g; g.build()'` or `make -C hellblast_b200/csrc`")
+                L = ctypes.CDLL(LIB_PATH)
+                for name, (res, args) in SIGNATURES.items():
+                    f = getattr(L, name)
+                    f.restype = res
+                    f.argtypes = args
+                _lib = L
+    return _lib
+
+
+def check(rc: int, what: str) -> None:
+    if rc == HB_OK:
+        return
+    msg = lib().hb_last_error_string().decode(errors="replace")
+    if rc == HB_ERR_INVALID:
+        raise ValueError(f"{what}: {msg}")
+    if rc == HB_ERR_UNSUPPORTED:
+        raise NotImplementedError(f"{what}: {msg}")
+    raise HBError(f"{what} failed ({rc}): {msg}")
+
+
+def call(name: str, *args) -> None:
+    check(getattr(lib(), name)(*args), name)

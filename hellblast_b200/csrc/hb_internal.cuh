@@ -1,0 +1,113 @@
+// Internal definitions shared by the hbsht CUDA sources (sm_100a).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <string>
+
+#include "../../include/hbsht.h"
+
+#define HB_MAX_L 16383
+
+namespace hb {
+
+// ----------------------------------------------------------------------------- errors
+void set_error(const std::string &msg);
+int fail(int code, const std::string &msg);
+#define HB_CUDA_TRY(call)                                                                         \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess)                                                                    \
+            return ::hb::fail(HB_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_));   \
+    } while (0)
+#define HB_CHECK_LAUNCH()                                                                         \
+    do {                                                                                          \
+        cudaError_t e_ = cudaGetLastError();                                                      \
+        if (e_ != cudaSuccess)                                                                    \
+            return ::hb::fail(HB_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+// ----------------------------------------------------------------------------- complex helpers
+template <typename T> struct C2;
+template <> struct C2<float> { using type = float2; };
+template <> struct C2<double> { using type = double2; };
+template <typename T> using c2_t = typename C2<T>::type;
+
+__host__ __device__ __forceinline__ float2 mk2(float a, float b) { return make_float2(a, b); }
+__host__ __device__ __forceinline__ double2 mk2(double a, double b) { return make_double2(a, b); }
+template <typename V> __host__ __device__ __forceinline__ V cadd(V a, V b) { return mk2(a.x + b.x, a.y + b.y); }
+template <typename V> __host__ __device__ __forceinline__ V csub(V a, V b) { return mk2(a.x - b.x, a.y - b.y); }
+template <typename V> __host__ __device__ __forceinline__ V cmul(V a, V b) {
+    return mk2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+template <typename V> __host__ __device__ __forceinline__ V cconj(V a) { return mk2(a.x, -a.y); }
+template <typename V, typename S> __host__ __device__ __forceinline__ V cscale(V a, S s) {
+    return mk2(a.x * s, a.y * s);
+}
+
+__device__ __forceinline__ void sincospi_t(float x, float *s, float *c) { sincospif(x, s, c); }
+__device__ __forceinline__ void sincospi_t(double x, double *s, double *c) { sincospi(x, s, c); }
+
+// ----------------------------------------------------------------------------- layout
+__host__ __device__ __forceinline__ int64_t alm_idx(int64_t lmax, int64_t l, int64_t m) {
+    return m * (2 * lmax + 1 - m) / 2 + l;
+}
+inline int64_t alm_size(int lmax, int mmax) { return alm_idx(lmax, lmax, mmax) + 1; }
+
+// ----------------------------------------------------------------------------- geometry
+// Device-resident ring/pair tables.  A "pair" is a north ring and its mirror south ring
+// (theta_S = pi - theta_N) that share |cos theta|; unpaired rings (the equator, or rings of a
+// non-symmetric geometry) have south = -1.
+struct GeomDev {
+    int64_t nr, npix, npairs;
+    int32_t *nphi;         // [nr]
+    int64_t *ofs;          // [nr] first pixel of ring
+    double *phi0_pi;       // [nr] phi0 / pi
+    double *w;             // [nr] default per-ring weight (dz convention)
+    int32_t *ring_pair;    // [nr]
+    int32_t *ring_side;    // [nr] 0 = north/unpaired, 1 = south
+    int32_t *pair_ring;    // [npairs][2] ring index of north, south (-1)
+    double *pair_x;        // [npairs] cos theta of the north ring
+    float *pair_xhi;       // [npairs] float(x)
+    float *pair_xlo;       // [npairs] float(x - xhi)
+    double *pair_log2sin;  // [npairs] log2 sin theta
+    double *pair_log2ch;   // [npairs] log2 cos(theta/2)
+    double *pair_log2sh;   // [npairs] log2 sin(theta/2)
+    // ragged FFT: per ring the convolution length L (== nphi/2 when that is a power of two:
+    // direct FFT; otherwise Bluestein) and the offset of its chirp spectrum in blu_*.
+    int32_t *fft_len;      // [nr]
+    int64_t *blu_ofs;      // [nr] (-1 for direct)
+    double2 *blu_f64;      // concatenated chirp spectra, bit-reversed order, scaled by 1/L
+    float2 *blu_f32;
+    int max_fft_len;       // max L over rings
+    int max_nphi;
+    double *log2cm;        // [HB_MAX_L+1] log2 sqrt((2m+1)!!/((2m)!! 4 pi)), scalar lambda_mm
+    double *log2spin;      // [HB_MAX_L+1] log2 of the constant of N_l0 d^l0_{m,+-2}
+};
+
+}  // namespace hb
+
+struct hb_geom {
+    hb::GeomDev d;
+    int64_t nside;  // 0 when not a HEALPix grid
+    void *alloc_base;
+};
+
+namespace hb {
+// kernels' host launchers (implemented in the .cu files)
+int launch_ring_analysis(const GeomDev &g, int precision, int nmaps, const void *maps, int64_t map_stride,
+                         const double *w, void *Fm, int mmax, int flags, bool unit_weights, bool mdouble,
+                         cudaStream_t st);
+int launch_ring_synthesis(const GeomDev &g, int precision, int nmaps, const void *Gm, int mmax, void *maps,
+                          int64_t map_stride, const double *w, bool apply_weights, bool mdouble, int flags,
+                          cudaStream_t st);
+int launch_leg_analysis(const GeomDev &g, int precision, int nmaps, int lmax, int mmax, const void *Fm,
+                        void *alm, cudaStream_t st);
+int launch_leg_synthesis(const GeomDev &g, int precision, int nmaps, int lmax, int mmax, const void *alm,
+                         void *Gm, cudaStream_t st);
+int launch_spin_analysis(const GeomDev &g, int precision, int nmaps, int lmax, int mmax, const void *QFm,
+                         const void *UFm, void *E, void *B, cudaStream_t st);
+int launch_spin_synthesis(const GeomDev &g, int precision, int nmaps, int lmax, int mmax, const void *E,
+                          const void *B, void *QGm, void *UGm, cudaStream_t st);
+int build_bluestein_tables(GeomDev &g, cudaStream_t st);
+int fft_smem_bytes(int L, int precision);
+}  // namespace hb

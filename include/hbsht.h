@@ -1,0 +1,188 @@
+/*
+ * hbsht: B200-native (sm_100a) HEALPix spherical-harmonic transforms -- public C ABI.
+ *
+ * Drop-in boundary for the SHT hot path of hellblast.  Every entry point:
+ *   - returns int (HB_OK = 0, negative = error; hb_last_error_string() explains),
+ *   - takes device pointers plus explicit sizes and an explicit cudaStream_t,
+ *   - allocates nothing on the hot path: transforms take a caller-provided device workspace
+ *     whose size the matching *_workspace_size() query returns.
+ * Geometry handles (hb_geom) are created once (this allocates) and are immutable afterwards,
+ * so one handle may be shared by several host threads and streams.
+ *
+ * alm layout: healpy m-major, idx(l,m) = m*(2*lmax+1-m)/2 + l, size hb_alm_size(lmax,mmax),
+ * complex interleaved (re, im) in the transform's precision.  Maps: RING-ordered flat arrays.
+ * Batches: nmaps maps back to back ([nmaps][npix]) and nmaps alm vectors ([nmaps][nalm]).
+ *
+ * Reference interfaces replaced (file:line within Luce-Morningstar/hellblast):
+ *   hb_ring_tables            HealpixRingTables.__init__ + build_ring_tables
+ *                             (ring_tables.py:17-37, ring_tables_healpix.cu:5-52);
+ *                             weights_dz (ring_tables.py:39-40)
+ *   hb_geom_create*           the (thetas, nphi_per_ring, weights_dz) arguments of
+ *                             map2alm_gpu / alm2map_gpu (sht_raw.py:30, isht.py:5)
+ *   hb_map2alm_{f32,f64}      map2alm_gpu (sht.py:1-4 -> sht_raw.py:30-57, sht_fallback.py:36-65)
+ *   hb_alm2map_{f32,f64}      alm2map_gpu (isht.py:5-26)
+ *   hb_map2alm_spin2_{f32,f64} map2alm_spin_gpu + eb_from_qu_gpu (spin.py:32-78)
+ *   hb_alm2map_spin2_{f32,f64} qu_from_eb_gpu (spin.py:80-115)
+ *   hb_alm2cl_{f32,f64}       alm2cl (alm_ops.py:19-32), the reduction inside anafast_ring
+ *                             (anafast.py:5-7)
+ *   hb_map2alm_adjoint_*, hb_alm2map_adjoint_*, hb_*_spin2_adjoint_*
+ *                             no reference counterpart (the reference has no gradients);
+ *                             exact transposes used by the autograd wrappers
+ */
+#ifndef HBSHT_H
+#define HBSHT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define HB_API __attribute__((visibility("default")))
+#else
+#define HB_API
+#endif
+
+typedef struct CUstream_st *hb_stream_t; /* same handle as cudaStream_t */
+typedef struct hb_geom hb_geom;
+
+enum {
+    HB_OK = 0,
+    HB_ERR_INVALID = -1,     /* bad argument (size, nside, lmax, null pointer, ...) */
+    HB_ERR_UNSUPPORTED = -2, /* valid request outside what this build implements */
+    HB_ERR_CUDA = -3,        /* a CUDA runtime call failed */
+    HB_ERR_WORKSPACE = -4,   /* workspace pointer null or smaller than the size query */
+    HB_ERR_ALLOC = -5        /* allocation failed while creating a handle */
+};
+
+/* phi0 convention of a HEALPix geometry */
+enum { HB_PHI0_HEALPIX = 0, HB_PHI0_REFERENCE = 1 };
+/* default ring weights of a HEALPix geometry */
+enum { HB_WEIGHTS_DZ = 0, HB_WEIGHTS_UNIFORM = 1 };
+
+/* flags of the forward transforms (reference-compatibility switches, all off by default) */
+enum {
+    HB_F_NOPHASE = 1, /* drop exp(-i m phi0): the reference omits it (sht_raw.py:41) */
+    HB_F_NOFOLD = 2,  /* zero for m >= nphi instead of folding m mod nphi (sht_raw.py:51) */
+    HB_F_NO2PI = 4    /* omit the 2*pi factor, like sht_raw.py:53 (sht_fallback.py:63 has it) */
+};
+
+/* Last error message of the calling thread ("" if none). */
+HB_API const char *hb_last_error_string(void);
+/* Library version string. */
+HB_API const char *hb_version(void);
+
+/* alm vector length for (lmax, mmax), healpy layout. */
+HB_API int64_t hb_alm_size(int lmax, int mmax);
+
+/* HEALPix ring tables on the device, nside a power of two (ring_tables.py:19).
+ * Outputs (device, any may be NULL): z[Nr], theta[Nr], nphi[Nr], phi0[Nr],
+ * ring_start[Nr+1], z_edges[Nr+1], weights_dz[Nr], Nr = 4*nside-1.
+ * Integer outputs are bit-exact with the reference; phi0_mode selects HB_PHI0_*. */
+HB_API int hb_ring_tables(int64_t nside, int phi0_mode, double *z, double *theta, int32_t *nphi, double *phi0,
+                   int64_t *ring_start, double *z_edges, double *weights_dz, hb_stream_t stream);
+
+/* Geometry of a HEALPix RING grid.  weights_mode selects HB_WEIGHTS_*. */
+HB_API int hb_geom_create_healpix(int64_t nside, int phi0_mode, int weights_mode, hb_geom **out);
+/* Geometry of arbitrary iso-latitude rings (host arrays, length nr).  weights are the
+ * reference's per-ring weights (sum 2 for a full sphere): pixel weight = 2*pi*w_r/nphi_r.
+ * phi0 may be NULL (all zero).  Ring r's pixels start at the running sum of nphi.
+ * nphi_r must be a positive multiple of 2. */
+HB_API int hb_geom_create(int64_t nr, const double *theta, const int32_t *nphi, const double *phi0,
+                   const double *weights, hb_geom **out);
+HB_API int hb_geom_destroy(hb_geom *g);
+/* nr, npix, ring pairs used by the Legendre kernels, nside (0 if not HEALPix) */
+HB_API int hb_geom_info(const hb_geom *g, int64_t *nr, int64_t *npix, int64_t *npairs, int64_t *nside);
+
+/* Workspace bytes for one call of the transform family; precision 32 or 64. */
+HB_API size_t hb_sht_workspace_size(const hb_geom *g, int lmax, int mmax, int precision, int nmaps);
+HB_API size_t hb_spin2_workspace_size(const hb_geom *g, int lmax, int mmax, int precision, int nmaps);
+
+/* map2alm: alm = sum_pix (2 pi w_r / nphi_r) f(pix) conj(Y_lm(pix)).  maps [nmaps][npix],
+ * alm [nmaps][nalm] complex.  weights: device [nr] per-ring weights or NULL (geometry's). */
+HB_API int hb_map2alm_f32(const hb_geom *g, int lmax, int mmax, int nmaps, const float *maps, const double *weights,
+                   float *alm, void *ws, size_t ws_bytes, int flags, hb_stream_t stream);
+HB_API int hb_map2alm_f64(const hb_geom *g, int lmax, int mmax, int nmaps, const double *maps, const double *weights,
+                   double *alm, void *ws, size_t ws_bytes, int flags, hb_stream_t stream);
+
+/* alm2map: f(pix) = sum_lm a_lm Y_lm(pix) (real field: m>0 counted twice). */
+HB_API int hb_alm2map_f32(const hb_geom *g, int lmax, int mmax, int nmaps, const float *alm, float *maps,
+                   void *ws, size_t ws_bytes, int flags, hb_stream_t stream);
+HB_API int hb_alm2map_f64(const hb_geom *g, int lmax, int mmax, int nmaps, const double *alm, double *maps,
+                   void *ws, size_t ws_bytes, int flags, hb_stream_t stream);
+
+/* Exact adjoints (transposes, Re and Im of alm as independent real coordinates):
+ *   hb_alm2map_adjoint: map-space vector -> alm-space vector, includes the m>0 doubling;
+ *   hb_map2alm_adjoint: alm-space vector -> map-space vector, includes the pixel weights. */
+HB_API int hb_alm2map_adjoint_f32(const hb_geom *g, int lmax, int mmax, int nmaps, const float *maps, float *alm,
+                           void *ws, size_t ws_bytes, int flags, hb_stream_t stream);
+HB_API int hb_alm2map_adjoint_f64(const hb_geom *g, int lmax, int mmax, int nmaps, const double *maps, double *alm,
+                           void *ws, size_t ws_bytes, int flags, hb_stream_t stream);
+HB_API int hb_map2alm_adjoint_f32(const hb_geom *g, int lmax, int mmax, int nmaps, const float *alm, const double *weights,
+                           float *maps, void *ws, size_t ws_bytes, int flags, hb_stream_t stream);
+HB_API int hb_map2alm_adjoint_f64(const hb_geom *g, int lmax, int mmax, int nmaps, const double *alm, const double *weights,
+                           double *maps, void *ws, size_t ws_bytes, int flags, hb_stream_t stream);
+
+/* Spin-2: Q/U maps -> E/B alm (E = -(a2+a-2)/2, B = i(a2-a-2)/2, healpy convention) and back. */
+HB_API int hb_map2alm_spin2_f32(const hb_geom *g, int lmax, int mmax, int nmaps, const float *Q, const float *U,
+                         const double *weights, float *E, float *B, void *ws, size_t ws_bytes, int flags,
+                         hb_stream_t stream);
+HB_API int hb_map2alm_spin2_f64(const hb_geom *g, int lmax, int mmax, int nmaps, const double *Q, const double *U,
+                         const double *weights, double *E, double *B, void *ws, size_t ws_bytes, int flags,
+                         hb_stream_t stream);
+HB_API int hb_alm2map_spin2_f32(const hb_geom *g, int lmax, int mmax, int nmaps, const float *E, const float *B,
+                         float *Q, float *U, void *ws, size_t ws_bytes, int flags, hb_stream_t stream);
+HB_API int hb_alm2map_spin2_f64(const hb_geom *g, int lmax, int mmax, int nmaps, const double *E, const double *B,
+                         double *Q, double *U, void *ws, size_t ws_bytes, int flags, hb_stream_t stream);
+
+/* Exact adjoints of the spin-2 pair (transposes over Re/Im of E and B):
+ *   hb_alm2map_spin2_adjoint: (gQ, gU) -> (gE, gB), includes the m>0 doubling;
+ *   hb_map2alm_spin2_adjoint: (gE, gB) -> (gQ, gU), includes the pixel weights. */
+HB_API int hb_alm2map_spin2_adjoint_f32(const hb_geom *g, int lmax, int mmax, int nmaps, const float *gQ,
+                                        const float *gU, float *gE, float *gB, void *ws, size_t ws_bytes, int flags,
+                                        hb_stream_t stream);
+HB_API int hb_alm2map_spin2_adjoint_f64(const hb_geom *g, int lmax, int mmax, int nmaps, const double *gQ,
+                                        const double *gU, double *gE, double *gB, void *ws, size_t ws_bytes,
+                                        int flags, hb_stream_t stream);
+HB_API int hb_map2alm_spin2_adjoint_f32(const hb_geom *g, int lmax, int mmax, int nmaps, const float *gE,
+                                        const float *gB, const double *weights, float *gQ, float *gU, void *ws,
+                                        size_t ws_bytes, int flags, hb_stream_t stream);
+HB_API int hb_map2alm_spin2_adjoint_f64(const hb_geom *g, int lmax, int mmax, int nmaps, const double *gE,
+                                        const double *gB, const double *weights, double *gQ, double *gU, void *ws,
+                                        size_t ws_bytes, int flags, hb_stream_t stream);
+
+/* alm2cl: cl[l] = (Re a_l0 b_l0* + 2 sum_{m>0} Re a_lm b_lm*) / (2l+1); alm2 may be NULL
+ * (auto spectrum).  cl is always double [nmaps][lmax+1]. */
+HB_API int hb_alm2cl_f32(int lmax, int mmax, int nmaps, const float *alm1, const float *alm2, double *cl,
+                  hb_stream_t stream);
+HB_API int hb_alm2cl_f64(int lmax, int mmax, int nmaps, const double *alm1, const double *alm2, double *cl,
+                  hb_stream_t stream);
+
+/* Pipeline stages (what the transforms are made of), for callers that keep the per-ring
+ * Fourier coefficients resident or time the stages.  F / G: complex, precision 32 or 64,
+ * layout [nmaps][mmax+1][npairs][2] (north, south ring of each pair), npairs from hb_geom_info.
+ *   hb_ring_analysis:      maps -> F (weights, phi0 phase, alias fold; flags as map2alm)
+ *   hb_legendre_analysis:  F -> alm
+ *   hb_legendre_synthesis: alm -> G
+ *   hb_ring_synthesis:     G -> maps
+ * (sht_raw.py:38-43 / 46-56 and isht.py:11-25 are the reference's versions of these steps.) */
+HB_API int hb_ring_analysis(const hb_geom *g, int precision, int mmax, int nmaps, const void *maps,
+                            const double *weights, void *F, int flags, hb_stream_t stream);
+HB_API int hb_ring_synthesis(const hb_geom *g, int precision, int mmax, int nmaps, const void *G, void *maps, int flags,
+                             hb_stream_t stream);
+HB_API int hb_legendre_analysis(const hb_geom *g, int precision, int lmax, int mmax, int nmaps, const void *F,
+                                void *alm, hb_stream_t stream);
+HB_API int hb_legendre_synthesis(const hb_geom *g, int precision, int lmax, int mmax, int nmaps, const void *alm,
+                                 void *G, hb_stream_t stream);
+
+/* Diagnostics (no reference counterpart): FP32 FMA throughput probe, blocks*threads threads
+ * each running iters*8 FMAs; out holds blocks*threads floats.  Used by bench.py to measure the
+ * FP32-pipe roofline on the running GPU. */
+HB_API int hb_probe_fp32(int blocks, int threads, int iters, float *out, hb_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* HBSHT_H */

@@ -1,0 +1,219 @@
+"""GPU parity tests of the scalar transforms: the CUDA path (through the C ABI / torch ops)
+against the reference's own outputs (golden fixtures) and against the FP64 oracle.
+
+Tolerances: FP64 path <= 1e-10 relative (max-abs over max-abs), FP32 path <= 1e-5 relative
+(L2 norm of the error over L2 norm of the FP64 result).  Integer ring tables bit-exact.
+"""
+import math
+import os
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import GOLDEN
+
+pytestmark = pytest.mark.gpu
+
+TOL64 = 1e-10
+TOL32 = 1e-5
+
+
+def relmax(a, b):
+    a = np.asarray(a); b = np.asarray(b)
+    return float(np.max(np.abs(a - b)) / max(np.max(np.abs(b)), 1e-300))
+
+
+def rel2(a, b):
+    a = np.asarray(a); b = np.asarray(b)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+def npy(t):
+    return t.detach().cpu().numpy()
+
+
+@pytest.fixture(scope="module")
+def hb():
+    import hellblast_b200
+    return hellblast_b200
+
+
+CASES = ["sht_nside8_lmax16", "sht_nside32_lmax64", "sht_nside32_lmax85", "sht_nside16_lmax40_m0"]
+
+
+def test_ring_tables_kernel_bit_exact(hb):
+    import hashlib
+    d = np.load(os.path.join(GOLDEN, "ring_tables.npz"))
+    for nside in (1, 2, 4, 8, 16, 32, 64):
+        t = hb.HealpixRingTables(nside, phi0="reference").dump_host()
+        for k in ("nphi", "ring_start", "z_centers", "phi_center0", "z_edges"):
+            assert np.array_equal(t[k], d[f"n{nside}_{k}"]), (nside, k)
+        # theta = acos(z): CUDA's acos and the host C library's may differ in the last bit
+        assert np.allclose(t["theta_centers"], d[f"n{nside}_theta_centers"], rtol=0, atol=1e-15)
+    for nside in (128, 256, 512, 1024, 2048, 4096, 8192):
+        t = hb.HealpixRingTables(nside, phi0="reference").dump_host()
+        h = hashlib.sha256(t["nphi"].astype(np.int32).tobytes() + t["ring_start"].astype(np.int64).tobytes())
+        assert h.hexdigest() == str(d[f"n{nside}_int_sha256"])
+        assert t["npix"] == int(d[f"n{nside}_npix"])
+
+
+@pytest.mark.parametrize("name", CASES)
+@pytest.mark.parametrize("flavour", ["fallback", "raw"])
+def test_ref_compat_parity_with_reference(hb, name, flavour):
+    """map2alm_gpu(ref_compat=...) in FP64 == the reference's own sht_fallback / sht_raw output."""
+    d = np.load(os.path.join(GOLDEN, name + ".npz"))
+    nside, lmax = int(d["nside"]), int(d["lmax"])
+    tabs = hb.HealpixRingTables(nside, phi0="reference")
+    flat = torch.from_numpy(d["map"]).cuda()
+    rings = [flat[int(tabs.ring_start[r]):int(tabs.ring_start[r + 1])] for r in range(tabs.Nr)]
+    alm = hb.map2alm_gpu(rings, tabs.theta_centers, tabs.nphi, tabs.weights_dz(), lmax, ref_compat=flavour,
+                         alm_layout="ref_lsquare")
+    ref = d["ref_sht_fallback"] if flavour == "fallback" else d["ref_sht_raw"]
+    assert alm.dtype == torch.complex128
+    assert relmax(npy(alm), ref) < TOL64
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_correct_transform_m0_parity_and_anafast(hb, name, oracle):
+    d = np.load(os.path.join(GOLDEN, name + ".npz"))
+    nside, lmax = int(d["nside"]), int(d["lmax"])
+    tabs = hb.HealpixRingTables(nside)
+    flat = torch.from_numpy(d["map"]).cuda()
+    alm = npy(hb.map2alm_gpu(flat, tabs.theta_centers, tabs.nphi, tabs.weights_dz(), lmax))
+    l = np.arange(lmax + 1)
+    assert relmax(alm[hb.alm_index(lmax, l, 0)], d["ref_sht_fallback"][l * (l + 1)]) < TOL64
+    g = oracle.ring_tables(nside)
+    assert relmax(alm, oracle.map2alm(d["map"], g, lmax)) < TOL64
+    # anafast_ring on the reference-convention path == reference anafast_ring
+    tref = hb.HealpixRingTables(nside, phi0="reference")
+    raw = hb.map2alm_gpu(flat, tref.theta_centers, tref.nphi, tref.weights_dz(), lmax, ref_compat="raw")
+    assert relmax(npy(hb.alm2cl(raw)), d["ref_anafast_ring"]) < TOL64
+    fb = hb.map2alm_gpu(flat, tref.theta_centers, tref.nphi, tref.weights_dz(), lmax, ref_compat="fallback")
+    assert relmax(npy(hb.alm2cl(fb)), d["ref_alm2cl_fallback"]) < TOL64
+
+
+def test_isht_m0_parity(hb):
+    d = np.load(os.path.join(GOLDEN, "sht_nside16_lmax40_m0.npz"))
+    nside, lmax = int(d["nside"]), int(d["lmax"])
+    tabs = hb.HealpixRingTables(nside)
+    a = torch.from_numpy(d["alm_in"]).cuda()
+    rings = hb.alm2map_gpu(a, tabs.theta_centers, tabs.nphi, lmax)
+    mp = torch.cat(rings)
+    assert relmax(npy(mp), d["ref_isht_map"]) < TOL64
+
+
+def _alm(oracle, lmax, seed, mmax=None):
+    cl = 1.0 / (np.arange(lmax + 1) + 1.0) ** 2
+    cl[:2] = 0.0
+    a = oracle.synalm(cl, seed=seed)
+    if mmax is not None and mmax < lmax:
+        keep = np.concatenate([oracle.alm_index(lmax, np.arange(m, lmax + 1), m) for m in range(mmax + 1)])
+        a = a[np.sort(keep)]
+    return a
+
+
+@pytest.mark.parametrize("nside,lmax", [(1, 3), (2, 8), (8, 23), (16, 47), (32, 95), (64, 191), (16, 200)])
+def test_fp64_vs_oracle(hb, oracle, nside, lmax):
+    g = oracle.ring_tables(nside)
+    a = _alm(oracle, lmax, seed=nside)
+    mp_ref = oracle.alm2map(a, g, lmax)
+    mp = npy(hb.hp_compat.alm2map(torch.from_numpy(a).cuda(), nside, lmax=lmax))
+    assert relmax(mp, mp_ref) < TOL64
+    alm_ref = oracle.map2alm(mp_ref, g, lmax)
+    alm = npy(hb.hp_compat.map2alm(torch.from_numpy(mp_ref).cuda(), lmax=lmax))
+    assert relmax(alm, alm_ref) < TOL64
+
+
+@pytest.mark.parametrize("nside,lmax", [(8, 23), (64, 191), (256, 767)])
+def test_fp32_vs_oracle(hb, oracle, nside, lmax):
+    g = oracle.ring_tables(nside)
+    a = _alm(oracle, lmax, seed=3 + nside)
+    mp_ref = oracle.alm2map(a, g, lmax)
+    mp = npy(hb.hp_compat.alm2map(torch.from_numpy(a).cuda().to(torch.complex64), nside, lmax=lmax))
+    assert mp.dtype == np.float32
+    assert rel2(mp, mp_ref) < TOL32
+    alm_ref = oracle.map2alm(mp_ref, g, lmax)
+    alm = npy(hb.hp_compat.map2alm(torch.from_numpy(mp_ref).cuda().float(), lmax=lmax))
+    assert alm.dtype == np.complex64
+    assert rel2(alm, alm_ref) < TOL32
+
+
+def test_mmax_less_than_lmax_and_batch(hb, oracle):
+    nside, lmax, mmax = 16, 40, 13
+    g = oracle.ring_tables(nside)
+    alms = [_alm(oracle, lmax, seed=s, mmax=mmax) for s in range(3)]
+    ref = np.stack([oracle.alm2map(a, g, lmax, mmax) for a in alms])
+    out = npy(hb.hp_compat.alm2map(torch.from_numpy(np.stack(alms)).cuda(), nside, lmax=lmax, mmax=mmax))
+    assert out.shape == ref.shape
+    assert relmax(out, ref) < TOL64
+    back = npy(hb.hp_compat.map2alm(torch.from_numpy(ref).cuda(), lmax=lmax, mmax=mmax))
+    assert relmax(back, np.stack([oracle.map2alm(r, g, lmax, mmax) for r in ref])) < TOL64
+
+
+def test_generic_rings_unpaired(hb, oracle):
+    """Arbitrary iso-latitude rings (not HEALPix, no mirror pairs, odd-half lengths)."""
+    rng = np.random.default_rng(1)
+    th = np.sort(rng.uniform(0.05, 3.0, 23))
+    nphi = (2 * rng.integers(3, 40, 23)).astype(np.int32)
+    w = rng.uniform(0.05, 0.15, 23)
+    phi0 = rng.uniform(0, 1, 23)
+    g = oracle.generic_geometry(th, nphi, phi0=phi0, weights=w)
+    lmax = 30
+    mp = rng.standard_normal(int(nphi.sum()))
+    ref = oracle.map2alm(mp, g, lmax, weights=w)
+    alm = npy(hb.map2alm_gpu(torch.from_numpy(mp).cuda(), th, nphi, w, lmax, phi0=phi0))
+    assert relmax(alm, ref) < TOL64
+    a = _alm(oracle, lmax, 4)
+    out = npy(hb.alm2map_gpu(torch.from_numpy(a).cuda(), th, nphi, lmax, phi0=phi0, flat=True))
+    assert relmax(out, oracle.alm2map(a, g, lmax)) < TOL64
+
+
+def test_high_lmax_small_nside_underflow_paths(hb, oracle):
+    """lmax far above 4*nside: heavy aliasing fold and lambda_mm underflow near the poles."""
+    nside, lmax = 4, 300
+    g = oracle.ring_tables(nside)
+    rng = np.random.default_rng(2)
+    mp = rng.standard_normal(12 * nside * nside)
+    ref = oracle.map2alm(mp, g, lmax)
+    for prec, tol in (("fp64", TOL64), ("fp32", TOL32)):
+        alm = npy(hb.hp_compat.map2alm(torch.from_numpy(mp).cuda(), lmax=lmax, precision=prec))
+        assert rel2(alm, ref) < tol, prec
+
+
+def test_alm2cl_kernel(hb, oracle):
+    lmax, mmax = 300, 250
+    rng = np.random.default_rng(3)
+    n = oracle.alm_size(lmax, mmax)
+    a = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    b = rng.standard_normal(n) + 1j * rng.standard_normal(n)
+    ta, tb = torch.from_numpy(a).cuda(), torch.from_numpy(b).cuda()
+    assert relmax(npy(hb.alm2cl(ta, mmax=mmax)), oracle.alm2cl(a, lmax, mmax)) < 1e-13
+    assert relmax(npy(hb.alm2cl(ta, tb, mmax=mmax)), oracle.alm2cl(a, lmax, mmax, alm2=b)) < 1e-13
+    assert relmax(npy(hb.alm2cl(ta.to(torch.complex64), mmax=mmax)), oracle.alm2cl(a, lmax, mmax)) < 1e-6
+
+
+def test_lmax_zero_and_tiny(hb, oracle):
+    for lmax in (0, 1):
+        g = oracle.ring_tables(1)
+        a = np.zeros(oracle.alm_size(lmax), complex); a[0] = 2.0
+        mp = npy(hb.hp_compat.alm2map(torch.from_numpy(a).cuda(), 1, lmax=lmax))
+        assert relmax(mp, oracle.alm2map(a, g, lmax)) < TOL64
+
+
+def test_errors_raise(hb):
+    with pytest.raises(ValueError):
+        hb.hp_compat.map2alm(torch.zeros(1000, device="cuda", dtype=torch.float64))
+    with pytest.raises(ValueError):
+        hb.hp_compat.alm2map(torch.zeros(7, device="cuda", dtype=torch.complex128), 4, lmax=3)
+
+
+def test_cupy_style_ring_list_input(hb, oracle):
+    """The reference passes a Python list of per-ring arrays (sht_raw.py:38-40)."""
+    nside, lmax = 8, 16
+    g = oracle.ring_tables(nside)
+    rng = np.random.default_rng(9)
+    mp = rng.standard_normal(12 * nside * nside)
+    rings = [mp[g["ring_start"][r]:g["ring_start"][r + 1]] for r in range(g["nr"])]
+    alm = npy(hb.map2alm_gpu(rings, g["theta"], g["nphi"], g["weights_dz"], lmax))
+    assert relmax(alm, oracle.map2alm(mp, g, lmax)) < TOL64
