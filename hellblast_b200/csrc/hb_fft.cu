@@ -231,13 +231,9 @@ __global__ void __launch_bounds__(256) ring_synthesis_kernel(GeomDev g, const c2
 // for |t| < N (circular), one CTA per ring, computed in place in global memory (FP64), then
 // rounded to FP32 for the single-precision kernels.
 __global__ void __launch_bounds__(1024) bluestein_table_kernel(GeomDev g) {
-    const int r = blockIdx.x;
+    // one CTA per distinct convolution table (rings of equal nphi share one)
+    const int r = g.blu_owner[blockIdx.x];
     const int64_t bo = g.blu_ofs[r];
-    if (bo < 0) return;
-    if (g.ring_side[r] == 1) {  // mirror of a north ring with the same table
-        int north = g.pair_ring[2 * g.ring_pair[r]];
-        if (g.blu_ofs[north] == bo) return;
-    }
     const int N = g.nphi[r] >> 1, L = g.fft_len[r];
     double2 *buf = g.blu_f64 + bo;
     for (int t = threadIdx.x; t < L; t += blockDim.x) {
@@ -273,7 +269,8 @@ __global__ void __launch_bounds__(1024) bluestein_table_kernel(GeomDev g) {
 }
 
 int build_bluestein_tables(GeomDev &g, cudaStream_t st) {
-    bluestein_table_kernel<<<(unsigned)g.nr, 1024, 0, st>>>(g);
+    if (g.n_blu == 0) return HB_OK;
+    bluestein_table_kernel<<<(unsigned)g.n_blu, 1024, 0, st>>>(g);
     HB_CHECK_LAUNCH();
     return HB_OK;
 }

@@ -107,7 +107,7 @@ static void fill_log2_tables(std::vector<double> &cm, std::vector<double> &spin)
 }
 
 struct HostGeom {
-    std::vector<int32_t> nphi, ring_pair, ring_side, pair_ring, fft_len;
+    std::vector<int32_t> nphi, ring_pair, ring_side, pair_ring, fft_len, blu_owner;
     std::vector<int64_t> ofs, blu_ofs;
     std::vector<double> phi0_pi, w, pair_x, pair_log2sin, pair_log2ch, pair_log2sh;
     std::vector<float> pair_xhi, pair_xlo;
@@ -137,6 +137,7 @@ static int finish_geom(HostGeom &h, int64_t nside, const std::vector<double> &xn
             if (it == blu_of_N.end()) {
                 blu_of_N[N] = h.blu_total;
                 h.blu_ofs[r] = h.blu_total;
+                h.blu_owner.push_back((int32_t)r);
                 h.blu_total += L;
             } else {
                 h.blu_ofs[r] = it->second;
@@ -159,7 +160,7 @@ static int finish_geom(HostGeom &h, int64_t nside, const std::vector<double> &xn
            o_rp = carve(4 * nr), o_rs = carve(4 * nr), o_pr = carve(8 * np), o_px = carve(8 * np),
            o_pxh = carve(4 * np), o_pxl = carve(4 * np), o_pls = carve(8 * np), o_plc = carve(8 * np),
            o_plh = carve(8 * np), o_fl = carve(4 * nr), o_bo = carve(8 * nr), o_b64 = carve(16 * (h.blu_total + 1)),
-           o_b32 = carve(8 * (h.blu_total + 1)), o_cm = carve(8 * (HB_MAX_L + 1)), o_sp = carve(8 * (HB_MAX_L + 1));
+           o_b32 = carve(8 * (h.blu_total + 1)), o_bw = carve(4 * (h.blu_owner.size() + 1)), o_cm = carve(8 * (HB_MAX_L + 1)), o_sp = carve(8 * (HB_MAX_L + 1));
     char *base = nullptr;
     if (cudaMalloc(&base, total) != cudaSuccess) {
         cudaGetLastError();
@@ -177,6 +178,7 @@ static int finish_geom(HostGeom &h, int64_t nside, const std::vector<double> &xn
     d.pair_log2ch = (double *)(base + o_plc); d.pair_log2sh = (double *)(base + o_plh);
     d.fft_len = (int32_t *)(base + o_fl); d.blu_ofs = (int64_t *)(base + o_bo);
     d.blu_f64 = (double2 *)(base + o_b64); d.blu_f32 = (float2 *)(base + o_b32);
+    d.blu_owner = (int32_t *)(base + o_bw); d.n_blu = (int64_t)h.blu_owner.size();
     d.log2cm = (double *)(base + o_cm); d.log2spin = (double *)(base + o_sp);
     d.max_fft_len = h.max_fft_len; d.max_nphi = h.max_nphi;
     struct Up { void *dst; const void *src; size_t n; } ups[] = {
@@ -187,7 +189,8 @@ static int finish_geom(HostGeom &h, int64_t nside, const std::vector<double> &xn
         {d.pair_xhi, h.pair_xhi.data(), 4 * (size_t)np}, {d.pair_xlo, h.pair_xlo.data(), 4 * (size_t)np},
         {d.pair_log2sin, h.pair_log2sin.data(), 8 * (size_t)np}, {d.pair_log2ch, h.pair_log2ch.data(), 8 * (size_t)np},
         {d.pair_log2sh, h.pair_log2sh.data(), 8 * (size_t)np}, {d.fft_len, h.fft_len.data(), 4 * (size_t)nr},
-        {d.blu_ofs, h.blu_ofs.data(), 8 * (size_t)nr}, {d.log2cm, cm.data(), 8 * (size_t)(HB_MAX_L + 1)},
+        {d.blu_ofs, h.blu_ofs.data(), 8 * (size_t)nr},
+        {d.blu_owner, h.blu_owner.data(), 4 * h.blu_owner.size()}, {d.log2cm, cm.data(), 8 * (size_t)(HB_MAX_L + 1)},
         {d.log2spin, spin.data(), 8 * (size_t)(HB_MAX_L + 1)}};
     for (auto &u : ups) {
         if (cudaMemcpy(u.dst, u.src, u.n, cudaMemcpyHostToDevice) != cudaSuccess) {

@@ -78,6 +78,8 @@ struct GeomDev {
     int64_t *blu_ofs;      // [nr] (-1 for direct)
     double2 *blu_f64;      // concatenated chirp spectra, bit-reversed order, scaled by 1/L
     float2 *blu_f32;
+    int32_t *blu_owner;    // [n_blu] first ring using each distinct chirp table
+    int64_t n_blu;
     int max_fft_len;       // max L over rings
     int max_nphi;
     double *log2cm;        // [HB_MAX_L+1] log2 sqrt((2m+1)!!/((2m)!! 4 pi)), scalar lambda_mm

@@ -210,7 +210,8 @@ __global__ void __launch_bounds__(NT) spin_analysis_kernel(GeomDev g, int lmax, 
                     }
                     if (em[k] < 0 && fabs(M1[k]) > s_huge<T>()) {
                         M1[k] *= s_down<T>(); M2[k] *= s_down<T>();
-                        ch = ch || (++em[k] == 0);
+                        ++em[k];
+                        if (em[k] == 0) ch = true;
                     }
                     if (ch) load_w(k, (int64_t)chunk * NT * K + (int64_t)k * NT + tid, ep[k] >= 0, em[k] >= 0);
                     anyneg |= (ep[k] < 0) || (em[k] < 0);
