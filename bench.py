@@ -172,6 +172,7 @@ def main():
     npix = 12 * nside * nside
     P = 2 * nside
     g = G.healpix(nside)
+    plan = G.plan(g, lmax, mmax, precision=32)
     st = torch.cuda.current_stream(dev)
     sp = st.cuda_stream
 
@@ -181,20 +182,20 @@ def main():
     alm = alm_h.to(dev).reshape(1, -1).repeat(B, 1).contiguous()
     maps = torch.empty(B, npix, dtype=torch.float32, device=dev)
     alm_out = torch.empty_like(alm)
-    ws = torch.empty(g.workspace_bytes(lmax, mmax, 32, B), dtype=torch.uint8, device=dev)
+    ws = torch.empty(plan.workspace_bytes(32, B), dtype=torch.uint8, device=dev)
 
     def stage_events():
         return [torch.cuda.Event(enable_timing=True) for _ in range(5)]
 
     def step(ev=None):
         if ev: ev[0].record(st)
-        L.call("hb_legendre_synthesis", g.handle, 32, lmax, mmax, B, alm.data_ptr(), ws.data_ptr(), sp)
+        L.call("hb_legendre_synthesis", plan.handle, 32, B, alm.data_ptr(), ws.data_ptr(), sp)
         if ev: ev[1].record(st)
-        L.call("hb_ring_synthesis", g.handle, 32, mmax, B, ws.data_ptr(), maps.data_ptr(), 0, sp)
+        L.call("hb_ring_synthesis", plan.handle, 32, B, ws.data_ptr(), maps.data_ptr(), 0, sp)
         if ev: ev[2].record(st)
-        L.call("hb_ring_analysis", g.handle, 32, mmax, B, maps.data_ptr(), None, ws.data_ptr(), 0, sp)
+        L.call("hb_ring_analysis", plan.handle, 32, B, maps.data_ptr(), None, ws.data_ptr(), 0, sp)
         if ev: ev[3].record(st)
-        L.call("hb_legendre_analysis", g.handle, 32, lmax, mmax, B, ws.data_ptr(), alm_out.data_ptr(), sp)
+        L.call("hb_legendre_analysis", plan.handle, 32, B, ws.data_ptr(), alm_out.data_ptr(), sp)
         if ev: ev[4].record(st)
 
     # FP32-pipe peak measured on this GPU (FFMA probe)

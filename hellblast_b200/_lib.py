@@ -44,25 +44,31 @@ SIGNATURES = {
     "hb_geom_create": (i32, [i64, vp, vp, vp, vp, ctypes.POINTER(vp)]),
     "hb_geom_destroy": (i32, [vp]),
     "hb_geom_info": (i32, [vp, ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.POINTER(i64)]),
-    "hb_sht_workspace_size": (sz, [vp, i32, i32, i32, i32]),
-    "hb_spin2_workspace_size": (sz, [vp, i32, i32, i32, i32]),
+    "hb_plan_create": (i32, [vp, i32, i32, i32, ctypes.POINTER(vp)]),
+    "hb_plan_destroy": (i32, [vp]),
+    "hb_plan_bytes": (sz, [vp]),
+    "hb_sht_workspace_size": (sz, [vp, i32, i32]),
+    "hb_spin2_workspace_size": (sz, [vp, i32, i32]),
     "hb_alm2cl_f32": (i32, [i32, i32, i32, vp, vp, vp, vp]),
-    "hb_ring_analysis": (i32, [vp, i32, i32, i32, vp, vp, vp, i32, vp]),
-    "hb_ring_synthesis": (i32, [vp, i32, i32, i32, vp, vp, i32, vp]),
-    "hb_legendre_analysis": (i32, [vp, i32, i32, i32, i32, vp, vp, vp]),
-    "hb_legendre_synthesis": (i32, [vp, i32, i32, i32, i32, vp, vp, vp]),
-    "hb_probe_fp32": (i32, [i32, i32, i32, vp, vp]),
     "hb_alm2cl_f64": (i32, [i32, i32, i32, vp, vp, vp, vp]),
+    "hb_ring_analysis": (i32, [vp, i32, i32, vp, vp, vp, i32, vp]),
+    "hb_ring_synthesis": (i32, [vp, i32, i32, vp, vp, i32, vp]),
+    "hb_legendre_analysis": (i32, [vp, i32, i32, vp, vp, vp]),
+    "hb_legendre_synthesis": (i32, [vp, i32, i32, vp, vp, vp]),
+    "hb_probe_fp32": (i32, [i32, i32, i32, vp, vp]),
 }
 for _p in ("f32", "f64"):
-    SIGNATURES[f"hb_map2alm_{_p}"] = (i32, [vp, i32, i32, i32, vp, vp, vp, vp, sz, i32, vp])
-    SIGNATURES[f"hb_alm2map_{_p}"] = (i32, [vp, i32, i32, i32, vp, vp, vp, sz, i32, vp])
-    SIGNATURES[f"hb_alm2map_adjoint_{_p}"] = (i32, [vp, i32, i32, i32, vp, vp, vp, sz, i32, vp])
-    SIGNATURES[f"hb_map2alm_adjoint_{_p}"] = (i32, [vp, i32, i32, i32, vp, vp, vp, vp, sz, i32, vp])
-    SIGNATURES[f"hb_map2alm_spin2_{_p}"] = (i32, [vp, i32, i32, i32, vp, vp, vp, vp, vp, vp, sz, i32, vp])
-    SIGNATURES[f"hb_alm2map_spin2_{_p}"] = (i32, [vp, i32, i32, i32, vp, vp, vp, vp, vp, sz, i32, vp])
-    SIGNATURES[f"hb_alm2map_spin2_adjoint_{_p}"] = (i32, [vp, i32, i32, i32, vp, vp, vp, vp, vp, sz, i32, vp])
-    SIGNATURES[f"hb_map2alm_spin2_adjoint_{_p}"] = (i32, [vp, i32, i32, i32, vp, vp, vp, vp, vp, vp, sz, i32, vp])
+    SIGNATURES[f"hb_map2alm_{_p}"] = (i32, [vp, i32, vp, vp, vp, vp, sz, i32, vp])
+    SIGNATURES[f"hb_alm2map_{_p}"] = (i32, [vp, i32, vp, vp, vp, sz, i32, vp])
+    SIGNATURES[f"hb_alm2map_adjoint_{_p}"] = (i32, [vp, i32, vp, vp, vp, sz, i32, vp])
+    SIGNATURES[f"hb_map2alm_adjoint_{_p}"] = (i32, [vp, i32, vp, vp, vp, vp, sz, i32, vp])
+    SIGNATURES[f"hb_map2alm_spin2_{_p}"] = (i32, [vp, i32, vp, vp, vp, vp, vp, vp, sz, i32, vp])
+    SIGNATURES[f"hb_alm2map_spin2_{_p}"] = (i32, [vp, i32, vp, vp, vp, vp, vp, sz, i32, vp])
+    SIGNATURES[f"hb_alm2map_spin2_adjoint_{_p}"] = (i32, [vp, i32, vp, vp, vp, vp, vp, sz, i32, vp])
+    SIGNATURES[f"hb_map2alm_spin2_adjoint_{_p}"] = (i32, [vp, i32, vp, vp, vp, vp, vp, vp, sz, i32, vp])
+
+HB_PLAN_FP32 = 1
+HB_PLAN_SPIN2_FP32 = 2
 
 
 class HBError(RuntimeError):

@@ -16,61 +16,54 @@ from .transforms import device_weights
 
 class Map2Alm(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, maps, gid, lmax, mmax, weights):
+    def forward(ctx, maps, pid, weights):
         ctx.save_for_backward(weights)
-        ctx.cfg = (gid, lmax, mmax)
-        return ops.map2alm(maps, gid, lmax, mmax, weights, 0)
+        ctx.pid = pid
+        return ops.map2alm(maps, pid, weights, 0)
 
     @staticmethod
     def backward(ctx, galm):
         (weights,) = ctx.saved_tensors
-        gid, lmax, mmax = ctx.cfg
-        gm = ops.map2alm_adjoint(galm.contiguous(), gid, lmax, mmax, weights, 0)
-        return gm, None, None, None, None
+        return ops.map2alm_adjoint(galm.contiguous(), ctx.pid, weights, 0), None, None
 
 
 class Alm2Map(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, alm, gid, lmax, mmax):
-        ctx.cfg = (gid, lmax, mmax)
-        return ops.alm2map(alm, gid, lmax, mmax, 0)
+    def forward(ctx, alm, pid):
+        ctx.pid = pid
+        return ops.alm2map(alm, pid, 0)
 
     @staticmethod
     def backward(ctx, gmap):
-        gid, lmax, mmax = ctx.cfg
-        return ops.alm2map_adjoint(gmap.contiguous(), gid, lmax, mmax, 0), None, None, None
+        return ops.alm2map_adjoint(gmap.contiguous(), ctx.pid, 0), None
 
 
 class Map2AlmSpin2(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, Q, U, gid, lmax, mmax, weights):
+    def forward(ctx, Q, U, pid, weights):
         ctx.save_for_backward(weights)
-        ctx.cfg = (gid, lmax, mmax)
-        return ops.map2alm_spin2(Q, U, gid, lmax, mmax, weights, 0)
+        ctx.pid = pid
+        return ops.map2alm_spin2(Q, U, pid, weights, 0)
 
     @staticmethod
     def backward(ctx, gE, gB):
         (weights,) = ctx.saved_tensors
-        gid, lmax, mmax = ctx.cfg
-        gE = torch.zeros_like(gE) if gE is None else gE.contiguous()
-        gB = torch.zeros_like(gB) if gB is None else gB.contiguous()
-        gQ, gU = ops.map2alm_spin2_adjoint(gE, gB, gid, lmax, mmax, weights, 0)
-        return gQ, gU, None, None, None, None
+        gE = gE.contiguous()
+        gB = gB.contiguous()
+        gQ, gU = ops.map2alm_spin2_adjoint(gE, gB, ctx.pid, weights, 0)
+        return gQ, gU, None, None
 
 
 class Alm2MapSpin2(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, E, B, gid, lmax, mmax):
-        ctx.cfg = (gid, lmax, mmax)
-        return ops.alm2map_spin2(E, B, gid, lmax, mmax, 0)
+    def forward(ctx, E, B, pid):
+        ctx.pid = pid
+        return ops.alm2map_spin2(E, B, pid, 0)
 
     @staticmethod
     def backward(ctx, gQ, gU):
-        gid, lmax, mmax = ctx.cfg
-        gQ = torch.zeros_like(gQ) if gQ is None else gQ.contiguous()
-        gU = torch.zeros_like(gU) if gU is None else gU.contiguous()
-        gE, gB = ops.alm2map_spin2_adjoint(gQ, gU, gid, lmax, mmax, 0)
-        return gE, gB, None, None, None
+        gE, gB = ops.alm2map_spin2_adjoint(gQ.contiguous(), gU.contiguous(), ctx.pid, 0)
+        return gE, gB, None
 
 
 class Alm2Cl(torch.autograd.Function):
@@ -96,29 +89,33 @@ class Alm2Cl(torch.autograd.Function):
         return alm * w, None, None
 
 
+def _prec(t: torch.Tensor) -> int:
+    return 32 if t.dtype in (torch.float32, torch.complex64) else 64
+
+
 def map2alm(maps: torch.Tensor, nside: int, lmax: int, mmax: int | None = None, weights="dz") -> torch.Tensor:
     """Differentiable map2alm on a HEALPix grid; maps [nmaps, npix] (float32 or float64)."""
-    mmax = lmax if mmax is None else mmax
     g = G.healpix(nside, weights="uniform" if weights == "uniform" else "dz")
     w = None if isinstance(weights, str) else device_weights(weights, g, maps.device)
-    return Map2Alm.apply(maps.contiguous(), g.gid, lmax, mmax, w)
+    p = G.plan(g, lmax, mmax, precision=_prec(maps))
+    return Map2Alm.apply(maps.contiguous(), p.pid, w)
 
 
 def alm2map(alm: torch.Tensor, nside: int, lmax: int, mmax: int | None = None) -> torch.Tensor:
-    mmax = lmax if mmax is None else mmax
-    return Alm2Map.apply(alm.contiguous(), G.healpix(nside).gid, lmax, mmax)
+    p = G.plan(G.healpix(nside), lmax, mmax, precision=_prec(alm))
+    return Alm2Map.apply(alm.contiguous(), p.pid)
 
 
 def map2alm_spin(Q: torch.Tensor, U: torch.Tensor, nside: int, lmax: int, mmax: int | None = None, weights="dz"):
-    mmax = lmax if mmax is None else mmax
     g = G.healpix(nside, weights="uniform" if weights == "uniform" else "dz")
     w = None if isinstance(weights, str) else device_weights(weights, g, Q.device)
-    return Map2AlmSpin2.apply(Q.contiguous(), U.contiguous(), g.gid, lmax, mmax, w)
+    p = G.plan(g, lmax, mmax, precision=_prec(Q), spin=True)
+    return Map2AlmSpin2.apply(Q.contiguous(), U.contiguous(), p.pid, w)
 
 
 def alm2map_spin(E: torch.Tensor, B: torch.Tensor, nside: int, lmax: int, mmax: int | None = None):
-    mmax = lmax if mmax is None else mmax
-    return Alm2MapSpin2.apply(E.contiguous(), B.contiguous(), G.healpix(nside).gid, lmax, mmax)
+    p = G.plan(G.healpix(nside), lmax, mmax, precision=_prec(E), spin=True)
+    return Alm2MapSpin2.apply(E.contiguous(), B.contiguous(), p.pid)
 
 
 def alm2cl(alm: torch.Tensor, lmax: int, mmax: int | None = None) -> torch.Tensor:

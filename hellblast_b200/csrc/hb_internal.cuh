@@ -94,6 +94,18 @@ struct hb_geom {
     void *alloc_base;
 };
 
+// A geometry plus (lmax, mmax) and the FP32 recursion checkpoints (see hb_plan.cu).
+struct hb_plan {
+    const hb_geom *g;
+    int lmax, mmax, flags;
+    void *alloc_base;
+    size_t bytes;
+    int64_t *blk_ofs;       // [mmax+2] first checkpoint block of each m (scalar)
+    int64_t *blk_ofs_spin;  // [mmax+2] same for the spin-2 recursions (blocks from max(m,2))
+    float4 *ck;             // scalar checkpoints, or null
+    float4 *ckP, *ckM;      // spin-2 checkpoints, or null
+};
+
 namespace hb {
 // kernels' host launchers (implemented in the .cu files)
 int launch_ring_analysis(const GeomDev &g, int precision, int nmaps, const void *maps, int64_t map_stride,
@@ -102,14 +114,17 @@ int launch_ring_analysis(const GeomDev &g, int precision, int nmaps, const void 
 int launch_ring_synthesis(const GeomDev &g, int precision, int nmaps, const void *Gm, int mmax, void *maps,
                           int64_t map_stride, const double *w, bool apply_weights, bool mdouble, int flags,
                           cudaStream_t st);
+// ck / blk_ofs: FP32 recursion checkpoints of a plan (null: no re-anchoring; FP64 ignores them)
 int launch_leg_analysis(const GeomDev &g, int precision, int nmaps, int lmax, int mmax, const void *Fm,
-                        void *alm, cudaStream_t st);
+                        void *alm, cudaStream_t st, const float4 *ck, const int64_t *blk_ofs);
 int launch_leg_synthesis(const GeomDev &g, int precision, int nmaps, int lmax, int mmax, const void *alm,
-                         void *Gm, cudaStream_t st);
+                         void *Gm, cudaStream_t st, const float4 *ck, const int64_t *blk_ofs);
 int launch_spin_analysis(const GeomDev &g, int precision, int nmaps, int lmax, int mmax, const void *QFm,
-                         const void *UFm, void *E, void *B, cudaStream_t st);
+                         const void *UFm, void *E, void *B, cudaStream_t st, const float4 *ckP, const float4 *ckM,
+                         const int64_t *blk_ofs);
 int launch_spin_synthesis(const GeomDev &g, int precision, int nmaps, int lmax, int mmax, const void *E,
-                          const void *B, void *QGm, void *UGm, cudaStream_t st);
+                          const void *B, void *QGm, void *UGm, cudaStream_t st, const float4 *ckP,
+                          const float4 *ckM, const int64_t *blk_ofs);
 int build_bluestein_tables(GeomDev &g, cudaStream_t st);
 int fft_smem_bytes(int L, int precision);
 }  // namespace hb

@@ -95,9 +95,11 @@ template <> __device__ __forceinline__ double down_v<double>() { return 0x1p-512
 constexpr int COEF_CH = 256;  // l values per shared-memory coefficient chunk
 
 template <typename T, int K, int NT>
-__global__ void __launch_bounds__(NT) leg_analysis_kernel(GeomDev g, int lmax, int mmax, const c2_t<T> *__restrict__ Fm,
-                                                          int64_t fm_stride, c2_t<T> *__restrict__ alm,
-                                                          int64_t alm_stride, int atomic) {
+__global__ void __launch_bounds__(NT, 2) leg_analysis_kernel(GeomDev g, int lmax, int mmax, const c2_t<T> *__restrict__ Fm,
+                                                             int64_t fm_stride, c2_t<T> *__restrict__ alm,
+                                                             int64_t alm_stride, int atomic,
+                                                             const float4 *__restrict__ ck,
+                                                             const int64_t *__restrict__ blk_ofs) {
     using V = c2_t<T>;
     constexpr int TL = LegCfg<T>::TL;
     constexpr int TPS = NT / TL;  // threads reducing one l slot
@@ -150,6 +152,33 @@ __global__ void __launch_bounds__(NT) leg_analysis_kernel(GeomDev g, int lmax, i
                 coef[i] = mk2((T)A, (T)B);
             }
             __syncthreads();
+            if constexpr (sizeof(T) == 4) {
+                if (ck != nullptr && lrel > 0) {  // re-anchor on the FP64-computed state
+                    const float4 *cb = ck + (blk_ofs[m] + lrel / COEF_CH) * np;
+                    anyneg = false;
+#pragma unroll
+                    for (int k = 0; k < K; ++k) {
+                        const int64_t p = (int64_t)chunk * NT * K + (int64_t)k * NT + tid;
+                        if (p < np) {
+                            const float4 c = cb[p];
+                            l1[k] = c.x;
+                            l2[k] = c.y;
+                            const int en = __float_as_int(c.z);
+                            if (en != e[k]) {
+                                e[k] = en;
+                                if (en == 0) {
+                                    V fn = F[2 * p], fs = F[2 * p + 1];
+                                    ge[k] = cadd(fn, fs);
+                                    go[k] = csub(fn, fs);
+                                } else {
+                                    ge[k] = go[k] = mk2((T)0, (T)0);
+                                }
+                            }
+                            anyneg |= e[k] < 0;
+                        }
+                    }
+                }
+            }
         }
         const V *cf = coef + (lrel % COEF_CH);
 #pragma unroll
@@ -217,9 +246,10 @@ __global__ void __launch_bounds__(NT) leg_analysis_kernel(GeomDev g, int lmax, i
 }
 
 template <typename T, int K, int NT>
-__global__ void __launch_bounds__(NT) leg_synthesis_kernel(GeomDev g, int lmax, int mmax, const c2_t<T> *__restrict__ alm,
-                                                           int64_t alm_stride, c2_t<T> *__restrict__ Gm,
-                                                           int64_t gm_stride) {
+__global__ void __launch_bounds__(NT, 2) leg_synthesis_kernel(GeomDev g, int lmax, int mmax, const c2_t<T> *__restrict__ alm,
+                                                              int64_t alm_stride, c2_t<T> *__restrict__ Gm,
+                                                              int64_t gm_stride, const float4 *__restrict__ ck,
+                                                              const int64_t *__restrict__ blk_ofs) {
     using V = c2_t<T>;
     __shared__ V coef[COEF_CH];
     __shared__ V acoef[COEF_CH];
@@ -261,6 +291,29 @@ __global__ void __launch_bounds__(NT) leg_synthesis_kernel(GeomDev g, int lmax, 
                 acoef[i] = (l0 + i <= lmax) ? a[alm_idx(lmax, l0 + i, m)] : mk2((T)0, (T)0);
             }
             __syncthreads();
+            if constexpr (sizeof(T) == 4) {
+                if (ck != nullptr && lrel > 0) {  // re-anchor on the FP64-computed state
+                    const float4 *cb = ck + (blk_ofs[m] + lrel / COEF_CH) * np;
+                    anyneg = false;
+#pragma unroll
+                    for (int k = 0; k < K; ++k) {
+                        const int64_t p = (int64_t)chunk * NT * K + (int64_t)k * NT + tid;
+                        if (p < np) {
+                            const float4 c = cb[p];
+                            l1[k] = c.x;
+                            l2[k] = c.y;
+                            const int en = __float_as_int(c.z);
+                            if (en != e[k]) {  // accumulators are kept in units of 2^(64 e)
+                                const float f = ldexpf(1.0f, 64 * max(-3, e[k] - en));
+                                ae[k] = cscale(ae[k], f);
+                                ao[k] = cscale(ao[k], f);
+                                e[k] = en;
+                            }
+                            anyneg |= e[k] < 0;
+                        }
+                    }
+                }
+            }
         }
         const int i0 = lrel % COEF_CH;
 #pragma unroll
@@ -311,7 +364,7 @@ __global__ void __launch_bounds__(NT) leg_synthesis_kernel(GeomDev g, int lmax, 
 
 template <typename T, int K, int NT>
 static int run_analysis(const GeomDev &g, int nmaps, int lmax, int mmax, const c2_t<T> *Fm, c2_t<T> *alm,
-                        cudaStream_t st) {
+                        cudaStream_t st, const float4 *ck, const int64_t *bo) {
     const int64_t per = (int64_t)K * NT;
     const int nchunks = (int)((g.npairs + per - 1) / per);
     const int64_t fm_stride = (int64_t)(mmax + 1) * g.npairs * 2;
@@ -320,52 +373,55 @@ static int run_analysis(const GeomDev &g, int nmaps, int lmax, int mmax, const c
     const int smem = 2 * LegCfg<T>::TL * NT * (int)sizeof(c2_t<T>);
     HB_CUDA_TRY(cudaFuncSetAttribute(leg_analysis_kernel<T, K, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     dim3 grid((unsigned)(mmax + 1), (unsigned)nchunks, (unsigned)nmaps);
-    leg_analysis_kernel<T, K, NT><<<grid, NT, smem, st>>>(g, lmax, mmax, Fm, fm_stride, alm, alm_stride, nchunks > 1);
+    leg_analysis_kernel<T, K, NT><<<grid, NT, smem, st>>>(g, lmax, mmax, Fm, fm_stride, alm, alm_stride, nchunks > 1,
+                                                           ck, bo);
     HB_CHECK_LAUNCH();
     return HB_OK;
 }
 
 template <typename T, int K, int NT>
 static int run_synthesis(const GeomDev &g, int nmaps, int lmax, int mmax, const c2_t<T> *alm, c2_t<T> *Gm,
-                         cudaStream_t st) {
+                         cudaStream_t st, const float4 *ck, const int64_t *bo) {
     const int64_t per = (int64_t)K * NT;
     const int nchunks = (int)((g.npairs + per - 1) / per);
     const int64_t gm_stride = (int64_t)(mmax + 1) * g.npairs * 2;
     const int64_t alm_stride = alm_size(lmax, mmax);
     dim3 grid((unsigned)(mmax + 1), (unsigned)nchunks, (unsigned)nmaps);
-    leg_synthesis_kernel<T, K, NT><<<grid, NT, 0, st>>>(g, lmax, mmax, alm, alm_stride, Gm, gm_stride);
+    leg_synthesis_kernel<T, K, NT><<<grid, NT, 0, st>>>(g, lmax, mmax, alm, alm_stride, Gm, gm_stride, ck, bo);
     HB_CHECK_LAUNCH();
     return HB_OK;
 }
 
 template <typename T>
 static int analysis_t(const GeomDev &g, int nmaps, int lmax, int mmax, const c2_t<T> *Fm, c2_t<T> *alm,
-                      cudaStream_t st) {
-    if (g.npairs >= 1024) return run_analysis<T, 8, 256>(g, nmaps, lmax, mmax, Fm, alm, st);
-    if (g.npairs >= 256) return run_analysis<T, 4, 128>(g, nmaps, lmax, mmax, Fm, alm, st);
-    if (g.npairs >= 64) return run_analysis<T, 2, 64>(g, nmaps, lmax, mmax, Fm, alm, st);
-    return run_analysis<T, 1, 64>(g, nmaps, lmax, mmax, Fm, alm, st);
+                      cudaStream_t st, const float4 *ck, const int64_t *bo) {
+    if (g.npairs >= 1024) return run_analysis<T, 8, 256>(g, nmaps, lmax, mmax, Fm, alm, st, ck, bo);
+    if (g.npairs >= 256) return run_analysis<T, 4, 128>(g, nmaps, lmax, mmax, Fm, alm, st, ck, bo);
+    if (g.npairs >= 64) return run_analysis<T, 2, 64>(g, nmaps, lmax, mmax, Fm, alm, st, ck, bo);
+    return run_analysis<T, 1, 64>(g, nmaps, lmax, mmax, Fm, alm, st, ck, bo);
 }
 
 template <typename T>
 static int synthesis_t(const GeomDev &g, int nmaps, int lmax, int mmax, const c2_t<T> *alm, c2_t<T> *Gm,
-                       cudaStream_t st) {
-    if (g.npairs >= 1024) return run_synthesis<T, 8, 256>(g, nmaps, lmax, mmax, alm, Gm, st);
-    if (g.npairs >= 256) return run_synthesis<T, 4, 128>(g, nmaps, lmax, mmax, alm, Gm, st);
-    if (g.npairs >= 64) return run_synthesis<T, 2, 64>(g, nmaps, lmax, mmax, alm, Gm, st);
-    return run_synthesis<T, 1, 64>(g, nmaps, lmax, mmax, alm, Gm, st);
+                       cudaStream_t st, const float4 *ck, const int64_t *bo) {
+    if (g.npairs >= 1024) return run_synthesis<T, 8, 256>(g, nmaps, lmax, mmax, alm, Gm, st, ck, bo);
+    if (g.npairs >= 256) return run_synthesis<T, 4, 128>(g, nmaps, lmax, mmax, alm, Gm, st, ck, bo);
+    if (g.npairs >= 64) return run_synthesis<T, 2, 64>(g, nmaps, lmax, mmax, alm, Gm, st, ck, bo);
+    return run_synthesis<T, 1, 64>(g, nmaps, lmax, mmax, alm, Gm, st, ck, bo);
 }
 
 int launch_leg_analysis(const GeomDev &g, int precision, int nmaps, int lmax, int mmax, const void *Fm, void *alm,
-                        cudaStream_t st) {
-    if (precision == 32) return analysis_t<float>(g, nmaps, lmax, mmax, (const float2 *)Fm, (float2 *)alm, st);
-    return analysis_t<double>(g, nmaps, lmax, mmax, (const double2 *)Fm, (double2 *)alm, st);
+                        cudaStream_t st, const float4 *ck, const int64_t *bo) {
+    if (precision == 32)
+        return analysis_t<float>(g, nmaps, lmax, mmax, (const float2 *)Fm, (float2 *)alm, st, ck, bo);
+    return analysis_t<double>(g, nmaps, lmax, mmax, (const double2 *)Fm, (double2 *)alm, st, nullptr, nullptr);
 }
 
 int launch_leg_synthesis(const GeomDev &g, int precision, int nmaps, int lmax, int mmax, const void *alm, void *Gm,
-                         cudaStream_t st) {
-    if (precision == 32) return synthesis_t<float>(g, nmaps, lmax, mmax, (const float2 *)alm, (float2 *)Gm, st);
-    return synthesis_t<double>(g, nmaps, lmax, mmax, (const double2 *)alm, (double2 *)Gm, st);
+                         cudaStream_t st, const float4 *ck, const int64_t *bo) {
+    if (precision == 32)
+        return synthesis_t<float>(g, nmaps, lmax, mmax, (const float2 *)alm, (float2 *)Gm, st, ck, bo);
+    return synthesis_t<double>(g, nmaps, lmax, mmax, (const double2 *)alm, (double2 *)Gm, st, nullptr, nullptr);
 }
 
 }  // namespace hb

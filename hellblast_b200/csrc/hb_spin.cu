@@ -93,7 +93,7 @@ __device__ __forceinline__ void spin_start(const GeomDev &g, int m, int64_t p, T
     mm = (T)(sm * exp2(LM - (double)SE * em));
 }
 
-constexpr int SCOEF_CH = 128;
+constexpr int SCOEF_CH = 256;  // == the plan's checkpoint block length
 
 // Per pair and parity class (even / odd l-m, slots s&1 after the l0 parity swap), the weights
 //   E += P WPE + M WME,   B += P WPB + M WMB
@@ -116,7 +116,10 @@ template <typename T, int K, int NT>
 __global__ void __launch_bounds__(NT) spin_analysis_kernel(GeomDev g, int lmax, int mmax, const c2_t<T> *__restrict__ QF,
                                                            const c2_t<T> *__restrict__ UF, int64_t fm_stride,
                                                            c2_t<T> *__restrict__ Eo, c2_t<T> *__restrict__ Bo,
-                                                           int64_t alm_stride, int atomic) {
+                                                           int64_t alm_stride, int atomic,
+                                                           const float4 *__restrict__ ckP,
+                                                           const float4 *__restrict__ ckM,
+                                                           const int64_t *__restrict__ blk_ofs) {
     using V = c2_t<T>;
     using W = v4_t<T>;
     constexpr int TL = SpinCfg<T>::TL;
@@ -179,6 +182,27 @@ __global__ void __launch_bounds__(NT) spin_analysis_kernel(GeomDev g, int lmax, 
                 coef[i] = mk4((T)a, (T)bb, (T)c, (T)0);
             }
             __syncthreads();
+            if constexpr (sizeof(T) == 4) {
+                if (ckP != nullptr && lrel > 0) {  // re-anchor both recursions on the FP64 states
+                    const int64_t row = (blk_ofs[m] + lrel / SCOEF_CH) * np;
+                    anyneg = false;
+#pragma unroll
+                    for (int k = 0; k < K; ++k) {
+                        const int64_t p = (int64_t)chunk * NT * K + (int64_t)k * NT + tid;
+                        if (p < np) {
+                            const float4 cp = ckP[row + p], cm = ckM[row + p];
+                            P1[k] = cp.x; P2[k] = cp.y; M1[k] = cm.x; M2[k] = cm.y;
+                            const int np_ = __float_as_int(cp.z), nm_ = __float_as_int(cm.z);
+                            if (np_ != ep[k] || nm_ != em[k]) {
+                                ep[k] = np_;
+                                em[k] = nm_;
+                                load_w(k, p, ep[k] >= 0, em[k] >= 0);
+                            }
+                            anyneg |= (ep[k] < 0) || (em[k] < 0);
+                        }
+                    }
+                }
+            }
         }
         const W *cf = coef + (lrel % SCOEF_CH);
 #pragma unroll
@@ -262,7 +286,9 @@ template <typename T, int K, int NT>
 __global__ void __launch_bounds__(NT) spin_synthesis_kernel(GeomDev g, int lmax, int mmax, const c2_t<T> *__restrict__ E,
                                                             const c2_t<T> *__restrict__ B, int64_t alm_stride,
                                                             c2_t<T> *__restrict__ QG, c2_t<T> *__restrict__ UG,
-                                                            int64_t gm_stride) {
+                                                            int64_t gm_stride, const float4 *__restrict__ ckP,
+                                                            const float4 *__restrict__ ckM,
+                                                            const int64_t *__restrict__ blk_ofs) {
     using V = c2_t<T>;
     using W = v4_t<T>;
     __shared__ W coef[SCOEF_CH];
@@ -314,6 +340,32 @@ __global__ void __launch_bounds__(NT) spin_synthesis_kernel(GeomDev g, int lmax,
                 aco[i] = mk4(e.x - bv.y, e.y + bv.x, e.x + bv.y, e.y - bv.x);
             }
             __syncthreads();
+            if constexpr (sizeof(T) == 4) {
+                if (ckP != nullptr && lrel > 0) {  // re-anchor both recursions on the FP64 states
+                    const int64_t row = (blk_ofs[m] + lrel / SCOEF_CH) * np;
+                    anyneg = false;
+#pragma unroll
+                    for (int k = 0; k < K; ++k) {
+                        const int64_t p = (int64_t)chunk * NT * K + (int64_t)k * NT + tid;
+                        if (p < np) {
+                            const float4 cp = ckP[row + p], cm = ckM[row + p];
+                            P1[k] = cp.x; P2[k] = cp.y; M1[k] = cm.x; M2[k] = cm.y;
+                            const int np_ = __float_as_int(cp.z), nm_ = __float_as_int(cm.z);
+                            if (np_ != ep[k]) {  // accumulators are kept in units of 2^(64 e)
+                                const float f = ldexpf(1.0f, 64 * max(-3, ep[k] - np_));
+                                for (int q = 0; q < 2; ++q) { X1[q][k] = cscale(X1[q][k], f); X3[q][k] = cscale(X3[q][k], f); }
+                                ep[k] = np_;
+                            }
+                            if (nm_ != em[k]) {
+                                const float f = ldexpf(1.0f, 64 * max(-3, em[k] - nm_));
+                                for (int q = 0; q < 2; ++q) { X2[q][k] = cscale(X2[q][k], f); X4[q][k] = cscale(X4[q][k], f); }
+                                em[k] = nm_;
+                            }
+                            anyneg |= (ep[k] < 0) || (em[k] < 0);
+                        }
+                    }
+                }
+            }
         }
         const int i0 = lrel % SCOEF_CH;
 #pragma unroll
@@ -385,7 +437,8 @@ __global__ void __launch_bounds__(NT) spin_synthesis_kernel(GeomDev g, int lmax,
 
 template <typename T, int K, int NT>
 static int run_spin_analysis(const GeomDev &g, int nmaps, int lmax, int mmax, const c2_t<T> *QF, const c2_t<T> *UF,
-                             c2_t<T> *E, c2_t<T> *B, cudaStream_t st) {
+                             c2_t<T> *E, c2_t<T> *B, cudaStream_t st, const float4 *ckP, const float4 *ckM,
+                             const int64_t *bo) {
     const int64_t per = (int64_t)K * NT;
     const int nchunks = (int)((g.npairs + per - 1) / per);
     const int64_t fm_stride = (int64_t)(mmax + 1) * g.npairs * 2;
@@ -398,56 +451,62 @@ static int run_spin_analysis(const GeomDev &g, int nmaps, int lmax, int mmax, co
     HB_CUDA_TRY(cudaFuncSetAttribute(spin_analysis_kernel<T, K, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     dim3 grid((unsigned)(mmax + 1), (unsigned)nchunks, (unsigned)nmaps);
     spin_analysis_kernel<T, K, NT><<<grid, NT, smem, st>>>(g, lmax, mmax, QF, UF, fm_stride, E, B, alm_stride,
-                                                            nchunks > 1);
+                                                            nchunks > 1, ckP, ckM, bo);
     HB_CHECK_LAUNCH();
     return HB_OK;
 }
 
 template <typename T, int K, int NT>
 static int run_spin_synthesis(const GeomDev &g, int nmaps, int lmax, int mmax, const c2_t<T> *E, const c2_t<T> *B,
-                              c2_t<T> *QG, c2_t<T> *UG, cudaStream_t st) {
+                              c2_t<T> *QG, c2_t<T> *UG, cudaStream_t st, const float4 *ckP, const float4 *ckM,
+                              const int64_t *bo) {
     const int64_t per = (int64_t)K * NT;
     const int nchunks = (int)((g.npairs + per - 1) / per);
     const int64_t gm_stride = (int64_t)(mmax + 1) * g.npairs * 2;
     const int64_t alm_stride = alm_size(lmax, mmax);
     dim3 grid((unsigned)(mmax + 1), (unsigned)nchunks, (unsigned)nmaps);
-    spin_synthesis_kernel<T, K, NT><<<grid, NT, 0, st>>>(g, lmax, mmax, E, B, alm_stride, QG, UG, gm_stride);
+    spin_synthesis_kernel<T, K, NT><<<grid, NT, 0, st>>>(g, lmax, mmax, E, B, alm_stride, QG, UG, gm_stride, ckP,
+                                                          ckM, bo);
     HB_CHECK_LAUNCH();
     return HB_OK;
 }
 
 template <typename T>
 static int spin_analysis_t(const GeomDev &g, int nmaps, int lmax, int mmax, const c2_t<T> *QF, const c2_t<T> *UF,
-                           c2_t<T> *E, c2_t<T> *B, cudaStream_t st) {
-    if (g.npairs >= 512) return run_spin_analysis<T, 4, 128>(g, nmaps, lmax, mmax, QF, UF, E, B, st);
-    if (g.npairs >= 128) return run_spin_analysis<T, 2, 64>(g, nmaps, lmax, mmax, QF, UF, E, B, st);
-    return run_spin_analysis<T, 1, 64>(g, nmaps, lmax, mmax, QF, UF, E, B, st);
+                           c2_t<T> *E, c2_t<T> *B, cudaStream_t st, const float4 *ckP, const float4 *ckM,
+                           const int64_t *bo) {
+    if (g.npairs >= 512) return run_spin_analysis<T, 4, 128>(g, nmaps, lmax, mmax, QF, UF, E, B, st, ckP, ckM, bo);
+    if (g.npairs >= 128) return run_spin_analysis<T, 2, 64>(g, nmaps, lmax, mmax, QF, UF, E, B, st, ckP, ckM, bo);
+    return run_spin_analysis<T, 1, 64>(g, nmaps, lmax, mmax, QF, UF, E, B, st, ckP, ckM, bo);
 }
 
 template <typename T>
 static int spin_synthesis_t(const GeomDev &g, int nmaps, int lmax, int mmax, const c2_t<T> *E, const c2_t<T> *B,
-                            c2_t<T> *QG, c2_t<T> *UG, cudaStream_t st) {
-    if (g.npairs >= 512) return run_spin_synthesis<T, 4, 128>(g, nmaps, lmax, mmax, E, B, QG, UG, st);
-    if (g.npairs >= 128) return run_spin_synthesis<T, 2, 64>(g, nmaps, lmax, mmax, E, B, QG, UG, st);
-    return run_spin_synthesis<T, 1, 64>(g, nmaps, lmax, mmax, E, B, QG, UG, st);
+                            c2_t<T> *QG, c2_t<T> *UG, cudaStream_t st, const float4 *ckP, const float4 *ckM,
+                            const int64_t *bo) {
+    if (g.npairs >= 512) return run_spin_synthesis<T, 4, 128>(g, nmaps, lmax, mmax, E, B, QG, UG, st, ckP, ckM, bo);
+    if (g.npairs >= 128) return run_spin_synthesis<T, 2, 64>(g, nmaps, lmax, mmax, E, B, QG, UG, st, ckP, ckM, bo);
+    return run_spin_synthesis<T, 1, 64>(g, nmaps, lmax, mmax, E, B, QG, UG, st, ckP, ckM, bo);
 }
 
 int launch_spin_analysis(const GeomDev &g, int precision, int nmaps, int lmax, int mmax, const void *QFm,
-                         const void *UFm, void *E, void *B, cudaStream_t st) {
+                         const void *UFm, void *E, void *B, cudaStream_t st, const float4 *ckP, const float4 *ckM,
+                         const int64_t *bo) {
     if (precision == 32)
         return spin_analysis_t<float>(g, nmaps, lmax, mmax, (const float2 *)QFm, (const float2 *)UFm, (float2 *)E,
-                                      (float2 *)B, st);
+                                      (float2 *)B, st, ckP, ckM, bo);
     return spin_analysis_t<double>(g, nmaps, lmax, mmax, (const double2 *)QFm, (const double2 *)UFm, (double2 *)E,
-                                   (double2 *)B, st);
+                                   (double2 *)B, st, nullptr, nullptr, nullptr);
 }
 
 int launch_spin_synthesis(const GeomDev &g, int precision, int nmaps, int lmax, int mmax, const void *E,
-                          const void *B, void *QGm, void *UGm, cudaStream_t st) {
+                          const void *B, void *QGm, void *UGm, cudaStream_t st, const float4 *ckP,
+                          const float4 *ckM, const int64_t *bo) {
     if (precision == 32)
         return spin_synthesis_t<float>(g, nmaps, lmax, mmax, (const float2 *)E, (const float2 *)B, (float2 *)QGm,
-                                       (float2 *)UGm, st);
+                                       (float2 *)UGm, st, ckP, ckM, bo);
     return spin_synthesis_t<double>(g, nmaps, lmax, mmax, (const double2 *)E, (const double2 *)B, (double2 *)QGm,
-                                    (double2 *)UGm, st);
+                                    (double2 *)UGm, st, nullptr, nullptr, nullptr);
 }
 
 }  // namespace hb

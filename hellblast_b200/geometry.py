@@ -41,10 +41,6 @@ class Geometry:
             _next_id[0] += 1
             _registry[self.gid] = self
 
-    def workspace_bytes(self, lmax: int, mmax: int, precision: int, nmaps: int, spin: bool = False) -> int:
-        fn = "hb_spin2_workspace_size" if spin else "hb_sht_workspace_size"
-        return int(getattr(L.lib(), fn)(self.handle, lmax, mmax, precision, nmaps))
-
     def __del__(self):  # pragma: no cover - interpreter shutdown order
         try:
             if self.handle:
@@ -56,6 +52,63 @@ class Geometry:
 
 def get(gid: int) -> Geometry:
     return _registry[gid]
+
+
+class Plan:
+    """Owns an ``hb_plan``: a geometry, (lmax, mmax) and, for FP32, the FP64-computed recursion
+    checkpoints.  ``pid`` is the integer the torch ops take."""
+
+    def __init__(self, geom: Geometry, lmax: int, mmax: int, flags: int):
+        self.geom = geom
+        self.lmax, self.mmax, self.flags = int(lmax), int(mmax), int(flags)
+        out = ctypes.c_void_p()
+        L.call("hb_plan_create", geom.handle, self.lmax, self.mmax, self.flags, ctypes.byref(out))
+        self.handle = out
+        self.nbytes = int(L.lib().hb_plan_bytes(out))
+        with _lock:
+            self.pid = _next_id[0]
+            _next_id[0] += 1
+            _plans[self.pid] = self
+
+    @property
+    def npix(self):
+        return self.geom.npix
+
+    def workspace_bytes(self, precision: int, nmaps: int, spin: bool = False) -> int:
+        fn = "hb_spin2_workspace_size" if spin else "hb_sht_workspace_size"
+        return int(getattr(L.lib(), fn)(self.handle, precision, nmaps))
+
+    def __del__(self):  # pragma: no cover - interpreter shutdown order
+        try:
+            if self.handle:
+                L.lib().hb_plan_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+
+_plans: dict[int, Plan] = {}
+
+
+def get_plan(pid: int) -> Plan:
+    return _plans[pid]
+
+
+def plan(geom: Geometry, lmax: int, mmax: int | None = None, precision: int = 64, spin: bool = False) -> Plan:
+    """Cached plan for (geometry, lmax, mmax); FP32 plans carry the checkpoint tables (scalar, or
+    spin-2 with ``spin=True``)."""
+    mmax = lmax if mmax is None else mmax
+    flags = 0
+    if precision == 32:
+        flags = L.HB_PLAN_SPIN2_FP32 if spin else L.HB_PLAN_FP32
+    key = ("plan", geom.gid, int(lmax), int(mmax), flags)
+    with _lock:
+        p = _cache.get(key)
+    if p is None:
+        p = Plan(geom, lmax, mmax, flags)
+        with _lock:
+            _cache[key] = p
+    return p
 
 
 def _current_device() -> int:

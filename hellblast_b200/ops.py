@@ -1,6 +1,6 @@
 """The C ABI exposed as PyTorch custom ops (``torch.ops.hb.*``): CUDA tensors in and out, the
-caller's current stream, workspace from torch's caching allocator.  Geometry handles are
-passed as integer ids (see geometry.py)."""
+caller's current stream, workspace from torch's caching allocator.  Plans (geometry + lmax +
+mmax + FP32 recursion checkpoints) are passed as integer ids (see geometry.py)."""
 from __future__ import annotations
 
 from typing import Optional
@@ -33,8 +33,8 @@ def _check_cuda(*ts):
             raise ValueError("hellblast_b200 ops take CUDA tensors (no CPU path exists)")
 
 
-def _ws(g: G.Geometry, lmax, mmax, prec, nmaps, dev, spin=False):
-    n = g.workspace_bytes(lmax, mmax, prec, nmaps, spin)
+def _ws(p: G.Plan, prec, nmaps, dev, spin=False):
+    n = p.workspace_bytes(prec, nmaps, spin)
     return torch.empty(max(n, 1), dtype=torch.uint8, device=dev)
 
 
@@ -46,137 +46,170 @@ def _wptr(w: Optional[torch.Tensor]) -> Optional[int]:
     return w.data_ptr()
 
 
+def _ctype(prec):
+    return torch.complex64 if prec == 32 else torch.complex128
+
+
+def _rtype(prec):
+    return torch.float32 if prec == 32 else torch.float64
+
+
 @torch.library.custom_op("hb::map2alm", mutates_args=())
-def map2alm(maps: torch.Tensor, gid: int, lmax: int, mmax: int, weights: Optional[torch.Tensor],
-            flags: int) -> torch.Tensor:
+def map2alm(maps: torch.Tensor, pid: int, weights: Optional[torch.Tensor], flags: int) -> torch.Tensor:
     _check_cuda(maps, weights)
-    g = G.get(gid)
+    p = G.get_plan(pid)
     maps = maps.contiguous()
-    nmaps = maps.shape[0]
-    prec = _prec(maps.dtype)
-    out = torch.empty(nmaps, alm_size(lmax, mmax), dtype=torch.complex64 if prec == 32 else torch.complex128,
-                      device=maps.device)
-    ws = _ws(g, lmax, mmax, prec, nmaps, maps.device)
-    L.call(f"hb_map2alm_f{prec}", g.handle, lmax, mmax, nmaps, maps.data_ptr(), _wptr(weights), out.data_ptr(),
-           ws.data_ptr(), ws.numel(), flags, _stream(maps.device))
+    nmaps, prec = maps.shape[0], _prec(maps.dtype)
+    out = torch.empty(nmaps, alm_size(p.lmax, p.mmax), dtype=_ctype(prec), device=maps.device)
+    ws = _ws(p, prec, nmaps, maps.device)
+    L.call(f"hb_map2alm_f{prec}", p.handle, nmaps, maps.data_ptr(), _wptr(weights), out.data_ptr(), ws.data_ptr(),
+           ws.numel(), flags, _stream(maps.device))
     return out
 
 
 @map2alm.register_fake
-def _(maps, gid, lmax, mmax, weights, flags):
-    ct = torch.complex64 if maps.dtype == torch.float32 else torch.complex128
-    return maps.new_empty((maps.shape[0], alm_size(lmax, mmax)), dtype=ct)
+def _(maps, pid, weights, flags):
+    p = G.get_plan(pid)
+    return maps.new_empty((maps.shape[0], alm_size(p.lmax, p.mmax)), dtype=_ctype(_prec(maps.dtype)))
 
 
 @torch.library.custom_op("hb::alm2map", mutates_args=())
-def alm2map(alm: torch.Tensor, gid: int, lmax: int, mmax: int, flags: int) -> torch.Tensor:
+def alm2map(alm: torch.Tensor, pid: int, flags: int) -> torch.Tensor:
     _check_cuda(alm)
-    g = G.get(gid)
+    p = G.get_plan(pid)
     alm = alm.contiguous()
-    nmaps = alm.shape[0]
-    prec = _prec(alm.dtype)
-    out = torch.empty(nmaps, g.npix, dtype=torch.float32 if prec == 32 else torch.float64, device=alm.device)
-    ws = _ws(g, lmax, mmax, prec, nmaps, alm.device)
-    L.call(f"hb_alm2map_f{prec}", g.handle, lmax, mmax, nmaps, alm.data_ptr(), out.data_ptr(), ws.data_ptr(),
-           ws.numel(), flags, _stream(alm.device))
+    nmaps, prec = alm.shape[0], _prec(alm.dtype)
+    out = torch.empty(nmaps, p.npix, dtype=_rtype(prec), device=alm.device)
+    ws = _ws(p, prec, nmaps, alm.device)
+    L.call(f"hb_alm2map_f{prec}", p.handle, nmaps, alm.data_ptr(), out.data_ptr(), ws.data_ptr(), ws.numel(), flags,
+           _stream(alm.device))
     return out
 
 
 @alm2map.register_fake
-def _(alm, gid, lmax, mmax, flags):
-    rt = torch.float32 if alm.dtype == torch.complex64 else torch.float64
-    return alm.new_empty((alm.shape[0], G.get(gid).npix), dtype=rt)
+def _(alm, pid, flags):
+    return alm.new_empty((alm.shape[0], G.get_plan(pid).npix), dtype=_rtype(_prec(alm.dtype)))
 
 
 @torch.library.custom_op("hb::alm2map_adjoint", mutates_args=())
-def alm2map_adjoint(maps: torch.Tensor, gid: int, lmax: int, mmax: int, flags: int) -> torch.Tensor:
+def alm2map_adjoint(maps: torch.Tensor, pid: int, flags: int) -> torch.Tensor:
     _check_cuda(maps)
-    g = G.get(gid)
+    p = G.get_plan(pid)
     maps = maps.contiguous()
-    nmaps = maps.shape[0]
-    prec = _prec(maps.dtype)
-    out = torch.empty(nmaps, alm_size(lmax, mmax), dtype=torch.complex64 if prec == 32 else torch.complex128,
-                      device=maps.device)
-    ws = _ws(g, lmax, mmax, prec, nmaps, maps.device)
-    L.call(f"hb_alm2map_adjoint_f{prec}", g.handle, lmax, mmax, nmaps, maps.data_ptr(), out.data_ptr(),
-           ws.data_ptr(), ws.numel(), flags, _stream(maps.device))
+    nmaps, prec = maps.shape[0], _prec(maps.dtype)
+    out = torch.empty(nmaps, alm_size(p.lmax, p.mmax), dtype=_ctype(prec), device=maps.device)
+    ws = _ws(p, prec, nmaps, maps.device)
+    L.call(f"hb_alm2map_adjoint_f{prec}", p.handle, nmaps, maps.data_ptr(), out.data_ptr(), ws.data_ptr(),
+           ws.numel(), flags, _stream(maps.device))
     return out
 
 
 @alm2map_adjoint.register_fake
-def _(maps, gid, lmax, mmax, flags):
-    ct = torch.complex64 if maps.dtype == torch.float32 else torch.complex128
-    return maps.new_empty((maps.shape[0], alm_size(lmax, mmax)), dtype=ct)
+def _(maps, pid, flags):
+    p = G.get_plan(pid)
+    return maps.new_empty((maps.shape[0], alm_size(p.lmax, p.mmax)), dtype=_ctype(_prec(maps.dtype)))
 
 
 @torch.library.custom_op("hb::map2alm_adjoint", mutates_args=())
-def map2alm_adjoint(alm: torch.Tensor, gid: int, lmax: int, mmax: int, weights: Optional[torch.Tensor],
-                    flags: int) -> torch.Tensor:
+def map2alm_adjoint(alm: torch.Tensor, pid: int, weights: Optional[torch.Tensor], flags: int) -> torch.Tensor:
     _check_cuda(alm, weights)
-    g = G.get(gid)
+    p = G.get_plan(pid)
     alm = alm.contiguous()
-    nmaps = alm.shape[0]
-    prec = _prec(alm.dtype)
-    out = torch.empty(nmaps, g.npix, dtype=torch.float32 if prec == 32 else torch.float64, device=alm.device)
-    ws = _ws(g, lmax, mmax, prec, nmaps, alm.device)
-    L.call(f"hb_map2alm_adjoint_f{prec}", g.handle, lmax, mmax, nmaps, alm.data_ptr(), _wptr(weights),
-           out.data_ptr(), ws.data_ptr(), ws.numel(), flags, _stream(alm.device))
+    nmaps, prec = alm.shape[0], _prec(alm.dtype)
+    out = torch.empty(nmaps, p.npix, dtype=_rtype(prec), device=alm.device)
+    ws = _ws(p, prec, nmaps, alm.device)
+    L.call(f"hb_map2alm_adjoint_f{prec}", p.handle, nmaps, alm.data_ptr(), _wptr(weights), out.data_ptr(),
+           ws.data_ptr(), ws.numel(), flags, _stream(alm.device))
     return out
 
 
 @map2alm_adjoint.register_fake
-def _(alm, gid, lmax, mmax, weights, flags):
-    rt = torch.float32 if alm.dtype == torch.complex64 else torch.float64
-    return alm.new_empty((alm.shape[0], G.get(gid).npix), dtype=rt)
+def _(alm, pid, weights, flags):
+    return alm.new_empty((alm.shape[0], G.get_plan(pid).npix), dtype=_rtype(_prec(alm.dtype)))
 
 
 @torch.library.custom_op("hb::map2alm_spin2", mutates_args=())
-def map2alm_spin2(Q: torch.Tensor, U: torch.Tensor, gid: int, lmax: int, mmax: int,
-                  weights: Optional[torch.Tensor], flags: int) -> tuple[torch.Tensor, torch.Tensor]:
+def map2alm_spin2(Q: torch.Tensor, U: torch.Tensor, pid: int, weights: Optional[torch.Tensor],
+                  flags: int) -> tuple[torch.Tensor, torch.Tensor]:
     _check_cuda(Q, U, weights)
-    g = G.get(gid)
-    Q = Q.contiguous()
-    U = U.contiguous()
-    nmaps = Q.shape[0]
-    prec = _prec(Q.dtype)
-    ct = torch.complex64 if prec == 32 else torch.complex128
-    E = torch.empty(nmaps, alm_size(lmax, mmax), dtype=ct, device=Q.device)
+    p = G.get_plan(pid)
+    Q, U = Q.contiguous(), U.contiguous()
+    nmaps, prec = Q.shape[0], _prec(Q.dtype)
+    E = torch.empty(nmaps, alm_size(p.lmax, p.mmax), dtype=_ctype(prec), device=Q.device)
     B = torch.empty_like(E)
-    ws = _ws(g, lmax, mmax, prec, nmaps, Q.device, spin=True)
-    L.call(f"hb_map2alm_spin2_f{prec}", g.handle, lmax, mmax, nmaps, Q.data_ptr(), U.data_ptr(), _wptr(weights),
-           E.data_ptr(), B.data_ptr(), ws.data_ptr(), ws.numel(), flags, _stream(Q.device))
+    ws = _ws(p, prec, nmaps, Q.device, spin=True)
+    L.call(f"hb_map2alm_spin2_f{prec}", p.handle, nmaps, Q.data_ptr(), U.data_ptr(), _wptr(weights), E.data_ptr(),
+           B.data_ptr(), ws.data_ptr(), ws.numel(), flags, _stream(Q.device))
     return E, B
 
 
 @map2alm_spin2.register_fake
-def _(Q, U, gid, lmax, mmax, weights, flags):
-    ct = torch.complex64 if Q.dtype == torch.float32 else torch.complex128
-    e = Q.new_empty((Q.shape[0], alm_size(lmax, mmax)), dtype=ct)
+def _(Q, U, pid, weights, flags):
+    p = G.get_plan(pid)
+    e = Q.new_empty((Q.shape[0], alm_size(p.lmax, p.mmax)), dtype=_ctype(_prec(Q.dtype)))
     return e, torch.empty_like(e)
 
 
 @torch.library.custom_op("hb::alm2map_spin2", mutates_args=())
-def alm2map_spin2(E: torch.Tensor, B: torch.Tensor, gid: int, lmax: int, mmax: int,
-                  flags: int) -> tuple[torch.Tensor, torch.Tensor]:
+def alm2map_spin2(E: torch.Tensor, B: torch.Tensor, pid: int, flags: int) -> tuple[torch.Tensor, torch.Tensor]:
     _check_cuda(E, B)
-    g = G.get(gid)
-    E = E.contiguous()
-    B = B.contiguous()
-    nmaps = E.shape[0]
-    prec = _prec(E.dtype)
-    rt = torch.float32 if prec == 32 else torch.float64
-    Q = torch.empty(nmaps, g.npix, dtype=rt, device=E.device)
+    p = G.get_plan(pid)
+    E, B = E.contiguous(), B.contiguous()
+    nmaps, prec = E.shape[0], _prec(E.dtype)
+    Q = torch.empty(nmaps, p.npix, dtype=_rtype(prec), device=E.device)
     U = torch.empty_like(Q)
-    ws = _ws(g, lmax, mmax, prec, nmaps, E.device, spin=True)
-    L.call(f"hb_alm2map_spin2_f{prec}", g.handle, lmax, mmax, nmaps, E.data_ptr(), B.data_ptr(), Q.data_ptr(),
-           U.data_ptr(), ws.data_ptr(), ws.numel(), flags, _stream(E.device))
+    ws = _ws(p, prec, nmaps, E.device, spin=True)
+    L.call(f"hb_alm2map_spin2_f{prec}", p.handle, nmaps, E.data_ptr(), B.data_ptr(), Q.data_ptr(), U.data_ptr(),
+           ws.data_ptr(), ws.numel(), flags, _stream(E.device))
     return Q, U
 
 
 @alm2map_spin2.register_fake
-def _(E, B, gid, lmax, mmax, flags):
-    rt = torch.float32 if E.dtype == torch.complex64 else torch.float64
-    q = E.new_empty((E.shape[0], G.get(gid).npix), dtype=rt)
+def _(E, B, pid, flags):
+    q = E.new_empty((E.shape[0], G.get_plan(pid).npix), dtype=_rtype(_prec(E.dtype)))
+    return q, torch.empty_like(q)
+
+
+@torch.library.custom_op("hb::alm2map_spin2_adjoint", mutates_args=())
+def alm2map_spin2_adjoint(gQ: torch.Tensor, gU: torch.Tensor, pid: int,
+                          flags: int) -> tuple[torch.Tensor, torch.Tensor]:
+    _check_cuda(gQ, gU)
+    p = G.get_plan(pid)
+    gQ, gU = gQ.contiguous(), gU.contiguous()
+    nmaps, prec = gQ.shape[0], _prec(gQ.dtype)
+    gE = torch.empty(nmaps, alm_size(p.lmax, p.mmax), dtype=_ctype(prec), device=gQ.device)
+    gB = torch.empty_like(gE)
+    ws = _ws(p, prec, nmaps, gQ.device, spin=True)
+    L.call(f"hb_alm2map_spin2_adjoint_f{prec}", p.handle, nmaps, gQ.data_ptr(), gU.data_ptr(), gE.data_ptr(),
+           gB.data_ptr(), ws.data_ptr(), ws.numel(), flags, _stream(gQ.device))
+    return gE, gB
+
+
+@alm2map_spin2_adjoint.register_fake
+def _(gQ, gU, pid, flags):
+    p = G.get_plan(pid)
+    e = gQ.new_empty((gQ.shape[0], alm_size(p.lmax, p.mmax)), dtype=_ctype(_prec(gQ.dtype)))
+    return e, torch.empty_like(e)
+
+
+@torch.library.custom_op("hb::map2alm_spin2_adjoint", mutates_args=())
+def map2alm_spin2_adjoint(gE: torch.Tensor, gB: torch.Tensor, pid: int, weights: Optional[torch.Tensor],
+                          flags: int) -> tuple[torch.Tensor, torch.Tensor]:
+    _check_cuda(gE, gB, weights)
+    p = G.get_plan(pid)
+    gE, gB = gE.contiguous(), gB.contiguous()
+    nmaps, prec = gE.shape[0], _prec(gE.dtype)
+    gQ = torch.empty(nmaps, p.npix, dtype=_rtype(prec), device=gE.device)
+    gU = torch.empty_like(gQ)
+    ws = _ws(p, prec, nmaps, gE.device, spin=True)
+    L.call(f"hb_map2alm_spin2_adjoint_f{prec}", p.handle, nmaps, gE.data_ptr(), gB.data_ptr(), _wptr(weights),
+           gQ.data_ptr(), gU.data_ptr(), ws.data_ptr(), ws.numel(), flags, _stream(gE.device))
+    return gQ, gU
+
+
+@map2alm_spin2_adjoint.register_fake
+def _(gE, gB, pid, weights, flags):
+    q = gE.new_empty((gE.shape[0], G.get_plan(pid).npix), dtype=_rtype(_prec(gE.dtype)))
     return q, torch.empty_like(q)
 
 
@@ -186,8 +219,7 @@ def alm2cl(alm1: torch.Tensor, alm2: Optional[torch.Tensor], lmax: int, mmax: in
     alm1 = alm1.contiguous()
     if alm2 is not None:
         alm2 = alm2.contiguous().to(alm1.dtype)
-    nmaps = alm1.shape[0]
-    prec = _prec(alm1.dtype)
+    nmaps, prec = alm1.shape[0], _prec(alm1.dtype)
     cl = torch.empty(nmaps, lmax + 1, dtype=torch.float64, device=alm1.device)
     L.call(f"hb_alm2cl_f{prec}", lmax, mmax, nmaps, alm1.data_ptr(), None if alm2 is None else alm2.data_ptr(),
            cl.data_ptr(), _stream(alm1.device))
@@ -212,53 +244,3 @@ def ring_tables(nside: int, phi0_mode: int, device) -> dict:
            out["phi0"].data_ptr(), out["ring_start"].data_ptr(), out["z_edges"].data_ptr(),
            out["weights_dz"].data_ptr(), _stream(dev))
     return out
-
-
-@torch.library.custom_op("hb::alm2map_spin2_adjoint", mutates_args=())
-def alm2map_spin2_adjoint(gQ: torch.Tensor, gU: torch.Tensor, gid: int, lmax: int, mmax: int,
-                          flags: int) -> tuple[torch.Tensor, torch.Tensor]:
-    _check_cuda(gQ, gU)
-    g = G.get(gid)
-    gQ = gQ.contiguous()
-    gU = gU.contiguous()
-    nmaps = gQ.shape[0]
-    prec = _prec(gQ.dtype)
-    ct = torch.complex64 if prec == 32 else torch.complex128
-    gE = torch.empty(nmaps, alm_size(lmax, mmax), dtype=ct, device=gQ.device)
-    gB = torch.empty_like(gE)
-    ws = _ws(g, lmax, mmax, prec, nmaps, gQ.device, spin=True)
-    L.call(f"hb_alm2map_spin2_adjoint_f{prec}", g.handle, lmax, mmax, nmaps, gQ.data_ptr(), gU.data_ptr(),
-           gE.data_ptr(), gB.data_ptr(), ws.data_ptr(), ws.numel(), flags, _stream(gQ.device))
-    return gE, gB
-
-
-@alm2map_spin2_adjoint.register_fake
-def _(gQ, gU, gid, lmax, mmax, flags):
-    ct = torch.complex64 if gQ.dtype == torch.float32 else torch.complex128
-    e = gQ.new_empty((gQ.shape[0], alm_size(lmax, mmax)), dtype=ct)
-    return e, torch.empty_like(e)
-
-
-@torch.library.custom_op("hb::map2alm_spin2_adjoint", mutates_args=())
-def map2alm_spin2_adjoint(gE: torch.Tensor, gB: torch.Tensor, gid: int, lmax: int, mmax: int,
-                          weights: Optional[torch.Tensor], flags: int) -> tuple[torch.Tensor, torch.Tensor]:
-    _check_cuda(gE, gB, weights)
-    g = G.get(gid)
-    gE = gE.contiguous()
-    gB = gB.contiguous()
-    nmaps = gE.shape[0]
-    prec = _prec(gE.dtype)
-    rt = torch.float32 if prec == 32 else torch.float64
-    gQ = torch.empty(nmaps, g.npix, dtype=rt, device=gE.device)
-    gU = torch.empty_like(gQ)
-    ws = _ws(g, lmax, mmax, prec, nmaps, gE.device, spin=True)
-    L.call(f"hb_map2alm_spin2_adjoint_f{prec}", g.handle, lmax, mmax, nmaps, gE.data_ptr(), gB.data_ptr(),
-           _wptr(weights), gQ.data_ptr(), gU.data_ptr(), ws.data_ptr(), ws.numel(), flags, _stream(gE.device))
-    return gQ, gU
-
-
-@map2alm_spin2_adjoint.register_fake
-def _(gE, gB, gid, lmax, mmax, weights, flags):
-    rt = torch.float32 if gE.dtype == torch.complex64 else torch.float64
-    q = gE.new_empty((gE.shape[0], G.get(gid).npix), dtype=rt)
-    return q, torch.empty_like(q)

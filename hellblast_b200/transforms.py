@@ -63,7 +63,8 @@ def map2alm(maps, g: G.Geometry, lmax: int, mmax: int | None = None, weights=Non
     t = t.reshape(-1, g.npix).to(rt).contiguous()
     if ref_compat not in REF_COMPAT:
         raise ValueError("ref_compat must be None, 'fallback' or 'raw'")
-    alm = ops.map2alm(t, g.gid, lmax, mmax, device_weights(weights, g, t.device), REF_COMPAT[ref_compat])
+    p = G.plan(g, lmax, mmax, precision=32 if rt == torch.float32 else 64)
+    alm = ops.map2alm(t, p.pid, device_weights(weights, g, t.device), REF_COMPAT[ref_compat])
     if ref_compat == "raw":
         mcut = min(mmax, int(np.max(g.nphi)) // 2)  # sht_raw.py:43 mmax_eff
         if mcut < mmax:
@@ -82,7 +83,8 @@ def alm2map(alm, g: G.Geometry, lmax: int, mmax: int | None = None, precision=No
         raise ValueError(f"alm has {t.shape[-1]} entries, expected {ops.alm_size(lmax, mmax)} for "
                          f"lmax={lmax}, mmax={mmax}")
     flags = L.HB_F_NOPHASE if ref_compat else 0
-    out = ops.alm2map(t, g.gid, lmax, mmax, flags)
+    p = G.plan(g, lmax, mmax, precision=32 if rt == torch.float32 else 64)
+    out = ops.alm2map(t, p.pid, flags)
     return out[0] if squeeze else out
 
 
@@ -94,7 +96,8 @@ def map2alm_spin2(Q, U, g: G.Geometry, lmax: int, mmax: int | None = None, weigh
     squeeze = q.dim() == 1
     q = q.reshape(-1, g.npix).to(rt).contiguous()
     u = u.reshape(-1, g.npix).to(rt).contiguous()
-    E, B = ops.map2alm_spin2(q, u, g.gid, lmax, mmax, device_weights(weights, g, q.device), 0)
+    p = G.plan(g, lmax, mmax, precision=32 if rt == torch.float32 else 64, spin=True)
+    E, B = ops.map2alm_spin2(q, u, p.pid, device_weights(weights, g, q.device), 0)
     return (E[0], B[0]) if squeeze else (E, B)
 
 
@@ -107,7 +110,8 @@ def alm2map_spin2(E, B, g: G.Geometry, lmax: int, mmax: int | None = None, preci
     squeeze = e.dim() == 1
     e = e.reshape(-1, e.shape[-1]).to(ct).contiguous()
     b = b.reshape(-1, b.shape[-1]).to(ct).contiguous()
-    Q, U = ops.alm2map_spin2(e, b, g.gid, lmax, mmax, 0)
+    p = G.plan(g, lmax, mmax, precision=32 if rt == torch.float32 else 64, spin=True)
+    Q, U = ops.alm2map_spin2(e, b, p.pid, 0)
     return (Q[0], U[0]) if squeeze else (Q, U)
 
 

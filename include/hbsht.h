@@ -96,62 +96,74 @@ HB_API int hb_geom_destroy(hb_geom *g);
 /* nr, npix, ring pairs used by the Legendre kernels, nside (0 if not HEALPix) */
 HB_API int hb_geom_info(const hb_geom *g, int64_t *nr, int64_t *npix, int64_t *npairs, int64_t *nside);
 
+/* Transform plans: a geometry plus (lmax, mmax) plus the FP64-computed checkpoints that
+ * re-anchor the FP32 Legendre recursions every 256 l (FP32 transforms need them to stay within
+ * 1e-5 of FP64 at lmax ~ 4000; FP64 transforms do not use them).  Creating a plan allocates
+ * (about 16 bytes per (m, 256-block of l, ring pair) per table) and runs one FP64 pass; plans
+ * are immutable afterwards and may be shared across threads and streams.  The geometry must
+ * outlive the plan. */
+typedef struct hb_plan hb_plan;
+enum { HB_PLAN_FP32 = 1, HB_PLAN_SPIN2_FP32 = 2 };
+HB_API int hb_plan_create(const hb_geom *g, int lmax, int mmax, int flags, hb_plan **out);
+HB_API int hb_plan_destroy(hb_plan *p);
+HB_API size_t hb_plan_bytes(const hb_plan *p);
+
 /* Workspace bytes for one call of the transform family; precision 32 or 64. */
-HB_API size_t hb_sht_workspace_size(const hb_geom *g, int lmax, int mmax, int precision, int nmaps);
-HB_API size_t hb_spin2_workspace_size(const hb_geom *g, int lmax, int mmax, int precision, int nmaps);
+HB_API size_t hb_sht_workspace_size(const hb_plan *p, int precision, int nmaps);
+HB_API size_t hb_spin2_workspace_size(const hb_plan *p, int precision, int nmaps);
 
 /* map2alm: alm = sum_pix (2 pi w_r / nphi_r) f(pix) conj(Y_lm(pix)).  maps [nmaps][npix],
- * alm [nmaps][nalm] complex.  weights: device [nr] per-ring weights or NULL (geometry's). */
-HB_API int hb_map2alm_f32(const hb_geom *g, int lmax, int mmax, int nmaps, const float *maps, const double *weights,
-                   float *alm, void *ws, size_t ws_bytes, int flags, hb_stream_t stream);
-HB_API int hb_map2alm_f64(const hb_geom *g, int lmax, int mmax, int nmaps, const double *maps, const double *weights,
-                   double *alm, void *ws, size_t ws_bytes, int flags, hb_stream_t stream);
+ * alm [nmaps][nalm] complex.  weights: device [nr] per-ring weights or NULL (geometry's).
+ * FP32 needs a plan made with HB_PLAN_FP32. */
+HB_API int hb_map2alm_f32(const hb_plan *p, int nmaps, const float *maps, const double *weights, float *alm,
+                          void *ws, size_t ws_bytes, int flags, hb_stream_t stream);
+HB_API int hb_map2alm_f64(const hb_plan *p, int nmaps, const double *maps, const double *weights, double *alm,
+                          void *ws, size_t ws_bytes, int flags, hb_stream_t stream);
 
 /* alm2map: f(pix) = sum_lm a_lm Y_lm(pix) (real field: m>0 counted twice). */
-HB_API int hb_alm2map_f32(const hb_geom *g, int lmax, int mmax, int nmaps, const float *alm, float *maps,
-                   void *ws, size_t ws_bytes, int flags, hb_stream_t stream);
-HB_API int hb_alm2map_f64(const hb_geom *g, int lmax, int mmax, int nmaps, const double *alm, double *maps,
-                   void *ws, size_t ws_bytes, int flags, hb_stream_t stream);
+HB_API int hb_alm2map_f32(const hb_plan *p, int nmaps, const float *alm, float *maps, void *ws, size_t ws_bytes,
+                          int flags, hb_stream_t stream);
+HB_API int hb_alm2map_f64(const hb_plan *p, int nmaps, const double *alm, double *maps, void *ws, size_t ws_bytes,
+                          int flags, hb_stream_t stream);
 
 /* Exact adjoints (transposes, Re and Im of alm as independent real coordinates):
  *   hb_alm2map_adjoint: map-space vector -> alm-space vector, includes the m>0 doubling;
  *   hb_map2alm_adjoint: alm-space vector -> map-space vector, includes the pixel weights. */
-HB_API int hb_alm2map_adjoint_f32(const hb_geom *g, int lmax, int mmax, int nmaps, const float *maps, float *alm,
-                           void *ws, size_t ws_bytes, int flags, hb_stream_t stream);
-HB_API int hb_alm2map_adjoint_f64(const hb_geom *g, int lmax, int mmax, int nmaps, const double *maps, double *alm,
-                           void *ws, size_t ws_bytes, int flags, hb_stream_t stream);
-HB_API int hb_map2alm_adjoint_f32(const hb_geom *g, int lmax, int mmax, int nmaps, const float *alm, const double *weights,
-                           float *maps, void *ws, size_t ws_bytes, int flags, hb_stream_t stream);
-HB_API int hb_map2alm_adjoint_f64(const hb_geom *g, int lmax, int mmax, int nmaps, const double *alm, const double *weights,
-                           double *maps, void *ws, size_t ws_bytes, int flags, hb_stream_t stream);
+HB_API int hb_alm2map_adjoint_f32(const hb_plan *p, int nmaps, const float *maps, float *alm, void *ws,
+                                  size_t ws_bytes, int flags, hb_stream_t stream);
+HB_API int hb_alm2map_adjoint_f64(const hb_plan *p, int nmaps, const double *maps, double *alm, void *ws,
+                                  size_t ws_bytes, int flags, hb_stream_t stream);
+HB_API int hb_map2alm_adjoint_f32(const hb_plan *p, int nmaps, const float *alm, const double *weights, float *maps,
+                                  void *ws, size_t ws_bytes, int flags, hb_stream_t stream);
+HB_API int hb_map2alm_adjoint_f64(const hb_plan *p, int nmaps, const double *alm, const double *weights,
+                                  double *maps, void *ws, size_t ws_bytes, int flags, hb_stream_t stream);
 
-/* Spin-2: Q/U maps -> E/B alm (E = -(a2+a-2)/2, B = i(a2-a-2)/2, healpy convention) and back. */
-HB_API int hb_map2alm_spin2_f32(const hb_geom *g, int lmax, int mmax, int nmaps, const float *Q, const float *U,
-                         const double *weights, float *E, float *B, void *ws, size_t ws_bytes, int flags,
-                         hb_stream_t stream);
-HB_API int hb_map2alm_spin2_f64(const hb_geom *g, int lmax, int mmax, int nmaps, const double *Q, const double *U,
-                         const double *weights, double *E, double *B, void *ws, size_t ws_bytes, int flags,
-                         hb_stream_t stream);
-HB_API int hb_alm2map_spin2_f32(const hb_geom *g, int lmax, int mmax, int nmaps, const float *E, const float *B,
-                         float *Q, float *U, void *ws, size_t ws_bytes, int flags, hb_stream_t stream);
-HB_API int hb_alm2map_spin2_f64(const hb_geom *g, int lmax, int mmax, int nmaps, const double *E, const double *B,
-                         double *Q, double *U, void *ws, size_t ws_bytes, int flags, hb_stream_t stream);
+/* Spin-2: Q/U maps -> E/B alm (E = -(a2+a-2)/2, B = i(a2-a-2)/2, healpy convention) and back.
+ * FP32 needs a plan made with HB_PLAN_SPIN2_FP32. */
+HB_API int hb_map2alm_spin2_f32(const hb_plan *p, int nmaps, const float *Q, const float *U, const double *weights,
+                                float *E, float *B, void *ws, size_t ws_bytes, int flags, hb_stream_t stream);
+HB_API int hb_map2alm_spin2_f64(const hb_plan *p, int nmaps, const double *Q, const double *U,
+                                const double *weights, double *E, double *B, void *ws, size_t ws_bytes, int flags,
+                                hb_stream_t stream);
+HB_API int hb_alm2map_spin2_f32(const hb_plan *p, int nmaps, const float *E, const float *B, float *Q, float *U,
+                                void *ws, size_t ws_bytes, int flags, hb_stream_t stream);
+HB_API int hb_alm2map_spin2_f64(const hb_plan *p, int nmaps, const double *E, const double *B, double *Q, double *U,
+                                void *ws, size_t ws_bytes, int flags, hb_stream_t stream);
 
 /* Exact adjoints of the spin-2 pair (transposes over Re/Im of E and B):
  *   hb_alm2map_spin2_adjoint: (gQ, gU) -> (gE, gB), includes the m>0 doubling;
  *   hb_map2alm_spin2_adjoint: (gE, gB) -> (gQ, gU), includes the pixel weights. */
-HB_API int hb_alm2map_spin2_adjoint_f32(const hb_geom *g, int lmax, int mmax, int nmaps, const float *gQ,
-                                        const float *gU, float *gE, float *gB, void *ws, size_t ws_bytes, int flags,
+HB_API int hb_alm2map_spin2_adjoint_f32(const hb_plan *p, int nmaps, const float *gQ, const float *gU, float *gE,
+                                        float *gB, void *ws, size_t ws_bytes, int flags, hb_stream_t stream);
+HB_API int hb_alm2map_spin2_adjoint_f64(const hb_plan *p, int nmaps, const double *gQ, const double *gU,
+                                        double *gE, double *gB, void *ws, size_t ws_bytes, int flags,
                                         hb_stream_t stream);
-HB_API int hb_alm2map_spin2_adjoint_f64(const hb_geom *g, int lmax, int mmax, int nmaps, const double *gQ,
-                                        const double *gU, double *gE, double *gB, void *ws, size_t ws_bytes,
+HB_API int hb_map2alm_spin2_adjoint_f32(const hb_plan *p, int nmaps, const float *gE, const float *gB,
+                                        const double *weights, float *gQ, float *gU, void *ws, size_t ws_bytes,
                                         int flags, hb_stream_t stream);
-HB_API int hb_map2alm_spin2_adjoint_f32(const hb_geom *g, int lmax, int mmax, int nmaps, const float *gE,
-                                        const float *gB, const double *weights, float *gQ, float *gU, void *ws,
-                                        size_t ws_bytes, int flags, hb_stream_t stream);
-HB_API int hb_map2alm_spin2_adjoint_f64(const hb_geom *g, int lmax, int mmax, int nmaps, const double *gE,
-                                        const double *gB, const double *weights, double *gQ, double *gU, void *ws,
-                                        size_t ws_bytes, int flags, hb_stream_t stream);
+HB_API int hb_map2alm_spin2_adjoint_f64(const hb_plan *p, int nmaps, const double *gE, const double *gB,
+                                        const double *weights, double *gQ, double *gU, void *ws, size_t ws_bytes,
+                                        int flags, hb_stream_t stream);
 
 /* alm2cl: cl[l] = (Re a_l0 b_l0* + 2 sum_{m>0} Re a_lm b_lm*) / (2l+1); alm2 may be NULL
  * (auto spectrum).  cl is always double [nmaps][lmax+1]. */
@@ -168,14 +180,14 @@ HB_API int hb_alm2cl_f64(int lmax, int mmax, int nmaps, const double *alm1, cons
  *   hb_legendre_synthesis: alm -> G
  *   hb_ring_synthesis:     G -> maps
  * (sht_raw.py:38-43 / 46-56 and isht.py:11-25 are the reference's versions of these steps.) */
-HB_API int hb_ring_analysis(const hb_geom *g, int precision, int mmax, int nmaps, const void *maps,
-                            const double *weights, void *F, int flags, hb_stream_t stream);
-HB_API int hb_ring_synthesis(const hb_geom *g, int precision, int mmax, int nmaps, const void *G, void *maps, int flags,
+HB_API int hb_ring_analysis(const hb_plan *p, int precision, int nmaps, const void *maps, const double *weights,
+                            void *F, int flags, hb_stream_t stream);
+HB_API int hb_ring_synthesis(const hb_plan *p, int precision, int nmaps, const void *G, void *maps, int flags,
                              hb_stream_t stream);
-HB_API int hb_legendre_analysis(const hb_geom *g, int precision, int lmax, int mmax, int nmaps, const void *F,
-                                void *alm, hb_stream_t stream);
-HB_API int hb_legendre_synthesis(const hb_geom *g, int precision, int lmax, int mmax, int nmaps, const void *alm,
-                                 void *G, hb_stream_t stream);
+HB_API int hb_legendre_analysis(const hb_plan *p, int precision, int nmaps, const void *F, void *alm,
+                                hb_stream_t stream);
+HB_API int hb_legendre_synthesis(const hb_plan *p, int precision, int nmaps, const void *alm, void *G,
+                                 hb_stream_t stream);
 
 /* Diagnostics (no reference counterpart): FP32 FMA throughput probe, blocks*threads threads
  * each running iters*8 FMAs; out holds blocks*threads floats.  Used by bench.py to measure the

@@ -61,7 +61,9 @@ def test_host_side_argument_errors():
     assert b"power of 2" in lib.hb_last_error_string()
     assert lib.hb_geom_create_healpix(8, 7, 0, ctypes.byref(out)) == L.HB_ERR_INVALID
     assert lib.hb_ring_tables(6, 0, None, None, None, None, None, None, None, None) == L.HB_ERR_INVALID
-    assert lib.hb_map2alm_f32(None, 10, 10, 1, None, None, None, None, 0, 0, None) == L.HB_ERR_INVALID
+    assert lib.hb_map2alm_f32(None, 1, None, None, None, None, 0, 0, None) == L.HB_ERR_INVALID
+    assert b"null plan" in lib.hb_last_error_string()
+    assert lib.hb_plan_create(None, 10, 10, 0, ctypes.byref(out)) == L.HB_ERR_INVALID
     assert lib.hb_alm2cl_f64(-1, 0, 1, None, None, None, None) == L.HB_ERR_INVALID
     th = np.array([0.5, 4.0]); nphi = np.array([4, 3], dtype=np.int32); w = np.ones(2)
     assert lib.hb_geom_create(2, th.ctypes.data, nphi.ctypes.data, None, w.ctypes.data,

@@ -217,3 +217,19 @@ def test_cupy_style_ring_list_input(hb, oracle):
     rings = [mp[g["ring_start"][r]:g["ring_start"][r + 1]] for r in range(g["nr"])]
     alm = npy(hb.map2alm_gpu(rings, g["theta"], g["nphi"], g["weights_dz"], lmax))
     assert relmax(alm, oracle.map2alm(mp, g, lmax)) < TOL64
+
+
+@pytest.mark.parametrize("nside", [1024, 2048])
+def test_fp32_pair_accuracy_at_full_size(hb, nside):
+    """The north-star accuracy bar: FP32 alm2map + map2alm within 1e-5 (relative L2) of the same
+    pair in FP64 at lmax = 2 nside - 1 (the FP64 path itself is pinned to the oracle above)."""
+    lmax = 2 * nside - 1
+    cl = 1.0 / (np.arange(lmax + 1) + 10.0) ** 2
+    a64 = hb.synalm(cl, lmax=lmax, seed=1, device="cuda")
+    m64 = hb.hp_compat.alm2map(a64, nside, lmax=lmax)
+    b64 = hb.hp_compat.map2alm(m64, lmax=lmax)
+    m32 = hb.hp_compat.alm2map(a64.to(torch.complex64), nside, lmax=lmax)
+    b32 = hb.hp_compat.map2alm(m32, lmax=lmax)
+    err_map = float(torch.linalg.norm(m32.double() - m64) / torch.linalg.norm(m64))
+    err_alm = float(torch.linalg.norm(b32.to(torch.complex128) - b64) / torch.linalg.norm(b64))
+    assert err_map < TOL32 and err_alm < TOL32, (err_map, err_alm)

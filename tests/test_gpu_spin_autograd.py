@@ -100,18 +100,19 @@ def test_adjoint_dot_products(hb, prec):
     ct = torch.complex128 if prec == "fp64" else torch.complex64
     tol = 1e-12 if prec == "fp64" else 1e-5
     g = hb.geometry.healpix(nside)
+    pid = hb.geometry.plan(g, lmax, precision=32 if prec == "fp32" else 64).pid
     x = torch.randn(1, g.npix, dtype=torch.float64, generator=torch.Generator().manual_seed(0)).to(rt).cuda()
     y = _rand_alm(hb, lmax, 1, ct)[None]
-    A_x = torch.ops.hb.map2alm(x, g.gid, lmax, lmax, None, 0)
-    At_y = torch.ops.hb.map2alm_adjoint(y, g.gid, lmax, lmax, None, 0)
+    A_x = torch.ops.hb.map2alm(x, pid, None, 0)
+    At_y = torch.ops.hb.map2alm_adjoint(y, pid, None, 0)
     lhs, rhs = _dot_c(A_x, y), float((x * At_y).sum())
     assert abs(lhs - rhs) <= tol * abs(lhs)
-    S_y = torch.ops.hb.alm2map(y, g.gid, lmax, lmax, 0)
-    St_x = torch.ops.hb.alm2map_adjoint(x, g.gid, lmax, lmax, 0)
+    S_y = torch.ops.hb.alm2map(y, pid, 0)
+    St_x = torch.ops.hb.alm2map_adjoint(x, pid, 0)
     # imaginary parts of m = 0 do not enter a real map: drop them from y for the identity
     y0 = y.clone()
     y0[:, :lmax + 1] = y0[:, :lmax + 1].real.to(ct)
-    lhs, rhs = float((torch.ops.hb.alm2map(y0, g.gid, lmax, lmax, 0) * x).sum()), _dot_c(St_x, y0)
+    lhs, rhs = float((torch.ops.hb.alm2map(y0, pid, 0) * x).sum()), _dot_c(St_x, y0)
     assert abs(lhs - rhs) <= tol * abs(lhs)
     assert torch.all(St_x[:, :lmax + 1].imag == 0)
     del S_y
@@ -120,17 +121,18 @@ def test_adjoint_dot_products(hb, prec):
 def test_spin_adjoint_dot_products(hb):
     nside, lmax = 16, 40
     g = hb.geometry.healpix(nside)
+    pid = hb.geometry.plan(g, lmax, precision=64, spin=True).pid
     gen = torch.Generator().manual_seed(3)
     Q = torch.randn(1, g.npix, dtype=torch.float64, generator=gen).cuda()
     U = torch.randn(1, g.npix, dtype=torch.float64, generator=gen).cuda()
     e, b = _rand_alm(hb, lmax, 4)[None], _rand_alm(hb, lmax, 5)[None]
-    E, B = torch.ops.hb.map2alm_spin2(Q, U, g.gid, lmax, lmax, None, 0)
-    gQ, gU = torch.ops.hb.map2alm_spin2_adjoint(e, b, g.gid, lmax, lmax, None, 0)
+    E, B = torch.ops.hb.map2alm_spin2(Q, U, pid, None, 0)
+    gQ, gU = torch.ops.hb.map2alm_spin2_adjoint(e, b, pid, None, 0)
     lhs = _dot_c(E, e) + _dot_c(B, b)
     rhs = float((Q * gQ).sum() + (U * gU).sum())
     assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
-    q, u = torch.ops.hb.alm2map_spin2(e, b, g.gid, lmax, lmax, 0)
-    ge, gb = torch.ops.hb.alm2map_spin2_adjoint(Q, U, g.gid, lmax, lmax, 0)
+    q, u = torch.ops.hb.alm2map_spin2(e, b, pid, 0)
+    ge, gb = torch.ops.hb.alm2map_spin2_adjoint(Q, U, pid, 0)
     # l < 2 and the m = 0 imaginary parts do not enter Q/U
     mask = torch.ones_like(e.real)
     for m in range(0, 2):
@@ -140,7 +142,7 @@ def test_spin_adjoint_dot_products(hb):
     b0 = b * mask
     e0[:, :lmax + 1] = e0[:, :lmax + 1].real.to(e.dtype)
     b0[:, :lmax + 1] = b0[:, :lmax + 1].real.to(e.dtype)
-    q0, u0 = torch.ops.hb.alm2map_spin2(e0, b0, g.gid, lmax, lmax, 0)
+    q0, u0 = torch.ops.hb.alm2map_spin2(e0, b0, pid, 0)
     lhs = float((q0 * Q).sum() + (u0 * U).sum())
     rhs = _dot_c(ge, e0) + _dot_c(gb, b0)
     assert abs(lhs - rhs) <= 1e-12 * abs(lhs)
@@ -152,6 +154,7 @@ def test_dense_matrix_small_nside(hb, oracle):
     GPU kernels) and check the adjoint kernels reproduce their transposes exactly."""
     nside, lmax = 2, 5
     g = hb.geometry.healpix(nside)
+    pid = hb.geometry.plan(g, lmax).pid
     n = hb.alm_size(lmax)
     npix = g.npix
     # real coordinates of alm: Re(a_lm) for all, Im(a_lm) for m > 0
@@ -159,14 +162,14 @@ def test_dense_matrix_small_nside(hb, oracle):
     eye = torch.zeros(len(coords), n, dtype=torch.complex128, device="cuda")
     for j, (k, part) in enumerate(coords):
         eye[j, k] = 1.0 if part == 0 else 1j
-    S = torch.ops.hb.alm2map(eye, g.gid, lmax, lmax, 0).T  # [npix, ncoord]
+    S = torch.ops.hb.alm2map(eye, pid, 0).T  # [npix, ncoord]
     pix = torch.eye(npix, dtype=torch.float64, device="cuda")
-    St = torch.ops.hb.alm2map_adjoint(pix, g.gid, lmax, lmax, 0)  # [npix, n] complex
+    St = torch.ops.hb.alm2map_adjoint(pix, pid, 0)  # [npix, n] complex
     St_real = torch.stack([St[:, k].real if part == 0 else St[:, k].imag for (k, part) in coords], 1)
     assert torch.allclose(St_real, S, rtol=0, atol=1e-13)
-    A = torch.ops.hb.map2alm(pix, g.gid, lmax, lmax, None, 0)  # [npix, n]: row i = alm of unit pixel i
+    A = torch.ops.hb.map2alm(pix, pid, None, 0)  # [npix, n]: row i = alm of unit pixel i
     A_real = torch.stack([A[:, k].real if part == 0 else A[:, k].imag for (k, part) in coords], 1)  # [npix, nc]
-    At = torch.ops.hb.map2alm_adjoint(eye, g.gid, lmax, lmax, None, 0)  # [ncoord, npix]
+    At = torch.ops.hb.map2alm_adjoint(eye, pid, None, 0)  # [ncoord, npix]
     assert torch.allclose(At.T, A_real, rtol=0, atol=1e-13)
     # and the matrices agree with the oracle
     go = oracle.ring_tables(nside)
