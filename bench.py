@@ -34,10 +34,10 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--mode", default="plain", choices=["plain"])
+    p.add_argument("--mode", default="batched", choices=["plain", "batched"])
     p.add_argument("--nside", type=int, default=2048)
     p.add_argument("--lmax", type=int, default=None)
-    p.add_argument("--nmaps", type=int, default=1)
+    p.add_argument("--nmaps", type=int, default=None, help="maps per GPU (default 64 batched, 1 plain)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-sample-m", type=int, default=12)
     return p.parse_args()
@@ -167,36 +167,22 @@ def main():
     nside = args.nside
     lmax = 2 * nside - 1 if args.lmax is None else args.lmax
     mmax = lmax
-    B = args.nmaps
     nalm = n_lm(lmax)
     npix = 12 * nside * nside
     P = 2 * nside
+    B = args.nmaps if args.nmaps is not None else (64 if args.mode == "batched" else 1)
     g = G.healpix(nside)
-    plan = G.plan(g, lmax, mmax, precision=32)
     st = torch.cuda.current_stream(dev)
     sp = st.cuda_stream
 
-    # synthetic Gaussian alm, C_l = (l+10)^-2, seeded per rank (independent maps)
+    # synthetic Gaussian alm, C_l = (l+10)^-2, seeded per rank and map (independent maps)
     cl = 1.0 / (np.arange(lmax + 1) + 10.0) ** 2
-    alm_h = hb.synalm(cl, lmax=lmax, seed=1 + rank, device="cpu", dtype=torch.complex64)
-    alm = alm_h.to(dev).reshape(1, -1).repeat(B, 1).contiguous()
+    alm_h = torch.stack([hb.synalm(cl, lmax=lmax, seed=1000 * rank + i, device="cpu", dtype=torch.complex64)
+                         for i in range(min(B, 4))])
+    alm_h = alm_h.repeat((B + alm_h.shape[0] - 1) // alm_h.shape[0], 1)[:B].contiguous()
+    alm = alm_h.to(dev)
     maps = torch.empty(B, npix, dtype=torch.float32, device=dev)
     alm_out = torch.empty_like(alm)
-    ws = torch.empty(plan.workspace_bytes(32, B), dtype=torch.uint8, device=dev)
-
-    def stage_events():
-        return [torch.cuda.Event(enable_timing=True) for _ in range(5)]
-
-    def step(ev=None):
-        if ev: ev[0].record(st)
-        L.call("hb_legendre_synthesis", plan.handle, 32, B, alm.data_ptr(), ws.data_ptr(), sp)
-        if ev: ev[1].record(st)
-        L.call("hb_ring_synthesis", plan.handle, 32, B, ws.data_ptr(), maps.data_ptr(), 0, sp)
-        if ev: ev[2].record(st)
-        L.call("hb_ring_analysis", plan.handle, 32, B, maps.data_ptr(), None, ws.data_ptr(), 0, sp)
-        if ev: ev[3].record(st)
-        L.call("hb_legendre_analysis", plan.handle, 32, B, ws.data_ptr(), alm_out.data_ptr(), sp)
-        if ev: ev[4].record(st)
 
     # FP32-pipe peak measured on this GPU (FFMA probe)
     probe_out = torch.empty(148 * 8 * 256, dtype=torch.float32, device=dev)
@@ -208,46 +194,107 @@ def main():
     e1.record(st)
     torch.cuda.synchronize(dev)
     fp32_peak = 148 * 8 * 256 * iters * 8 * 2 / (e0.elapsed_time(e1) * 1e-3) / 1e12
+    peaks = {}
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            peaks = json.load(f)
+    except Exception:
+        pass
+    bf16_peak = float(peaks.get("bf16_tflops", 1590.0))
+
+    if args.mode == "plain":
+        plan = G.plan(g, lmax, mmax, precision=32)
+        ws = torch.empty(plan.workspace_bytes(32, B), dtype=torch.uint8, device=dev)
+
+        def step(ev=None):
+            if ev: ev[0].record(st)
+            L.call("hb_legendre_synthesis", plan.handle, 32, B, alm.data_ptr(), ws.data_ptr(), sp)
+            if ev: ev[1].record(st)
+            L.call("hb_ring_synthesis", plan.handle, 32, B, ws.data_ptr(), maps.data_ptr(), 0, sp)
+            if ev: ev[2].record(st)
+            L.call("hb_ring_analysis", plan.handle, 32, B, maps.data_ptr(), None, ws.data_ptr(), 0, sp)
+            if ev: ev[3].record(st)
+            L.call("hb_legendre_analysis", plan.handle, 32, B, ws.data_ptr(), alm_out.data_ptr(), sp)
+            if ev: ev[4].record(st)
+
+        def stage_times(evs):
+            s = np.array([[ev[i].elapsed_time(ev[i + 1]) for i in range(4)] for ev in evs]).mean(0)
+            return {"legendre_synthesis": s[0], "ring_synthesis": s[1], "ring_analysis": s[2],
+                    "legendre_analysis": s[3]}
+        n_launch = 4
+        def make_ev():
+            return [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+    else:
+        bp = hb.batched.plan(nside, lmax, B)
+        bp.profile(True)
+        alm_flat, maps_flat, out_flat = alm.reshape(-1), maps.reshape(-1), alm_out.reshape(-1)
+        stage_acc = []
+
+        def step(ev=None):
+            bp.alm2map(alm_flat, out=maps_flat)
+            bp.map2alm(maps_flat, out=out_flat)
+            if ev is not None:
+                stage_acc.append(bp.stage_ms())
+
+        def stage_times(evs):
+            keys = stage_acc[0].keys()
+            return {k: float(np.mean([s[k] for s in stage_acc])) for k in keys}
+        n_launch = 2 + 2 * len(bp.specs) + 2 + 2  # preps, tensor kernels, ring FFTs
+
+        def make_ev():
+            return True
 
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize(dev)
     if world > 1:
         dist.barrier()
-    evs = [stage_events() for _ in range(args.steps)]
+    if args.mode == "plain":
+        evs = [make_ev() for _ in range(args.steps)]
     with Clocks(local) as clk:
         torch.cuda.synchronize(dev)
         t0 = torch.cuda.Event(enable_timing=True); t1 = torch.cuda.Event(enable_timing=True)
         t0.record(st)
         for k in range(args.steps):
-            step(evs[k])
+            step(evs[k] if args.mode == "plain" else None)
         t1.record(st)
         torch.cuda.synchronize(dev)
     if world > 1:
         dist.barrier()
     ms = t0.elapsed_time(t1)
-    stage = np.array([[ev[i].elapsed_time(ev[i + 1]) for i in range(4)] for ev in evs]).mean(0)  # ms
+    if args.mode == "batched":  # stage breakdown from one extra, separately timed step
+        step(True)
+        torch.cuda.synchronize(dev)
+        stages = stage_times(None)
+        assert bp.status() == 0, f"tensor-core pipeline reported error {bp.status()}"
+    else:
+        stages = stage_times(evs)
     if world > 1:
         tt = torch.tensor([ms], device=dev)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         ms = float(tt.item())
     value = world * args.steps * B / (ms * 1e-3)
 
-    # accuracy of the FP32 pair vs the FP64 GPU path on the same input (this step's alm_out)
-    a64 = alm_h.to(dev, torch.complex128)
+    # accuracy of map 0 of the pair vs the FP64 pair on the same input
+    a64 = alm_h[0].to(dev, torch.complex128)
     m64 = hb.hp_compat.alm2map(a64, nside, lmax=lmax)
     b64 = hb.hp_compat.map2alm(m64, lmax=lmax)
     relerr = float(torch.linalg.norm(alm_out[0].to(torch.complex128) - b64) / torch.linalg.norm(b64))
+    del m64, b64
 
     # end to end through the public API: pinned host alm in, host alm out, copies timed
-    alm_pin = alm_h.reshape(1, -1).repeat(B, 1).contiguous().pin_memory()
+    alm_pin = alm_h.pin_memory()
     out_pin = torch.empty_like(alm_pin).pin_memory()
 
     def e2e_step():
         a = alm_pin.to(dev, non_blocking=True)
-        m = hb.hp_compat.alm2map(a, nside, lmax=lmax)
-        b = hb.hp_compat.map2alm(m, lmax=lmax)
-        out_pin.copy_(b, non_blocking=True)
+        if args.mode == "plain":
+            m = hb.hp_compat.alm2map(a, nside, lmax=lmax)
+            r = hb.hp_compat.map2alm(m, lmax=lmax)
+        else:
+            m = hb.batched.alm2map(a, nside, lmax)
+            r = hb.batched.map2alm(m, nside, lmax)
+        out_pin.copy_(r, non_blocking=True)
 
     for _ in range(max(1, args.warmup)):
         e2e_step()
@@ -267,28 +314,42 @@ def main():
         ms_e2e = float(tt.item())
     e2e = world * args.steps * B / (ms_e2e * 1e-3)
 
-    # roofline of the dominant kernels: the two Legendre launches of a step
-    flop = 8.0 * nalm * P * B  # per Legendre launch (one direction), FMA = 2
-    t_leg = (stage[0] + stage[3]) * 1e-3
-    achieved = 2 * flop / t_leg / 1e12
+    logical = 8.0 * nalm * P  # per map per direction: 4 recursion + 4 contraction flop per (l, m, pair)
+    if args.mode == "plain":
+        t_dom = (stages["legendre_synthesis"] + stages["legendre_analysis"]) * 1e-3
+        achieved = 2 * logical * B / t_dom / 1e12
+        roof = {"bound": "fp32", "kernel": "leg_synthesis_kernel + leg_analysis_kernel", "achieved": achieved,
+                "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
+                "peak_source": "FFMA probe (hb_probe_fp32) on this GPU in this run",
+                "flop_per_launch": logical * B}
+    else:
+        t_dom = (stages["tensor_synthesis"] + stages["tensor_analysis"]) * 1e-3
+        alg = (4.0 * B + 4.0) * nalm * P          # logical: contraction per map + shared recursion
+        executed = 3 * 2 * 2.0 * B * nalm * P     # 3 split passes x 2 flop x (Re, Im) columns
+        achieved = 2 * alg / t_dom / 1e12
+        roof = {"bound": "tensor", "kernel": "synth_tc_kernel + anal_tc_kernel", "achieved": achieved,
+                "peak": bf16_peak, "unit": "TFLOP/s", "frac": achieved / bf16_peak, "traffic": None,
+                "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)" if peaks else "fallback 1590 TFLOP/s",
+                "flop_per_launch": alg,
+                "tensor_flop_executed_per_launch": executed,
+                "tensor_achieved_executed": 2 * executed / t_dom / 1e12,
+                "tensor_frac_executed": 2 * executed / t_dom / 1e12 / bf16_peak}
     out = {
         "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (Gaussian alm, C_l=(l+10)^-2)",
-        "config": {"workload": f"scalar map2alm+alm2map pair, nside {nside}, lmax {lmax}, float32, plain per-map "
-                               f"FP32 path, {B} map(s) per GPU", "nside": nside, "lmax": lmax, "maps_per_gpu": B,
-                   "mode": args.mode, "l2": "inputs larger than L2 (map 201 MB, alm 67 MB)",
+        "config": {"workload": (f"scalar map2alm+alm2map pair, nside {nside}, lmax {lmax}, float32 maps, "
+                                + ("batched split-BF16 tcgen05 path, " if args.mode == "batched" else
+                                   "plain per-map FP32 path, ") + f"{B} maps per GPU per step"),
+                   "nside": nside, "lmax": lmax, "maps_per_gpu": B, "mode": args.mode,
+                   "l2": "inputs larger than L2 (one map 201 MB, one alm 67 MB)",
                    "parallelism": f"replicas x{world}"},
         "rel_err_vs_fp64": relerr,
-        "stages_ms": {"legendre_synthesis": stage[0], "ring_synthesis": stage[1], "ring_analysis": stage[2],
-                      "legendre_analysis": stage[3]},
-        "roofline": {"bound": "fp32", "kernel": "leg_synthesis + leg_analysis", "achieved": achieved,
-                     "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": None,
-                     "peak_source": "FFMA probe (hb_probe_fp32) on this GPU, this run",
-                     "flop_per_launch": flop},
+        "stages_ms": stages,
+        "roofline": roof,
         "e2e": {"value": e2e, "unit": "pairs/s", "h2d_bytes_per_step": int(alm_pin.numel() * 8),
                 "d2h_bytes_per_step": int(out_pin.numel() * 8)},
-        "gpu_launches": args.steps * 4,
+        "gpu_launches": args.steps * n_launch,
         "clocks": clk.summary(),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

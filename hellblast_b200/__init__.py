@@ -17,6 +17,7 @@ from .sht import map2alm_gpu
 from .spin import eb_from_qu_gpu, map2alm_spin_gpu, qu_from_eb_gpu
 from . import hp_compat  # noqa: F401
 from . import autograd  # noqa: F401
+from . import batched  # noqa: F401
 
 map2alm = map2alm_gpu
 alm2map = alm2map_gpu

@@ -56,6 +56,14 @@ SIGNATURES = {
     "hb_legendre_analysis": (i32, [vp, i32, i32, vp, vp, vp]),
     "hb_legendre_synthesis": (i32, [vp, i32, i32, vp, vp, vp]),
     "hb_probe_fp32": (i32, [i32, i32, i32, vp, vp]),
+    "hb_batched_plan_create": (i32, [ctypes.POINTER(vp), ctypes.POINTER(i32), i32, i32, ctypes.POINTER(vp)]),
+    "hb_batched_plan_destroy": (i32, [vp]),
+    "hb_batched_plan_bytes": (sz, [vp]),
+    "hb_batched_alm2map": (i32, [vp, vp, vp, vp]),
+    "hb_batched_map2alm": (i32, [vp, vp, vp, vp]),
+    "hb_batched_status": (i32, [vp, ctypes.POINTER(i32)]),
+    "hb_batched_profile": (i32, [vp, i32]),
+    "hb_batched_stage_ms": (i32, [vp, ctypes.POINTER(ctypes.c_float)]),
 }
 for _p in ("f32", "f64"):
     SIGNATURES[f"hb_map2alm_{_p}"] = (i32, [vp, i32, vp, vp, vp, vp, sz, i32, vp])

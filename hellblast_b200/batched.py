@@ -1,0 +1,98 @@
+"""Batched split-precision transforms (BF16 hi+lo three-pass products on the tcgen05 tensor
+cores, FP32 accumulation in TMEM): many maps of one or several (nside, lmax) in one persistent
+launch per direction.  Wraps hb_batched_plan_* of the C ABI."""
+from __future__ import annotations
+
+import ctypes
+import threading
+
+import torch
+
+from . import _lib as L
+from . import geometry as G
+from .ops import alm_size
+
+_cache: dict[tuple, "BatchedPlan"] = {}
+_lock = threading.Lock()
+
+
+class BatchedPlan:
+    """``specs``: list of (geometry, lmax, mmax, nmaps).  Inputs/outputs are flat CUDA tensors
+    holding the maps (float32) or alm (complex64, healpy layout) of all specs back to back."""
+
+    def __init__(self, specs):
+        self.specs = [(g, int(lmax), int(lmax if mmax is None else mmax), int(n)) for g, lmax, mmax, n in specs]
+        self.plans = [G.plan(g, lmax, mmax, precision=32) for g, lmax, mmax, _ in self.specs]
+        n = len(self.plans)
+        arr = (ctypes.c_void_p * n)(*[p.handle.value for p in self.plans])
+        nm = (ctypes.c_int * n)(*[s[3] for s in self.specs])
+        out = ctypes.c_void_p()
+        L.call("hb_batched_plan_create", arr, nm, n, 0, ctypes.byref(out))
+        self.handle = out
+        self.nbytes = int(L.lib().hb_batched_plan_bytes(out))
+        self.total_pix = sum(g.npix * k for g, _, _, k in self.specs)
+        self.total_alm = sum(alm_size(l, m) * k for _, l, m, k in self.specs)
+
+    def alm2map(self, alm: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+        alm = alm.reshape(-1).contiguous()
+        if alm.dtype != torch.complex64 or alm.numel() != self.total_alm or not alm.is_cuda:
+            raise ValueError(f"alm must be a CUDA complex64 tensor of {self.total_alm} elements")
+        out = torch.empty(self.total_pix, dtype=torch.float32, device=alm.device) if out is None else out
+        L.call("hb_batched_alm2map", self.handle, alm.data_ptr(), out.data_ptr(),
+               torch.cuda.current_stream(alm.device).cuda_stream)
+        return out
+
+    def map2alm(self, maps: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+        maps = maps.reshape(-1).contiguous()
+        if maps.dtype != torch.float32 or maps.numel() != self.total_pix or not maps.is_cuda:
+            raise ValueError(f"maps must be a CUDA float32 tensor of {self.total_pix} elements")
+        out = torch.empty(self.total_alm, dtype=torch.complex64, device=maps.device) if out is None else out
+        L.call("hb_batched_map2alm", self.handle, maps.data_ptr(), out.data_ptr(),
+               torch.cuda.current_stream(maps.device).cuda_stream)
+        return out
+
+    def profile(self, enable: bool = True) -> None:
+        L.call("hb_batched_profile", self.handle, 1 if enable else 0)
+
+    def stage_ms(self) -> dict:
+        ms = (ctypes.c_float * 6)()
+        L.call("hb_batched_stage_ms", self.handle, ms)
+        keys = ("prep_alm", "tensor_synthesis", "ring_synthesis", "ring_analysis", "prep_f", "tensor_analysis")
+        return dict(zip(keys, [float(v) for v in ms]))
+
+    def status(self) -> int:
+        code = ctypes.c_int(0)
+        L.call("hb_batched_status", self.handle, ctypes.byref(code))
+        return code.value
+
+    def __del__(self):  # pragma: no cover
+        try:
+            if self.handle:
+                L.lib().hb_batched_plan_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+
+def plan(nside: int, lmax: int, nmaps: int, mmax: int | None = None, weights: str = "dz") -> BatchedPlan:
+    """Cached single-geometry batched plan (HEALPix nside, lmax, nmaps maps)."""
+    key = (int(nside), int(lmax), mmax, int(nmaps), weights, torch.cuda.current_device())
+    with _lock:
+        bp = _cache.get(key)
+    if bp is None:
+        bp = BatchedPlan([(G.healpix(nside, weights=weights), lmax, mmax, nmaps)])
+        with _lock:
+            _cache[key] = bp
+    return bp
+
+
+def alm2map(alm: torch.Tensor, nside: int, lmax: int, mmax: int | None = None) -> torch.Tensor:
+    """[nmaps, nalm] complex64 -> [nmaps, npix] float32 through the tensor-core path."""
+    nmaps = alm.shape[0]
+    return plan(nside, lmax, nmaps, mmax).alm2map(alm).reshape(nmaps, -1)
+
+
+def map2alm(maps: torch.Tensor, nside: int, lmax: int, mmax: int | None = None) -> torch.Tensor:
+    """[nmaps, npix] float32 -> [nmaps, nalm] complex64 through the tensor-core path."""
+    nmaps = maps.shape[0]
+    return plan(nside, lmax, nmaps, mmax).map2alm(maps).reshape(nmaps, -1)

@@ -1,0 +1,879 @@
+// Batched split-precision Legendre transforms on the 5th-generation tensor cores (tcgen05).
+//
+// Many maps that share a geometry and lmax reuse every Legendre value lambda_lm(x_p): the
+// contraction over l (synthesis) or over ring pairs (analysis) becomes a GEMM whose one operand
+// is generated on the fly by the FP32 recursion and whose other operand is the batch.  Both
+// operands are split into BF16 hi + lo parts and multiplied in three passes (hi*hi + hi*lo +
+// lo*hi) with FP32 accumulation in TMEM; lambda is never written to global memory.
+//
+// Synthesis (alm -> G_N/S(m) per ring pair), work unit = (group, m, block of 128 ring pairs):
+//   D_q[pair, n] = sum_{l = m+q mod 2} lambda_l(x_pair) a_l[n],   q = parity of l-m,
+//   MMA M = 128 pairs, N = 2 * maps (Re/Im columns), K = l (32 per parity per stage).
+//   Four producer warps run the recursion (one pair per thread) and write the A tiles (K-major);
+//   a loader warp streams pre-split alm tiles with bulk copies; one thread issues the MMAs.
+//   Epilogue: G_N = D_0 + D_1, G_S = D_0 - D_1.
+// Analysis (F -> alm), work unit = (group, m, block of 256 consecutive l):
+//   D_q[l, n] = sum_pairs lambda_l(x_pair) (E|O)_pair[n],  E = F_N + F_S, O = F_N - F_S,
+//   MMA M = 128 l of one parity, N = 2 * maps, K = ring pairs (32 per stage).  The recursion
+//   restarts at the block from the plan's FP64-computed checkpoint; three producer warps each
+//   own one pipeline stage (one pair per thread, 256 steps) and write MN-major A tiles.
+//
+// Every mbarrier wait is bounded (HB_TC_WAIT_NS); on expiry the kernel records an error code in
+// *err and returns after releasing its tensor memory.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
+#include "hb_internal.cuh"
+#include "hb_tc.cuh"
+
+namespace hb {
+
+constexpr uint64_t HB_TC_WAIT_NS = 2000000000ull;  // 2 s
+constexpr int TC_STAGES = 3;
+constexpr int A_TILE = 8192;       // 128 rows x 32 K x bf16
+constexpr int A_STAGE = 4 * A_TILE;  // [parity][hi/lo]
+
+struct TcGroup {
+    GeomDev g;
+    int lmax, mmax, nmaps;
+    int64_t npb;             // blocks of 128 pairs (synthesis)
+    int64_t npc;             // chunks of 32 pairs (analysis)
+    const float4 *ck;        // plan checkpoints
+    const int64_t *blk_ofs;
+    // synthesis
+    const uint4 *alm_tiles;  // [chunk][4][N x 32] bf16, chunk = tile_ofs[m] + c
+    const int64_t *alm_tile_ofs;
+    float2 *Gm;              // [map][m][pair][2]
+    int64_t gm_stride;
+    // analysis
+    const uint4 *g_tiles;    // [m][pc][4][N x 32] bf16
+    int64_t alm_out_ofs;     // this group's first alm in the caller's output buffer (complex elements)
+    int64_t alm_stride;
+};
+
+__device__ __forceinline__ void set_err(int *err, int code) { atomicCAS(err, 0, code); }
+
+// lane 0 waits (bounded), the result is broadcast so the whole warp takes the same path
+__device__ __forceinline__ bool warp_wait(uint64_t *bar, uint32_t parity) {
+    bool okw = true;
+    if ((threadIdx.x & 31) == 0) okw = tc::mbar_wait(bar, parity, HB_TC_WAIT_NS);
+    return __shfl_sync(0xffffffffu, (int)okw, 0) != 0;
+}
+
+// ------------------------------------------------------------------------------------ prep
+// alm [map][nalm] complex64 -> per (m, 64-l chunk) the synthesis B tiles:
+// [q][h][N rows (2*map + re/im) x 32 K (l = l0 + 2k + q)], K-major core matrices
+// (row%8)*16 B + (row/8)*512 B + (k/8)*128 B.
+template <int N>
+__global__ void prep_alm_tiles_kernel(const TcGroup *groups, int gi, const float2 *__restrict__ alm, int64_t alm_stride) {
+    const TcGroup &G = groups[gi];
+    const int m = blockIdx.x;
+    if (m > G.mmax) return;
+    const int lmax = G.lmax;
+    const int nch = (lmax - m + 64) / 64;
+    __nv_bfloat16 *base = (__nv_bfloat16 *)(G.alm_tiles + G.alm_tile_ofs[m] * (16 * N));
+    // thread -> (n, k, q); consecutive threads walk l
+    const int per_chunk = N * 64;  // (n, k, q)
+    for (int idx = threadIdx.x; idx < nch * per_chunk; idx += blockDim.x) {
+        const int c = idx / per_chunk, r = idx % per_chunk;
+        const int n = r / 64, kq = r % 64, k = kq >> 1, q = kq & 1;
+        const int l = m + 64 * c + 2 * k + q;
+        const int b = n >> 1;
+        float v = 0.f;
+        if (l <= lmax && b < G.nmaps) {
+            const float2 a = alm[(int64_t)b * alm_stride + alm_idx(lmax, l, m)];
+            v = (n & 1) ? a.y : a.x;
+        }
+        const __nv_bfloat16 hi = __float2bfloat16_rn(v);
+        const __nv_bfloat16 lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+        const int64_t off = (n & 7) * 8 + (n >> 3) * 256 + (k >> 3) * 64 + (k & 7);
+        __nv_bfloat16 *chunk = base + (int64_t)c * (4 * N * 32);
+        chunk[(q * 2 + 0) * N * 32 + off] = hi;
+        chunk[(q * 2 + 1) * N * 32 + off] = lo;
+    }
+}
+
+// F [map][m][pair][2] -> per (m, 32-pair chunk) the analysis B tiles [q][h][N x 32 pairs]
+// (E = F_N + F_S for q = 0, O = F_N - F_S for q = 1), K-major like above.
+template <int N>
+__global__ void prep_g_tiles_kernel(const TcGroup *groups, int gi, const float2 *__restrict__ F, int64_t f_stride) {
+    const TcGroup &G = groups[gi];
+    const int m = blockIdx.x;
+    if (m > G.mmax) return;
+    const int64_t np = G.g.npairs;
+    __nv_bfloat16 *base = (__nv_bfloat16 *)(G.g_tiles + (int64_t)m * G.npc * (16 * N));
+    const int per_chunk = N * 32;
+    for (int64_t idx = threadIdx.x; idx < G.npc * per_chunk; idx += blockDim.x) {
+        const int64_t c = idx / per_chunk;
+        const int r = (int)(idx % per_chunk);
+        const int n = r / 32, k = r % 32;
+        const int64_t p = c * 32 + k;
+        const int b = n >> 1;
+        float e = 0.f, o = 0.f;
+        if (p < np && b < G.nmaps) {
+            const float2 *f = F + (int64_t)b * f_stride + ((int64_t)m * np + p) * 2;
+            const float2 fn = f[0], fs = f[1];
+            e = (n & 1) ? fn.y + fs.y : fn.x + fs.x;
+            o = (n & 1) ? fn.y - fs.y : fn.x - fs.x;
+        }
+        const int64_t off = (n & 7) * 8 + (n >> 3) * 256 + (k >> 3) * 64 + (k & 7);
+        __nv_bfloat16 *chunk = base + c * (4 * N * 32);
+        __nv_bfloat16 ehi = __float2bfloat16_rn(e), ohi = __float2bfloat16_rn(o);
+        chunk[0 * N * 32 + off] = ehi;
+        chunk[1 * N * 32 + off] = __float2bfloat16_rn(e - __bfloat162float(ehi));
+        chunk[2 * N * 32 + off] = ohi;
+        chunk[3 * N * 32 + off] = __float2bfloat16_rn(o - __bfloat162float(ohi));
+    }
+}
+
+// ------------------------------------------------------------------------------------ recursion
+// One recursion step in the scaled FP32 form used by the plain kernels: lambda = mu * 2^(64 e),
+// contributions only while e == 0; rescale by 2^-64 when |mu| passes 2^32 with e < 0.
+struct Rec {
+    float l1, l2, xh, xl;
+    int e;
+    __device__ __forceinline__ float step(float A, float B) {
+        float v = A * fmaf(xh, l1, xl * l1) + B * l2;
+        l2 = l1;
+        l1 = v;
+        return v;
+    }
+    __device__ __forceinline__ void check() {
+        if (e < 0 && fabsf(l1) > 4294967296.0f) {
+            l1 *= 5.42101086242752217e-20f;
+            l2 *= 5.42101086242752217e-20f;
+            ++e;
+        }
+    }
+    __device__ __forceinline__ float val(float v) const { return e == 0 ? v : 0.f; }
+    __device__ __forceinline__ void load(float4 c) {
+        l1 = c.x;
+        l2 = c.y;
+        e = __float_as_int(c.z);
+    }
+};
+
+__device__ __forceinline__ void coef_scalar(int l, int m, int lmax, float2 &out) {
+    double A = 0.0, B = 0.0;
+    if (l == m) {
+        B = 1.0;
+    } else if (l <= lmax) {
+        const double ll = l, mm = m;
+        A = sqrt((4.0 * ll * ll - 1.0) / ((ll - mm) * (ll + mm)));
+        B = (l - 1 > m) ? -A * sqrt(((ll - 1.0 - mm) * (ll - 1.0 + mm)) / (4.0 * (ll - 1.0) * (ll - 1.0) - 1.0)) : 0.0;
+    }
+    out = make_float2((float)A, (float)B);
+}
+
+// ------------------------------------------------------------------------------------ synthesis
+constexpr int SYN_THREADS = 192;  // warps 0-3 producers/epilogue, 4 MMA, 5 loader
+
+template <int N>
+__global__ void __launch_bounds__(SYN_THREADS, 1)
+    synth_tc_kernel(const TcGroup *__restrict__ groups, const int4 *__restrict__ units, int nunits, int *err) {
+    constexpr int B_STAGE = 4 * N * 64;  // [q][h][N x 32] bf16
+    constexpr int STAGE = A_STAGE + B_STAGE;
+    constexpr uint32_t IDESC = tc::idesc_bf16(128, N, 0, 0);
+    constexpr int TCOLS = (2 * N < 32) ? 32 : 2 * N;
+    extern __shared__ __align__(1024) uint8_t smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // one private copy of the 256 recursion coefficients per producer warp (no cross-warp barrier)
+    float2 *coef = reinterpret_cast<float2 *>(smem + TC_STAGES * STAGE) + (warp & 3) * 256;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + TC_STAGES * STAGE + 4 * 256 * sizeof(float2));
+    uint64_t *full = bars, *empty = bars + TC_STAGES, *accum = bars + 2 * TC_STAGES, *tfree = accum + 1;
+    uint64_t *drain = tfree + 1;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < TC_STAGES; ++s) {
+            tc::mbar_init(&full[s], 128 + 1);
+            tc::mbar_init(&empty[s], 1);
+        }
+        tc::mbar_init(accum, 1);
+        tc::mbar_init(tfree, 128);
+        tc::mbar_init(drain, 1);
+        tc::fence_mbar_init();
+    }
+    if (warp == 4) {
+        tc::tmem_alloc(tmem_slot, TCOLS);
+        tc::tmem_relinquish();
+    }
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    const uint32_t tmem = *tmem_slot;
+    bool ok = true;
+
+    if (warp < 4) {
+        // ---------------- producers + epilogue
+        const int r = threadIdx.x;  // row = pair within the block
+        uint32_t it = 0;
+        int ui = 0;
+        for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++ui) {
+            const int4 U = units[u];
+            const TcGroup &G = groups[U.x];
+            const int m = U.y, lmax = G.lmax;
+            const int64_t np = G.g.npairs, p = (int64_t)U.z * 128 + r;
+            const bool live = p < np;
+            Rec R;
+            R.xh = live ? G.g.pair_xhi[p] : 0.f;
+            R.xl = live ? G.g.pair_xlo[p] : 0.f;
+            R.load(live ? G.ck[G.blk_ofs[m] * np + p] : make_float4(0.f, 0.f, 0.f, 0.f));
+            const int nch = (lmax - m + 64) / 64;
+            for (int c = 0; c < nch && ok; ++c, ++it) {
+                const int l0 = m + 64 * c;
+                if ((c & 3) == 0) {
+                    __syncwarp();
+                    for (int i = lane; i < 256; i += 32) coef_scalar(l0 + i, m, lmax, coef[i]);
+                    __syncwarp();
+                    if (c > 0 && live) R.load(G.ck[(G.blk_ofs[m] + c / 4) * np + p]);
+                }
+                const int s = it % TC_STAGES;
+                if (it >= TC_STAGES && !warp_wait(&empty[s], ((it / TC_STAGES) + 1) & 1)) {
+                    if (lane == 0) set_err(err, 1);
+                    ok = false;
+                    break;
+                }
+                uint8_t *A = smem + s * STAGE;
+                const float2 *cf = coef + (c & 3) * 64;
+#pragma unroll
+                for (int grp = 0; grp < 4; ++grp) {
+                    float ev[8], od[8];
+#pragma unroll
+                    for (int t = 0; t < 8; ++t) {
+                        const float2 ce = cf[16 * grp + 2 * t], co = cf[16 * grp + 2 * t + 1];
+                        ev[t] = R.val(R.step(ce.x, ce.y));
+                        od[t] = R.val(R.step(co.x, co.y));
+                        if (t & 1) R.check();
+                    }
+                    uint4 hi, lo;
+                    const int off = (r & 7) * 16 + (r >> 3) * 512 + grp * 128;
+                    tc::split8(ev, hi, lo);
+                    *reinterpret_cast<uint4 *>(A + 0 * A_TILE + off) = hi;
+                    *reinterpret_cast<uint4 *>(A + 1 * A_TILE + off) = lo;
+                    tc::split8(od, hi, lo);
+                    *reinterpret_cast<uint4 *>(A + 2 * A_TILE + off) = hi;
+                    *reinterpret_cast<uint4 *>(A + 3 * A_TILE + off) = lo;
+                }
+                tc::fence_proxy_async_smem();
+                tc::mbar_arrive(&full[s]);
+            }
+            if (!ok) break;
+            // epilogue
+            if (!warp_wait(accum, ui & 1)) {
+                if (lane == 0) set_err(err, 2);
+                ok = false;
+                break;
+            }
+            tc::fence_after();
+            const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+#pragma unroll
+            for (int j = 0; j < N / 16; ++j) {
+                float de[16], dd[16];
+                tc::tmem_ld16(tmem + lane_base + j * 16, de);
+                tc::tmem_ld16(tmem + lane_base + N + j * 16, dd);
+                tc::tmem_wait_ld();
+                if (live) {
+#pragma unroll
+                    for (int h = 0; h < 8; ++h) {
+                        const int b = j * 8 + h;
+                        if (b < G.nmaps) {
+                            float2 *dst = G.Gm + (int64_t)b * G.gm_stride + ((int64_t)m * np + p) * 2;
+                            const float re = de[2 * h], im = de[2 * h + 1], ro = dd[2 * h], io = dd[2 * h + 1];
+                            *reinterpret_cast<float4 *>(dst) = make_float4(re + ro, im + io, re - ro, im - io);
+                        }
+                    }
+                }
+            }
+            tc::fence_before();
+            tc::mbar_arrive(tfree);
+        }
+    } else if (warp == 4) {
+        // ---------------- MMA issuer
+        if (lane == 0) {
+            uint32_t it = 0;
+            int ui = 0;
+            for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++ui) {
+                const int4 U = units[u];
+                const TcGroup &G = groups[U.x];
+                const int m = U.y;
+                const int nch = (G.lmax - m + 64) / 64;
+                if (ui > 0 && !tc::mbar_wait(tfree, (ui - 1) & 1, HB_TC_WAIT_NS)) {
+                    set_err(err, 3);
+                    ok = false;
+                    break;
+                }
+                tc::fence_after();
+                for (int c = 0; c < nch; ++c, ++it) {
+                    const int s = it % TC_STAGES;
+                    if (!tc::mbar_wait(&full[s], (it / TC_STAGES) & 1, HB_TC_WAIT_NS)) {
+                        set_err(err, 4);
+                        ok = false;
+                        break;
+                    }
+                    tc::fence_after();
+                    const uint32_t a0 = tc::smem_u32(smem + s * STAGE), b0 = a0 + A_STAGE;
+#pragma unroll
+                    for (int q = 0; q < 2; ++q) {
+                        const uint32_t d = tmem + q * N;
+#pragma unroll
+                        for (int j = 0; j < 2; ++j) {
+                            const uint64_t ah = tc::sdesc(a0 + (q * 2 + 0) * A_TILE + j * 256, 128, 512);
+                            const uint64_t al = tc::sdesc(a0 + (q * 2 + 1) * A_TILE + j * 256, 128, 512);
+                            const uint64_t bh = tc::sdesc(b0 + (q * 2 + 0) * (N * 64) + j * 256, 128, 512);
+                            const uint64_t bl = tc::sdesc(b0 + (q * 2 + 1) * (N * 64) + j * 256, 128, 512);
+                            tc::mma_bf16(d, ah, bh, IDESC, (c > 0 || j > 0) ? 1u : 0u);
+                            tc::mma_bf16(d, ah, bl, IDESC, 1u);
+                            tc::mma_bf16(d, al, bh, IDESC, 1u);
+                        }
+                    }
+                    tc::mma_commit(&empty[s]);
+                }
+                if (!ok) break;
+                tc::mma_commit(accum);
+            }
+            if (!ok) {  // let issued MMAs finish before the tensor memory is released
+                tc::mma_commit(drain);
+                tc::mbar_wait(drain, 0, HB_TC_WAIT_NS);
+            }
+        }
+        __syncwarp();
+    } else {
+        // ---------------- loader of the pre-split alm tiles
+        if (lane == 0) {
+            uint32_t it = 0;
+            for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+                const int4 U = units[u];
+                const TcGroup &G = groups[U.x];
+                const int m = U.y;
+                const int nch = (G.lmax - m + 64) / 64;
+                const uint4 *src = G.alm_tiles + G.alm_tile_ofs[m] * (16 * N);
+                for (int c = 0; c < nch; ++c, ++it) {
+                    const int s = it % TC_STAGES;
+                    if (it >= TC_STAGES && !tc::mbar_wait(&empty[s], ((it / TC_STAGES) + 1) & 1, HB_TC_WAIT_NS)) {
+                        set_err(err, 5);
+                        ok = false;
+                        break;
+                    }
+                    tc::mbar_arrive_expect_tx(&full[s], B_STAGE);
+                    tc::bulk_g2s(smem + s * STAGE + A_STAGE, src + (int64_t)c * (16 * N), B_STAGE, &full[s]);
+                }
+            }
+        }
+        __syncwarp();
+    }
+    tc::fence_before();
+    __syncthreads();
+    if (warp == 4) {
+        tc::fence_after();
+        tc::tmem_dealloc(tmem, TCOLS);
+    }
+}
+
+// ------------------------------------------------------------------------------------ analysis
+constexpr int ANA_THREADS = 160;  // warps 0-2 producers (+ epilogue), 3 MMA (+ epilogue), 4 loader
+
+template <int N>
+__global__ void __launch_bounds__(ANA_THREADS, 1)
+    anal_tc_kernel(const TcGroup *__restrict__ groups, const int4 *__restrict__ units, int nunits, float2 *alm_out,
+                   int *err) {
+    constexpr int B_STAGE = 4 * N * 64;
+    constexpr int STAGE = A_STAGE + B_STAGE;
+    constexpr uint32_t IDESC = tc::idesc_bf16(128, N, 1, 0);
+    constexpr int TCOLS = (2 * N < 32) ? 32 : 2 * N;
+    extern __shared__ __align__(1024) uint8_t smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float2 *coef = reinterpret_cast<float2 *>(smem + TC_STAGES * STAGE) + (warp & 3) * 256;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + TC_STAGES * STAGE + 4 * 256 * sizeof(float2));
+    uint64_t *full = bars, *empty = bars + TC_STAGES, *accum = bars + 2 * TC_STAGES, *tfree = accum + 1;
+    uint64_t *drain = tfree + 1;
+    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < TC_STAGES; ++s) {
+            tc::mbar_init(&full[s], 32 + 1);
+            tc::mbar_init(&empty[s], 1);
+        }
+        tc::mbar_init(accum, 1);
+        tc::mbar_init(tfree, 128);
+        tc::mbar_init(drain, 1);
+        tc::fence_mbar_init();
+    }
+    if (warp == 3) {
+        tc::tmem_alloc(tmem_slot, TCOLS);
+        tc::tmem_relinquish();
+    }
+    tc::fence_before();
+    __syncthreads();
+    tc::fence_after();
+    const uint32_t tmem = *tmem_slot;
+    bool ok = true;
+
+    if (warp < 4) {
+        uint32_t it = 0;  // running chunk counter: stage = it % 3, phase = it / 3
+        int ui = 0;
+        for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++ui) {
+            const int4 U = units[u];
+            const TcGroup &G = groups[U.x];
+            const int m = U.y, jb = U.z, lmax = G.lmax;
+            const int l0 = m + 256 * jb;
+            const int64_t np = G.g.npairs;
+            const int npc = (int)G.npc;
+            if (warp < 3) {
+                // ---------------- producers: warp w fills the chunks with it % 3 == w
+                __syncwarp();
+                for (int i = lane; i < 256; i += 32) coef_scalar(l0 + i, m, lmax, coef[i]);
+                __syncwarp();
+                for (int c = 0; c < npc; ++c, ++it) {
+                    const int s = it % TC_STAGES;
+                    if (s != warp) continue;
+                    const int64_t p = (int64_t)c * 32 + lane;
+                    const bool live = p < np;
+                    Rec R;
+                    R.xh = live ? G.g.pair_xhi[p] : 0.f;
+                    R.xl = live ? G.g.pair_xlo[p] : 0.f;
+                    R.load(live ? G.ck[(G.blk_ofs[m] + jb) * np + p] : make_float4(0.f, 0.f, 0.f, 0.f));
+                    if (it >= TC_STAGES && !warp_wait(&empty[s], ((it / TC_STAGES) + 1) & 1)) {
+                        if (lane == 0) set_err(err, 11);
+                        ok = false;
+                        break;
+                    }
+                    uint8_t *A = smem + s * STAGE;
+#pragma unroll 1
+                    for (int grp = 0; grp < 16; ++grp) {
+                        float ev[8], od[8];
+#pragma unroll
+                        for (int t = 0; t < 8; ++t) {
+                            const float2 ce = coef[16 * grp + 2 * t], co = coef[16 * grp + 2 * t + 1];
+                            ev[t] = R.val(R.step(ce.x, ce.y));
+                            od[t] = R.val(R.step(co.x, co.y));
+                            if (t & 1) R.check();
+                        }
+                        uint4 hi, lo;
+                        // MN-major: 8 consecutive rows (l of one parity) of pair `lane`
+                        const int off = (lane & 7) * 16 + grp * 512 + (lane >> 3) * 128;
+                        tc::split8(ev, hi, lo);
+                        *reinterpret_cast<uint4 *>(A + 0 * A_TILE + off) = hi;
+                        *reinterpret_cast<uint4 *>(A + 1 * A_TILE + off) = lo;
+                        tc::split8(od, hi, lo);
+                        *reinterpret_cast<uint4 *>(A + 2 * A_TILE + off) = hi;
+                        *reinterpret_cast<uint4 *>(A + 3 * A_TILE + off) = lo;
+                    }
+                    tc::fence_proxy_async_smem();
+                    tc::mbar_arrive(&full[s]);
+                }
+            } else {
+                // ---------------- MMA issuer: one thread of warp 3
+                if (lane == 0) {
+                    if (ui > 0 && !tc::mbar_wait(tfree, (ui - 1) & 1, HB_TC_WAIT_NS)) {
+                        set_err(err, 13);
+                        ok = false;
+                    }
+                    tc::fence_after();
+                    for (int c = 0; c < npc && ok; ++c, ++it) {
+                        const int s = it % TC_STAGES;
+                        if (!tc::mbar_wait(&full[s], (it / TC_STAGES) & 1, HB_TC_WAIT_NS)) {
+                            set_err(err, 14);
+                            ok = false;
+                            break;
+                        }
+                        tc::fence_after();
+                        const uint32_t a0 = tc::smem_u32(smem + s * STAGE), b0 = a0 + A_STAGE;
+#pragma unroll
+                        for (int q = 0; q < 2; ++q) {
+                            const uint32_t d = tmem + q * N;
+#pragma unroll
+                            for (int k = 0; k < 2; ++k) {
+                                const uint64_t ah = tc::sdesc(a0 + (q * 2 + 0) * A_TILE + k * 256, 128, 512);
+                                const uint64_t al = tc::sdesc(a0 + (q * 2 + 1) * A_TILE + k * 256, 128, 512);
+                                const uint64_t bh = tc::sdesc(b0 + (q * 2 + 0) * (N * 64) + k * 256, 128, 512);
+                                const uint64_t bl = tc::sdesc(b0 + (q * 2 + 1) * (N * 64) + k * 256, 128, 512);
+                                tc::mma_bf16(d, ah, bh, IDESC, (c > 0 || k > 0) ? 1u : 0u);
+                                tc::mma_bf16(d, ah, bl, IDESC, 1u);
+                                tc::mma_bf16(d, al, bh, IDESC, 1u);
+                            }
+                        }
+                        tc::mma_commit(&empty[s]);
+                    }
+                    if (ok) {
+                        tc::mma_commit(accum);
+                    } else {
+                        tc::mma_commit(drain);
+                        tc::mbar_wait(drain, 0, HB_TC_WAIT_NS);
+                    }
+                }
+                __syncwarp();
+                ok = __shfl_sync(0xffffffffu, ok, 0);
+                it = __shfl_sync(0xffffffffu, it, 0);
+            }
+            if (!ok) break;
+            // ---------------- epilogue (warps 0-3: TMEM lane quarters 0-3 = rows 32w..32w+31)
+            if (!warp_wait(accum, ui & 1)) {
+                if (lane == 0) set_err(err, 12);
+                ok = false;
+                break;
+            }
+            tc::fence_after();
+            const int row = warp * 32 + lane;
+            const int le = l0 + 2 * row;
+            const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+#pragma unroll
+            for (int j = 0; j < N / 16; ++j) {
+                float de[16], dd[16];
+                tc::tmem_ld16(tmem + lane_base + j * 16, de);
+                tc::tmem_ld16(tmem + lane_base + N + j * 16, dd);
+                tc::tmem_wait_ld();
+#pragma unroll
+                for (int h = 0; h < 8; ++h) {
+                    const int b = j * 8 + h;
+                    if (b < G.nmaps) {
+                        float2 *dst = alm_out + G.alm_out_ofs + (int64_t)b * G.alm_stride + alm_idx(lmax, le, m);
+                        if (le <= lmax) dst[0] = make_float2(de[2 * h], de[2 * h + 1]);
+                        if (le + 1 <= lmax) dst[1] = make_float2(dd[2 * h], dd[2 * h + 1]);
+                    }
+                }
+            }
+            tc::fence_before();
+            tc::mbar_arrive(tfree);
+        }
+    } else {
+        // ---------------- loader of the pre-split E/O tiles (warp 4, one thread)
+        if (lane == 0) {
+            uint32_t it = 0;
+            for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+                const int4 U = units[u];
+                const TcGroup &G = groups[U.x];
+                const int m = U.y;
+                const int npc = (int)G.npc;
+                const uint4 *src = G.g_tiles + (int64_t)m * npc * (16 * N);
+                for (int c = 0; c < npc; ++c, ++it) {
+                    const int s = it % TC_STAGES;
+                    if (it >= TC_STAGES && !tc::mbar_wait(&empty[s], ((it / TC_STAGES) + 1) & 1, HB_TC_WAIT_NS)) {
+                        set_err(err, 15);
+                        ok = false;
+                        break;
+                    }
+                    tc::mbar_arrive_expect_tx(&full[s], B_STAGE);
+                    tc::bulk_g2s(smem + s * STAGE + A_STAGE, src + (int64_t)c * (16 * N), B_STAGE, &full[s]);
+                }
+            }
+        }
+        __syncwarp();
+    }
+    tc::fence_before();
+    __syncthreads();
+    if (warp == 3) {
+        tc::fence_after();
+        tc::tmem_dealloc(tmem, TCOLS);
+    }
+}
+
+// ------------------------------------------------------------------------------------ host
+template <int N> constexpr int syn_smem() { return TC_STAGES * (A_STAGE + 4 * N * 64) + 4 * 256 * 8 + 8 * 16 + 16; }
+
+}  // namespace hb
+
+using namespace hb;
+
+struct hb_batched_plan {
+    struct PlanPart {
+        const hb_plan *p;
+        int nmaps;
+        int64_t map_ofs, alm_ofs;     // offsets of this plan's maps / alm in the caller's buffers (elements)
+        float2 *GF;                   // G (synthesis) / F (analysis) buffer [nmaps][mmax+1][np][2]
+        int64_t gf_stride;
+        int64_t *tile_ofs;            // device [mmax+1] alm chunk offsets
+    };
+    std::vector<PlanPart> parts;
+    std::vector<TcGroup> hgroups;
+    std::vector<int> group_part, group_first_map;
+    TcGroup *dgroups = nullptr;
+    int4 *syn_units = nullptr, *ana_units = nullptr;
+    int n_syn = 0, n_ana = 0, N = 128;
+    int *err = nullptr;
+    void *base = nullptr;
+    size_t bytes = 0;
+    bool profile = false;
+    cudaEvent_t ev[8] = {};  // synthesis: 0 prep 1 tensor 2 ring 3 end; analysis: 4 ring 5 prep 6 tensor 7 end
+    int64_t total_maps = 0, total_pix = 0, total_alm = 0;
+};
+
+namespace hb {
+
+static int sm_count() {
+    static int v = 0;
+    if (!v) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev);
+        if (v <= 0) v = 148;
+    }
+    return v;
+}
+
+template <int N>
+static int launch_syn(hb_batched_plan *bp, cudaStream_t st) {
+    const int smem = syn_smem<N>();
+    HB_CUDA_TRY(cudaFuncSetAttribute(synth_tc_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    const int grid = std::min(bp->n_syn, sm_count());
+    synth_tc_kernel<N><<<grid, SYN_THREADS, smem, st>>>(bp->dgroups, bp->syn_units, bp->n_syn, bp->err);
+    HB_CHECK_LAUNCH();
+    return HB_OK;
+}
+template <int N>
+static int launch_ana(hb_batched_plan *bp, float2 *alm_out, cudaStream_t st) {
+    const int smem = syn_smem<N>();
+    HB_CUDA_TRY(cudaFuncSetAttribute(anal_tc_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    const int grid = std::min(bp->n_ana, sm_count());
+    anal_tc_kernel<N><<<grid, ANA_THREADS, smem, st>>>(bp->dgroups, bp->ana_units, bp->n_ana, alm_out, bp->err);
+    HB_CHECK_LAUNCH();
+    return HB_OK;
+}
+template <int N>
+static int launch_prep_alm(hb_batched_plan *bp, int gi, const float2 *alm, int64_t stride, cudaStream_t st) {
+    prep_alm_tiles_kernel<N><<<bp->hgroups[gi].mmax + 1, 256, 0, st>>>(bp->dgroups, gi, alm, stride);
+    HB_CHECK_LAUNCH();
+    return HB_OK;
+}
+template <int N>
+static int launch_prep_g(hb_batched_plan *bp, int gi, const float2 *F, int64_t stride, cudaStream_t st) {
+    prep_g_tiles_kernel<N><<<bp->hgroups[gi].mmax + 1, 256, 0, st>>>(bp->dgroups, gi, F, stride);
+    HB_CHECK_LAUNCH();
+    return HB_OK;
+}
+
+#define HB_DISPATCH_N(N_, call)                                  \
+    ((N_) == 32 ? call<32> : (N_) == 64 ? call<64> : call<128>)
+
+}  // namespace hb
+
+extern "C" {
+
+int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int nplans, int flags,
+                           hb_batched_plan **out) {
+    (void)flags;
+    if (!plans || !nmaps || nplans <= 0 || !out) return fail(HB_ERR_INVALID, "hb_batched_plan_create: bad arguments");
+    hb_batched_plan *bp = new hb_batched_plan();
+    int maxg = 0;
+    for (int i = 0; i < nplans; ++i) {
+        if (!plans[i] || !plans[i]->ck || nmaps[i] <= 0) {
+            delete bp;
+            return fail(HB_ERR_INVALID, "hb_batched_plan_create: every plan needs HB_PLAN_FP32 and nmaps > 0");
+        }
+        maxg = std::max(maxg, std::min(nmaps[i], 64));
+    }
+    bp->N = (2 * maxg <= 32) ? 32 : (2 * maxg <= 64 ? 64 : 128);
+    const int N = bp->N;
+    // sizes and layout of the single allocation
+    size_t total = 0;
+    auto carve = [&](size_t b) { size_t o = total; total += (b + 255) & ~(size_t)255; return o; };
+    struct Off { size_t gf, tofs, tiles_a, tiles_g; };
+    std::vector<Off> offs(nplans);
+    std::vector<std::vector<int64_t>> tile_ofs(nplans);
+    std::vector<int64_t> chunks_a(nplans);
+    int64_t map_ofs = 0, alm_ofs = 0;
+    for (int i = 0; i < nplans; ++i) {
+        const hb_plan *p = plans[i];
+        const int64_t np = p->g->d.npairs;
+        auto &to = tile_ofs[i];
+        to.resize(p->mmax + 2);
+        to[0] = 0;
+        for (int m = 0; m <= p->mmax; ++m) to[m + 1] = to[m] + (p->lmax - m + 64) / 64;
+        chunks_a[i] = to[p->mmax + 1];
+        const int ng = (nmaps[i] + 63) / 64;
+        offs[i].gf = carve((size_t)nmaps[i] * (p->mmax + 1) * np * 2 * sizeof(float2));
+        offs[i].tofs = carve(8 * (size_t)(p->mmax + 2));
+        offs[i].tiles_a = carve((size_t)ng * chunks_a[i] * 256 * N);
+        offs[i].tiles_g = carve((size_t)ng * (p->mmax + 1) * ((np + 31) / 32) * 256 * N);
+        hb_batched_plan::PlanPart part;
+        part.p = p;
+        part.nmaps = nmaps[i];
+        part.map_ofs = map_ofs;
+        part.alm_ofs = alm_ofs;
+        map_ofs += (int64_t)nmaps[i] * p->g->d.npix;
+        alm_ofs += (int64_t)nmaps[i] * alm_size(p->lmax, p->mmax);
+        bp->parts.push_back(part);
+    }
+    bp->total_pix = map_ofs;
+    bp->total_alm = alm_ofs;
+    const size_t o_err = carve(256);
+    // groups of <= 64 maps
+    for (int i = 0; i < nplans; ++i) {
+        const hb_plan *p = plans[i];
+        const int ng = (nmaps[i] + 63) / 64;
+        for (int k = 0; k < ng; ++k) {
+            TcGroup G{};
+            G.g = p->g->d;
+            G.lmax = p->lmax;
+            G.mmax = p->mmax;
+            G.nmaps = std::min(64, nmaps[i] - 64 * k);
+            G.npb = (p->g->d.npairs + 127) / 128;
+            G.npc = (p->g->d.npairs + 31) / 32;
+            G.ck = p->ck;
+            G.blk_ofs = p->blk_ofs;
+            bp->hgroups.push_back(G);
+            bp->group_part.push_back(i);
+            bp->group_first_map.push_back(64 * k);
+        }
+    }
+    const int ngroups = (int)bp->hgroups.size();
+    const size_t o_groups = carve(sizeof(TcGroup) * ngroups);
+    // units, sorted by decreasing work
+    std::vector<std::pair<double, int4>> su, au;
+    for (int gi = 0; gi < ngroups; ++gi) {
+        const TcGroup &G = bp->hgroups[gi];
+        for (int m = 0; m <= G.mmax; ++m) {
+            for (int64_t pb = 0; pb < G.npb; ++pb)
+                su.push_back({-(double)(G.lmax - m + 1) * N, make_int4(gi, m, (int)pb, 0)});
+            for (int jb = 0; m + 256 * jb <= G.lmax; ++jb)
+                au.push_back({-(double)std::min(256, G.lmax - m - 256 * jb + 1) * G.npc * N, make_int4(gi, m, jb, 0)});
+        }
+    }
+    std::stable_sort(su.begin(), su.end(), [](auto &a, auto &b) { return a.first < b.first; });
+    std::stable_sort(au.begin(), au.end(), [](auto &a, auto &b) { return a.first < b.first; });
+    bp->n_syn = (int)su.size();
+    bp->n_ana = (int)au.size();
+    const size_t o_su = carve(sizeof(int4) * su.size()), o_au = carve(sizeof(int4) * au.size());
+    char *base = nullptr;
+    if (cudaMalloc(&base, total) != cudaSuccess) {
+        cudaGetLastError();
+        delete bp;
+        return fail(HB_ERR_ALLOC, "hb_batched_plan_create: cudaMalloc of " + std::to_string(total) + " bytes failed");
+    }
+    bp->base = base;
+    bp->bytes = total;
+    bp->err = (int *)(base + o_err);
+    bp->dgroups = (TcGroup *)(base + o_groups);
+    bp->syn_units = (int4 *)(base + o_su);
+    bp->ana_units = (int4 *)(base + o_au);
+    for (int i = 0; i < nplans; ++i) {
+        auto &part = bp->parts[i];
+        part.GF = (float2 *)(base + offs[i].gf);
+        part.gf_stride = (int64_t)(part.p->mmax + 1) * part.p->g->d.npairs * 2;
+        part.tile_ofs = (int64_t *)(base + offs[i].tofs);
+    }
+    {
+        int gi = 0;
+        for (int i = 0; i < nplans; ++i) {
+            const hb_plan *p = plans[i];
+            const int ng = (nmaps[i] + 63) / 64;
+            for (int k = 0; k < ng; ++k, ++gi) {
+                TcGroup &G = bp->hgroups[gi];
+                G.alm_tiles = (const uint4 *)(base + offs[i].tiles_a) + (size_t)k * chunks_a[i] * 16 * N;
+                G.alm_tile_ofs = bp->parts[i].tile_ofs;
+                G.Gm = bp->parts[i].GF + (int64_t)64 * k * bp->parts[i].gf_stride;
+                G.gm_stride = bp->parts[i].gf_stride;
+                G.g_tiles = (const uint4 *)(base + offs[i].tiles_g) +
+                            (size_t)k * (p->mmax + 1) * G.npc * 16 * N;
+                G.alm_stride = alm_size(p->lmax, p->mmax);
+                G.alm_out_ofs = bp->parts[i].alm_ofs + (int64_t)64 * k * G.alm_stride;
+            }
+        }
+    }
+    std::vector<int4> suv, auv;
+    for (auto &x : su) suv.push_back(x.second);
+    for (auto &x : au) auv.push_back(x.second);
+    int rc = HB_OK;
+    for (int i = 0; i < nplans && rc == HB_OK; ++i)
+        if (cudaMemcpy(bp->parts[i].tile_ofs, tile_ofs[i].data(), 8 * tile_ofs[i].size(), cudaMemcpyHostToDevice) !=
+            cudaSuccess)
+            rc = fail(HB_ERR_CUDA, "hb_batched_plan_create: upload");
+    if (rc == HB_OK &&
+        (cudaMemcpy(bp->dgroups, bp->hgroups.data(), sizeof(TcGroup) * ngroups, cudaMemcpyHostToDevice) != cudaSuccess ||
+         cudaMemcpy(bp->syn_units, suv.data(), sizeof(int4) * suv.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+         cudaMemcpy(bp->ana_units, auv.data(), sizeof(int4) * auv.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+         cudaMemset(bp->err, 0, sizeof(int)) != cudaSuccess))
+        rc = fail(HB_ERR_CUDA, "hb_batched_plan_create: upload");
+    if (rc != HB_OK) {
+        cudaFree(base);
+        delete bp;
+        return rc;
+    }
+    *out = bp;
+    return HB_OK;
+}
+
+int hb_batched_plan_destroy(hb_batched_plan *bp) {
+    if (!bp) return HB_OK;
+    for (auto &e : bp->ev)
+        if (e) cudaEventDestroy(e);
+    cudaFree(bp->base);
+    delete bp;
+    return HB_OK;
+}
+
+size_t hb_batched_plan_bytes(const hb_batched_plan *bp) { return bp ? bp->bytes : 0; }
+
+int hb_batched_alm2map(hb_batched_plan *bp, const float *alm, float *maps, hb_stream_t stream) {
+    if (!bp || !alm || !maps) return fail(HB_ERR_INVALID, "hb_batched_alm2map: null argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc;
+    if (bp->profile) HB_CUDA_TRY(cudaEventRecord(bp->ev[0], st));
+    for (size_t gi = 0; gi < bp->hgroups.size(); ++gi) {
+        const auto &part = bp->parts[bp->group_part[gi]];
+        const float2 *a = (const float2 *)alm + part.alm_ofs +
+                          (int64_t)bp->group_first_map[gi] * alm_size(part.p->lmax, part.p->mmax);
+        if ((rc = HB_DISPATCH_N(bp->N, launch_prep_alm)(bp, (int)gi, a, alm_size(part.p->lmax, part.p->mmax), st)))
+            return rc;
+    }
+    if (bp->profile) HB_CUDA_TRY(cudaEventRecord(bp->ev[1], st));
+    if ((rc = HB_DISPATCH_N(bp->N, launch_syn)(bp, st))) return rc;
+    if (bp->profile) HB_CUDA_TRY(cudaEventRecord(bp->ev[2], st));
+    for (const auto &part : bp->parts) {
+        const GeomDev &d = part.p->g->d;
+        if ((rc = launch_ring_synthesis(d, 32, part.nmaps, part.GF, part.p->mmax, maps + part.map_ofs, d.npix, nullptr,
+                                        false, true, 0, st)))
+            return rc;
+    }
+    if (bp->profile) HB_CUDA_TRY(cudaEventRecord(bp->ev[3], st));
+    return HB_OK;
+}
+
+int hb_batched_map2alm(hb_batched_plan *bp, const float *maps, float *alm, hb_stream_t stream) {
+    if (!bp || !alm || !maps) return fail(HB_ERR_INVALID, "hb_batched_map2alm: null argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    int rc;
+    if (bp->profile) HB_CUDA_TRY(cudaEventRecord(bp->ev[4], st));
+    for (const auto &part : bp->parts) {
+        const GeomDev &d = part.p->g->d;
+        if ((rc = launch_ring_analysis(d, 32, part.nmaps, maps + part.map_ofs, d.npix, nullptr, part.GF, part.p->mmax, 0,
+                                       false, false, st)))
+            return rc;
+    }
+    if (bp->profile) HB_CUDA_TRY(cudaEventRecord(bp->ev[5], st));
+    for (size_t gi = 0; gi < bp->hgroups.size(); ++gi) {
+        const auto &part = bp->parts[bp->group_part[gi]];
+        const float2 *F = part.GF + (int64_t)bp->group_first_map[gi] * part.gf_stride;
+        if ((rc = HB_DISPATCH_N(bp->N, launch_prep_g)(bp, (int)gi, F, part.gf_stride, st))) return rc;
+    }
+    if (bp->profile) HB_CUDA_TRY(cudaEventRecord(bp->ev[6], st));
+    if ((rc = HB_DISPATCH_N(bp->N, launch_ana)(bp, (float2 *)alm, st))) return rc;
+    if (bp->profile) HB_CUDA_TRY(cudaEventRecord(bp->ev[7], st));
+    return HB_OK;
+}
+
+int hb_batched_profile(hb_batched_plan *bp, int enable) {
+    if (!bp) return fail(HB_ERR_INVALID, "hb_batched_profile: null plan");
+    if (enable && !bp->ev[0])
+        for (auto &e : bp->ev) HB_CUDA_TRY(cudaEventCreate(&e));
+    bp->profile = enable != 0;
+    return HB_OK;
+}
+
+int hb_batched_stage_ms(hb_batched_plan *bp, float *ms) {
+    if (!bp || !ms || !bp->ev[0]) return fail(HB_ERR_INVALID, "hb_batched_stage_ms: profiling not enabled");
+    HB_CUDA_TRY(cudaEventSynchronize(bp->ev[3]));
+    HB_CUDA_TRY(cudaEventSynchronize(bp->ev[7]));
+    const int pairs[6][2] = {{0, 1}, {1, 2}, {2, 3}, {4, 5}, {5, 6}, {6, 7}};
+    for (int i = 0; i < 6; ++i) HB_CUDA_TRY(cudaEventElapsedTime(&ms[i], bp->ev[pairs[i][0]], bp->ev[pairs[i][1]]));
+    return HB_OK;
+}
+
+int hb_batched_status(hb_batched_plan *bp, int *code) {
+    if (!bp || !code) return fail(HB_ERR_INVALID, "hb_batched_status: null argument");
+    HB_CUDA_TRY(cudaMemcpy(code, bp->err, sizeof(int), cudaMemcpyDeviceToHost));
+    return HB_OK;
+}
+
+}  // extern "C"

@@ -172,6 +172,31 @@ HB_API int hb_alm2cl_f32(int lmax, int mmax, int nmaps, const float *alm1, const
 HB_API int hb_alm2cl_f64(int lmax, int mmax, int nmaps, const double *alm1, const double *alm2, double *cl,
                   hb_stream_t stream);
 
+/* Batched split-precision transforms on the tcgen05 tensor cores (FP32 data, BF16 hi+lo
+ * three-pass products, FP32 accumulation in TMEM).  One batched plan covers nplans plans (each a
+ * geometry + lmax, made with HB_PLAN_FP32) with nmaps[i] maps each; all maps of all plans run
+ * in one persistent launch per direction, driven by a (plan, m, ring-block or l-block) work list
+ * sorted by decreasing work.  Creating it allocates the operand staging buffers.
+ * Buffers: alm = concatenation over plans of [nmaps_i][nalm_i] complex64, maps = concatenation
+ * over plans of [nmaps_i][npix_i] float32.  map2alm uses each geometry's default ring weights.
+ * hb_batched_status returns the kernels' error word (0 = fine; nonzero = a pipeline wait timed
+ * out and the results are invalid); it synchronises with the device.
+ * (Replaces, for batches, the per-map loops of sht_raw.py:30-57 and isht.py:5-26.) */
+typedef struct hb_batched_plan hb_batched_plan;
+HB_API int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int nplans, int flags,
+                                  hb_batched_plan **out);
+HB_API int hb_batched_plan_destroy(hb_batched_plan *bp);
+HB_API size_t hb_batched_plan_bytes(const hb_batched_plan *bp);
+HB_API int hb_batched_alm2map(hb_batched_plan *bp, const float *alm, float *maps, hb_stream_t stream);
+HB_API int hb_batched_map2alm(hb_batched_plan *bp, const float *maps, float *alm, hb_stream_t stream);
+HB_API int hb_batched_status(hb_batched_plan *bp, int *code);
+/* Profiling: with enable != 0 every exec records CUDA events between its kernels (do not enable
+ * while capturing a CUDA graph); hb_batched_stage_ms then returns the last calls' stage times in
+ * ms: [alm tile prep, tensor synthesis, ring synthesis, ring analysis, F tile prep, tensor
+ * analysis] (synchronises). */
+HB_API int hb_batched_profile(hb_batched_plan *bp, int enable);
+HB_API int hb_batched_stage_ms(hb_batched_plan *bp, float *ms);
+
 /* Pipeline stages (what the transforms are made of), for callers that keep the per-ring
  * Fourier coefficients resident or time the stages.  F / G: complex, precision 32 or 64,
  * layout [nmaps][mmax+1][npairs][2] (north, south ring of each pair), npairs from hb_geom_info.
