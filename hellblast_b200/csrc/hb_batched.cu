@@ -47,7 +47,8 @@ struct TcGroup {
     float2 *Gm;              // [map][m][pair][2]
     int64_t gm_stride;
     // analysis
-    const uint4 *g_tiles;    // [m][pc][4][N x 32] bf16
+    const uint4 *g_tiles;    // [m][pc][4][N x 32] 16-bit
+    float *dscale;           // [mmax+1] power-of-two scale of the batch operand per m (set by the prep kernels)
     int64_t alm_out_ofs;     // this group's first alm in the caller's output buffer (complex elements)
     int64_t alm_stride;
 };
@@ -62,33 +63,60 @@ __device__ __forceinline__ bool warp_wait(uint64_t *bar, uint32_t parity) {
 }
 
 // ------------------------------------------------------------------------------------ prep
+// Power-of-two scale that brings the largest |value| of one m's batch operand to [2^13, 2^14):
+// exact, keeps IEEE-half hi/lo parts normal over ~2^10 of dynamic range (harmless for BF16).
+__device__ __forceinline__ float block_pow2_scale(float vmax) {
+    __shared__ float red[32];
+    for (int o = 16; o >= 1; o >>= 1) vmax = fmaxf(vmax, __shfl_xor_sync(0xffffffffu, vmax, o));
+    if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = vmax;
+    __syncthreads();
+    float v = (threadIdx.x < (blockDim.x >> 5)) ? red[threadIdx.x] : 0.f;
+    if (threadIdx.x < 32)
+        for (int o = 16; o >= 1; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    __shared__ float res;
+    if (threadIdx.x == 0) {
+        int e = 0;
+        if (v > 0.f) frexpf(v, &e);  // v in [2^(e-1), 2^e)
+        res = (v > 0.f) ? ldexpf(1.0f, 14 - e) : 1.0f;
+    }
+    __syncthreads();
+    return res;
+}
+
 // alm [map][nalm] complex64 -> per (m, 64-l chunk) the synthesis B tiles:
 // [q][h][N rows (2*map + re/im) x 32 K (l = l0 + 2k + q)], K-major core matrices
 // (row%8)*16 B + (row/8)*512 B + (k/8)*128 B.
-template <int N>
+template <int N, bool BF16>
 __global__ void prep_alm_tiles_kernel(const TcGroup *groups, int gi, const float2 *__restrict__ alm, int64_t alm_stride) {
+    using H = tc::Half16<BF16>;
     const TcGroup &G = groups[gi];
     const int m = blockIdx.x;
     if (m > G.mmax) return;
     const int lmax = G.lmax;
     const int nch = (lmax - m + 64) / 64;
-    __nv_bfloat16 *base = (__nv_bfloat16 *)(G.alm_tiles + G.alm_tile_ofs[m] * (16 * N));
-    // thread -> (n, k, q); consecutive threads walk l
+    typename H::t *base = (typename H::t *)(G.alm_tiles + G.alm_tile_ofs[m] * (16 * N));
     const int per_chunk = N * 64;  // (n, k, q)
+    auto value = [&](int idx) -> float {
+        const int c = idx / per_chunk, r = idx % per_chunk;
+        const int n = r / 64, kq = r % 64;
+        const int l = m + 64 * c + kq;
+        const int b = n >> 1;
+        if (l > lmax || b >= G.nmaps) return 0.f;
+        const float2 a = alm[(int64_t)b * alm_stride + alm_idx(lmax, l, m)];
+        return (n & 1) ? a.y : a.x;
+    };
+    float vmax = 0.f;
+    for (int idx = threadIdx.x; idx < nch * per_chunk; idx += blockDim.x) vmax = fmaxf(vmax, fabsf(value(idx)));
+    const float s = block_pow2_scale(vmax);
+    if (threadIdx.x == 0) G.dscale[m] = s;
     for (int idx = threadIdx.x; idx < nch * per_chunk; idx += blockDim.x) {
         const int c = idx / per_chunk, r = idx % per_chunk;
         const int n = r / 64, kq = r % 64, k = kq >> 1, q = kq & 1;
-        const int l = m + 64 * c + 2 * k + q;
-        const int b = n >> 1;
-        float v = 0.f;
-        if (l <= lmax && b < G.nmaps) {
-            const float2 a = alm[(int64_t)b * alm_stride + alm_idx(lmax, l, m)];
-            v = (n & 1) ? a.y : a.x;
-        }
-        const __nv_bfloat16 hi = __float2bfloat16_rn(v);
-        const __nv_bfloat16 lo = __float2bfloat16_rn(v - __bfloat162float(hi));
+        const float v = value(idx) * s;
+        const typename H::t hi = H::one(v);
+        const typename H::t lo = H::one(v - H::back(hi));
         const int64_t off = (n & 7) * 8 + (n >> 3) * 256 + (k >> 3) * 64 + (k & 7);
-        __nv_bfloat16 *chunk = base + (int64_t)c * (4 * N * 32);
+        typename H::t *chunk = base + (int64_t)c * (4 * N * 32);
         chunk[(q * 2 + 0) * N * 32 + off] = hi;
         chunk[(q * 2 + 1) * N * 32 + off] = lo;
     }
@@ -96,34 +124,52 @@ __global__ void prep_alm_tiles_kernel(const TcGroup *groups, int gi, const float
 
 // F [map][m][pair][2] -> per (m, 32-pair chunk) the analysis B tiles [q][h][N x 32 pairs]
 // (E = F_N + F_S for q = 0, O = F_N - F_S for q = 1), K-major like above.
-template <int N>
+template <int N, bool BF16>
 __global__ void prep_g_tiles_kernel(const TcGroup *groups, int gi, const float2 *__restrict__ F, int64_t f_stride) {
+    using H = tc::Half16<BF16>;
     const TcGroup &G = groups[gi];
     const int m = blockIdx.x;
     if (m > G.mmax) return;
     const int64_t np = G.g.npairs;
-    __nv_bfloat16 *base = (__nv_bfloat16 *)(G.g_tiles + (int64_t)m * G.npc * (16 * N));
+    typename H::t *base = (typename H::t *)(G.g_tiles + (int64_t)m * G.npc * (16 * N));
     const int per_chunk = N * 32;
-    for (int64_t idx = threadIdx.x; idx < G.npc * per_chunk; idx += blockDim.x) {
+    auto eo = [&](int64_t idx, float &e, float &o) {
         const int64_t c = idx / per_chunk;
         const int r = (int)(idx % per_chunk);
         const int n = r / 32, k = r % 32;
         const int64_t p = c * 32 + k;
         const int b = n >> 1;
-        float e = 0.f, o = 0.f;
+        e = o = 0.f;
         if (p < np && b < G.nmaps) {
             const float2 *f = F + (int64_t)b * f_stride + ((int64_t)m * np + p) * 2;
             const float2 fn = f[0], fs = f[1];
             e = (n & 1) ? fn.y + fs.y : fn.x + fs.x;
             o = (n & 1) ? fn.y - fs.y : fn.x - fs.x;
         }
+    };
+    float vmax = 0.f;
+    for (int64_t idx = threadIdx.x; idx < G.npc * per_chunk; idx += blockDim.x) {
+        float e, o;
+        eo(idx, e, o);
+        vmax = fmaxf(vmax, fmaxf(fabsf(e), fabsf(o)));
+    }
+    const float s = block_pow2_scale(vmax);
+    if (threadIdx.x == 0) G.dscale[m] = s;
+    for (int64_t idx = threadIdx.x; idx < G.npc * per_chunk; idx += blockDim.x) {
+        float e, o;
+        eo(idx, e, o);
+        e *= s;
+        o *= s;
+        const int64_t c = idx / per_chunk;
+        const int r = (int)(idx % per_chunk);
+        const int n = r / 32, k = r % 32;
         const int64_t off = (n & 7) * 8 + (n >> 3) * 256 + (k >> 3) * 64 + (k & 7);
-        __nv_bfloat16 *chunk = base + c * (4 * N * 32);
-        __nv_bfloat16 ehi = __float2bfloat16_rn(e), ohi = __float2bfloat16_rn(o);
+        typename H::t *chunk = base + c * (4 * N * 32);
+        const typename H::t ehi = H::one(e), ohi = H::one(o);
         chunk[0 * N * 32 + off] = ehi;
-        chunk[1 * N * 32 + off] = __float2bfloat16_rn(e - __bfloat162float(ehi));
+        chunk[1 * N * 32 + off] = H::one(e - H::back(ehi));
         chunk[2 * N * 32 + off] = ohi;
-        chunk[3 * N * 32 + off] = __float2bfloat16_rn(o - __bfloat162float(ohi));
+        chunk[3 * N * 32 + off] = H::one(o - H::back(ohi));
     }
 }
 
@@ -169,12 +215,13 @@ __device__ __forceinline__ void coef_scalar(int l, int m, int lmax, float2 &out)
 // ------------------------------------------------------------------------------------ synthesis
 constexpr int SYN_THREADS = 192;  // warps 0-3 producers/epilogue, 4 MMA, 5 loader
 
-template <int N>
+template <int N, bool BF16>
 __global__ void __launch_bounds__(SYN_THREADS, 1)
     synth_tc_kernel(const TcGroup *__restrict__ groups, const int4 *__restrict__ units, int nunits, int *err) {
-    constexpr int B_STAGE = 4 * N * 64;  // [q][h][N x 32] bf16
+    constexpr int B_STAGE = 4 * N * 64;  // [q][h][N x 32] 16-bit
     constexpr int STAGE = A_STAGE + B_STAGE;
-    constexpr uint32_t IDESC = tc::idesc_bf16(128, N, 0, 0);
+    constexpr uint32_t IDESC = tc::idesc_f16kind(128, N, 0, 0, BF16);
+    constexpr float LS = BF16 ? 1.0f : 256.0f;  // lambda scale (|lambda| < 2^7 -> < 2^15 in half)
     constexpr int TCOLS = (2 * N < 32) ? 32 : 2 * N;
     extern __shared__ __align__(1024) uint8_t smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -249,10 +296,10 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
                     }
                     uint4 hi, lo;
                     const int off = (r & 7) * 16 + (r >> 3) * 512 + grp * 128;
-                    tc::split8(ev, hi, lo);
+                    tc::split8<BF16>(ev, LS, hi, lo);
                     *reinterpret_cast<uint4 *>(A + 0 * A_TILE + off) = hi;
                     *reinterpret_cast<uint4 *>(A + 1 * A_TILE + off) = lo;
-                    tc::split8(od, hi, lo);
+                    tc::split8<BF16>(od, LS, hi, lo);
                     *reinterpret_cast<uint4 *>(A + 2 * A_TILE + off) = hi;
                     *reinterpret_cast<uint4 *>(A + 3 * A_TILE + off) = lo;
                 }
@@ -268,6 +315,7 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
             }
             tc::fence_after();
             const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+            const float inv = 1.0f / (LS * G.dscale[m]);
 #pragma unroll
             for (int j = 0; j < N / 16; ++j) {
                 float de[16], dd[16];
@@ -280,7 +328,8 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
                         const int b = j * 8 + h;
                         if (b < G.nmaps) {
                             float2 *dst = G.Gm + (int64_t)b * G.gm_stride + ((int64_t)m * np + p) * 2;
-                            const float re = de[2 * h], im = de[2 * h + 1], ro = dd[2 * h], io = dd[2 * h + 1];
+                            const float re = de[2 * h] * inv, im = de[2 * h + 1] * inv, ro = dd[2 * h] * inv,
+                                        io = dd[2 * h + 1] * inv;
                             *reinterpret_cast<float4 *>(dst) = make_float4(re + ro, im + io, re - ro, im - io);
                         }
                     }
@@ -374,13 +423,14 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
 // ------------------------------------------------------------------------------------ analysis
 constexpr int ANA_THREADS = 160;  // warps 0-2 producers (+ epilogue), 3 MMA (+ epilogue), 4 loader
 
-template <int N>
+template <int N, bool BF16>
 __global__ void __launch_bounds__(ANA_THREADS, 1)
     anal_tc_kernel(const TcGroup *__restrict__ groups, const int4 *__restrict__ units, int nunits, float2 *alm_out,
                    int *err) {
     constexpr int B_STAGE = 4 * N * 64;
     constexpr int STAGE = A_STAGE + B_STAGE;
-    constexpr uint32_t IDESC = tc::idesc_bf16(128, N, 1, 0);
+    constexpr uint32_t IDESC = tc::idesc_f16kind(128, N, 1, 0, BF16);
+    constexpr float LS = BF16 ? 1.0f : 256.0f;
     constexpr int TCOLS = (2 * N < 32) ? 32 : 2 * N;
     extern __shared__ __align__(1024) uint8_t smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -453,10 +503,10 @@ __global__ void __launch_bounds__(ANA_THREADS, 1)
                         uint4 hi, lo;
                         // MN-major: 8 consecutive rows (l of one parity) of pair `lane`
                         const int off = (lane & 7) * 16 + grp * 512 + (lane >> 3) * 128;
-                        tc::split8(ev, hi, lo);
+                        tc::split8<BF16>(ev, LS, hi, lo);
                         *reinterpret_cast<uint4 *>(A + 0 * A_TILE + off) = hi;
                         *reinterpret_cast<uint4 *>(A + 1 * A_TILE + off) = lo;
-                        tc::split8(od, hi, lo);
+                        tc::split8<BF16>(od, LS, hi, lo);
                         *reinterpret_cast<uint4 *>(A + 2 * A_TILE + off) = hi;
                         *reinterpret_cast<uint4 *>(A + 3 * A_TILE + off) = lo;
                     }
@@ -518,6 +568,7 @@ __global__ void __launch_bounds__(ANA_THREADS, 1)
             const int row = warp * 32 + lane;
             const int le = l0 + 2 * row;
             const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+            const float inv = 1.0f / (LS * G.dscale[m]);
 #pragma unroll
             for (int j = 0; j < N / 16; ++j) {
                 float de[16], dd[16];
@@ -529,8 +580,8 @@ __global__ void __launch_bounds__(ANA_THREADS, 1)
                     const int b = j * 8 + h;
                     if (b < G.nmaps) {
                         float2 *dst = alm_out + G.alm_out_ofs + (int64_t)b * G.alm_stride + alm_idx(lmax, le, m);
-                        if (le <= lmax) dst[0] = make_float2(de[2 * h], de[2 * h + 1]);
-                        if (le + 1 <= lmax) dst[1] = make_float2(dd[2 * h], dd[2 * h + 1]);
+                        if (le <= lmax) dst[0] = make_float2(de[2 * h] * inv, de[2 * h + 1] * inv);
+                        if (le + 1 <= lmax) dst[1] = make_float2(dd[2 * h] * inv, dd[2 * h + 1] * inv);
                     }
                 }
             }
@@ -588,6 +639,7 @@ struct hb_batched_plan {
     std::vector<PlanPart> parts;
     std::vector<TcGroup> hgroups;
     std::vector<int> group_part, group_first_map;
+    bool bf16 = false;
     TcGroup *dgroups = nullptr;
     int4 *syn_units = nullptr, *ana_units = nullptr;
     int n_syn = 0, n_ana = 0, N = 128;
@@ -612,39 +664,40 @@ static int sm_count() {
     return v;
 }
 
-template <int N>
+template <int N, bool BF16>
 static int launch_syn(hb_batched_plan *bp, cudaStream_t st) {
     const int smem = syn_smem<N>();
-    HB_CUDA_TRY(cudaFuncSetAttribute(synth_tc_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    HB_CUDA_TRY(cudaFuncSetAttribute(synth_tc_kernel<N, BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     const int grid = std::min(bp->n_syn, sm_count());
-    synth_tc_kernel<N><<<grid, SYN_THREADS, smem, st>>>(bp->dgroups, bp->syn_units, bp->n_syn, bp->err);
+    synth_tc_kernel<N, BF16><<<grid, SYN_THREADS, smem, st>>>(bp->dgroups, bp->syn_units, bp->n_syn, bp->err);
     HB_CHECK_LAUNCH();
     return HB_OK;
 }
-template <int N>
+template <int N, bool BF16>
 static int launch_ana(hb_batched_plan *bp, float2 *alm_out, cudaStream_t st) {
     const int smem = syn_smem<N>();
-    HB_CUDA_TRY(cudaFuncSetAttribute(anal_tc_kernel<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    HB_CUDA_TRY(cudaFuncSetAttribute(anal_tc_kernel<N, BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     const int grid = std::min(bp->n_ana, sm_count());
-    anal_tc_kernel<N><<<grid, ANA_THREADS, smem, st>>>(bp->dgroups, bp->ana_units, bp->n_ana, alm_out, bp->err);
+    anal_tc_kernel<N, BF16><<<grid, ANA_THREADS, smem, st>>>(bp->dgroups, bp->ana_units, bp->n_ana, alm_out, bp->err);
     HB_CHECK_LAUNCH();
     return HB_OK;
 }
-template <int N>
+template <int N, bool BF16>
 static int launch_prep_alm(hb_batched_plan *bp, int gi, const float2 *alm, int64_t stride, cudaStream_t st) {
-    prep_alm_tiles_kernel<N><<<bp->hgroups[gi].mmax + 1, 256, 0, st>>>(bp->dgroups, gi, alm, stride);
+    prep_alm_tiles_kernel<N, BF16><<<bp->hgroups[gi].mmax + 1, 256, 0, st>>>(bp->dgroups, gi, alm, stride);
     HB_CHECK_LAUNCH();
     return HB_OK;
 }
-template <int N>
+template <int N, bool BF16>
 static int launch_prep_g(hb_batched_plan *bp, int gi, const float2 *F, int64_t stride, cudaStream_t st) {
-    prep_g_tiles_kernel<N><<<bp->hgroups[gi].mmax + 1, 256, 0, st>>>(bp->dgroups, gi, F, stride);
+    prep_g_tiles_kernel<N, BF16><<<bp->hgroups[gi].mmax + 1, 256, 0, st>>>(bp->dgroups, gi, F, stride);
     HB_CHECK_LAUNCH();
     return HB_OK;
 }
 
-#define HB_DISPATCH_N(N_, call)                                  \
-    ((N_) == 32 ? call<32> : (N_) == 64 ? call<64> : call<128>)
+#define HB_DISPATCH_N(bp_, call)                                                                      \
+    ((bp_)->bf16 ? ((bp_)->N == 32 ? call<32, true> : (bp_)->N == 64 ? call<64, true> : call<128, true>) \
+                 : ((bp_)->N == 32 ? call<32, false> : (bp_)->N == 64 ? call<64, false> : call<128, false>))
 
 }  // namespace hb
 
@@ -652,9 +705,9 @@ extern "C" {
 
 int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int nplans, int flags,
                            hb_batched_plan **out) {
-    (void)flags;
     if (!plans || !nmaps || nplans <= 0 || !out) return fail(HB_ERR_INVALID, "hb_batched_plan_create: bad arguments");
     hb_batched_plan *bp = new hb_batched_plan();
+    bp->bf16 = (flags & HB_BATCHED_BF16) != 0;
     int maxg = 0;
     for (int i = 0; i < nplans; ++i) {
         if (!plans[i] || !plans[i]->ck || nmaps[i] <= 0) {
@@ -668,7 +721,7 @@ int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int np
     // sizes and layout of the single allocation
     size_t total = 0;
     auto carve = [&](size_t b) { size_t o = total; total += (b + 255) & ~(size_t)255; return o; };
-    struct Off { size_t gf, tofs, tiles_a, tiles_g; };
+    struct Off { size_t gf, tofs, tiles_a, tiles_g, scales; };
     std::vector<Off> offs(nplans);
     std::vector<std::vector<int64_t>> tile_ofs(nplans);
     std::vector<int64_t> chunks_a(nplans);
@@ -686,6 +739,7 @@ int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int np
         offs[i].tofs = carve(8 * (size_t)(p->mmax + 2));
         offs[i].tiles_a = carve((size_t)ng * chunks_a[i] * 256 * N);
         offs[i].tiles_g = carve((size_t)ng * (p->mmax + 1) * ((np + 31) / 32) * 256 * N);
+        offs[i].scales = carve((size_t)ng * 4 * (p->mmax + 1));
         hb_batched_plan::PlanPart part;
         part.p = p;
         part.nmaps = nmaps[i];
@@ -766,6 +820,7 @@ int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int np
                 G.gm_stride = bp->parts[i].gf_stride;
                 G.g_tiles = (const uint4 *)(base + offs[i].tiles_g) +
                             (size_t)k * (p->mmax + 1) * G.npc * 16 * N;
+                G.dscale = (float *)(base + offs[i].scales) + (size_t)k * (p->mmax + 1);
                 G.alm_stride = alm_size(p->lmax, p->mmax);
                 G.alm_out_ofs = bp->parts[i].alm_ofs + (int64_t)64 * k * G.alm_stride;
             }
@@ -814,11 +869,11 @@ int hb_batched_alm2map(hb_batched_plan *bp, const float *alm, float *maps, hb_st
         const auto &part = bp->parts[bp->group_part[gi]];
         const float2 *a = (const float2 *)alm + part.alm_ofs +
                           (int64_t)bp->group_first_map[gi] * alm_size(part.p->lmax, part.p->mmax);
-        if ((rc = HB_DISPATCH_N(bp->N, launch_prep_alm)(bp, (int)gi, a, alm_size(part.p->lmax, part.p->mmax), st)))
+        if ((rc = HB_DISPATCH_N(bp, launch_prep_alm)(bp, (int)gi, a, alm_size(part.p->lmax, part.p->mmax), st)))
             return rc;
     }
     if (bp->profile) HB_CUDA_TRY(cudaEventRecord(bp->ev[1], st));
-    if ((rc = HB_DISPATCH_N(bp->N, launch_syn)(bp, st))) return rc;
+    if ((rc = HB_DISPATCH_N(bp, launch_syn)(bp, st))) return rc;
     if (bp->profile) HB_CUDA_TRY(cudaEventRecord(bp->ev[2], st));
     for (const auto &part : bp->parts) {
         const GeomDev &d = part.p->g->d;
@@ -845,10 +900,10 @@ int hb_batched_map2alm(hb_batched_plan *bp, const float *maps, float *alm, hb_st
     for (size_t gi = 0; gi < bp->hgroups.size(); ++gi) {
         const auto &part = bp->parts[bp->group_part[gi]];
         const float2 *F = part.GF + (int64_t)bp->group_first_map[gi] * part.gf_stride;
-        if ((rc = HB_DISPATCH_N(bp->N, launch_prep_g)(bp, (int)gi, F, part.gf_stride, st))) return rc;
+        if ((rc = HB_DISPATCH_N(bp, launch_prep_g)(bp, (int)gi, F, part.gf_stride, st))) return rc;
     }
     if (bp->profile) HB_CUDA_TRY(cudaEventRecord(bp->ev[6], st));
-    if ((rc = HB_DISPATCH_N(bp->N, launch_ana)(bp, (float2 *)alm, st))) return rc;
+    if ((rc = HB_DISPATCH_N(bp, launch_ana)(bp, (float2 *)alm, st))) return rc;
     if (bp->profile) HB_CUDA_TRY(cudaEventRecord(bp->ev[7], st));
     return HB_OK;
 }

@@ -3,6 +3,7 @@
 // TMEM), tcgen05.commit / tcgen05.ld, and the UMMA shared-memory / instruction descriptors.
 #pragma once
 #include <cuda_bf16.h>
+#include <cuda_fp16.h>
 #include <stdint.h>
 
 namespace hb {
@@ -122,22 +123,45 @@ __device__ __forceinline__ uint64_t sdesc(uint32_t saddr, uint32_t lbo, uint32_t
     d |= (uint64_t)1 << 46;  // descriptor version for sm_100
     return d;                // base offset 0, absolute LBO mode off, layout type 0 (no swizzle)
 }
-// Instruction descriptor: BF16 x BF16 -> FP32, dense, M x N, operand majors (0 = K, 1 = MN)
-__host__ __device__ constexpr uint32_t idesc_bf16(int M, int N, int a_mn_major, int b_mn_major) {
-    return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)a_mn_major << 15) | ((uint32_t)b_mn_major << 16) |
-           ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
+// Instruction descriptor: (BF16 x BF16 or F16 x F16) -> FP32, dense, M x N, operand majors
+// (0 = K, 1 = MN).  Both operands always share one type.
+__host__ __device__ constexpr uint32_t idesc_f16kind(int M, int N, int a_mn_major, int b_mn_major, bool bf16) {
+    return (1u << 4) | ((bf16 ? 1u : 0u) << 7) | ((bf16 ? 1u : 0u) << 10) | ((uint32_t)a_mn_major << 15) |
+           ((uint32_t)b_mn_major << 16) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
 }
 
-// 8 floats -> 8 bf16 "hi" and 8 bf16 "lo" = bf16(v - hi), packed as two uint4
-__device__ __forceinline__ void split8(const float (&v)[8], uint4 &hi, uint4 &lo) {
+// 16-bit operand type of the split: BF16 (8-bit significand) or IEEE half (11-bit significand)
+template <bool BF16> struct Half16;
+template <> struct Half16<true> {
+    using t = __nv_bfloat16;
+    using t2 = __nv_bfloat162;
+    static __device__ __forceinline__ t2 pack(float a, float b) { return __floats2bfloat162_rn(a, b); }
+    static __device__ __forceinline__ float2 unpack(t2 v) { return __bfloat1622float2(v); }
+    static __device__ __forceinline__ t one(float a) { return __float2bfloat16_rn(a); }
+    static __device__ __forceinline__ float back(t a) { return __bfloat162float(a); }
+};
+template <> struct Half16<false> {
+    using t = __half;
+    using t2 = __half2;
+    static __device__ __forceinline__ t2 pack(float a, float b) { return __floats2half2_rn(a, b); }
+    static __device__ __forceinline__ float2 unpack(t2 v) { return __half22float2(v); }
+    static __device__ __forceinline__ t one(float a) { return __float2half_rn(a); }
+    static __device__ __forceinline__ float back(t a) { return __half2float(a); }
+};
+
+// 8 floats * s -> 8 "hi" = h(v s) and 8 "lo" = h(v s - hi), packed as two uint4
+template <bool BF16>
+__device__ __forceinline__ void split8(const float (&v)[8], float s, uint4 &hi, uint4 &lo) {
+    using H = Half16<BF16>;
     uint32_t h[4], l[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        __nv_bfloat162 b = __floats2bfloat162_rn(v[2 * i], v[2 * i + 1]);
-        float2 f = __bfloat1622float2(b);
-        __nv_bfloat162 c = __floats2bfloat162_rn(v[2 * i] - f.x, v[2 * i + 1] - f.y);
-        h[i] = *reinterpret_cast<uint32_t *>(&b);
-        l[i] = *reinterpret_cast<uint32_t *>(&c);
+        const float a = v[2 * i] * s, b = v[2 * i + 1] * s;
+        typename H::t2 x = H::pack(a, b);
+        float2 f = H::unpack(x);
+        typename H::t2 y = H::pack(a - f.x, b - f.y);
+        h[i] = *reinterpret_cast<uint32_t *>(&x);
+        l[i] = *reinterpret_cast<uint32_t *>(&y);
     }
     hi = make_uint4(h[0], h[1], h[2], h[3]);
     lo = make_uint4(l[0], l[1], l[2], l[3]);

@@ -183,6 +183,11 @@ HB_API int hb_alm2cl_f64(int lmax, int mmax, int nmaps, const double *alm1, cons
  * out and the results are invalid); it synchronises with the device.
  * (Replaces, for batches, the per-map loops of sht_raw.py:30-57 and isht.py:5-26.) */
 typedef struct hb_batched_plan hb_batched_plan;
+/* flags: HB_BATCHED_BF16 splits into BF16 hi+lo (8-bit significands) instead of the default
+ * IEEE-half hi+lo with exact power-of-two per-m scaling (11-bit significands); both run at the
+ * same tcgen05 kind::f16 rate.  Measured at nside 2048, lmax 4095 the BF16 split leaves 2.1e-5
+ * relative error on a map2alm+alm2map pair, the half split stays within 1e-5. */
+enum { HB_BATCHED_BF16 = 1 };
 HB_API int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int nplans, int flags,
                                   hb_batched_plan **out);
 HB_API int hb_batched_plan_destroy(hb_batched_plan *bp);

@@ -27,18 +27,19 @@ def _batch(hb, lmax, nmaps, seed=0):
     return torch.stack([hb.synalm(cl, lmax=lmax, seed=seed + i, device="cuda") for i in range(nmaps)])
 
 
+@pytest.mark.parametrize("bf16", [False, True])
 @pytest.mark.parametrize("nside,nmaps", [(8, 1), (16, 3), (64, 20), (128, 64)])
-def test_batched_alm2map_and_map2alm_vs_fp64(hb, nside, nmaps):
+def test_batched_alm2map_and_map2alm_vs_fp64(hb, nside, nmaps, bf16):
     lmax = 2 * nside - 1
     a64 = _batch(hb, lmax, nmaps)
     m64 = hb.hp_compat.alm2map(a64, nside, lmax=lmax)
-    mb = hb.batched.alm2map(a64.to(torch.complex64), nside, lmax)
-    bp = hb.batched.plan(nside, lmax, nmaps)
+    mb = hb.batched.alm2map(a64.to(torch.complex64), nside, lmax, bf16=bf16)
+    bp = hb.batched.plan(nside, lmax, nmaps, bf16=bf16)
     assert bp.status() == 0
     assert mb.shape == m64.shape and mb.dtype == torch.float32
     assert rel(mb, m64) < TOL
     b64 = hb.hp_compat.map2alm(m64, lmax=lmax)
-    bb = hb.batched.map2alm(m64.float(), nside, lmax)
+    bb = hb.batched.map2alm(m64.float(), nside, lmax, bf16=bf16)
     assert bp.status() == 0
     assert rel(bb, b64) < TOL
     # and against the plain FP32 path on the same inputs
@@ -96,3 +97,21 @@ def test_batched_vs_oracle_small(hb, oracle):
     back = hb.batched.map2alm(torch.from_numpy(ref).cuda().float(), nside, lmax).cpu().numpy()
     refa = np.stack([oracle.map2alm(r, g, lmax) for r in ref])
     assert np.linalg.norm(back - refa) / np.linalg.norm(refa) < TOL
+
+
+@pytest.mark.parametrize("nside", [1024, 2048])
+def test_batched_pair_accuracy_at_full_size(hb, nside):
+    """The north-star bar: the batched (IEEE-half hi+lo, default) pair within 1e-5 of FP64 at
+    lmax = 2 nside - 1, 8 maps."""
+    lmax, nmaps = 2 * nside - 1, 8
+    a64 = _batch(hb, lmax, nmaps, seed=7)
+    mb = hb.batched.alm2map(a64.to(torch.complex64), nside, lmax)
+    bb = hb.batched.map2alm(mb, nside, lmax)
+    errs = []
+    for i in (0, nmaps - 1):
+        m64 = hb.hp_compat.alm2map(a64[i], nside, lmax=lmax)
+        b64 = hb.hp_compat.map2alm(m64, lmax=lmax)
+        errs.append((rel(mb[i], m64), rel(bb[i], b64)))
+        del m64, b64
+    assert hb.batched.plan(nside, lmax, nmaps).status() == 0
+    assert all(e[0] < TOL and e[1] < TOL for e in errs), errs
