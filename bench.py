@@ -38,6 +38,8 @@ def parse():
     p.add_argument("--nside", type=int, default=2048)
     p.add_argument("--lmax", type=int, default=None)
     p.add_argument("--nmaps", type=int, default=None, help="maps per GPU (default 64 batched, 1 plain)")
+    p.add_argument("--split", default="f16", choices=["f16", "bf16"], help="16-bit type of the hi+lo split")
+    p.add_argument("--wide", action="store_true", help="groups of 64 maps (two accumulator sets)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-sample-m", type=int, default=12)
     return p.parse_args()
@@ -225,7 +227,8 @@ def main():
         def make_ev():
             return [torch.cuda.Event(enable_timing=True) for _ in range(5)]
     else:
-        bp = hb.batched.plan(nside, lmax, B)
+        bf16 = args.split == "bf16"
+        bp = hb.batched.plan(nside, lmax, B, bf16=bf16, wide=args.wide)
         bp.profile(True)
         alm_flat, maps_flat, out_flat = alm.reshape(-1), maps.reshape(-1), alm_out.reshape(-1)
         stage_acc = []
@@ -292,8 +295,8 @@ def main():
             m = hb.hp_compat.alm2map(a, nside, lmax=lmax)
             r = hb.hp_compat.map2alm(m, lmax=lmax)
         else:
-            m = hb.batched.alm2map(a, nside, lmax)
-            r = hb.batched.map2alm(m, nside, lmax)
+            m = bp.alm2map(a).reshape(B, -1)
+            r = bp.map2alm(m).reshape(B, -1)
         out_pin.copy_(r, non_blocking=True)
 
     for _ in range(max(1, args.warmup)):
@@ -339,8 +342,9 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (Gaussian alm, C_l=(l+10)^-2)",
         "config": {"workload": (f"scalar map2alm+alm2map pair, nside {nside}, lmax {lmax}, float32 maps, "
-                                + ("batched split-BF16 tcgen05 path, " if args.mode == "batched" else
-                                   "plain per-map FP32 path, ") + f"{B} maps per GPU per step"),
+                                + (f"batched hi+lo split-{args.split.upper()} tcgen05 path"
+                                   f" ({'64' if args.wide else '32'} maps per group), " if args.mode == "batched"
+                                   else "plain per-map FP32 path, ") + f"{B} maps per GPU per step"),
                    "nside": nside, "lmax": lmax, "maps_per_gpu": B, "mode": args.mode,
                    "l2": "inputs larger than L2 (one map 201 MB, one alm 67 MB)",
                    "parallelism": f"replicas x{world}"},

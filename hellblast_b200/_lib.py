@@ -77,6 +77,8 @@ for _p in ("f32", "f64"):
 
 HB_PLAN_FP32 = 1
 HB_PLAN_SPIN2_FP32 = 2
+HB_BATCHED_BF16 = 1
+HB_BATCHED_WIDE = 2
 
 
 class HBError(RuntimeError):

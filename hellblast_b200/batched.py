@@ -1,6 +1,10 @@
-"""Batched split-precision transforms (BF16 hi+lo three-pass products on the tcgen05 tensor
+"""Batched split-precision transforms (16-bit hi+lo three-pass products on the tcgen05 tensor
 cores, FP32 accumulation in TMEM): many maps of one or several (nside, lmax) in one persistent
-launch per direction.  Wraps hb_batched_plan_* of the C ABI."""
+launch per direction.  Wraps hb_batched_plan_* of the C ABI.
+
+The default split is IEEE half with exact power-of-two per-m scaling (``bf16=True``: BF16).
+Maps run in groups of 32 with four TMEM accumulator sets per output tile (``wide=True``: groups
+of 64 with two sets, fewer recursion passes, about twice the accumulation error)."""
 from __future__ import annotations
 
 import ctypes
@@ -20,15 +24,17 @@ class BatchedPlan:
     """``specs``: list of (geometry, lmax, mmax, nmaps).  Inputs/outputs are flat CUDA tensors
     holding the maps (float32) or alm (complex64, healpy layout) of all specs back to back."""
 
-    def __init__(self, specs, bf16: bool = False):
+    def __init__(self, specs, bf16: bool = False, wide: bool = False):
         self.specs = [(g, int(lmax), int(lmax if mmax is None else mmax), int(n)) for g, lmax, mmax, n in specs]
         self.plans = [G.plan(g, lmax, mmax, precision=32) for g, lmax, mmax, _ in self.specs]
         n = len(self.plans)
         arr = (ctypes.c_void_p * n)(*[p.handle.value for p in self.plans])
         nm = (ctypes.c_int * n)(*[s[3] for s in self.specs])
         out = ctypes.c_void_p()
-        L.call("hb_batched_plan_create", arr, nm, n, 1 if bf16 else 0, ctypes.byref(out))
+        flags = (L.HB_BATCHED_BF16 if bf16 else 0) | (L.HB_BATCHED_WIDE if wide else 0)
+        L.call("hb_batched_plan_create", arr, nm, n, flags, ctypes.byref(out))
         self.bf16 = bf16
+        self.wide = wide
         self.handle = out
         self.nbytes = int(L.lib().hb_batched_plan_bytes(out))
         self.total_pix = sum(g.npix * k for g, _, _, k in self.specs)
@@ -76,26 +82,28 @@ class BatchedPlan:
 
 
 def plan(nside: int, lmax: int, nmaps: int, mmax: int | None = None, weights: str = "dz",
-         bf16: bool = False) -> BatchedPlan:
+         bf16: bool = False, wide: bool = False) -> BatchedPlan:
     """Cached single-geometry batched plan (HEALPix nside, lmax, nmaps maps).  ``bf16`` selects
-    the BF16 hi+lo split instead of the default IEEE-half hi+lo split."""
-    key = (int(nside), int(lmax), mmax, int(nmaps), weights, bool(bf16), torch.cuda.current_device())
+    the BF16 hi+lo split instead of the default IEEE-half hi+lo split, ``wide`` groups of 64 maps."""
+    key = (int(nside), int(lmax), mmax, int(nmaps), weights, bool(bf16), bool(wide), torch.cuda.current_device())
     with _lock:
         bp = _cache.get(key)
     if bp is None:
-        bp = BatchedPlan([(G.healpix(nside, weights=weights), lmax, mmax, nmaps)], bf16=bf16)
+        bp = BatchedPlan([(G.healpix(nside, weights=weights), lmax, mmax, nmaps)], bf16=bf16, wide=wide)
         with _lock:
             _cache[key] = bp
     return bp
 
 
-def alm2map(alm: torch.Tensor, nside: int, lmax: int, mmax: int | None = None, bf16: bool = False) -> torch.Tensor:
+def alm2map(alm: torch.Tensor, nside: int, lmax: int, mmax: int | None = None, bf16: bool = False,
+            wide: bool = False) -> torch.Tensor:
     """[nmaps, nalm] complex64 -> [nmaps, npix] float32 through the tensor-core path."""
     nmaps = alm.shape[0]
-    return plan(nside, lmax, nmaps, mmax, bf16=bf16).alm2map(alm).reshape(nmaps, -1)
+    return plan(nside, lmax, nmaps, mmax, bf16=bf16, wide=wide).alm2map(alm).reshape(nmaps, -1)
 
 
-def map2alm(maps: torch.Tensor, nside: int, lmax: int, mmax: int | None = None, bf16: bool = False) -> torch.Tensor:
+def map2alm(maps: torch.Tensor, nside: int, lmax: int, mmax: int | None = None, bf16: bool = False,
+            wide: bool = False) -> torch.Tensor:
     """[nmaps, npix] float32 -> [nmaps, nalm] complex64 through the tensor-core path."""
     nmaps = maps.shape[0]
-    return plan(nside, lmax, nmaps, mmax, bf16=bf16).map2alm(maps).reshape(nmaps, -1)
+    return plan(nside, lmax, nmaps, mmax, bf16=bf16, wide=wide).map2alm(maps).reshape(nmaps, -1)

@@ -215,14 +215,18 @@ __device__ __forceinline__ void coef_scalar(int l, int m, int lmax, float2 &out)
 // ------------------------------------------------------------------------------------ synthesis
 constexpr int SYN_THREADS = 192;  // warps 0-3 producers/epilogue, 4 MMA, 5 loader
 
-template <int N, bool BF16>
+template <int N, bool BF16, int S>
 __global__ void __launch_bounds__(SYN_THREADS, 1)
     synth_tc_kernel(const TcGroup *__restrict__ groups, const int4 *__restrict__ units, int nunits, int *err) {
     constexpr int B_STAGE = 4 * N * 64;  // [q][h][N x 32] 16-bit
     constexpr int STAGE = A_STAGE + B_STAGE;
     constexpr uint32_t IDESC = tc::idesc_f16kind(128, N, 0, 0, BF16);
     constexpr float LS = BF16 ? 1.0f : 256.0f;  // lambda scale (|lambda| < 2^7 -> < 2^15 in half)
-    constexpr int TCOLS = (2 * N < 32) ? 32 : 2 * N;
+    // S accumulator sets, chunk c accumulates into set c % S: the tensor core's FP32 accumulation
+    // error grows with the number of accumulate steps into one set; the epilogue sums the sets
+    // in IEEE FP32.
+    constexpr int TCOLS = (2 * N * S < 32) ? 32 : 2 * N * S;
+    static_assert(2 * N * S <= 512, "TMEM holds 512 columns");
     extern __shared__ __align__(1024) uint8_t smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // one private copy of the 256 recursion coefficients per producer warp (no cross-warp barrier)
@@ -316,12 +320,24 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
             tc::fence_after();
             const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
             const float inv = 1.0f / (LS * G.dscale[m]);
-#pragma unroll
+            const int nsets = nch < S ? nch : S;
+#pragma unroll 1
             for (int j = 0; j < N / 16; ++j) {
                 float de[16], dd[16];
                 tc::tmem_ld16(tmem + lane_base + j * 16, de);
                 tc::tmem_ld16(tmem + lane_base + N + j * 16, dd);
                 tc::tmem_wait_ld();
+                for (int st = 1; st < nsets; ++st) {
+                    float xe[16], xd[16];
+                    tc::tmem_ld16(tmem + lane_base + st * 2 * N + j * 16, xe);
+                    tc::tmem_ld16(tmem + lane_base + st * 2 * N + N + j * 16, xd);
+                    tc::tmem_wait_ld();
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) {
+                        de[i] += xe[i];
+                        dd[i] += xd[i];
+                    }
+                }
                 if (live) {
 #pragma unroll
                     for (int h = 0; h < 8; ++h) {
@@ -363,16 +379,17 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
                     }
                     tc::fence_after();
                     const uint32_t a0 = tc::smem_u32(smem + s * STAGE), b0 = a0 + A_STAGE;
+                    const int set = c % S;
 #pragma unroll
                     for (int q = 0; q < 2; ++q) {
-                        const uint32_t d = tmem + q * N;
+                        const uint32_t d = tmem + set * 2 * N + q * N;
 #pragma unroll
                         for (int j = 0; j < 2; ++j) {
                             const uint64_t ah = tc::sdesc(a0 + (q * 2 + 0) * A_TILE + j * 256, 128, 512);
                             const uint64_t al = tc::sdesc(a0 + (q * 2 + 1) * A_TILE + j * 256, 128, 512);
                             const uint64_t bh = tc::sdesc(b0 + (q * 2 + 0) * (N * 64) + j * 256, 128, 512);
                             const uint64_t bl = tc::sdesc(b0 + (q * 2 + 1) * (N * 64) + j * 256, 128, 512);
-                            tc::mma_bf16(d, ah, bh, IDESC, (c > 0 || j > 0) ? 1u : 0u);
+                            tc::mma_bf16(d, ah, bh, IDESC, (c >= S || j > 0) ? 1u : 0u);
                             tc::mma_bf16(d, ah, bl, IDESC, 1u);
                             tc::mma_bf16(d, al, bh, IDESC, 1u);
                         }
@@ -423,7 +440,7 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
 // ------------------------------------------------------------------------------------ analysis
 constexpr int ANA_THREADS = 160;  // warps 0-2 producers (+ epilogue), 3 MMA (+ epilogue), 4 loader
 
-template <int N, bool BF16>
+template <int N, bool BF16, int S>
 __global__ void __launch_bounds__(ANA_THREADS, 1)
     anal_tc_kernel(const TcGroup *__restrict__ groups, const int4 *__restrict__ units, int nunits, float2 *alm_out,
                    int *err) {
@@ -431,7 +448,8 @@ __global__ void __launch_bounds__(ANA_THREADS, 1)
     constexpr int STAGE = A_STAGE + B_STAGE;
     constexpr uint32_t IDESC = tc::idesc_f16kind(128, N, 1, 0, BF16);
     constexpr float LS = BF16 ? 1.0f : 256.0f;
-    constexpr int TCOLS = (2 * N < 32) ? 32 : 2 * N;
+    constexpr int TCOLS = (2 * N * S < 32) ? 32 : 2 * N * S;  // S accumulator sets, see synth_tc_kernel
+    static_assert(2 * N * S <= 512, "TMEM holds 512 columns");
     extern __shared__ __align__(1024) uint8_t smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     float2 *coef = reinterpret_cast<float2 *>(smem + TC_STAGES * STAGE) + (warp & 3) * 256;
@@ -530,16 +548,17 @@ __global__ void __launch_bounds__(ANA_THREADS, 1)
                         }
                         tc::fence_after();
                         const uint32_t a0 = tc::smem_u32(smem + s * STAGE), b0 = a0 + A_STAGE;
+                        const int set = c % S;
 #pragma unroll
                         for (int q = 0; q < 2; ++q) {
-                            const uint32_t d = tmem + q * N;
+                            const uint32_t d = tmem + set * 2 * N + q * N;
 #pragma unroll
                             for (int k = 0; k < 2; ++k) {
                                 const uint64_t ah = tc::sdesc(a0 + (q * 2 + 0) * A_TILE + k * 256, 128, 512);
                                 const uint64_t al = tc::sdesc(a0 + (q * 2 + 1) * A_TILE + k * 256, 128, 512);
                                 const uint64_t bh = tc::sdesc(b0 + (q * 2 + 0) * (N * 64) + k * 256, 128, 512);
                                 const uint64_t bl = tc::sdesc(b0 + (q * 2 + 1) * (N * 64) + k * 256, 128, 512);
-                                tc::mma_bf16(d, ah, bh, IDESC, (c > 0 || k > 0) ? 1u : 0u);
+                                tc::mma_bf16(d, ah, bh, IDESC, (c >= S || k > 0) ? 1u : 0u);
                                 tc::mma_bf16(d, ah, bl, IDESC, 1u);
                                 tc::mma_bf16(d, al, bh, IDESC, 1u);
                             }
@@ -569,12 +588,24 @@ __global__ void __launch_bounds__(ANA_THREADS, 1)
             const int le = l0 + 2 * row;
             const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
             const float inv = 1.0f / (LS * G.dscale[m]);
-#pragma unroll
+            const int nsets = npc < S ? npc : S;
+#pragma unroll 1
             for (int j = 0; j < N / 16; ++j) {
                 float de[16], dd[16];
                 tc::tmem_ld16(tmem + lane_base + j * 16, de);
                 tc::tmem_ld16(tmem + lane_base + N + j * 16, dd);
                 tc::tmem_wait_ld();
+                for (int st = 1; st < nsets; ++st) {
+                    float xe[16], xd[16];
+                    tc::tmem_ld16(tmem + lane_base + st * 2 * N + j * 16, xe);
+                    tc::tmem_ld16(tmem + lane_base + st * 2 * N + N + j * 16, xd);
+                    tc::tmem_wait_ld();
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) {
+                        de[i] += xe[i];
+                        dd[i] += xd[i];
+                    }
+                }
 #pragma unroll
                 for (int h = 0; h < 8; ++h) {
                     const int b = j * 8 + h;
@@ -664,21 +695,26 @@ static int sm_count() {
     return v;
 }
 
+template <int N> constexpr int nsets() { return 512 / (2 * N) > 4 ? 4 : 512 / (2 * N); }
+
 template <int N, bool BF16>
 static int launch_syn(hb_batched_plan *bp, cudaStream_t st) {
     const int smem = syn_smem<N>();
-    HB_CUDA_TRY(cudaFuncSetAttribute(synth_tc_kernel<N, BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    constexpr int S = nsets<N>();
+    HB_CUDA_TRY(cudaFuncSetAttribute(synth_tc_kernel<N, BF16, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     const int grid = std::min(bp->n_syn, sm_count());
-    synth_tc_kernel<N, BF16><<<grid, SYN_THREADS, smem, st>>>(bp->dgroups, bp->syn_units, bp->n_syn, bp->err);
+    synth_tc_kernel<N, BF16, S><<<grid, SYN_THREADS, smem, st>>>(bp->dgroups, bp->syn_units, bp->n_syn, bp->err);
     HB_CHECK_LAUNCH();
     return HB_OK;
 }
 template <int N, bool BF16>
 static int launch_ana(hb_batched_plan *bp, float2 *alm_out, cudaStream_t st) {
     const int smem = syn_smem<N>();
-    HB_CUDA_TRY(cudaFuncSetAttribute(anal_tc_kernel<N, BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    constexpr int S = nsets<N>();
+    HB_CUDA_TRY(cudaFuncSetAttribute(anal_tc_kernel<N, BF16, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     const int grid = std::min(bp->n_ana, sm_count());
-    anal_tc_kernel<N, BF16><<<grid, ANA_THREADS, smem, st>>>(bp->dgroups, bp->ana_units, bp->n_ana, alm_out, bp->err);
+    anal_tc_kernel<N, BF16, S><<<grid, ANA_THREADS, smem, st>>>(bp->dgroups, bp->ana_units, bp->n_ana, alm_out,
+                                                                 bp->err);
     HB_CHECK_LAUNCH();
     return HB_OK;
 }
@@ -708,13 +744,14 @@ int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int np
     if (!plans || !nmaps || nplans <= 0 || !out) return fail(HB_ERR_INVALID, "hb_batched_plan_create: bad arguments");
     hb_batched_plan *bp = new hb_batched_plan();
     bp->bf16 = (flags & HB_BATCHED_BF16) != 0;
+    const int GM = (flags & HB_BATCHED_WIDE) ? 64 : 32;  // maps per group (MMA N = 2 GM)
     int maxg = 0;
     for (int i = 0; i < nplans; ++i) {
         if (!plans[i] || !plans[i]->ck || nmaps[i] <= 0) {
             delete bp;
             return fail(HB_ERR_INVALID, "hb_batched_plan_create: every plan needs HB_PLAN_FP32 and nmaps > 0");
         }
-        maxg = std::max(maxg, std::min(nmaps[i], 64));
+        maxg = std::max(maxg, std::min(nmaps[i], GM));
     }
     bp->N = (2 * maxg <= 32) ? 32 : (2 * maxg <= 64 ? 64 : 128);
     const int N = bp->N;
@@ -734,7 +771,7 @@ int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int np
         to[0] = 0;
         for (int m = 0; m <= p->mmax; ++m) to[m + 1] = to[m] + (p->lmax - m + 64) / 64;
         chunks_a[i] = to[p->mmax + 1];
-        const int ng = (nmaps[i] + 63) / 64;
+        const int ng = (nmaps[i] + GM - 1) / GM;
         offs[i].gf = carve((size_t)nmaps[i] * (p->mmax + 1) * np * 2 * sizeof(float2));
         offs[i].tofs = carve(8 * (size_t)(p->mmax + 2));
         offs[i].tiles_a = carve((size_t)ng * chunks_a[i] * 256 * N);
@@ -755,20 +792,20 @@ int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int np
     // groups of <= 64 maps
     for (int i = 0; i < nplans; ++i) {
         const hb_plan *p = plans[i];
-        const int ng = (nmaps[i] + 63) / 64;
+        const int ng = (nmaps[i] + GM - 1) / GM;
         for (int k = 0; k < ng; ++k) {
             TcGroup G{};
             G.g = p->g->d;
             G.lmax = p->lmax;
             G.mmax = p->mmax;
-            G.nmaps = std::min(64, nmaps[i] - 64 * k);
+            G.nmaps = std::min(GM, nmaps[i] - GM * k);
             G.npb = (p->g->d.npairs + 127) / 128;
             G.npc = (p->g->d.npairs + 31) / 32;
             G.ck = p->ck;
             G.blk_ofs = p->blk_ofs;
             bp->hgroups.push_back(G);
             bp->group_part.push_back(i);
-            bp->group_first_map.push_back(64 * k);
+            bp->group_first_map.push_back(GM * k);
         }
     }
     const int ngroups = (int)bp->hgroups.size();
@@ -811,18 +848,18 @@ int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int np
         int gi = 0;
         for (int i = 0; i < nplans; ++i) {
             const hb_plan *p = plans[i];
-            const int ng = (nmaps[i] + 63) / 64;
+            const int ng = (nmaps[i] + GM - 1) / GM;
             for (int k = 0; k < ng; ++k, ++gi) {
                 TcGroup &G = bp->hgroups[gi];
                 G.alm_tiles = (const uint4 *)(base + offs[i].tiles_a) + (size_t)k * chunks_a[i] * 16 * N;
                 G.alm_tile_ofs = bp->parts[i].tile_ofs;
-                G.Gm = bp->parts[i].GF + (int64_t)64 * k * bp->parts[i].gf_stride;
+                G.Gm = bp->parts[i].GF + (int64_t)GM * k * bp->parts[i].gf_stride;
                 G.gm_stride = bp->parts[i].gf_stride;
                 G.g_tiles = (const uint4 *)(base + offs[i].tiles_g) +
                             (size_t)k * (p->mmax + 1) * G.npc * 16 * N;
                 G.dscale = (float *)(base + offs[i].scales) + (size_t)k * (p->mmax + 1);
                 G.alm_stride = alm_size(p->lmax, p->mmax);
-                G.alm_out_ofs = bp->parts[i].alm_ofs + (int64_t)64 * k * G.alm_stride;
+                G.alm_out_ofs = bp->parts[i].alm_ofs + (int64_t)GM * k * G.alm_stride;
             }
         }
     }

@@ -172,7 +172,7 @@ HB_API int hb_alm2cl_f32(int lmax, int mmax, int nmaps, const float *alm1, const
 HB_API int hb_alm2cl_f64(int lmax, int mmax, int nmaps, const double *alm1, const double *alm2, double *cl,
                   hb_stream_t stream);
 
-/* Batched split-precision transforms on the tcgen05 tensor cores (FP32 data, BF16 hi+lo
+/* Batched split-precision transforms on the tcgen05 tensor cores (FP32 data, 16-bit hi+lo
  * three-pass products, FP32 accumulation in TMEM).  One batched plan covers nplans plans (each a
  * geometry + lmax, made with HB_PLAN_FP32) with nmaps[i] maps each; all maps of all plans run
  * in one persistent launch per direction, driven by a (plan, m, ring-block or l-block) work list
@@ -185,9 +185,14 @@ HB_API int hb_alm2cl_f64(int lmax, int mmax, int nmaps, const double *alm1, cons
 typedef struct hb_batched_plan hb_batched_plan;
 /* flags: HB_BATCHED_BF16 splits into BF16 hi+lo (8-bit significands) instead of the default
  * IEEE-half hi+lo with exact power-of-two per-m scaling (11-bit significands); both run at the
- * same tcgen05 kind::f16 rate.  Measured at nside 2048, lmax 4095 the BF16 split leaves 2.1e-5
- * relative error on a map2alm+alm2map pair, the half split stays within 1e-5. */
-enum { HB_BATCHED_BF16 = 1 };
+ * same tcgen05 kind::f16 rate.
+ * The maps run in groups of 32 (MMA N = 64) with four TMEM accumulator sets per output tile,
+ * chunk c of the l (or ring-pair) contraction accumulating into set c mod 4, the sets summed in
+ * FP32 at the end: the tensor core's FP32 accumulation error grows with the number of
+ * accumulate steps into one set.  HB_BATCHED_WIDE uses groups of 64 (N = 128) with two sets:
+ * one recursion pass serves twice as many maps, at about twice the accumulation error.
+ * Measured relative error of a map2alm+alm2map pair against FP64 at nside 2048, lmax 4095:
+ * default 7.3e-6, BF16 8.3e-6, WIDE 1.2e-5 (one set: 2.3e-5). */
 HB_API int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int nplans, int flags,
                                   hb_batched_plan **out);
 HB_API int hb_batched_plan_destroy(hb_batched_plan *bp);
