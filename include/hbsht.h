@@ -193,6 +193,7 @@ typedef struct hb_batched_plan hb_batched_plan;
  * one recursion pass serves twice as many maps, at about twice the accumulation error.
  * Measured relative error of a map2alm+alm2map pair against FP64 at nside 2048, lmax 4095:
  * default 7.3e-6, BF16 8.3e-6, WIDE 1.2e-5 (one set: 2.3e-5). */
+enum { HB_BATCHED_BF16 = 1, HB_BATCHED_WIDE = 2 };
 HB_API int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int nplans, int flags,
                                   hb_batched_plan **out);
 HB_API int hb_batched_plan_destroy(hb_batched_plan *bp);
