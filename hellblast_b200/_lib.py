@@ -74,6 +74,7 @@ for _p in ("f32", "f64"):
     SIGNATURES[f"hb_alm2map_spin2_{_p}"] = (i32, [vp, i32, vp, vp, vp, vp, vp, sz, i32, vp])
     SIGNATURES[f"hb_alm2map_spin2_adjoint_{_p}"] = (i32, [vp, i32, vp, vp, vp, vp, vp, sz, i32, vp])
     SIGNATURES[f"hb_map2alm_spin2_adjoint_{_p}"] = (i32, [vp, i32, vp, vp, vp, vp, vp, vp, sz, i32, vp])
+SIGNATURES["hb_map2alm_f32_noalloc"] = (i32, [vp, i32, vp, vp, vp, i32, vp])
 
 HB_PLAN_FP32 = 1
 HB_PLAN_SPIN2_FP32 = 2

@@ -28,6 +28,8 @@
  *   hb_map2alm_adjoint_*, hb_alm2map_adjoint_*, hb_*_spin2_adjoint_*
  *                             no reference counterpart (the reference has no gradients);
  *                             exact transposes used by the autograd wrappers
+ *   hb_map2alm_f32_noalloc    no reference counterpart: hb_map2alm_f32 with a static scratch
+ *                             for callers that cannot allocate or pass a workspace
  */
 #ifndef HBSHT_H
 #define HBSHT_H
@@ -119,6 +121,21 @@ HB_API int hb_map2alm_f32(const hb_plan *p, int nmaps, const float *maps, const 
                           void *ws, size_t ws_bytes, int flags, hb_stream_t stream);
 HB_API int hb_map2alm_f64(const hb_plan *p, int nmaps, const double *maps, const double *weights, double *alm,
                           void *ws, size_t ws_bytes, int flags, hb_stream_t stream);
+/* hb_map2alm_f32 without a workspace and without allocating: its F(m, ring pair) scratch is a
+ * fixed static device array of HB_NOALLOC_SCRATCH_BYTES that every GPU loading this library
+ * holds until the process exits.  For callers that may not allocate device memory per call
+ * and have no way to pass a workspace (an allocator owned by the host runtime, a plugin ABI
+ * without a workspace argument).  No counterpart in the reference.
+ * - Calls needing more than the scratch (nmaps * (mmax+1) * npairs * 16 bytes; 64 MiB holds
+ *   one map at nside 1024, lmax 2047) return HB_ERR_INVALID.
+ * - The first call with a given device current looks up the array's device address (and may
+ *   load the module onto that device); make that first call before any stream capture.
+ * - All calls share the one array per device: calls that overlap in time on the same device
+ *   (two streams, two threads) race on it and give wrong results.  Each call overwrites every
+ *   scratch entry it reads, so the leftover contents of an earlier call do not matter. */
+#define HB_NOALLOC_SCRATCH_BYTES (64u << 20)
+HB_API int hb_map2alm_f32_noalloc(const hb_plan *p, int nmaps, const float *maps, const double *weights,
+                                  float *alm, int flags, hb_stream_t stream);
 
 /* alm2map: f(pix) = sum_lm a_lm Y_lm(pix) (real field: m>0 counted twice). */
 HB_API int hb_alm2map_f32(const hb_plan *p, int nmaps, const float *alm, float *maps, void *ws, size_t ws_bytes,
