@@ -30,7 +30,6 @@
 namespace hb {
 
 constexpr uint64_t HB_TC_WAIT_NS = 2000000000ull;  // 2 s
-constexpr int TC_STAGES = 3;
 constexpr int A_TILE = 8192;       // 128 rows x 32 K x bf16
 constexpr int A_STAGE = 4 * A_TILE;  // [parity][hi/lo]
 
@@ -41,6 +40,8 @@ struct TcGroup {
     int64_t npc;             // chunks of 32 pairs (analysis)
     const float4 *ck;        // plan checkpoints
     const int64_t *blk_ofs;
+    const float4 *ckh;       // checkpoints at l0 + 128 of every block (same indexing as ck)
+    const float2 *coef;      // recursion coefficients (A_l, B_l): [(blk_ofs[m] + b) * 256 + i], l = m + 256 b + i
     // synthesis
     const uint4 *alm_tiles;  // [chunk][4][N x 32] bf16, chunk = tile_ofs[m] + c
     const int64_t *alm_tile_ofs;
@@ -179,8 +180,14 @@ __global__ void prep_g_tiles_kernel(const TcGroup *groups, int gi, const float2 
 struct Rec {
     float l1, l2, xh, xl;
     int e;
+    // lambda_l = A x lambda_{l-1} + B lambda_{l-2}.  A x is formed off the dependency chain as an
+    // unevaluated sum ah + al (ah = fl(A xh), al = exact remainder + A xl): a single rounded A x
+    // would carry nearly the same relative error at every l (A_l -> 2 slowly), i.e. a systematic
+    // shift of x, which the hi + lo x exists to avoid.  The chain is two FMAs per step.
     __device__ __forceinline__ float step(float A, float B) {
-        float v = A * fmaf(xh, l1, xl * l1) + B * l2;
+        const float ah = A * xh;
+        const float al = fmaf(A, xl, fmaf(A, xh, -ah));
+        const float v = fmaf(ah, l1, fmaf(al, l1, B * l2));
         l2 = l1;
         l1 = v;
         return v;
@@ -193,12 +200,32 @@ struct Rec {
         }
     }
     __device__ __forceinline__ float val(float v) const { return e == 0 ? v : 0.f; }
-    __device__ __forceinline__ void load(float4 c) {
-        l1 = c.x;
-        l2 = c.y;
+    // checkpoint state, values multiplied by the operand scale ls (a power of two)
+    __device__ __forceinline__ void load(float4 c, float ls) {
+        l1 = c.x * ls;
+        l2 = c.y * ls;
         e = __float_as_int(c.z);
     }
 };
+
+// 8 even-parity and 8 odd-parity values l0+2t, l0+2t+1 (t < 8) from the coefficients cf[0..15].
+// CHECKED: some row of the warp still carries a negative exponent, so values are gated and the
+// state rescaled; otherwise (all rows at e == 0, the common case) neither is needed.
+template <bool CHECKED>
+__device__ __forceinline__ void gen16(Rec &R, const float2 *cf, float (&ev)[8], float (&od)[8]) {
+    const float4 *c4 = reinterpret_cast<const float4 *>(cf);
+#pragma unroll
+    for (int t = 0; t < 8; ++t) {
+        const float4 c = c4[t];
+        ev[t] = R.step(c.x, c.y);
+        if (CHECKED) ev[t] = R.val(ev[t]);
+        od[t] = R.step(c.z, c.w);
+        if (CHECKED) {
+            od[t] = R.val(od[t]);
+            if (t & 1) R.check();
+        }
+    }
+}
 
 __device__ __forceinline__ void coef_scalar(int l, int m, int lmax, float2 &out) {
     double A = 0.0, B = 0.0;
@@ -212,13 +239,120 @@ __device__ __forceinline__ void coef_scalar(int l, int m, int lmax, float2 &out)
     out = make_float2((float)A, (float)B);
 }
 
-// ------------------------------------------------------------------------------------ synthesis
-constexpr int SYN_THREADS = 192;  // warps 0-3 producers/epilogue, 4 MMA, 5 loader
+// (A_l, B_l) of every (m, l), in the plan's 256-l block layout, zero past lmax; one CTA per m.
+__global__ void coef_table_kernel(int lmax, const int64_t *__restrict__ blk_ofs, float2 *__restrict__ tab) {
+    const int m = blockIdx.x;
+    const int64_t b0 = blk_ofs[m], nb = blk_ofs[m + 1] - b0;
+    for (int64_t i = threadIdx.x; i < nb * 256; i += blockDim.x) coef_scalar(m + (int)i, m, lmax, tab[b0 * 256 + i]);
+}
 
+// ------------------------------------------------------------------------------------ pipeline
+// Both kernels: warps 0-7 produce A tiles (recursion, one ring pair per thread) and run the
+// epilogue (TMEM lane quarter = warp % 4, columns split between warps w and w + 4); warp 8
+// allocates TMEM and one of its threads issues the MMAs; one thread of warp 9 streams the
+// pre-split batch tiles with bulk copies.  Two producer warps per SM sub-partition hide the
+// recursion's dependency latency.  The recursion restarts from the plan's FP64 checkpoints at
+// every 128 l (block starts and the mid-block table), which is what lets two warps share one
+// row's l range.
+constexpr int TC_THREADS = 320;
+constexpr int TC_PRODUCERS = 256;
+template <int N> constexpr int tc_b_stage() { return 4 * N * 64; }  // [q][h][N x 32] 16-bit
+template <int N> constexpr int syn_stages() { return N >= 128 ? 2 : 4; }  // two rings
+template <int N> constexpr int ana_stages() { return N >= 128 ? 3 : 4; }
+template <int ST, int N> constexpr int tc_smem() { return ST * (A_STAGE + tc_b_stage<N>()) + 8 * 128 * 8 + 128; }
+
+struct TcSmem {
+    float2 *coef;  // this producer warp's 128 recursion coefficients
+    uint64_t *full, *empty, *accum, *tfree, *drain;
+    uint32_t *tmem_slot;
+};
+template <int ST, int N>
+__device__ __forceinline__ TcSmem tc_smem_layout(uint8_t *smem, int warp) {
+    constexpr int STAGE = A_STAGE + tc_b_stage<N>();
+    TcSmem L;
+    L.coef = reinterpret_cast<float2 *>(smem + ST * STAGE) + (warp & 7) * 128;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + ST * STAGE + 8 * 128 * sizeof(float2));
+    L.full = bars;
+    L.empty = bars + ST;
+    L.accum = bars + 2 * ST;
+    L.tfree = L.accum + 1;
+    L.drain = L.tfree + 1;
+    L.tmem_slot = reinterpret_cast<uint32_t *>(L.drain + 1);
+    return L;
+}
+
+template <int ST>
+__device__ __forceinline__ void tc_init_barriers(const TcSmem &L, int full_count) {
+    for (int s = 0; s < ST; ++s) {
+        tc::mbar_init(&L.full[s], full_count);
+        tc::mbar_init(&L.empty[s], 1);
+    }
+    tc::mbar_init(L.accum, 1);
+    tc::mbar_init(L.tfree, TC_PRODUCERS);
+    tc::mbar_init(L.drain, 1);
+    tc::fence_mbar_init();
+}
+
+// write 8 even + 8 odd split values of one A-tile row group: A + {0,1,2,3} * A_TILE + off
+template <bool BF16>
+__device__ __forceinline__ void store_split(uint8_t *A, int off, const float (&ev)[8], const float (&od)[8]) {
+    uint4 hi, lo;
+    tc::split8<BF16>(ev, hi, lo);
+    *reinterpret_cast<uint4 *>(A + 0 * A_TILE + off) = hi;
+    *reinterpret_cast<uint4 *>(A + 1 * A_TILE + off) = lo;
+    tc::split8<BF16>(od, hi, lo);
+    *reinterpret_cast<uint4 *>(A + 2 * A_TILE + off) = hi;
+    *reinterpret_cast<uint4 *>(A + 3 * A_TILE + off) = lo;
+}
+
+// the 12 MMAs of one stage (2 parities x 2 K-steps x 3 split passes) into accumulator set `set`
+template <int N>
+__device__ __forceinline__ void issue_stage(uint32_t tmem, uint32_t a0, int set, bool first, uint32_t idesc) {
+    const uint32_t b0 = a0 + A_STAGE;
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const uint32_t d = tmem + set * 2 * N + q * N;
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            const uint64_t ah = tc::sdesc(a0 + (q * 2 + 0) * A_TILE + k * 256, 128, 512);
+            const uint64_t al = tc::sdesc(a0 + (q * 2 + 1) * A_TILE + k * 256, 128, 512);
+            const uint64_t bh = tc::sdesc(b0 + (q * 2 + 0) * (N * 64) + k * 256, 128, 512);
+            const uint64_t bl = tc::sdesc(b0 + (q * 2 + 1) * (N * 64) + k * 256, 128, 512);
+            tc::mma_bf16(d, ah, bh, idesc, (!first || k > 0) ? 1u : 0u);
+            tc::mma_bf16(d, ah, bl, idesc, 1u);
+            tc::mma_bf16(d, al, bh, idesc, 1u);
+        }
+    }
+}
+
+// epilogue helper: columns [16j, 16j+16) of both parities, summed over the nsets accumulator sets
+template <int N>
+__device__ __forceinline__ void load_sets(uint32_t taddr, int j, int nsets, float (&de)[16], float (&dd)[16]) {
+    tc::tmem_ld16(taddr + j * 16, de);
+    tc::tmem_ld16(taddr + N + j * 16, dd);
+    tc::tmem_wait_ld();
+    for (int st = 1; st < nsets; ++st) {
+        float xe[16], xd[16];
+        tc::tmem_ld16(taddr + st * 2 * N + j * 16, xe);
+        tc::tmem_ld16(taddr + st * 2 * N + N + j * 16, xd);
+        tc::tmem_wait_ld();
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            de[i] += xe[i];
+            dd[i] += xd[i];
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------------ synthesis
+// Chunk c (64 l) of a unit belongs to half-block hb = c / 2 (128 l); half-blocks alternate
+// between the two producer warp groups (g = hb % 2), each with its own ring of SPR stages.  The
+// MMA thread and the loader walk the chunks in order, taking chunk c from ring (c / 2) % 2.
 template <int N, bool BF16, int S>
-__global__ void __launch_bounds__(SYN_THREADS, 1)
+__global__ void __launch_bounds__(TC_THREADS, 1)
     synth_tc_kernel(const TcGroup *__restrict__ groups, const int4 *__restrict__ units, int nunits, int *err) {
-    constexpr int B_STAGE = 4 * N * 64;  // [q][h][N x 32] 16-bit
+    constexpr int ST = syn_stages<N>(), SPR = ST / 2;
+    constexpr int B_STAGE = tc_b_stage<N>();
     constexpr int STAGE = A_STAGE + B_STAGE;
     constexpr uint32_t IDESC = tc::idesc_f16kind(128, N, 0, 0, BF16);
     constexpr float LS = BF16 ? 1.0f : 256.0f;  // lambda scale (|lambda| < 2^7 -> < 2^15 in half)
@@ -229,37 +363,24 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
     static_assert(2 * N * S <= 512, "TMEM holds 512 columns");
     extern __shared__ __align__(1024) uint8_t smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    // one private copy of the 256 recursion coefficients per producer warp (no cross-warp barrier)
-    float2 *coef = reinterpret_cast<float2 *>(smem + TC_STAGES * STAGE) + (warp & 3) * 256;
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + TC_STAGES * STAGE + 4 * 256 * sizeof(float2));
-    uint64_t *full = bars, *empty = bars + TC_STAGES, *accum = bars + 2 * TC_STAGES, *tfree = accum + 1;
-    uint64_t *drain = tfree + 1;
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+    const TcSmem L = tc_smem_layout<ST, N>(smem, warp);
 
-    if (threadIdx.x == 0) {
-        for (int s = 0; s < TC_STAGES; ++s) {
-            tc::mbar_init(&full[s], 128 + 1);
-            tc::mbar_init(&empty[s], 1);
-        }
-        tc::mbar_init(accum, 1);
-        tc::mbar_init(tfree, 128);
-        tc::mbar_init(drain, 1);
-        tc::fence_mbar_init();
-    }
-    if (warp == 4) {
-        tc::tmem_alloc(tmem_slot, TCOLS);
+    if (threadIdx.x == 0) tc_init_barriers<ST>(L, 128 + 1);
+    if (warp == 8) {
+        tc::tmem_alloc(L.tmem_slot, TCOLS);
         tc::tmem_relinquish();
     }
     tc::fence_before();
     __syncthreads();
     tc::fence_after();
-    const uint32_t tmem = *tmem_slot;
+    const uint32_t tmem = *L.tmem_slot;
     bool ok = true;
 
-    if (warp < 4) {
+    if (warp < 8) {
         // ---------------- producers + epilogue
-        const int r = threadIdx.x;  // row = pair within the block
-        uint32_t it = 0;
+        const int wg = warp >> 2;                   // half-blocks hb with hb % 2 == wg
+        const int r = ((warp & 3) << 5) | lane;     // row = pair within the block
+        uint32_t itr = 0;                           // chunks of this warp group's ring so far
         int ui = 0;
         for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++ui) {
             const int4 U = units[u];
@@ -270,74 +391,63 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
             Rec R;
             R.xh = live ? G.g.pair_xhi[p] : 0.f;
             R.xl = live ? G.g.pair_xlo[p] : 0.f;
-            R.load(live ? G.ck[G.blk_ofs[m] * np + p] : make_float4(0.f, 0.f, 0.f, 0.f));
-            const int nch = (lmax - m + 64) / 64;
-            for (int c = 0; c < nch && ok; ++c, ++it) {
-                const int l0 = m + 64 * c;
-                if ((c & 3) == 0) {
-                    __syncwarp();
-                    for (int i = lane; i < 256; i += 32) coef_scalar(l0 + i, m, lmax, coef[i]);
-                    __syncwarp();
-                    if (c > 0 && live) R.load(G.ck[(G.blk_ofs[m] + c / 4) * np + p]);
-                }
-                const int s = it % TC_STAGES;
-                if (it >= TC_STAGES && !warp_wait(&empty[s], ((it / TC_STAGES) + 1) & 1)) {
-                    if (lane == 0) set_err(err, 1);
-                    ok = false;
-                    break;
-                }
-                uint8_t *A = smem + s * STAGE;
-                const float2 *cf = coef + (c & 3) * 64;
+            const int nch = (lmax - m + 64) / 64, nhb = (nch + 1) / 2;
+            const int64_t b0 = G.blk_ofs[m];
+            // the next half-block's coefficients and checkpoint are fetched one half-block ahead
+            float2 cpre[4];
+            float4 kpre = make_float4(0.f, 0.f, 0.f, 0.f);
+            auto fetch = [&](int hb) {
+                const int64_t blk = b0 + (hb >> 1);
 #pragma unroll
-                for (int grp = 0; grp < 4; ++grp) {
-                    float ev[8], od[8];
+                for (int i = 0; i < 4; ++i) cpre[i] = G.coef[blk * 256 + (hb & 1) * 128 + lane + 32 * i];
+                kpre = live ? ((hb & 1) ? G.ckh : G.ck)[blk * np + p] : make_float4(0.f, 0.f, 0.f, 0.f);
+            };
+            if (wg < nhb) fetch(wg);
+            for (int hb = wg; hb < nhb && ok; hb += 2) {
+                __syncwarp();
 #pragma unroll
-                    for (int t = 0; t < 8; ++t) {
-                        const float2 ce = cf[16 * grp + 2 * t], co = cf[16 * grp + 2 * t + 1];
-                        ev[t] = R.val(R.step(ce.x, ce.y));
-                        od[t] = R.val(R.step(co.x, co.y));
-                        if (t & 1) R.check();
+                for (int i = 0; i < 4; ++i) L.coef[lane + 32 * i] = cpre[i];
+                __syncwarp();
+                R.load(kpre, LS);
+                const bool fast = __all_sync(0xffffffffu, R.e == 0);
+                if (hb + 2 < nhb) fetch(hb + 2);
+                for (int cc = 0; cc < 2 && 2 * hb + cc < nch; ++cc, ++itr) {
+                    const int s = wg * SPR + (int)(itr % SPR);
+                    if (itr >= SPR && !warp_wait(&L.empty[s], ((itr / SPR) + 1) & 1)) {
+                        if (lane == 0) set_err(err, 1);
+                        ok = false;
+                        break;
                     }
-                    uint4 hi, lo;
-                    const int off = (r & 7) * 16 + (r >> 3) * 512 + grp * 128;
-                    tc::split8<BF16>(ev, LS, hi, lo);
-                    *reinterpret_cast<uint4 *>(A + 0 * A_TILE + off) = hi;
-                    *reinterpret_cast<uint4 *>(A + 1 * A_TILE + off) = lo;
-                    tc::split8<BF16>(od, LS, hi, lo);
-                    *reinterpret_cast<uint4 *>(A + 2 * A_TILE + off) = hi;
-                    *reinterpret_cast<uint4 *>(A + 3 * A_TILE + off) = lo;
+                    uint8_t *A = smem + s * STAGE;
+                    const float2 *cf = L.coef + cc * 64;
+#pragma unroll
+                    for (int grp = 0; grp < 4; ++grp) {
+                        float ev[8], od[8];
+                        if (fast)
+                            gen16<false>(R, cf + 16 * grp, ev, od);
+                        else
+                            gen16<true>(R, cf + 16 * grp, ev, od);
+                        store_split<BF16>(A, (r & 7) * 16 + (r >> 3) * 512 + grp * 128, ev, od);
+                    }
+                    tc::fence_proxy_async_smem();
+                    tc::mbar_arrive(&L.full[s]);
                 }
-                tc::fence_proxy_async_smem();
-                tc::mbar_arrive(&full[s]);
             }
             if (!ok) break;
-            // epilogue
-            if (!warp_wait(accum, ui & 1)) {
+            // epilogue: this warp's lane quarter, column blocks j with j % 2 == wg
+            if (!warp_wait(L.accum, ui & 1)) {
                 if (lane == 0) set_err(err, 2);
                 ok = false;
                 break;
             }
             tc::fence_after();
-            const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+            const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
             const float inv = 1.0f / (LS * G.dscale[m]);
             const int nsets = nch < S ? nch : S;
 #pragma unroll 1
-            for (int j = 0; j < N / 16; ++j) {
+            for (int j = wg; j < N / 16; j += 2) {
                 float de[16], dd[16];
-                tc::tmem_ld16(tmem + lane_base + j * 16, de);
-                tc::tmem_ld16(tmem + lane_base + N + j * 16, dd);
-                tc::tmem_wait_ld();
-                for (int st = 1; st < nsets; ++st) {
-                    float xe[16], xd[16];
-                    tc::tmem_ld16(tmem + lane_base + st * 2 * N + j * 16, xe);
-                    tc::tmem_ld16(tmem + lane_base + st * 2 * N + N + j * 16, xd);
-                    tc::tmem_wait_ld();
-#pragma unroll
-                    for (int i = 0; i < 16; ++i) {
-                        de[i] += xe[i];
-                        dd[i] += xd[i];
-                    }
-                }
+                load_sets<N>(taddr, j, nsets, de, dd);
                 if (live) {
 #pragma unroll
                     for (int h = 0; h < 8; ++h) {
@@ -352,78 +462,67 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
                 }
             }
             tc::fence_before();
-            tc::mbar_arrive(tfree);
+            tc::mbar_arrive(L.tfree);
         }
-    } else if (warp == 4) {
+    } else if (warp == 8) {
         // ---------------- MMA issuer
         if (lane == 0) {
-            uint32_t it = 0;
+            uint32_t itr0 = 0, itr1 = 0;  // per-ring chunk counters
             int ui = 0;
             for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++ui) {
                 const int4 U = units[u];
-                const TcGroup &G = groups[U.x];
-                const int m = U.y;
-                const int nch = (G.lmax - m + 64) / 64;
-                if (ui > 0 && !tc::mbar_wait(tfree, (ui - 1) & 1, HB_TC_WAIT_NS)) {
+                const int nch = (groups[U.x].lmax - U.y + 64) / 64;
+                if (ui > 0 && !tc::mbar_wait(L.tfree, (ui - 1) & 1, HB_TC_WAIT_NS)) {
                     set_err(err, 3);
                     ok = false;
                     break;
                 }
                 tc::fence_after();
-                for (int c = 0; c < nch; ++c, ++it) {
-                    const int s = it % TC_STAGES;
-                    if (!tc::mbar_wait(&full[s], (it / TC_STAGES) & 1, HB_TC_WAIT_NS)) {
+                for (int c = 0; c < nch; ++c) {
+                    const int g = (c >> 1) & 1;
+                    uint32_t &itr = g ? itr1 : itr0;
+                    const int s = g * SPR + (int)(itr % SPR);
+                    if (!tc::mbar_wait(&L.full[s], (itr / SPR) & 1, HB_TC_WAIT_NS)) {
                         set_err(err, 4);
                         ok = false;
                         break;
                     }
+                    ++itr;
                     tc::fence_after();
-                    const uint32_t a0 = tc::smem_u32(smem + s * STAGE), b0 = a0 + A_STAGE;
-                    const int set = c % S;
-#pragma unroll
-                    for (int q = 0; q < 2; ++q) {
-                        const uint32_t d = tmem + set * 2 * N + q * N;
-#pragma unroll
-                        for (int j = 0; j < 2; ++j) {
-                            const uint64_t ah = tc::sdesc(a0 + (q * 2 + 0) * A_TILE + j * 256, 128, 512);
-                            const uint64_t al = tc::sdesc(a0 + (q * 2 + 1) * A_TILE + j * 256, 128, 512);
-                            const uint64_t bh = tc::sdesc(b0 + (q * 2 + 0) * (N * 64) + j * 256, 128, 512);
-                            const uint64_t bl = tc::sdesc(b0 + (q * 2 + 1) * (N * 64) + j * 256, 128, 512);
-                            tc::mma_bf16(d, ah, bh, IDESC, (c >= S || j > 0) ? 1u : 0u);
-                            tc::mma_bf16(d, ah, bl, IDESC, 1u);
-                            tc::mma_bf16(d, al, bh, IDESC, 1u);
-                        }
-                    }
-                    tc::mma_commit(&empty[s]);
+                    issue_stage<N>(tmem, tc::smem_u32(smem + s * STAGE), c % S, c < S, IDESC);
+                    tc::mma_commit(&L.empty[s]);
                 }
                 if (!ok) break;
-                tc::mma_commit(accum);
+                tc::mma_commit(L.accum);
             }
             if (!ok) {  // let issued MMAs finish before the tensor memory is released
-                tc::mma_commit(drain);
-                tc::mbar_wait(drain, 0, HB_TC_WAIT_NS);
+                tc::mma_commit(L.drain);
+                tc::mbar_wait(L.drain, 0, HB_TC_WAIT_NS);
             }
         }
         __syncwarp();
     } else {
         // ---------------- loader of the pre-split alm tiles
         if (lane == 0) {
-            uint32_t it = 0;
+            uint32_t itr0 = 0, itr1 = 0;  // per-ring chunk counters
             for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
                 const int4 U = units[u];
                 const TcGroup &G = groups[U.x];
                 const int m = U.y;
                 const int nch = (G.lmax - m + 64) / 64;
                 const uint4 *src = G.alm_tiles + G.alm_tile_ofs[m] * (16 * N);
-                for (int c = 0; c < nch; ++c, ++it) {
-                    const int s = it % TC_STAGES;
-                    if (it >= TC_STAGES && !tc::mbar_wait(&empty[s], ((it / TC_STAGES) + 1) & 1, HB_TC_WAIT_NS)) {
+                for (int c = 0; c < nch; ++c) {
+                    const int g = (c >> 1) & 1;
+                    uint32_t &itr = g ? itr1 : itr0;
+                    const int s = g * SPR + (int)(itr % SPR);
+                    if (itr >= SPR && !tc::mbar_wait(&L.empty[s], ((itr / SPR) + 1) & 1, HB_TC_WAIT_NS)) {
                         set_err(err, 5);
                         ok = false;
                         break;
                     }
-                    tc::mbar_arrive_expect_tx(&full[s], B_STAGE);
-                    tc::bulk_g2s(smem + s * STAGE + A_STAGE, src + (int64_t)c * (16 * N), B_STAGE, &full[s]);
+                    ++itr;
+                    tc::mbar_arrive_expect_tx(&L.full[s], B_STAGE);
+                    tc::bulk_g2s(smem + s * STAGE + A_STAGE, src + (int64_t)c * (16 * N), B_STAGE, &L.full[s]);
                 }
             }
         }
@@ -431,20 +530,22 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
     }
     tc::fence_before();
     __syncthreads();
-    if (warp == 4) {
+    if (warp == 8) {
         tc::fence_after();
         tc::tmem_dealloc(tmem, TCOLS);
     }
 }
 
 // ------------------------------------------------------------------------------------ analysis
-constexpr int ANA_THREADS = 160;  // warps 0-2 producers (+ epilogue), 3 MMA (+ epilogue), 4 loader
-
+// Chunk c (32 ring pairs) of a unit goes to stage c' % ST (c' = running chunk count); the two
+// warps w, w + 4 with w == c' % ST fill it, warp w the rows of l0 .. l0+127, warp w + 4 those of
+// l0+128 .. l0+255 (restarting from the mid-block checkpoint).
 template <int N, bool BF16, int S>
-__global__ void __launch_bounds__(ANA_THREADS, 1)
+__global__ void __launch_bounds__(TC_THREADS, 1)
     anal_tc_kernel(const TcGroup *__restrict__ groups, const int4 *__restrict__ units, int nunits, float2 *alm_out,
                    int *err) {
-    constexpr int B_STAGE = 4 * N * 64;
+    constexpr int ST = ana_stages<N>();
+    constexpr int B_STAGE = tc_b_stage<N>();
     constexpr int STAGE = A_STAGE + B_STAGE;
     constexpr uint32_t IDESC = tc::idesc_f16kind(128, N, 1, 0, BF16);
     constexpr float LS = BF16 ? 1.0f : 256.0f;
@@ -452,160 +553,98 @@ __global__ void __launch_bounds__(ANA_THREADS, 1)
     static_assert(2 * N * S <= 512, "TMEM holds 512 columns");
     extern __shared__ __align__(1024) uint8_t smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    float2 *coef = reinterpret_cast<float2 *>(smem + TC_STAGES * STAGE) + (warp & 3) * 256;
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + TC_STAGES * STAGE + 4 * 256 * sizeof(float2));
-    uint64_t *full = bars, *empty = bars + TC_STAGES, *accum = bars + 2 * TC_STAGES, *tfree = accum + 1;
-    uint64_t *drain = tfree + 1;
-    uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(drain + 1);
+    const TcSmem L = tc_smem_layout<ST, N>(smem, warp);
 
-    if (threadIdx.x == 0) {
-        for (int s = 0; s < TC_STAGES; ++s) {
-            tc::mbar_init(&full[s], 32 + 1);
-            tc::mbar_init(&empty[s], 1);
-        }
-        tc::mbar_init(accum, 1);
-        tc::mbar_init(tfree, 128);
-        tc::mbar_init(drain, 1);
-        tc::fence_mbar_init();
-    }
-    if (warp == 3) {
-        tc::tmem_alloc(tmem_slot, TCOLS);
+    if (threadIdx.x == 0) tc_init_barriers<ST>(L, 64 + 1);
+    if (warp == 8) {
+        tc::tmem_alloc(L.tmem_slot, TCOLS);
         tc::tmem_relinquish();
     }
     tc::fence_before();
     __syncthreads();
     tc::fence_after();
-    const uint32_t tmem = *tmem_slot;
+    const uint32_t tmem = *L.tmem_slot;
     bool ok = true;
 
-    if (warp < 4) {
-        uint32_t it = 0;  // running chunk counter: stage = it % 3, phase = it / 3
+    if (warp < 8) {
+        // ---------------- producers + epilogue
+        const int owner = warp & 3, half = warp >> 2;
+        uint32_t it = 0;
         int ui = 0;
         for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++ui) {
             const int4 U = units[u];
             const TcGroup &G = groups[U.x];
             const int m = U.y, jb = U.z, lmax = G.lmax;
             const int l0 = m + 256 * jb;
+            const bool active = l0 + 128 * half <= lmax;  // this half of the block has rows <= lmax
             const int64_t np = G.g.npairs;
             const int npc = (int)G.npc;
-            if (warp < 3) {
-                // ---------------- producers: warp w fills the chunks with it % 3 == w
-                __syncwarp();
-                for (int i = lane; i < 256; i += 32) coef_scalar(l0 + i, m, lmax, coef[i]);
-                __syncwarp();
-                for (int c = 0; c < npc; ++c, ++it) {
-                    const int s = it % TC_STAGES;
-                    if (s != warp) continue;
-                    const int64_t p = (int64_t)c * 32 + lane;
-                    const bool live = p < np;
-                    Rec R;
-                    R.xh = live ? G.g.pair_xhi[p] : 0.f;
-                    R.xl = live ? G.g.pair_xlo[p] : 0.f;
-                    R.load(live ? G.ck[(G.blk_ofs[m] + jb) * np + p] : make_float4(0.f, 0.f, 0.f, 0.f));
-                    if (it >= TC_STAGES && !warp_wait(&empty[s], ((it / TC_STAGES) + 1) & 1)) {
-                        if (lane == 0) set_err(err, 11);
-                        ok = false;
-                        break;
-                    }
-                    uint8_t *A = smem + s * STAGE;
+            const int64_t blk = G.blk_ofs[m] + jb;
+            const float4 *ckt = half ? G.ckh : G.ck;
+            __syncwarp();
+#pragma unroll
+            for (int i = 0; i < 4; ++i) L.coef[lane + 32 * i] = G.coef[blk * 256 + half * 128 + lane + 32 * i];
+            __syncwarp();
+            // this warp's next chunk (c + ST) has its checkpoint and x fetched one chunk ahead
+            float4 knext = make_float4(0.f, 0.f, 0.f, 0.f);
+            float xhn = 0.f, xln = 0.f;
+            auto fetch = [&](int cc) {
+                const int64_t pp = (int64_t)cc * 32 + lane;
+                const bool lv = active && cc < npc && pp < np;
+                knext = lv ? ckt[blk * np + pp] : make_float4(0.f, 0.f, 0.f, 0.f);
+                xhn = lv ? G.g.pair_xhi[pp] : 0.f;
+                xln = lv ? G.g.pair_xlo[pp] : 0.f;
+            };
+            bool first = true;
+            for (int c = 0; c < npc; ++c, ++it) {
+                const int s = it % ST;
+                if (s != owner) continue;
+                if (first) fetch(c);
+                first = false;
+                Rec R;
+                R.xh = xhn;
+                R.xl = xln;
+                R.load(knext, LS);
+                fetch(c + ST);
+                const bool fast = __all_sync(0xffffffffu, R.e == 0);
+                if (it >= ST && !warp_wait(&L.empty[s], ((it / ST) + 1) & 1)) {
+                    if (lane == 0) set_err(err, 11);
+                    ok = false;
+                    break;
+                }
+                uint8_t *A = smem + s * STAGE;
+                // MN-major: 8 consecutive rows (l of one parity) of pair `lane`
+                const int off0 = (lane & 7) * 16 + (lane >> 3) * 128 + half * 8 * 512;
 #pragma unroll 1
-                    for (int grp = 0; grp < 16; ++grp) {
-                        float ev[8], od[8];
-#pragma unroll
-                        for (int t = 0; t < 8; ++t) {
-                            const float2 ce = coef[16 * grp + 2 * t], co = coef[16 * grp + 2 * t + 1];
-                            ev[t] = R.val(R.step(ce.x, ce.y));
-                            od[t] = R.val(R.step(co.x, co.y));
-                            if (t & 1) R.check();
-                        }
-                        uint4 hi, lo;
-                        // MN-major: 8 consecutive rows (l of one parity) of pair `lane`
-                        const int off = (lane & 7) * 16 + grp * 512 + (lane >> 3) * 128;
-                        tc::split8<BF16>(ev, LS, hi, lo);
-                        *reinterpret_cast<uint4 *>(A + 0 * A_TILE + off) = hi;
-                        *reinterpret_cast<uint4 *>(A + 1 * A_TILE + off) = lo;
-                        tc::split8<BF16>(od, LS, hi, lo);
-                        *reinterpret_cast<uint4 *>(A + 2 * A_TILE + off) = hi;
-                        *reinterpret_cast<uint4 *>(A + 3 * A_TILE + off) = lo;
-                    }
-                    tc::fence_proxy_async_smem();
-                    tc::mbar_arrive(&full[s]);
+                for (int grp = 0; grp < 8; ++grp) {
+                    float ev[8], od[8];
+                    if (fast)
+                        gen16<false>(R, L.coef + 16 * grp, ev, od);
+                    else
+                        gen16<true>(R, L.coef + 16 * grp, ev, od);
+                    store_split<BF16>(A, off0 + grp * 512, ev, od);
                 }
-            } else {
-                // ---------------- MMA issuer: one thread of warp 3
-                if (lane == 0) {
-                    if (ui > 0 && !tc::mbar_wait(tfree, (ui - 1) & 1, HB_TC_WAIT_NS)) {
-                        set_err(err, 13);
-                        ok = false;
-                    }
-                    tc::fence_after();
-                    for (int c = 0; c < npc && ok; ++c, ++it) {
-                        const int s = it % TC_STAGES;
-                        if (!tc::mbar_wait(&full[s], (it / TC_STAGES) & 1, HB_TC_WAIT_NS)) {
-                            set_err(err, 14);
-                            ok = false;
-                            break;
-                        }
-                        tc::fence_after();
-                        const uint32_t a0 = tc::smem_u32(smem + s * STAGE), b0 = a0 + A_STAGE;
-                        const int set = c % S;
-#pragma unroll
-                        for (int q = 0; q < 2; ++q) {
-                            const uint32_t d = tmem + set * 2 * N + q * N;
-#pragma unroll
-                            for (int k = 0; k < 2; ++k) {
-                                const uint64_t ah = tc::sdesc(a0 + (q * 2 + 0) * A_TILE + k * 256, 128, 512);
-                                const uint64_t al = tc::sdesc(a0 + (q * 2 + 1) * A_TILE + k * 256, 128, 512);
-                                const uint64_t bh = tc::sdesc(b0 + (q * 2 + 0) * (N * 64) + k * 256, 128, 512);
-                                const uint64_t bl = tc::sdesc(b0 + (q * 2 + 1) * (N * 64) + k * 256, 128, 512);
-                                tc::mma_bf16(d, ah, bh, IDESC, (c >= S || k > 0) ? 1u : 0u);
-                                tc::mma_bf16(d, ah, bl, IDESC, 1u);
-                                tc::mma_bf16(d, al, bh, IDESC, 1u);
-                            }
-                        }
-                        tc::mma_commit(&empty[s]);
-                    }
-                    if (ok) {
-                        tc::mma_commit(accum);
-                    } else {
-                        tc::mma_commit(drain);
-                        tc::mbar_wait(drain, 0, HB_TC_WAIT_NS);
-                    }
-                }
-                __syncwarp();
-                ok = __shfl_sync(0xffffffffu, ok, 0);
-                it = __shfl_sync(0xffffffffu, it, 0);
+                tc::fence_proxy_async_smem();
+                tc::mbar_arrive(&L.full[s]);
             }
             if (!ok) break;
-            // ---------------- epilogue (warps 0-3: TMEM lane quarters 0-3 = rows 32w..32w+31)
-            if (!warp_wait(accum, ui & 1)) {
+            // epilogue: lane quarter warp % 4 = rows 32w'..32w'+31 (l = l0 + 2 row + parity),
+            // column blocks j with j % 2 == half
+            if (!warp_wait(L.accum, ui & 1)) {
                 if (lane == 0) set_err(err, 12);
                 ok = false;
                 break;
             }
             tc::fence_after();
-            const int row = warp * 32 + lane;
+            const int row = owner * 32 + lane;
             const int le = l0 + 2 * row;
-            const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
+            const uint32_t taddr = tmem + ((uint32_t)(owner * 32) << 16);
             const float inv = 1.0f / (LS * G.dscale[m]);
             const int nsets = npc < S ? npc : S;
 #pragma unroll 1
-            for (int j = 0; j < N / 16; ++j) {
+            for (int j = half; j < N / 16; j += 2) {
                 float de[16], dd[16];
-                tc::tmem_ld16(tmem + lane_base + j * 16, de);
-                tc::tmem_ld16(tmem + lane_base + N + j * 16, dd);
-                tc::tmem_wait_ld();
-                for (int st = 1; st < nsets; ++st) {
-                    float xe[16], xd[16];
-                    tc::tmem_ld16(tmem + lane_base + st * 2 * N + j * 16, xe);
-                    tc::tmem_ld16(tmem + lane_base + st * 2 * N + N + j * 16, xd);
-                    tc::tmem_wait_ld();
-#pragma unroll
-                    for (int i = 0; i < 16; ++i) {
-                        de[i] += xe[i];
-                        dd[i] += xd[i];
-                    }
-                }
+                load_sets<N>(taddr, j, nsets, de, dd);
 #pragma unroll
                 for (int h = 0; h < 8; ++h) {
                     const int b = j * 8 + h;
@@ -617,10 +656,43 @@ __global__ void __launch_bounds__(ANA_THREADS, 1)
                 }
             }
             tc::fence_before();
-            tc::mbar_arrive(tfree);
+            tc::mbar_arrive(L.tfree);
         }
+    } else if (warp == 8) {
+        // ---------------- MMA issuer
+        if (lane == 0) {
+            uint32_t it = 0;
+            int ui = 0;
+            for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++ui) {
+                const int npc = (int)groups[units[u].x].npc;
+                if (ui > 0 && !tc::mbar_wait(L.tfree, (ui - 1) & 1, HB_TC_WAIT_NS)) {
+                    set_err(err, 13);
+                    ok = false;
+                    break;
+                }
+                tc::fence_after();
+                for (int c = 0; c < npc; ++c, ++it) {
+                    const int s = it % ST;
+                    if (!tc::mbar_wait(&L.full[s], (it / ST) & 1, HB_TC_WAIT_NS)) {
+                        set_err(err, 14);
+                        ok = false;
+                        break;
+                    }
+                    tc::fence_after();
+                    issue_stage<N>(tmem, tc::smem_u32(smem + s * STAGE), c % S, c < S, IDESC);
+                    tc::mma_commit(&L.empty[s]);
+                }
+                if (!ok) break;
+                tc::mma_commit(L.accum);
+            }
+            if (!ok) {
+                tc::mma_commit(L.drain);
+                tc::mbar_wait(L.drain, 0, HB_TC_WAIT_NS);
+            }
+        }
+        __syncwarp();
     } else {
-        // ---------------- loader of the pre-split E/O tiles (warp 4, one thread)
+        // ---------------- loader of the pre-split E/O tiles
         if (lane == 0) {
             uint32_t it = 0;
             for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
@@ -630,14 +702,14 @@ __global__ void __launch_bounds__(ANA_THREADS, 1)
                 const int npc = (int)G.npc;
                 const uint4 *src = G.g_tiles + (int64_t)m * npc * (16 * N);
                 for (int c = 0; c < npc; ++c, ++it) {
-                    const int s = it % TC_STAGES;
-                    if (it >= TC_STAGES && !tc::mbar_wait(&empty[s], ((it / TC_STAGES) + 1) & 1, HB_TC_WAIT_NS)) {
+                    const int s = it % ST;
+                    if (it >= ST && !tc::mbar_wait(&L.empty[s], ((it / ST) + 1) & 1, HB_TC_WAIT_NS)) {
                         set_err(err, 15);
                         ok = false;
                         break;
                     }
-                    tc::mbar_arrive_expect_tx(&full[s], B_STAGE);
-                    tc::bulk_g2s(smem + s * STAGE + A_STAGE, src + (int64_t)c * (16 * N), B_STAGE, &full[s]);
+                    tc::mbar_arrive_expect_tx(&L.full[s], B_STAGE);
+                    tc::bulk_g2s(smem + s * STAGE + A_STAGE, src + (int64_t)c * (16 * N), B_STAGE, &L.full[s]);
                 }
             }
         }
@@ -645,14 +717,13 @@ __global__ void __launch_bounds__(ANA_THREADS, 1)
     }
     tc::fence_before();
     __syncthreads();
-    if (warp == 3) {
+    if (warp == 8) {
         tc::fence_after();
         tc::tmem_dealloc(tmem, TCOLS);
     }
 }
 
 // ------------------------------------------------------------------------------------ host
-template <int N> constexpr int syn_smem() { return TC_STAGES * (A_STAGE + 4 * N * 64) + 4 * 256 * 8 + 8 * 16 + 16; }
 
 }  // namespace hb
 
@@ -666,6 +737,8 @@ struct hb_batched_plan {
         float2 *GF;                   // G (synthesis) / F (analysis) buffer [nmaps][mmax+1][np][2]
         int64_t gf_stride;
         int64_t *tile_ofs;            // device [mmax+1] alm chunk offsets
+        float2 *coef;                 // recursion coefficient table (coef_table_kernel)
+        float4 *ckh;                  // mid-block recursion checkpoints (launch_ck_mid)
     };
     std::vector<PlanPart> parts;
     std::vector<TcGroup> hgroups;
@@ -699,21 +772,21 @@ template <int N> constexpr int nsets() { return 512 / (2 * N) > 4 ? 4 : 512 / (2
 
 template <int N, bool BF16>
 static int launch_syn(hb_batched_plan *bp, cudaStream_t st) {
-    const int smem = syn_smem<N>();
+    const int smem = tc_smem<syn_stages<N>(), N>();
     constexpr int S = nsets<N>();
     HB_CUDA_TRY(cudaFuncSetAttribute(synth_tc_kernel<N, BF16, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     const int grid = std::min(bp->n_syn, sm_count());
-    synth_tc_kernel<N, BF16, S><<<grid, SYN_THREADS, smem, st>>>(bp->dgroups, bp->syn_units, bp->n_syn, bp->err);
+    synth_tc_kernel<N, BF16, S><<<grid, TC_THREADS, smem, st>>>(bp->dgroups, bp->syn_units, bp->n_syn, bp->err);
     HB_CHECK_LAUNCH();
     return HB_OK;
 }
 template <int N, bool BF16>
 static int launch_ana(hb_batched_plan *bp, float2 *alm_out, cudaStream_t st) {
-    const int smem = syn_smem<N>();
+    const int smem = tc_smem<ana_stages<N>(), N>();
     constexpr int S = nsets<N>();
     HB_CUDA_TRY(cudaFuncSetAttribute(anal_tc_kernel<N, BF16, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     const int grid = std::min(bp->n_ana, sm_count());
-    anal_tc_kernel<N, BF16, S><<<grid, ANA_THREADS, smem, st>>>(bp->dgroups, bp->ana_units, bp->n_ana, alm_out,
+    anal_tc_kernel<N, BF16, S><<<grid, TC_THREADS, smem, st>>>(bp->dgroups, bp->ana_units, bp->n_ana, alm_out,
                                                                  bp->err);
     HB_CHECK_LAUNCH();
     return HB_OK;
@@ -758,7 +831,7 @@ int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int np
     // sizes and layout of the single allocation
     size_t total = 0;
     auto carve = [&](size_t b) { size_t o = total; total += (b + 255) & ~(size_t)255; return o; };
-    struct Off { size_t gf, tofs, tiles_a, tiles_g, scales; };
+    struct Off { size_t gf, tofs, tiles_a, tiles_g, scales, coef, ckh; };
     std::vector<Off> offs(nplans);
     std::vector<std::vector<int64_t>> tile_ofs(nplans);
     std::vector<int64_t> chunks_a(nplans);
@@ -777,6 +850,10 @@ int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int np
         offs[i].tiles_a = carve((size_t)ng * chunks_a[i] * 256 * N);
         offs[i].tiles_g = carve((size_t)ng * (p->mmax + 1) * ((np + 31) / 32) * 256 * N);
         offs[i].scales = carve((size_t)ng * 4 * (p->mmax + 1));
+        int64_t nblocks = 0;  // 256-l blocks over all m, the plan's checkpoint layout
+        for (int m = 0; m <= p->mmax; ++m) nblocks += (p->lmax - m) / 256 + 1;
+        offs[i].coef = carve((size_t)nblocks * 256 * sizeof(float2));
+        offs[i].ckh = carve((size_t)nblocks * np * sizeof(float4));
         hb_batched_plan::PlanPart part;
         part.p = p;
         part.nmaps = nmaps[i];
@@ -843,6 +920,8 @@ int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int np
         part.GF = (float2 *)(base + offs[i].gf);
         part.gf_stride = (int64_t)(part.p->mmax + 1) * part.p->g->d.npairs * 2;
         part.tile_ofs = (int64_t *)(base + offs[i].tofs);
+        part.coef = (float2 *)(base + offs[i].coef);
+        part.ckh = (float4 *)(base + offs[i].ckh);
     }
     {
         int gi = 0;
@@ -853,6 +932,8 @@ int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int np
                 TcGroup &G = bp->hgroups[gi];
                 G.alm_tiles = (const uint4 *)(base + offs[i].tiles_a) + (size_t)k * chunks_a[i] * 16 * N;
                 G.alm_tile_ofs = bp->parts[i].tile_ofs;
+                G.coef = bp->parts[i].coef;
+                G.ckh = bp->parts[i].ckh;
                 G.Gm = bp->parts[i].GF + (int64_t)GM * k * bp->parts[i].gf_stride;
                 G.gm_stride = bp->parts[i].gf_stride;
                 G.g_tiles = (const uint4 *)(base + offs[i].tiles_g) +
@@ -877,6 +958,13 @@ int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int np
          cudaMemcpy(bp->ana_units, auv.data(), sizeof(int4) * auv.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
          cudaMemset(bp->err, 0, sizeof(int)) != cudaSuccess))
         rc = fail(HB_ERR_CUDA, "hb_batched_plan_create: upload");
+    for (int i = 0; i < nplans && rc == HB_OK; ++i) {
+        const hb_plan *p = plans[i];
+        coef_table_kernel<<<p->mmax + 1, 256>>>(p->lmax, p->blk_ofs, bp->parts[i].coef);
+        if (cudaGetLastError() != cudaSuccess || launch_ck_mid(p, bp->parts[i].ckh) != HB_OK ||
+            cudaDeviceSynchronize() != cudaSuccess)
+            rc = fail(HB_ERR_CUDA, "hb_batched_plan_create: coefficient table");
+    }
     if (rc != HB_OK) {
         cudaFree(base);
         delete bp;

@@ -108,6 +108,9 @@ struct hb_plan {
 
 namespace hb {
 // kernels' host launchers (implemented in the .cu files)
+// the plan's scalar recursion states at l0 + 128 of every 256-l block (same indexing as ck);
+// default stream, asynchronous
+int launch_ck_mid(const hb_plan *p, float4 *ck_mid);
 int launch_ring_analysis(const GeomDev &g, int precision, int nmaps, const void *maps, int64_t map_stride,
                          const double *w, void *Fm, int mmax, int flags, bool unit_weights, bool mdouble,
                          cudaStream_t st);

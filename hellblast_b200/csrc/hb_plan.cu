@@ -43,8 +43,10 @@ __device__ __forceinline__ float4 to_f32_state(double v1, double v2, int e) {
 constexpr int CKR = 256;   // checkpoint block length (== COEF_CH of the Legendre kernels)
 constexpr int CK_NT = 128;
 
+// ck (may be null): states at the block starts; ck_mid (may be null): states at l0 + R/2 of every
+// block that reaches that far, same indexing.
 __global__ void __launch_bounds__(CK_NT) ck_scalar_kernel(GeomDev g, int lmax, const int64_t *__restrict__ blk_ofs,
-                                                          float4 *__restrict__ ck) {
+                                                          float4 *__restrict__ ck, float4 *__restrict__ ck_mid) {
     const int m = blockIdx.x;
     const int64_t p = (int64_t)blockIdx.y * CK_NT + threadIdx.x;
     __shared__ double2 cf[CKR];
@@ -55,10 +57,11 @@ __global__ void __launch_bounds__(CK_NT) ck_scalar_kernel(GeomDev g, int lmax, c
     int e = (int)floor((L + 256.0) / 512.0);
     double l1 = 0.0, l2 = exp2(L - 512.0 * e);
     if (m & 1) l2 = -l2;
-    float4 *out = ck + blk_ofs[m] * np;
+    const int64_t o = blk_ofs[m] * np;
     for (int l0 = m; l0 <= lmax; l0 += CKR) {
+        const int64_t oj = o + (int64_t)((l0 - m) / CKR) * np + p;
         // state at the start of this block: (lambda_{l0-1}, lambda_{l0-2}); block 0 holds (0, lambda_mm)
-        if (live) out[(int64_t)((l0 - m) / CKR) * np + p] = to_f32_state(l1, l2, e);
+        if (live && ck) ck[oj] = to_f32_state(l1, l2, e);
         __syncthreads();
         for (int i = threadIdx.x; i < CKR; i += CK_NT) {
             int l = l0 + i;
@@ -73,6 +76,7 @@ __global__ void __launch_bounds__(CK_NT) ck_scalar_kernel(GeomDev g, int lmax, c
         __syncthreads();
         const int n = min(CKR, lmax - l0 + 1);
         for (int i = 0; i < n; ++i) {
+            if (i == CKR / 2 && live && ck_mid) ck_mid[oj] = to_f32_state(l1, l2, e);
             double v = cf[i].x * x * l1 + cf[i].y * l2;
             l2 = l1;
             l1 = v;
@@ -141,6 +145,14 @@ __global__ void __launch_bounds__(CK_NT) ck_spin_kernel(GeomDev g, int lmax, con
     }
 }
 
+int launch_ck_mid(const hb_plan *p, float4 *ck_mid) {
+    const int64_t np = p->g->d.npairs;
+    dim3 grid((unsigned)(p->mmax + 1), (unsigned)((np + CK_NT - 1) / CK_NT));
+    ck_scalar_kernel<<<grid, CK_NT>>>(p->g->d, p->lmax, p->blk_ofs, nullptr, ck_mid);
+    HB_CUDA_TRY(cudaGetLastError());
+    return HB_OK;
+}
+
 }  // namespace hb
 
 using namespace hb;
@@ -191,7 +203,7 @@ int hb_plan_create(const hb_geom *g, int lmax, int mmax, int flags, hb_plan **ou
         rc = fail(HB_ERR_CUDA, "hb_plan_create: upload failed");
     dim3 grid((unsigned)(mmax + 1), (unsigned)((np + CK_NT - 1) / CK_NT));
     if (rc == HB_OK && scalar) {
-        ck_scalar_kernel<<<grid, CK_NT>>>(g->d, lmax, p->blk_ofs, p->ck);
+        ck_scalar_kernel<<<grid, CK_NT>>>(g->d, lmax, p->blk_ofs, p->ck, nullptr);
         if (cudaGetLastError() != cudaSuccess) rc = fail(HB_ERR_CUDA, "hb_plan_create: checkpoint kernel launch");
     }
     if (rc == HB_OK && spin) {

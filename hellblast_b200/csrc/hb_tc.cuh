@@ -149,14 +149,14 @@ template <> struct Half16<false> {
     static __device__ __forceinline__ float back(t a) { return __half2float(a); }
 };
 
-// 8 floats * s -> 8 "hi" = h(v s) and 8 "lo" = h(v s - hi), packed as two uint4
+// 8 floats -> 8 "hi" = h(v) and 8 "lo" = h(v - hi), packed as two uint4
 template <bool BF16>
-__device__ __forceinline__ void split8(const float (&v)[8], float s, uint4 &hi, uint4 &lo) {
+__device__ __forceinline__ void split8(const float (&v)[8], uint4 &hi, uint4 &lo) {
     using H = Half16<BF16>;
     uint32_t h[4], l[4];
 #pragma unroll
     for (int i = 0; i < 4; ++i) {
-        const float a = v[2 * i] * s, b = v[2 * i + 1] * s;
+        const float a = v[2 * i], b = v[2 * i + 1];
         typename H::t2 x = H::pack(a, b);
         float2 f = H::unpack(x);
         typename H::t2 y = H::pack(a - f.x, b - f.y);
