@@ -6,6 +6,7 @@
 // reference.  Differences by design: one thread per ring with ring_start in closed form
 // (no serial scan by thread 0), and phi0 in either the HEALPix convention (default) or the
 // reference's, which sits +1/2 pixel off on the equatorial belt (ring_tables_healpix.cu:25-27).
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -148,6 +149,26 @@ static int finish_geom(HostGeom &h, int64_t nside, const std::vector<double> &xn
     }
     std::vector<double> cm, spin;
     fill_log2_tables(cm, spin);
+    int log_tw = 1;
+    while ((1 << log_tw) < h.max_fft_len) ++log_tw;
+    // pair classes by convolution length
+    std::vector<std::pair<int32_t, int32_t>> pl;
+    for (int64_t p = 0; p < np; ++p) {
+        const int32_t rn = h.pair_ring[2 * p], rs = h.pair_ring[2 * p + 1];
+        pl.push_back({std::max(h.fft_len[rn], rs >= 0 ? h.fft_len[rs] : 0), (int32_t)p});
+    }
+    std::sort(pl.begin(), pl.end());
+    std::vector<int32_t> cls_pairs(np), cls_L;
+    std::vector<int64_t> cls_first;
+    for (int64_t i = 0; i < np; ++i) {
+        cls_pairs[i] = pl[i].second;
+        if (i == 0 || pl[i].first != pl[i - 1].first) {
+            cls_L.push_back(pl[i].first);
+            cls_first.push_back(i);
+        }
+    }
+    cls_first.push_back(np);
+    if (cls_L.size() > 32) return fail(HB_ERR_UNSUPPORTED, "hb_geom: more than 32 FFT length classes");
 
     // one device allocation carved into 256-byte aligned pieces
     size_t total = 0;
@@ -160,7 +181,9 @@ static int finish_geom(HostGeom &h, int64_t nside, const std::vector<double> &xn
            o_rp = carve(4 * nr), o_rs = carve(4 * nr), o_pr = carve(8 * np), o_px = carve(8 * np),
            o_pxh = carve(4 * np), o_pxl = carve(4 * np), o_pls = carve(8 * np), o_plc = carve(8 * np),
            o_plh = carve(8 * np), o_fl = carve(4 * nr), o_bo = carve(8 * nr), o_b64 = carve(16 * (h.blu_total + 1)),
-           o_b32 = carve(8 * (h.blu_total + 1)), o_bw = carve(4 * (h.blu_owner.size() + 1)), o_cm = carve(8 * (HB_MAX_L + 1)), o_sp = carve(8 * (HB_MAX_L + 1));
+           o_b32 = carve(8 * (h.blu_total + 1)), o_bw = carve(4 * (h.blu_owner.size() + 1)), o_cm = carve(8 * (HB_MAX_L + 1)), o_sp = carve(8 * (HB_MAX_L + 1)),
+           o_t64 = carve(16 * ((size_t)1 << (log_tw - 1))), o_t32 = carve(8 * ((size_t)1 << (log_tw - 1))),
+           o_cp = carve(4 * (size_t)np);
     char *base = nullptr;
     if (cudaMalloc(&base, total) != cudaSuccess) {
         cudaGetLastError();
@@ -181,6 +204,10 @@ static int finish_geom(HostGeom &h, int64_t nside, const std::vector<double> &xn
     d.blu_owner = (int32_t *)(base + o_bw); d.n_blu = (int64_t)h.blu_owner.size();
     d.log2cm = (double *)(base + o_cm); d.log2spin = (double *)(base + o_sp);
     d.max_fft_len = h.max_fft_len; d.max_nphi = h.max_nphi;
+    d.tw64 = (double2 *)(base + o_t64); d.tw32 = (float2 *)(base + o_t32); d.log_tw = log_tw;
+    d.cls_pairs = (int32_t *)(base + o_cp); d.n_cls = (int)cls_L.size();
+    for (size_t c = 0; c < cls_L.size(); ++c) { d.cls_L[c] = cls_L[c]; d.cls_first[c] = cls_first[c]; }
+    d.cls_first[cls_L.size()] = np;
     struct Up { void *dst; const void *src; size_t n; } ups[] = {
         {d.nphi, h.nphi.data(), 4 * (size_t)nr}, {d.ofs, h.ofs.data(), 8 * (size_t)nr},
         {d.phi0_pi, h.phi0_pi.data(), 8 * (size_t)nr}, {d.w, h.w.data(), 8 * (size_t)nr},
@@ -191,7 +218,7 @@ static int finish_geom(HostGeom &h, int64_t nside, const std::vector<double> &xn
         {d.pair_log2sh, h.pair_log2sh.data(), 8 * (size_t)np}, {d.fft_len, h.fft_len.data(), 4 * (size_t)nr},
         {d.blu_ofs, h.blu_ofs.data(), 8 * (size_t)nr},
         {d.blu_owner, h.blu_owner.data(), 4 * h.blu_owner.size()}, {d.log2cm, cm.data(), 8 * (size_t)(HB_MAX_L + 1)},
-        {d.log2spin, spin.data(), 8 * (size_t)(HB_MAX_L + 1)}};
+        {d.log2spin, spin.data(), 8 * (size_t)(HB_MAX_L + 1)}, {d.cls_pairs, cls_pairs.data(), 4 * (size_t)np}};
     for (auto &u : ups) {
         if (cudaMemcpy(u.dst, u.src, u.n, cudaMemcpyHostToDevice) != cudaSuccess) {
             cudaGetLastError();
@@ -200,7 +227,7 @@ static int finish_geom(HostGeom &h, int64_t nside, const std::vector<double> &xn
             return fail(HB_ERR_CUDA, "hb_geom: upload failed");
         }
     }
-    int rc = build_bluestein_tables(d, 0);
+    int rc = build_fft_tables(d, 0);
     if (rc == HB_OK && cudaStreamSynchronize(0) != cudaSuccess) rc = fail(HB_ERR_CUDA, "hb_geom: table build failed");
     if (rc != HB_OK) {
         cudaFree(base);

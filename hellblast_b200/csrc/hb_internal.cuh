@@ -76,11 +76,21 @@ struct GeomDev {
     // direct FFT; otherwise Bluestein) and the offset of its chirp spectrum in blu_*.
     int32_t *fft_len;      // [nr]
     int64_t *blu_ofs;      // [nr] (-1 for direct)
-    double2 *blu_f64;      // concatenated chirp spectra, bit-reversed order, scaled by 1/L
+    double2 *blu_f64;      // concatenated chirp spectra, forward-transform output order, scaled by 1/L
     float2 *blu_f32;
     int32_t *blu_owner;    // [n_blu] first ring using each distinct chirp table
     int64_t n_blu;
     int max_fft_len;       // max L over rings
+    // FFT twiddles exp(-2 pi i j / 2^log_tw), j < 2^(log_tw-1), 2^log_tw = max(2, max_fft_len)
+    double2 *tw64;
+    float2 *tw32;
+    int log_tw;
+    // pairs grouped by convolution length class (max L of the pair's rings), ascending:
+    // class c = pairs cls_pairs[cls_first[c] .. cls_first[c+1]) with length cls_L[c]
+    int32_t *cls_pairs;    // [npairs]
+    int n_cls;
+    int cls_L[32];
+    int64_t cls_first[33];
     int max_nphi;
     double *log2cm;        // [HB_MAX_L+1] log2 sqrt((2m+1)!!/((2m)!! 4 pi)), scalar lambda_mm
     double *log2spin;      // [HB_MAX_L+1] log2 of the constant of N_l0 d^l0_{m,+-2}
@@ -128,6 +138,6 @@ int launch_spin_analysis(const GeomDev &g, int precision, int nmaps, int lmax, i
 int launch_spin_synthesis(const GeomDev &g, int precision, int nmaps, int lmax, int mmax, const void *E,
                           const void *B, void *QGm, void *UGm, cudaStream_t st, const float4 *ckP,
                           const float4 *ckM, const int64_t *blk_ofs);
-int build_bluestein_tables(GeomDev &g, cudaStream_t st);
-int fft_smem_bytes(int L, int precision);
+// FFT twiddle table and Bluestein chirp spectra of a geometry
+int build_fft_tables(GeomDev &g, cudaStream_t st);
 }  // namespace hb
