@@ -40,35 +40,21 @@ namespace hb {
 // Stage plan of a length-2^logL transform: logL / 3 radix-8 stages, then one radix-2^(logL % 3)
 // stage.  Stage i works on sub-transforms of size S_i = 2^(logL - 3i).
 
-// Position (in the forward transform's output) of frequency k.
-__device__ __forceinline__ int freq_to_pos(int k, int logL) {
+// Digit reversal between frequency k and its position p in the forward transform's output:
+// p holds k's base-8 digits (lowest first) from the top down, then k's top logL % 3 bits.
+// Computed as a full bit reversal plus a fix-up that restores the bit order inside each digit.
+__device__ __forceinline__ unsigned digit_fix(unsigned x, int logL) {
     const int n8 = logL / 3, rem = logL - 3 * n8;
-    int p = 0, sh_out = logL;
-#pragma unroll
-    for (int i = 0; i < 10; ++i) {
-        if (i < n8) {
-            sh_out -= 3;
-            p |= ((k >> (3 * i)) & 7) << sh_out;
-        }
-    }
-    if (rem) p |= (k >> (3 * n8)) & ((1 << rem) - 1);
-    return p;
+    const unsigned low = (1u << (3 * n8)) - 1u;
+    const unsigned g = x & low, hi = x & ~low;
+    const unsigned m0 = 0x49249249u & low;
+    const unsigned gf = (g & (m0 << 1)) | ((g & m0) << 2) | ((g & (m0 << 2)) >> 2);
+    const unsigned hf = rem == 2 ? (((hi >> 1) & (1u << (3 * n8))) | ((hi << 1) & (2u << (3 * n8)))) : hi;
+    return gf | hf;
 }
-
-// Frequency held at position p of the forward transform's output (inverse of freq_to_pos).
-__device__ __forceinline__ int pos_to_freq(int p, int logL) {
-    const int n8 = logL / 3, rem = logL - 3 * n8;
-    int k = 0, sh_in = logL;
-#pragma unroll
-    for (int i = 0; i < 10; ++i) {
-        if (i < n8) {
-            sh_in -= 3;
-            k |= ((p >> sh_in) & 7) << (3 * i);
-        }
-    }
-    if (rem) k |= (p & ((1 << rem) - 1)) << (3 * n8);
-    return k;
-}
+__device__ __forceinline__ unsigned brev_n(unsigned x, int logL) { return logL ? __brev(x) >> (32 - logL) : 0u; }
+__device__ __forceinline__ int freq_to_pos(int k, int logL) { return (int)brev_n(digit_fix((unsigned)k, logL), logL); }
+__device__ __forceinline__ int pos_to_freq(int p, int logL) { return (int)digit_fix(brev_n((unsigned)p, logL), logL); }
 
 // Shared-memory FFT buffers carry one pad element per 16: the late stages' strided accesses and
 // the digit-reversed reads then spread over the banks.
@@ -139,6 +125,26 @@ template <int R, bool INV, typename V> __device__ __forceinline__ void dftR(V *x
         dft2<INV>(x);
 }
 
+// x[q] *= W_S^(pos q) (conjugated for INV), q = 1 .. R-1; radix 8 loads W^pos, W^2pos, W^4pos
+// and forms the other four by products (about two roundings more)
+template <int R, bool INV, typename T>
+__device__ __forceinline__ void twiddle_apply(c2_t<T> *x, const Tw<T> &tw, int pos, int logS) {
+    using V = c2_t<T>;
+    if constexpr (R == 8) {
+        const V w1 = tw.w(pos, logS), w2 = tw.w(2 * pos, logS), w4 = tw.w(4 * pos, logS);
+        const V w3 = cmul(w1, w2);
+        V w[8] = {w1, w1, w2, w3, w4, cmul(w4, w1), cmul(w4, w2), cmul(w4, w3)};
+#pragma unroll
+        for (int q = 1; q < 8; ++q) x[q] = cmul(x[q], INV ? cconj(w[q]) : w[q]);
+    } else {
+#pragma unroll
+        for (int q = 1; q < R; ++q) {
+            const V wq = tw.w(pos * q, logS);
+            x[q] = cmul(x[q], INV ? cconj(wq) : wq);
+        }
+    }
+}
+
 // one decimation-in-frequency stage of radix R on sub-transforms of size 2^logS
 template <int R, bool PAD, typename T>
 __device__ __forceinline__ void dif_stage(c2_t<T> *buf, const Tw<T> &tw, int logL, int logS) {
@@ -152,8 +158,7 @@ __device__ __forceinline__ void dif_stage(c2_t<T> *buf, const Tw<T> &tw, int log
 #pragma unroll
         for (int t = 0; t < R; ++t) x[t] = buf[ph<PAD>(base + (t << logh))];
         dftR<R, false>(x);
-#pragma unroll
-        for (int q = 1; q < R; ++q) x[q] = cmul(x[q], tw.w(pos * q, logS));
+        twiddle_apply<R, false>(x, tw, pos, logS);
 #pragma unroll
         for (int q = 0; q < R; ++q) buf[ph<PAD>(base + (q << logh))] = x[q];
     }
@@ -172,8 +177,7 @@ __device__ __forceinline__ void dit_inv_stage(c2_t<T> *buf, const Tw<T> &tw, int
         V x[R];
 #pragma unroll
         for (int q = 0; q < R; ++q) x[q] = buf[ph<PAD>(base + (q << logh))];
-#pragma unroll
-        for (int q = 1; q < R; ++q) x[q] = cmul(x[q], cconj(tw.w(pos * q, logS)));
+        twiddle_apply<R, true>(x, tw, pos, logS);
         dftR<R, true>(x);
 #pragma unroll
         for (int t = 0; t < R; ++t) buf[ph<PAD>(base + (t << logh))] = x[t];
@@ -263,6 +267,32 @@ __device__ RingTrig<T> build_trig(c2_t<T> *tab, int n, int N, double phi0_pi, in
     return R;
 }
 
+// tables of ring `side` of the pair; the south ring reuses the north ring's when its nphi and
+// phi0 match (always on HEALPix grids).  Ends with a barrier.
+template <typename T>
+__device__ __forceinline__ RingTrig<T> trig_for_ring(const GeomDev &g, c2_t<T> *tab, int pair, int side, int n,
+                                                     int N, int mmax, bool chirp) {
+    bool rebuild = true;
+    if (side == 1) {
+        const int rn = g.pair_ring[2 * pair];
+        const int rs = g.pair_ring[2 * pair + 1];
+        rebuild = g.nphi[rn] != g.nphi[rs] || g.phi0_pi[rn] != g.phi0_pi[rs];
+    }
+    if (rebuild) {
+        const RingTrig<T> R = build_trig<T>(tab, n, N, side ? g.phi0_pi[g.pair_ring[2 * pair + 1]] : g.phi0_pi[g.pair_ring[2 * pair]], mmax, chirp);
+        __syncthreads();
+        return R;
+    }
+    // same layout as build_trig produced for the north ring (same n, N, mmax, chirp)
+    RingTrig<T> R;
+    c2_t<T> *u1 = tab, *p1 = u1 + 64, *c1 = p1 + 64, *u2 = c1 + 64;
+    c2_t<T> *p2 = u2 + (N >> 6) + 1, *c2 = p2 + (mmax >> 6) + 1;
+    R.U = {u1, u2};
+    R.P = {p1, p2};
+    R.C = {c1, c2};
+    return R;
+}
+
 // chirp w_j = exp(-i pi j^2 / N)
 template <typename T> __device__ __forceinline__ c2_t<T> chirp(const RingTrig<T> &R, int64_t j, int N) {
     return R.C((j * j) % (2 * (int64_t)N));
@@ -279,7 +309,7 @@ __global__ void __launch_bounds__(512, 2) ring_analysis_kernel(GeomDev g, const 
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V *buf = reinterpret_cast<V *>(smem_raw);
     V *tab = buf + padded_len(Lcls);
-    const int pair = pairs[blockIdx.x], b = blockIdx.y;
+    const int pair = pairs[blockIdx.y], b = blockIdx.x;  // maps fastest: a pair's tables stay in L2
     const int64_t np = g.npairs;
     V *out = Fm + b * fm_stride;
     const Tw<T> tw = twiddles<T>(g);
@@ -294,8 +324,7 @@ __global__ void __launch_bounds__(512, 2) ring_analysis_kernel(GeomDev g, const 
         const int64_t bo = g.blu_ofs[r];
         const bool direct = bo < 0;
         __syncthreads();  // previous ring done with buf / tables
-        const RingTrig<T> R = build_trig<T>(tab, n, N, g.phi0_pi[r], mmax, !direct);
-        __syncthreads();
+        const RingTrig<T> R = trig_for_ring<T>(g, tab, pair, side, n, N, mmax, !direct);
         const V *f2 = reinterpret_cast<const V *>(maps + b * map_stride + g.ofs[r]);  // ring offsets: multiples of 4
         if (direct) {
             for (int j = threadIdx.x; j < N; j += blockDim.x) buf[ph<true>(j)] = f2[j];
@@ -360,7 +389,7 @@ __global__ void __launch_bounds__(512, 2) ring_synthesis_kernel(GeomDev g, const
     V *buf = reinterpret_cast<V *>(smem_raw);
     V *tab = buf + padded_len(Lcls);
     V *ts = tab + trig_entries<T>(Lcls, mmax);  // staged T_m, m <= mmax (when stage_t)
-    const int pair = pairs[blockIdx.x], b = blockIdx.y;
+    const int pair = pairs[blockIdx.y], b = blockIdx.x;  // maps fastest: a pair's tables stay in L2
     const int64_t np = g.npairs;
     const V *gin = Gm + b * gm_stride;
     const Tw<T> tw = twiddles<T>(g);
@@ -373,8 +402,7 @@ __global__ void __launch_bounds__(512, 2) ring_synthesis_kernel(GeomDev g, const
         const bool direct = bo < 0;
         const int side_in = g.ring_side[r];
         __syncthreads();
-        const RingTrig<T> R = build_trig<T>(tab, n, N, g.phi0_pi[r], mmax, !direct);
-        __syncthreads();
+        const RingTrig<T> R = trig_for_ring<T>(g, tab, pair, side, n, N, mmax, !direct);
         // T_m = c_m G(m) exp(+i m phi0)
         auto Tm_global = [&](int m) -> V {
             V v = gin[((int64_t)m * np + pair) * 2 + side_in];
@@ -527,7 +555,7 @@ static int launch_analysis_t(const GeomDev &g, int nmaps, const T *maps, int64_t
         HB_CUDA_TRY(cudaFuncSetAttribute(ring_analysis_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         HB_CUDA_TRY(cudaFuncSetAttribute(ring_analysis_kernel<T>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                          cudaSharedmemCarveoutMaxShared));
-        dim3 grid((unsigned)cnt, (unsigned)nmaps);
+        dim3 grid((unsigned)nmaps, (unsigned)cnt);
         ring_analysis_kernel<T><<<grid, class_threads(L), smem, st>>>(g, g.cls_pairs + first, maps, map_stride,
                                                                        w ? w : g.w, Fm, fm_stride, mmax, flags,
                                                                        unit_w ? 1 : 0, mdouble ? 1 : 0, L);
@@ -550,7 +578,7 @@ static int launch_synthesis_t(const GeomDev &g, int nmaps, const c2_t<T> *Gm, in
         HB_CUDA_TRY(cudaFuncSetAttribute(ring_synthesis_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         HB_CUDA_TRY(cudaFuncSetAttribute(ring_synthesis_kernel<T>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                          cudaSharedmemCarveoutMaxShared));
-        dim3 grid((unsigned)cnt, (unsigned)nmaps);
+        dim3 grid((unsigned)nmaps, (unsigned)cnt);
         ring_synthesis_kernel<T><<<grid, class_threads(L), smem, st>>>(g, g.cls_pairs + first, Gm, gm_stride, mmax,
                                                                         maps, map_stride, w ? w : g.w,
                                                                         apply_w ? 1 : 0, mdouble ? 1 : 0, flags, L,
