@@ -147,6 +147,19 @@ def run_reference(args):
 
 
 # ----------------------------------------------------------------------------- GPU side
+def fft_classes(nside):
+    """Number of ring-FFT launches per direction: one per distinct convolution length of the
+    ring pairs (N = nphi/2 direct when a power of two, else Bluestein at 2^ceil(log2(2N-1)))."""
+    from hellblast_b200 import geometry as G
+    nphi = G.host_ring_tables(nside)["nphi"].astype(np.int64)
+    N = nphi // 2
+    pow2 = (N & (N - 1)) == 0
+    L = np.where(pow2, N, 1 << np.ceil(np.log2(2 * N - 1)).astype(np.int64))
+    nr = len(L)
+    pair_L = np.maximum(L[: (nr + 1) // 2], L[::-1][: (nr + 1) // 2])
+    return len(np.unique(pair_L))
+
+
 def main():
     args = parse()
     if args.impl == "reference":
@@ -206,6 +219,7 @@ def main():
 
     if args.mode == "plain":
         plan = G.plan(g, lmax, mmax, precision=32)
+        n_launch = 2 + 2 * fft_classes(nside)
         ws = torch.empty(plan.workspace_bytes(32, B), dtype=torch.uint8, device=dev)
 
         def step(ev=None):
@@ -223,26 +237,31 @@ def main():
             s = np.array([[ev[i].elapsed_time(ev[i + 1]) for i in range(4)] for ev in evs]).mean(0)
             return {"legendre_synthesis": s[0], "ring_synthesis": s[1], "ring_analysis": s[2],
                     "legendre_analysis": s[3]}
-        n_launch = 4
         def make_ev():
             return [torch.cuda.Event(enable_timing=True) for _ in range(5)]
     else:
         bf16 = args.split == "bf16"
         bp = hb.batched.plan(nside, lmax, B, bf16=bf16, wide=args.wide)
-        bp.profile(True)
         alm_flat, maps_flat, out_flat = alm.reshape(-1), maps.reshape(-1), alm_out.reshape(-1)
+        # the whole step (both directions, every kernel) as one CUDA graph
+        bp.capture(alm_flat, maps_flat, out_flat)
         stage_acc = []
 
         def step(ev=None):
+            if ev is None:
+                bp.replay(st)
+                return
+            bp.profile(True)  # separately timed step with events between the kernels
             bp.alm2map(alm_flat, out=maps_flat)
             bp.map2alm(maps_flat, out=out_flat)
-            if ev is not None:
-                stage_acc.append(bp.stage_ms())
+            stage_acc.append(bp.stage_ms())
+            bp.profile(False)
 
         def stage_times(evs):
             keys = stage_acc[0].keys()
             return {k: float(np.mean([s[k] for s in stage_acc])) for k in keys}
-        n_launch = 2 + 2 * len(bp.specs) + 2 + 2  # preps, tensor kernels, ring FFTs
+        groups = (B + (63 if args.wide else 31)) // (64 if args.wide else 32)
+        n_launch = 2 * groups + 2 + 2 * fft_classes(nside)  # operand preps, tensor kernels, ring FFT classes
 
         def make_ev():
             return True
@@ -289,25 +308,31 @@ def main():
     alm_pin = alm_h.pin_memory()
     out_pin = torch.empty_like(alm_pin).pin_memory()
 
-    def e2e_step():
-        a = alm_pin.to(dev, non_blocking=True)
-        if args.mode == "plain":
-            m = hb.hp_compat.alm2map(a, nside, lmax=lmax)
-            r = hb.hp_compat.map2alm(m, lmax=lmax)
-        else:
-            m = bp.alm2map(a).reshape(B, -1)
-            r = bp.map2alm(m).reshape(B, -1)
-        out_pin.copy_(r, non_blocking=True)
+    if args.mode == "plain":
+        def e2e_run(k):
+            for _ in range(k):
+                a = alm_pin.to(dev, non_blocking=True)
+                m = hb.hp_compat.alm2map(a, nside, lmax=lmax)
+                r = hb.hp_compat.map2alm(m, lmax=lmax)
+                out_pin.copy_(r, non_blocking=True)
+    else:
+        # batches streamed from pinned host memory: copies in / out overlap the transforms
+        pipe = hb.batched.HostPipeline(bp, dev)
 
-    for _ in range(max(1, args.warmup)):
-        e2e_step()
+        def e2e_run(k):
+            pipe.run([alm_pin] * k, [out_pin] * k)
+            pipe.wait_on(st)
+
+    e2e_run(max(1, args.warmup))
     torch.cuda.synchronize(dev)
     if world > 1:
         dist.barrier()
     t2 = torch.cuda.Event(enable_timing=True); t3 = torch.cuda.Event(enable_timing=True)
     t2.record(st)
-    for _ in range(args.steps):
-        e2e_step()
+    if args.mode != "plain":
+        for s_ in (pipe.s_in, pipe.s_run, pipe.s_out):
+            s_.wait_stream(st)
+    e2e_run(args.steps)
     t3.record(st)
     torch.cuda.synchronize(dev)
     ms_e2e = t2.elapsed_time(t3)

@@ -64,6 +64,8 @@ SIGNATURES = {
     "hb_batched_status": (i32, [vp, ctypes.POINTER(i32)]),
     "hb_batched_profile": (i32, [vp, i32]),
     "hb_batched_stage_ms": (i32, [vp, ctypes.POINTER(ctypes.c_float)]),
+    "hb_batched_graph_capture": (i32, [vp, vp, vp, vp]),
+    "hb_batched_graph_launch": (i32, [vp, vp]),
 }
 for _p in ("f32", "f64"):
     SIGNATURES[f"hb_map2alm_{_p}"] = (i32, [vp, i32, vp, vp, vp, vp, sz, i32, vp])

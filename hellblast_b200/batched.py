@@ -58,6 +58,22 @@ class BatchedPlan:
                torch.cuda.current_stream(maps.device).cuda_stream)
         return out
 
+    def capture(self, alm: torch.Tensor | None, maps: torch.Tensor, out: torch.Tensor | None) -> None:
+        """Record alm2map(alm -> maps) then map2alm(maps -> out) (either direction may be None)
+        into a CUDA graph owned by the plan; ``replay()`` then runs the whole step as one graph
+        launch.  The tensors' storage is baked into the graph: keep them alive and in place."""
+        for t, dt, n in ((alm, torch.complex64, self.total_alm), (maps, torch.float32, self.total_pix),
+                         (out, torch.complex64, self.total_alm)):
+            if t is not None and (t.dtype != dt or t.numel() != n or not t.is_cuda or not t.is_contiguous()):
+                raise ValueError("capture: buffers must be contiguous CUDA tensors of the plan's sizes")
+        self._graph_buffers = (alm, maps, out)
+        L.call("hb_batched_graph_capture", self.handle, None if alm is None else alm.data_ptr(), maps.data_ptr(),
+               None if out is None else out.data_ptr())
+
+    def replay(self, stream: torch.cuda.Stream | None = None) -> None:
+        st = torch.cuda.current_stream() if stream is None else stream
+        L.call("hb_batched_graph_launch", self.handle, st.cuda_stream)
+
     def profile(self, enable: bool = True) -> None:
         L.call("hb_batched_profile", self.handle, 1 if enable else 0)
 
@@ -107,3 +123,58 @@ def map2alm(maps: torch.Tensor, nside: int, lmax: int, mmax: int | None = None, 
     """[nmaps, npix] float32 -> [nmaps, nalm] complex64 through the tensor-core path."""
     nmaps = maps.shape[0]
     return plan(nside, lmax, nmaps, mmax, bf16=bf16, wide=wide).map2alm(maps).reshape(nmaps, -1)
+
+
+class HostPipeline:
+    """Streams batches held in pinned host memory through a batched plan: alm2map + map2alm of
+    batch i runs on a compute stream while batch i+1 is copied in and batch i-1's alm is copied
+    out on two copy streams (two device buffer sets, CUDA events between the streams).
+
+    ``run(inputs, outputs)`` takes lists of pinned complex64 host tensors of the plan's alm size
+    (outputs receive map2alm(alm2map(input))); it returns after queueing all work, and
+    ``synchronize()`` waits for the last copy out."""
+
+    def __init__(self, bp: BatchedPlan, device=None):
+        dev = torch.device("cuda", torch.cuda.current_device()) if device is None else torch.device(device)
+        self.bp = bp
+        self.dev = dev
+        self.s_in, self.s_run, self.s_out = (torch.cuda.Stream(dev) for _ in range(3))
+        self.alm = [torch.empty(bp.total_alm, dtype=torch.complex64, device=dev) for _ in range(2)]
+        self.res = [torch.empty(bp.total_alm, dtype=torch.complex64, device=dev) for _ in range(2)]
+        self.maps = torch.empty(bp.total_pix, dtype=torch.float32, device=dev)
+        self.in_ready = [torch.cuda.Event() for _ in range(2)]
+        self.ran = [torch.cuda.Event() for _ in range(2)]
+        self.copied = [torch.cuda.Event() for _ in range(2)]
+        self.used = [False, False]
+
+    def run(self, inputs, outputs):
+        for x in list(inputs) + list(outputs):
+            if x.is_cuda or x.dtype != torch.complex64 or x.numel() != self.bp.total_alm or not x.is_pinned():
+                raise ValueError("HostPipeline.run takes pinned complex64 host tensors of the plan's alm size")
+        for i, (hin, hout) in enumerate(zip(inputs, outputs)):
+            s = i & 1
+            if self.used[s]:  # buffer set s is free once batch i-2 ran and was copied out
+                self.s_in.wait_event(self.ran[s])
+            with torch.cuda.stream(self.s_in):
+                self.alm[s].copy_(hin.reshape(-1), non_blocking=True)
+                self.in_ready[s].record(self.s_in)
+            self.s_run.wait_event(self.in_ready[s])
+            if self.used[s]:
+                self.s_run.wait_event(self.copied[s])
+            with torch.cuda.stream(self.s_run):
+                self.bp.alm2map(self.alm[s], out=self.maps)
+                self.bp.map2alm(self.maps, out=self.res[s])
+                self.ran[s].record(self.s_run)
+            self.s_out.wait_event(self.ran[s])
+            with torch.cuda.stream(self.s_out):
+                hout.reshape(-1).copy_(self.res[s], non_blocking=True)
+                self.copied[s].record(self.s_out)
+            self.used[s] = True
+
+    def wait_on(self, stream: torch.cuda.Stream) -> None:
+        """Make `stream` wait for everything queued so far (for timing with events on it)."""
+        for s in (self.s_in, self.s_run, self.s_out):
+            stream.wait_stream(s)
+
+    def synchronize(self) -> None:
+        self.s_out.synchronize()

@@ -130,34 +130,46 @@ static int alm2map_spin_impl(const hb_plan *p, int nmaps, const void *E, const v
                                  st);
 }
 
-// alm2cl (alm_ops.py:19-32): one thread per l, m-loop over the l-contiguous healpy columns,
-// FP64 accumulation.
+// alm2cl (alm_ops.py:19-32): a CTA owns 32 consecutive l of one map (the lanes) and its 8 warps
+// split the m range (m = warp mod 8), so every warp load reads 32 consecutive l of one healpy
+// m-column (256 B); FP64 accumulation, one shared-memory reduction over the warps, no atomics.
 template <typename V>
-__global__ void alm2cl_kernel(int lmax, int mmax, const V *__restrict__ a1, const V *__restrict__ a2, int64_t stride,
-                              double *__restrict__ cl) {
-    const int l = blockIdx.x * blockDim.x + threadIdx.x;
-    const int b = blockIdx.y;
-    if (l > lmax) return;
+__global__ void __launch_bounds__(256) alm2cl_kernel(int lmax, int mmax, const V *__restrict__ a1,
+                                                     const V *__restrict__ a2, int64_t stride, double *__restrict__ cl) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int l = blockIdx.x * 32 + lane, b = blockIdx.y;
     const V *p1 = a1 + b * stride, *p2 = (a2 ? a2 : a1) + b * stride;
     const int mtop = l < mmax ? l : mmax;
-    double acc0 = 0.0, acc = 0.0;
-    {
-        V u = p1[l], v = p2[l];
-        acc0 = (double)u.x * (double)v.x + (double)u.y * (double)v.y;
-    }
-    for (int m = 1; m <= mtop; ++m) {
+    auto term = [&](int m) -> double {
         const int64_t k = alm_idx(lmax, l, m);
-        V u = p1[k], v = p2[k];
-        acc += (double)u.x * (double)v.x + (double)u.y * (double)v.y;
+        const V u = p1[k], v = p2[k];
+        return (m == 0 ? 1.0 : 2.0) * ((double)u.x * (double)v.x + (double)u.y * (double)v.y);
+    };
+    double acc = 0.0;
+    if (l <= lmax) {
+        int m = warp;
+        for (; m + 24 <= mtop; m += 32) {  // four independent loads in flight per thread
+            const double t0 = term(m), t1 = term(m + 8), t2 = term(m + 16), t3 = term(m + 24);
+            acc += (t0 + t1) + (t2 + t3);
+        }
+        for (; m <= mtop; m += 8) acc += term(m);
     }
-    cl[(int64_t)b * (lmax + 1) + l] = (acc0 + 2.0 * acc) / (2.0 * l + 1.0);
+    __shared__ double red[8][33];
+    red[warp][lane] = acc;
+    __syncthreads();
+    if (warp == 0 && l <= lmax) {
+        double s = 0.0;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) s += red[w][lane];
+        cl[(int64_t)b * (lmax + 1) + l] = s / (2.0 * l + 1.0);
+    }
 }
 
 template <typename V>
 static int alm2cl_impl(int lmax, int mmax, int nmaps, const V *a1, const V *a2, double *cl, cudaStream_t st) {
     if (lmax < 0 || mmax < 0 || mmax > lmax || nmaps <= 0 || nmaps > 65535 || !a1 || !cl)
         return fail(HB_ERR_INVALID, "hb_alm2cl: bad arguments");
-    dim3 grid((unsigned)((lmax + 256) / 256), (unsigned)nmaps);
+    dim3 grid((unsigned)((lmax + 32) / 32), (unsigned)nmaps);
     alm2cl_kernel<V><<<grid, 256, 0, st>>>(lmax, mmax, a1, a2, alm_size(lmax, mmax), cl);
     HB_CHECK_LAUNCH();
     return HB_OK;

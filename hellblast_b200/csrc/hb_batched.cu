@@ -49,7 +49,7 @@ struct TcGroup {
     int64_t gm_stride;
     // analysis
     const uint4 *g_tiles;    // [m][pc][4][N x 32] 16-bit
-    float *dscale;           // [mmax+1] power-of-two scale of the batch operand per m (set by the prep kernels)
+    float *dscale;           // [mmax+1][N/2] power-of-two scale of the batch operand per (m, map column)
     int64_t alm_out_ofs;     // this group's first alm in the caller's output buffer (complex elements)
     int64_t alm_stride;
 };
@@ -84,93 +84,102 @@ __device__ __forceinline__ float block_pow2_scale(float vmax) {
     return res;
 }
 
+// Both prep kernels: one CTA per (m, map of the group).  The CTA reads the map's m-slice of the
+// batch operand once, coalesced, into shared memory (one pad entry per 8 or 16 so that the
+// per-thread runs below hit distinct banks), takes its maximum |value| for the power-of-two scale
+// of this (m, map), then each thread turns one run of 8 consecutive K positions into the hi/lo
+// rows of the K-major core matrices (row n = 2 map + re/im; element (n, k) at
+// (n%8)*8 + (n/8)*256 + (k/8)*64 + k%8), written as 16-byte stores; a thread's re and im rows
+// are adjacent and fill one 32-byte sector.  Map columns past the group's maps get zeros.
+template <bool BF16>
+__device__ __forceinline__ void store_rows8(uint4 *chunk, int N, int qh, int n, int g, const float (&v)[8]) {
+    uint4 hi, lo;
+    tc::split8<BF16>(v, hi, lo);
+    const int64_t e = (int64_t)(2 * qh) * N * 32 + (n & 7) * 8 + (n >> 3) * 256 + g * 64;  // 16-bit elements
+    chunk[e / 8] = hi;
+    chunk[(e + (int64_t)N * 32) / 8] = lo;
+}
+
 // alm [map][nalm] complex64 -> per (m, 64-l chunk) the synthesis B tiles:
-// [q][h][N rows (2*map + re/im) x 32 K (l = l0 + 2k + q)], K-major core matrices
-// (row%8)*16 B + (row/8)*512 B + (k/8)*128 B.
+// [q][h][N rows x 32 K (l = l0 + 2k + q)].
 template <int N, bool BF16>
-__global__ void prep_alm_tiles_kernel(const TcGroup *groups, int gi, const float2 *__restrict__ alm, int64_t alm_stride) {
-    using H = tc::Half16<BF16>;
+__global__ void __launch_bounds__(256) prep_alm_tiles_kernel(const TcGroup *groups, int gi, const float2 *__restrict__ alm,
+                                                             int64_t alm_stride) {
+    extern __shared__ float2 sa[];  // l - m = i at i + i / 16
     const TcGroup &G = groups[gi];
-    const int m = blockIdx.x;
+    const int m = blockIdx.x, b = blockIdx.y;
     if (m > G.mmax) return;
     const int lmax = G.lmax;
     const int nch = (lmax - m + 64) / 64;
-    typename H::t *base = (typename H::t *)(G.alm_tiles + G.alm_tile_ofs[m] * (16 * N));
-    const int per_chunk = N * 64;  // (n, k, q)
-    auto value = [&](int idx) -> float {
-        const int c = idx / per_chunk, r = idx % per_chunk;
-        const int n = r / 64, kq = r % 64;
-        const int l = m + 64 * c + kq;
-        const int b = n >> 1;
-        if (l > lmax || b >= G.nmaps) return 0.f;
-        const float2 a = alm[(int64_t)b * alm_stride + alm_idx(lmax, l, m)];
-        return (n & 1) ? a.y : a.x;
-    };
+    const bool live = b < G.nmaps;
+    const float2 *src = alm + (int64_t)b * alm_stride + alm_idx(lmax, m, m);
     float vmax = 0.f;
-    for (int idx = threadIdx.x; idx < nch * per_chunk; idx += blockDim.x) vmax = fmaxf(vmax, fabsf(value(idx)));
-    const float s = block_pow2_scale(vmax);
-    if (threadIdx.x == 0) G.dscale[m] = s;
-    for (int idx = threadIdx.x; idx < nch * per_chunk; idx += blockDim.x) {
-        const int c = idx / per_chunk, r = idx % per_chunk;
-        const int n = r / 64, kq = r % 64, k = kq >> 1, q = kq & 1;
-        const float v = value(idx) * s;
-        const typename H::t hi = H::one(v);
-        const typename H::t lo = H::one(v - H::back(hi));
-        const int64_t off = (n & 7) * 8 + (n >> 3) * 256 + (k >> 3) * 64 + (k & 7);
-        typename H::t *chunk = base + (int64_t)c * (4 * N * 32);
-        chunk[(q * 2 + 0) * N * 32 + off] = hi;
-        chunk[(q * 2 + 1) * N * 32 + off] = lo;
+    for (int i = threadIdx.x; i < nch * 64; i += blockDim.x) {
+        const float2 v = (live && m + i <= lmax) ? src[i] : make_float2(0.f, 0.f);
+        sa[i + (i >> 4)] = v;
+        vmax = fmaxf(vmax, fmaxf(fabsf(v.x), fabsf(v.y)));
+    }
+    const float s = block_pow2_scale(vmax);  // barriers: the slice is in shared memory after it
+    if (threadIdx.x == 0) G.dscale[(int64_t)m * (N / 2) + b] = s;
+    uint4 *base = const_cast<uint4 *>(G.alm_tiles) + G.alm_tile_ofs[m] * (16 * N);
+    for (int it = threadIdx.x; it < nch * 4; it += blockDim.x) {  // (chunk c, k8 group g): l = l0 + 16 g + 0..15
+        const int c = it >> 2, g = it & 3;
+        const float2 *run = sa + 17 * it;  // 16 (it) + it
+        uint4 *chunk = base + (int64_t)c * (16 * N);
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            float re[8], im[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const float2 v = run[2 * k + q];
+                re[k] = v.x * s;
+                im[k] = v.y * s;
+            }
+            store_rows8<BF16>(chunk, N, q, 2 * b, g, re);
+            store_rows8<BF16>(chunk, N, q, 2 * b + 1, g, im);
+        }
     }
 }
 
 // F [map][m][pair][2] -> per (m, 32-pair chunk) the analysis B tiles [q][h][N x 32 pairs]
-// (E = F_N + F_S for q = 0, O = F_N - F_S for q = 1), K-major like above.
+// (E = F_N + F_S for q = 0, O = F_N - F_S for q = 1).
 template <int N, bool BF16>
-__global__ void prep_g_tiles_kernel(const TcGroup *groups, int gi, const float2 *__restrict__ F, int64_t f_stride) {
-    using H = tc::Half16<BF16>;
+__global__ void __launch_bounds__(512) prep_g_tiles_kernel(const TcGroup *groups, int gi, const float2 *__restrict__ F,
+                                                           int64_t f_stride) {
+    extern __shared__ float4 sf[];  // pair p (north, south) at p + p / 8
     const TcGroup &G = groups[gi];
-    const int m = blockIdx.x;
+    const int m = blockIdx.x, b = blockIdx.y;
     if (m > G.mmax) return;
     const int64_t np = G.g.npairs;
-    typename H::t *base = (typename H::t *)(G.g_tiles + (int64_t)m * G.npc * (16 * N));
-    const int per_chunk = N * 32;
-    auto eo = [&](int64_t idx, float &e, float &o) {
-        const int64_t c = idx / per_chunk;
-        const int r = (int)(idx % per_chunk);
-        const int n = r / 32, k = r % 32;
-        const int64_t p = c * 32 + k;
-        const int b = n >> 1;
-        e = o = 0.f;
-        if (p < np && b < G.nmaps) {
-            const float2 *f = F + (int64_t)b * f_stride + ((int64_t)m * np + p) * 2;
-            const float2 fn = f[0], fs = f[1];
-            e = (n & 1) ? fn.y + fs.y : fn.x + fs.x;
-            o = (n & 1) ? fn.y - fs.y : fn.x - fs.x;
-        }
-    };
+    const int npc = (int)G.npc;
+    const bool live = b < G.nmaps;
+    const float4 *src = reinterpret_cast<const float4 *>(F + (int64_t)b * f_stride + (int64_t)m * np * 2);
     float vmax = 0.f;
-    for (int64_t idx = threadIdx.x; idx < G.npc * per_chunk; idx += blockDim.x) {
-        float e, o;
-        eo(idx, e, o);
-        vmax = fmaxf(vmax, fmaxf(fabsf(e), fabsf(o)));
+    for (int p = threadIdx.x; p < npc * 32; p += blockDim.x) {
+        const float4 f = (live && p < np) ? src[p] : make_float4(0.f, 0.f, 0.f, 0.f);
+        sf[p + (p >> 3)] = f;
+        vmax = fmaxf(vmax, fmaxf(fmaxf(fabsf(f.x + f.z), fabsf(f.y + f.w)), fmaxf(fabsf(f.x - f.z), fabsf(f.y - f.w))));
     }
     const float s = block_pow2_scale(vmax);
-    if (threadIdx.x == 0) G.dscale[m] = s;
-    for (int64_t idx = threadIdx.x; idx < G.npc * per_chunk; idx += blockDim.x) {
-        float e, o;
-        eo(idx, e, o);
-        e *= s;
-        o *= s;
-        const int64_t c = idx / per_chunk;
-        const int r = (int)(idx % per_chunk);
-        const int n = r / 32, k = r % 32;
-        const int64_t off = (n & 7) * 8 + (n >> 3) * 256 + (k >> 3) * 64 + (k & 7);
-        typename H::t *chunk = base + c * (4 * N * 32);
-        const typename H::t ehi = H::one(e), ohi = H::one(o);
-        chunk[0 * N * 32 + off] = ehi;
-        chunk[1 * N * 32 + off] = H::one(e - H::back(ehi));
-        chunk[2 * N * 32 + off] = ohi;
-        chunk[3 * N * 32 + off] = H::one(o - H::back(ohi));
+    if (threadIdx.x == 0) G.dscale[(int64_t)m * (N / 2) + b] = s;
+    uint4 *base = const_cast<uint4 *>(G.g_tiles) + (int64_t)m * npc * (16 * N);
+    for (int it = threadIdx.x; it < npc * 4; it += blockDim.x) {  // (chunk c, k8 group g): pairs 8 it .. 8 it + 7
+        const int c = it >> 2, g = it & 3;
+        const float4 *run = sf + 9 * it;
+        uint4 *chunk = base + (int64_t)c * (16 * N);
+        float er[8], ei[8], orr[8], oi[8];
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+            const float4 f = run[j];
+            er[j] = (f.x + f.z) * s;
+            ei[j] = (f.y + f.w) * s;
+            orr[j] = (f.x - f.z) * s;
+            oi[j] = (f.y - f.w) * s;
+        }
+        store_rows8<BF16>(chunk, N, 0, 2 * b, g, er);
+        store_rows8<BF16>(chunk, N, 0, 2 * b + 1, g, ei);
+        store_rows8<BF16>(chunk, N, 1, 2 * b, g, orr);
+        store_rows8<BF16>(chunk, N, 1, 2 * b + 1, g, oi);
     }
 }
 
@@ -442,7 +451,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             }
             tc::fence_after();
             const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
-            const float inv = 1.0f / (LS * G.dscale[m]);
+            const float *scl = G.dscale + (int64_t)m * (N / 2);
             const int nsets = nch < S ? nch : S;
 #pragma unroll 1
             for (int j = wg; j < N / 16; j += 2) {
@@ -454,6 +463,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         const int b = j * 8 + h;
                         if (b < G.nmaps) {
                             float2 *dst = G.Gm + (int64_t)b * G.gm_stride + ((int64_t)m * np + p) * 2;
+                            const float inv = 1.0f / (LS * scl[b]);
                             const float re = de[2 * h] * inv, im = de[2 * h + 1] * inv, ro = dd[2 * h] * inv,
                                         io = dd[2 * h + 1] * inv;
                             *reinterpret_cast<float4 *>(dst) = make_float4(re + ro, im + io, re - ro, im - io);
@@ -639,7 +649,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             const int row = owner * 32 + lane;
             const int le = l0 + 2 * row;
             const uint32_t taddr = tmem + ((uint32_t)(owner * 32) << 16);
-            const float inv = 1.0f / (LS * G.dscale[m]);
+            const float *scl = G.dscale + (int64_t)m * (N / 2);
             const int nsets = npc < S ? npc : S;
 #pragma unroll 1
             for (int j = half; j < N / 16; j += 2) {
@@ -650,6 +660,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     const int b = j * 8 + h;
                     if (b < G.nmaps) {
                         float2 *dst = alm_out + G.alm_out_ofs + (int64_t)b * G.alm_stride + alm_idx(lmax, le, m);
+                        const float inv = 1.0f / (LS * scl[b]);
                         if (le <= lmax) dst[0] = make_float2(de[2 * h] * inv, de[2 * h + 1] * inv);
                         if (le + 1 <= lmax) dst[1] = make_float2(dd[2 * h] * inv, dd[2 * h + 1] * inv);
                     }
@@ -752,6 +763,7 @@ struct hb_batched_plan {
     size_t bytes = 0;
     bool profile = false;
     cudaEvent_t ev[8] = {};  // synthesis: 0 prep 1 tensor 2 ring 3 end; analysis: 4 ring 5 prep 6 tensor 7 end
+    cudaGraphExec_t graph = nullptr;  // hb_batched_graph_capture
     int64_t total_maps = 0, total_pix = 0, total_alm = 0;
 };
 
@@ -793,13 +805,19 @@ static int launch_ana(hb_batched_plan *bp, float2 *alm_out, cudaStream_t st) {
 }
 template <int N, bool BF16>
 static int launch_prep_alm(hb_batched_plan *bp, int gi, const float2 *alm, int64_t stride, cudaStream_t st) {
-    prep_alm_tiles_kernel<N, BF16><<<bp->hgroups[gi].mmax + 1, 256, 0, st>>>(bp->dgroups, gi, alm, stride);
+    const TcGroup &G = bp->hgroups[gi];
+    const int smem = (int)(sizeof(float2) * (size_t)(((G.lmax + 64) / 64) * 68));  // 64 l + 4 pads per chunk
+    HB_CUDA_TRY(cudaFuncSetAttribute(prep_alm_tiles_kernel<N, BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    prep_alm_tiles_kernel<N, BF16><<<dim3(G.mmax + 1, N / 2), 256, smem, st>>>(bp->dgroups, gi, alm, stride);
     HB_CHECK_LAUNCH();
     return HB_OK;
 }
 template <int N, bool BF16>
 static int launch_prep_g(hb_batched_plan *bp, int gi, const float2 *F, int64_t stride, cudaStream_t st) {
-    prep_g_tiles_kernel<N, BF16><<<bp->hgroups[gi].mmax + 1, 256, 0, st>>>(bp->dgroups, gi, F, stride);
+    const TcGroup &G = bp->hgroups[gi];
+    const int smem = (int)(sizeof(float4) * (size_t)(G.npc * 36));  // 32 pairs + 4 pads per chunk
+    HB_CUDA_TRY(cudaFuncSetAttribute(prep_g_tiles_kernel<N, BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
+    prep_g_tiles_kernel<N, BF16><<<dim3(G.mmax + 1, N / 2), 512, smem, st>>>(bp->dgroups, gi, F, stride);
     HB_CHECK_LAUNCH();
     return HB_OK;
 }
@@ -849,7 +867,7 @@ int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int np
         offs[i].tofs = carve(8 * (size_t)(p->mmax + 2));
         offs[i].tiles_a = carve((size_t)ng * chunks_a[i] * 256 * N);
         offs[i].tiles_g = carve((size_t)ng * (p->mmax + 1) * ((np + 31) / 32) * 256 * N);
-        offs[i].scales = carve((size_t)ng * 4 * (p->mmax + 1));
+        offs[i].scales = carve((size_t)ng * 4 * (p->mmax + 1) * (N / 2));
         int64_t nblocks = 0;  // 256-l blocks over all m, the plan's checkpoint layout
         for (int m = 0; m <= p->mmax; ++m) nblocks += (p->lmax - m) / 256 + 1;
         offs[i].coef = carve((size_t)nblocks * 256 * sizeof(float2));
@@ -938,7 +956,7 @@ int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int np
                 G.gm_stride = bp->parts[i].gf_stride;
                 G.g_tiles = (const uint4 *)(base + offs[i].tiles_g) +
                             (size_t)k * (p->mmax + 1) * G.npc * 16 * N;
-                G.dscale = (float *)(base + offs[i].scales) + (size_t)k * (p->mmax + 1);
+                G.dscale = (float *)(base + offs[i].scales) + (size_t)k * (p->mmax + 1) * (N / 2);
                 G.alm_stride = alm_size(p->lmax, p->mmax);
                 G.alm_out_ofs = bp->parts[i].alm_ofs + (int64_t)GM * k * G.alm_stride;
             }
@@ -976,6 +994,7 @@ int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int np
 
 int hb_batched_plan_destroy(hb_batched_plan *bp) {
     if (!bp) return HB_OK;
+    if (bp->graph) cudaGraphExecDestroy(bp->graph);
     for (auto &e : bp->ev)
         if (e) cudaEventDestroy(e);
     cudaFree(bp->base);
@@ -1030,6 +1049,42 @@ int hb_batched_map2alm(hb_batched_plan *bp, const float *maps, float *alm, hb_st
     if (bp->profile) HB_CUDA_TRY(cudaEventRecord(bp->ev[6], st));
     if ((rc = HB_DISPATCH_N(bp, launch_ana)(bp, (float2 *)alm, st))) return rc;
     if (bp->profile) HB_CUDA_TRY(cudaEventRecord(bp->ev[7], st));
+    return HB_OK;
+}
+
+int hb_batched_graph_capture(hb_batched_plan *bp, const float *alm, float *maps, float *alm_out) {
+    if (!bp || !maps || (!alm && !alm_out)) return fail(HB_ERR_INVALID, "hb_batched_graph_capture: bad arguments");
+    cudaStream_t s = nullptr;
+    HB_CUDA_TRY(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+    const bool prof = bp->profile;
+    bp->profile = false;  // no event records inside the graph
+    int rc = HB_OK;
+    cudaGraph_t graph = nullptr;
+    if (cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal) != cudaSuccess) {
+        rc = fail(HB_ERR_CUDA, "hb_batched_graph_capture: begin capture failed");
+    } else {
+        if (alm) rc = hb_batched_alm2map(bp, alm, maps, s);
+        if (rc == HB_OK && alm_out) rc = hb_batched_map2alm(bp, maps, alm_out, s);
+        const cudaError_t e = cudaStreamEndCapture(s, &graph);
+        if (rc == HB_OK && e != cudaSuccess)
+            rc = fail(HB_ERR_CUDA, std::string("hb_batched_graph_capture: ") + cudaGetErrorString(e));
+    }
+    bp->profile = prof;
+    cudaGraphExec_t exec = nullptr;
+    if (rc == HB_OK && cudaGraphInstantiate(&exec, graph, 0) != cudaSuccess)
+        rc = fail(HB_ERR_CUDA, "hb_batched_graph_capture: instantiate failed");
+    if (graph) cudaGraphDestroy(graph);
+    cudaStreamDestroy(s);
+    cudaGetLastError();
+    if (rc != HB_OK) return rc;
+    if (bp->graph) cudaGraphExecDestroy(bp->graph);
+    bp->graph = exec;
+    return HB_OK;
+}
+
+int hb_batched_graph_launch(hb_batched_plan *bp, hb_stream_t stream) {
+    if (!bp || !bp->graph) return fail(HB_ERR_INVALID, "hb_batched_graph_launch: no captured graph");
+    HB_CUDA_TRY(cudaGraphLaunch(bp->graph, (cudaStream_t)stream));
     return HB_OK;
 }
 

@@ -9,20 +9,31 @@
 // Bluestein chirp-z transform (power-of-two convolution of length L >= 2N-1, chirp spectra
 // precomputed per distinct N in the geometry) otherwise.
 //
-// Work decomposition: one CTA per (ring pair, map); it transforms the pair's north ring, then
-// its south ring, in one shared-memory buffer, so the two halves of each F(m, pair) entry are
-// written close together in time (and adjacent pairs run side by side), which lets L2 merge the
-// partial sector writes.  Pairs are launched in classes of equal convolution length, each class
-// with its own shared-memory size.
+// Work decomposition: one CTA per (ring pair, map), pairs fastest in the grid; it transforms
+// the pair's north ring, then its south ring, in one shared-memory buffer.  The analysis keeps
+// the north ring's F(m) in shared memory and writes each m's (north, south) entry as one vector
+// store, so two neighbouring CTAs fill each 32-byte sector of F.  Pairs are launched in classes
+// of equal convolution length, each class with its own shared-memory size.
 //
-// FFT engine: in-place radix-8 stages (radix 4 or 2 for the last one) in shared memory.  The
-// forward transform is decimation-in-frequency (natural order in, digit-reversed out), the
-// inverse is its exact mirror, decimation-in-time (digit-reversed in, natural out), so no
-// reordering pass exists.  Twiddles come from one table per geometry, W^j = exp(-2 pi i j/Lmax)
-// for j < Lmax/2 (FP64-computed, rounded for FP32).  The per-m factors of the untangling
-// (exp(-2 pi i k/n)), the ring phase (exp(-i m phi0)) and the Bluestein chirp
-// (exp(-i pi q/N)) are products of two entries of small per-ring tables (64 fine steps x
-// coarse steps), built per CTA with a few hundred FP64 sincospi.
+// FFT engine: a length L = 2^logL transform runs logL / 4 radix-16 stages and, when logL % 4 = r
+// is not zero, one radix-2^r stage.  Every stage is a pass in registers: each thread loads the
+// R points of a butterfly, transforms them and stores them back, with one barrier per pass.
+// The passes at the ends read from or write to global memory directly where the order allows:
+//   * analysis, direct ring: decimation in frequency (DIF) from the ring in global memory; the
+//     untangling reads the digit-ordered spectrum;
+//   * analysis, Bluestein ring: DIF from global memory times the chirp, then one fused pass
+//     (last DIF stage, product with the stored chirp spectrum, first inverse DIT stage), then
+//     the inverse decimation-in-time (DIT) stages, which leave natural order;
+//   * synthesis, direct ring: the Hermitian spectrum is built from the folded T_m in one pass,
+//     then inverse DIF and a digit-order read for the coalesced ring store;
+//   * synthesis, Bluestein ring: the same fused middle, and the last inverse DIT pass writes the
+//     ring to global memory.
+// Twiddles come from one table per geometry, W^j = exp(-2 pi i j/Lmax), j < Lmax/2
+// (FP64-computed, rounded for FP32): a radix-16 butterfly loads W^p, W^2p, W^4p, W^8p and forms
+// the others by at most three products.  The Bluestein chirp exp(-i pi j^2/N) is a stored table
+// per distinct N (after its spectrum).  The per-m factors of the untangling (exp(-2 pi i k/n))
+// and the ring phase (exp(-i m phi0)) are products of two entries of small per-ring tables
+// (64 fine steps x coarse steps), built per CTA with a few hundred FP64 sincospi.
 //
 // Fused into the m-major write (the reference has none of these, see sht_raw.py:41,51):
 //   * the per-pixel quadrature weight 2*pi*w_r/nphi_r,
@@ -36,30 +47,28 @@
 
 namespace hb {
 
-// ------------------------------------------------------------------------------ FFT engine
-// Stage plan of a length-2^logL transform: logL / 3 radix-8 stages, then one radix-2^(logL % 3)
-// stage.  Stage i works on sub-transforms of size S_i = 2^(logL - 3i).
-
-// Digit reversal between frequency k and its position p in the forward transform's output:
-// p holds k's base-8 digits (lowest first) from the top down, then k's top logL % 3 bits.
-// Computed as a full bit reversal plus a fix-up that restores the bit order inside each digit.
-__device__ __forceinline__ unsigned digit_fix(unsigned x, int logL) {
-    const int n8 = logL / 3, rem = logL - 3 * n8;
-    const unsigned low = (1u << (3 * n8)) - 1u;
-    const unsigned g = x & low, hi = x & ~low;
-    const unsigned m0 = 0x49249249u & low;
-    const unsigned gf = (g & (m0 << 1)) | ((g & m0) << 2) | ((g & (m0 << 2)) >> 2);
-    const unsigned hf = rem == 2 ? (((hi >> 1) & (1u << (3 * n8))) | ((hi << 1) & (2u << (3 * n8)))) : hi;
-    return gf | hf;
+// ------------------------------------------------------------------------------ FFT plan
+// Digit order: DIF takes natural order to the order in which position p of frequency k holds
+// k's base-16 digits (lowest first) from the top down, then k's top r bits:
+//   p = (nibble_reverse(k mod 16^a) << r) | (k >> 4a),  a = logL / 4, r = logL % 4.
+// DIT (the mirror) takes digit order back to natural order.
+__device__ __forceinline__ unsigned nibrev(unsigned x, int a) {  // reverse the order of the a low nibbles
+    if (a == 0) return 0u;
+    x = __byte_perm(x, 0u, 0x0123);
+    x = ((x >> 4) & 0x0F0F0F0Fu) | ((x & 0x0F0F0F0Fu) << 4);
+    return x >> (32 - 4 * a);
 }
-__device__ __forceinline__ unsigned brev_n(unsigned x, int logL) { return logL ? __brev(x) >> (32 - logL) : 0u; }
-__device__ __forceinline__ int freq_to_pos(int k, int logL) { return (int)brev_n(digit_fix((unsigned)k, logL), logL); }
-__device__ __forceinline__ int pos_to_freq(int p, int logL) { return (int)digit_fix(brev_n((unsigned)p, logL), logL); }
+__device__ __forceinline__ int pos_of_freq(int k, int logL) {
+    const int a = logL >> 2, r = logL & 3;
+    const unsigned low = (1u << (4 * a)) - 1u;
+    return (int)((nibrev((unsigned)k & low, a) << r) | ((unsigned)k >> (4 * a)));
+}
 
-// Shared-memory FFT buffers carry one pad element per 16: the late stages' strided accesses and
-// the digit-reversed reads then spread over the banks.
-template <bool PAD> __device__ __forceinline__ int ph(int i) { return PAD ? i + (i >> 4) : i; }
-__host__ __device__ __forceinline__ int padded_len(int L) { return L + (L >> 4) + 1; }
+// Shared-memory FFT buffers carry one pad element per 16 and one more per 256: every pass's
+// half-warp accesses (stride 1 within a butterfly row, stride 16 in the last radix-16 stage,
+// stride 2^r in the remainder stage) and the digit-order reads then spread over the banks.
+__device__ __forceinline__ int ph(int i) { return i + (i >> 4) + (i >> 8); }
+__host__ __device__ __forceinline__ int padded_len(int L) { return L + (L >> 4) + (L >> 8) + 1; }
 
 template <typename T> struct Tw {
     using V = c2_t<T>;
@@ -116,8 +125,54 @@ template <bool INV, typename V> __device__ __forceinline__ void dft8(V *x) {
     x[7] = csub(e3, o3);
 }
 
+// x *= exp(-+ 2 pi i e / 16) for the constant exponents of the radix-16 butterfly
+template <int E, bool INV, typename V> __device__ __forceinline__ V w16(V a) {
+    using T = decltype(a.x);
+    constexpr double C[10] = {1.0, 0.92387953251128675612818318939678828682, 0.70710678118654752440084436210484903928,
+                              0.38268343236508977172845998403039886676, 0.0, -0.38268343236508977172845998403039886676,
+                              -0.70710678118654752440084436210484903928, -0.92387953251128675612818318939678828682, -1.0,
+                              -0.92387953251128675612818318939678828682};
+    constexpr double S[10] = {0.0, 0.38268343236508977172845998403039886676, 0.70710678118654752440084436210484903928,
+                              0.92387953251128675612818318939678828682, 1.0, 0.92387953251128675612818318939678828682,
+                              0.70710678118654752440084436210484903928, 0.38268343236508977172845998403039886676, 0.0,
+                              -0.38268343236508977172845998403039886676};
+    if constexpr (E == 0) return a;
+    else if constexpr (E == 4) return rot90<INV>(a);
+    else {
+        const T c = (T)C[E], s = INV ? (T)S[E] : (T)(-S[E]);  // (c, s) = cos - +i sin
+        return mk2(a.x * c - a.y * s, a.x * s + a.y * c);
+    }
+}
+
+// 16-point DFT as 4 x 4: inner DFT-4 over n2 (n = n1 + 4 n2), twiddles W16^(n1 k2), outer
+// DFT-4 over n1; X[4 k1 + k2] ends in register k1 + 4 k2 and is renamed into place.
+template <bool INV, typename V> __device__ __forceinline__ void dft16(V *x) {
+#pragma unroll
+    for (int n1 = 0; n1 < 4; ++n1) dft4<INV>(x[n1], x[n1 + 4], x[n1 + 8], x[n1 + 12]);
+    x[5] = w16<1, INV>(x[5]);
+    x[9] = w16<2, INV>(x[9]);
+    x[13] = w16<3, INV>(x[13]);
+    x[6] = w16<2, INV>(x[6]);
+    x[10] = w16<4, INV>(x[10]);
+    x[14] = w16<6, INV>(x[14]);
+    x[7] = w16<3, INV>(x[7]);
+    x[11] = w16<6, INV>(x[11]);
+    x[15] = w16<9, INV>(x[15]);
+#pragma unroll
+    for (int k2 = 0; k2 < 4; ++k2) dft4<INV>(x[4 * k2], x[4 * k2 + 1], x[4 * k2 + 2], x[4 * k2 + 3]);
+    V y[16];
+#pragma unroll
+    for (int k1 = 0; k1 < 4; ++k1)
+#pragma unroll
+        for (int k2 = 0; k2 < 4; ++k2) y[4 * k1 + k2] = x[k1 + 4 * k2];
+#pragma unroll
+    for (int i = 0; i < 16; ++i) x[i] = y[i];
+}
+
 template <int R, bool INV, typename V> __device__ __forceinline__ void dftR(V *x) {
-    if constexpr (R == 8)
+    if constexpr (R == 16)
+        dft16<INV>(x);
+    else if constexpr (R == 8)
         dft8<INV>(x);
     else if constexpr (R == 4)
         dft4<INV>(x);
@@ -125,81 +180,142 @@ template <int R, bool INV, typename V> __device__ __forceinline__ void dftR(V *x
         dft2<INV>(x);
 }
 
-// x[q] *= W_S^(pos q) (conjugated for INV), q = 1 .. R-1; radix 8 loads W^pos, W^2pos, W^4pos
-// and forms the other four by products (about two roundings more)
+template <int R> struct Log2R {
+    static constexpr int v = R == 16 ? 4 : (R == 8 ? 3 : (R == 4 ? 2 : 1));
+};
+
+// x[q] *= W_S^(pos q) (conjugated for INV), q = 1 .. R-1.  Radix 16 and 8 load W^pos, W^2pos,
+// W^4pos (and W^8pos) and form the other factors by at most three products.
 template <int R, bool INV, typename T>
 __device__ __forceinline__ void twiddle_apply(c2_t<T> *x, const Tw<T> &tw, int pos, int logS) {
     using V = c2_t<T>;
-    if constexpr (R == 8) {
+    auto app = [&](int q, V wq) { x[q] = cmul(x[q], INV ? cconj(wq) : wq); };
+    if constexpr (R == 16) {
+        const V w1 = tw.w(pos, logS), w2 = tw.w(2 * pos, logS), w4 = tw.w(4 * pos, logS), w8 = tw.w(8 * pos, logS);
+        const V w3 = cmul(w1, w2), w5 = cmul(w4, w1), w6 = cmul(w4, w2), w7 = cmul(w4, w3);
+        app(1, w1); app(2, w2); app(3, w3); app(4, w4); app(5, w5); app(6, w6); app(7, w7); app(8, w8);
+        app(9, cmul(w8, w1)); app(10, cmul(w8, w2)); app(11, cmul(w8, w3)); app(12, cmul(w8, w4));
+        app(13, cmul(w8, w5)); app(14, cmul(w8, w6)); app(15, cmul(w8, w7));
+    } else if constexpr (R == 8) {
         const V w1 = tw.w(pos, logS), w2 = tw.w(2 * pos, logS), w4 = tw.w(4 * pos, logS);
         const V w3 = cmul(w1, w2);
-        V w[8] = {w1, w1, w2, w3, w4, cmul(w4, w1), cmul(w4, w2), cmul(w4, w3)};
-#pragma unroll
-        for (int q = 1; q < 8; ++q) x[q] = cmul(x[q], INV ? cconj(w[q]) : w[q]);
+        app(1, w1); app(2, w2); app(3, w3); app(4, w4);
+        app(5, cmul(w4, w1)); app(6, cmul(w4, w2)); app(7, cmul(w4, w3));
     } else {
 #pragma unroll
-        for (int q = 1; q < R; ++q) {
-            const V wq = tw.w(pos * q, logS);
-            x[q] = cmul(x[q], INV ? cconj(wq) : wq);
-        }
+        for (int q = 1; q < R; ++q) app(q, tw.w(pos * q, logS));
     }
 }
 
-// one decimation-in-frequency stage of radix R on sub-transforms of size 2^logS
-template <int R, bool PAD, typename T>
-__device__ __forceinline__ void dif_stage(c2_t<T> *buf, const Tw<T> &tw, int logL, int logS) {
+// One stage of radix R on the sub-transforms of size 2^logS (butterfly b: pos = b mod h,
+// points base + t h, h = 2^logS / R).  DIF: DFT, then twiddles on the outputs; DIT (its
+// mirror): twiddles on the inputs, then DFT.  `ld(p)` / `st(p, v)` read and write point p
+// (shared or global memory); a thread stores exactly the points it loaded.
+template <int R, bool DIT, bool INV, typename T, class Ld, class St>
+__device__ __forceinline__ void fft_pass(int logL, int logS, const Tw<T> &tw, Ld &&ld, St &&st) {
     using V = c2_t<T>;
-    constexpr int logR = R == 8 ? 3 : (R == 4 ? 2 : 1);
-    const int logh = logS - logR, h = 1 << logh;
-    for (int b = threadIdx.x; b < (1 << (logL - logR)); b += blockDim.x) {
-        const int pos = b & (h - 1);
-        const int base = ((b >> logh) << logS) + pos;
+    constexpr int lr = Log2R<R>::v;
+    const int logh = logS - lr, h = 1 << logh;
+    for (int b = threadIdx.x; b < (1 << (logL - lr)); b += blockDim.x) {
+        const int pos = b & (h - 1), base = ((b >> logh) << logS) + pos;
         V x[R];
 #pragma unroll
-        for (int t = 0; t < R; ++t) x[t] = buf[ph<PAD>(base + (t << logh))];
+        for (int t = 0; t < R; ++t) x[t] = ld(base + (t << logh));
+        if (DIT && logh > 0) twiddle_apply<R, INV>(x, tw, pos, logS);
+        dftR<R, INV>(x);
+        if (!DIT && logh > 0) twiddle_apply<R, INV>(x, tw, pos, logS);
+#pragma unroll
+        for (int q = 0; q < R; ++q) st(base + (q << logh), x[q]);
+    }
+}
+
+// Bluestein middle: the last forward DIF stage (radix R, h = 1), the product with the chirp
+// spectrum (stored in digit order), the first inverse DIT stage; all in registers.
+template <int R, typename T, class Ld, class St>
+__device__ __forceinline__ void mid_pass(int logL, const c2_t<T> *__restrict__ Bt, Ld &&ld, St &&st) {
+    using V = c2_t<T>;
+    constexpr int lr = Log2R<R>::v;
+    for (int b = threadIdx.x; b < (1 << (logL - lr)); b += blockDim.x) {
+        const int base = b << lr;
+        V x[R];
+#pragma unroll
+        for (int t = 0; t < R; ++t) x[t] = ld(base + t);
         dftR<R, false>(x);
-        twiddle_apply<R, false>(x, tw, pos, logS);
 #pragma unroll
-        for (int q = 0; q < R; ++q) buf[ph<PAD>(base + (q << logh))] = x[q];
-    }
-    __syncthreads();
-}
-
-// the exact inverse of dif_stage (times R): conjugate twiddles, then the inverse radix-R DFT
-template <int R, bool PAD, typename T>
-__device__ __forceinline__ void dit_inv_stage(c2_t<T> *buf, const Tw<T> &tw, int logL, int logS) {
-    using V = c2_t<T>;
-    constexpr int logR = R == 8 ? 3 : (R == 4 ? 2 : 1);
-    const int logh = logS - logR, h = 1 << logh;
-    for (int b = threadIdx.x; b < (1 << (logL - logR)); b += blockDim.x) {
-        const int pos = b & (h - 1);
-        const int base = ((b >> logh) << logS) + pos;
-        V x[R];
-#pragma unroll
-        for (int q = 0; q < R; ++q) x[q] = buf[ph<PAD>(base + (q << logh))];
-        twiddle_apply<R, true>(x, tw, pos, logS);
+        for (int q = 0; q < R; ++q) x[q] = cmul(x[q], Bt[base + q]);
         dftR<R, true>(x);
 #pragma unroll
-        for (int t = 0; t < R; ++t) buf[ph<PAD>(base + (t << logh))] = x[t];
+        for (int t = 0; t < R; ++t) st(base + t, x[t]);
     }
+}
+
+// stage i of the plan in DIF order (i < logL / 4: radix 16; then the radix-2^(logL % 4) stage)
+template <bool DIT, bool INV, typename T, class Ld, class St>
+__device__ __forceinline__ void fft_stage(int i, int logL, const Tw<T> &tw, Ld &&ld, St &&st) {
+    const int a = logL >> 2, r = logL & 3;
+    if (i < a) {
+        fft_pass<16, DIT, INV, T>(logL, logL - 4 * i, tw, ld, st);
+    } else if (r == 3) {
+        fft_pass<8, DIT, INV, T>(logL, 3, tw, ld, st);
+    } else if (r == 2) {
+        fft_pass<4, DIT, INV, T>(logL, 2, tw, ld, st);
+    } else {
+        fft_pass<2, DIT, INV, T>(logL, 1, tw, ld, st);
+    }
+}
+template <typename T, class Ld, class St>
+__device__ __forceinline__ void fft_mid(int logL, const c2_t<T> *Bt, Ld &&ld, St &&st) {
+    const int r = logL & 3;
+    if (r == 0) mid_pass<16, T>(logL, Bt, ld, st);
+    else if (r == 3) mid_pass<8, T>(logL, Bt, ld, st);
+    else if (r == 2) mid_pass<4, T>(logL, Bt, ld, st);
+    else mid_pass<2, T>(logL, Bt, ld, st);
+}
+__host__ __device__ __forceinline__ int fft_nstages(int logL) { return (logL >> 2) + ((logL & 3) ? 1 : 0); }
+
+// Bluestein convolution of the natural-order input `ld_in` (zero-padded to L by the caller's
+// functor): DIF forward, fused middle, inverse DIT; the last inverse stage hands its points
+// (natural order, times L) to `st_out`.  Intermediate stages use the shared buffer `buf`.
+template <typename T, class LdIn, class StOut>
+__device__ __forceinline__ void bluestein(c2_t<T> *buf, int logL, const Tw<T> &tw, const c2_t<T> *Bt, LdIn &&ld_in,
+                                          StOut &&st_out) {
+    using V = c2_t<T>;
+    auto lds = [&](int p) -> V { return buf[ph(p)]; };
+    auto sts = [&](int p, V v) { buf[ph(p)] = v; };
+    const int P = fft_nstages(logL);
+    if (P == 1) {
+        fft_mid<T>(logL, Bt, ld_in, st_out);
+        return;
+    }
+    fft_stage<false, false, T>(0, logL, tw, ld_in, sts);
     __syncthreads();
+    for (int i = 1; i < P - 1; ++i) {
+        fft_stage<false, false, T>(i, logL, tw, lds, sts);
+        __syncthreads();
+    }
+    fft_mid<T>(logL, Bt, lds, sts);
+    __syncthreads();
+    for (int i = P - 2; i > 0; --i) {
+        fft_stage<true, true, T>(i, logL, tw, lds, sts);
+        __syncthreads();
+    }
+    fft_stage<true, true, T>(0, logL, tw, lds, st_out);
 }
 
-// forward DFT of buf[0 .. 2^logL): natural order in, X_k at freq_to_pos(k) out
-template <bool PAD, typename T> __device__ void fft_fwd(c2_t<T> *buf, const Tw<T> &tw, int logL) {
-    const int n8 = logL / 3, rem = logL - 3 * n8;
-    int logS = logL;
-    for (int i = 0; i < n8; ++i, logS -= 3) dif_stage<8, PAD>(buf, tw, logL, logS);
-    if (rem == 2) dif_stage<4, PAD>(buf, tw, logL, 2);
-    if (rem == 1) dif_stage<2, PAD>(buf, tw, logL, 1);
-}
-
-// unnormalised inverse DFT: X_k at freq_to_pos(k) in, natural order out
-template <bool PAD, typename T> __device__ void fft_inv(c2_t<T> *buf, const Tw<T> &tw, int logL) {
-    const int n8 = logL / 3, rem = logL - 3 * n8;
-    if (rem == 2) dit_inv_stage<4, PAD>(buf, tw, logL, 2);
-    if (rem == 1) dit_inv_stage<2, PAD>(buf, tw, logL, 1);
-    for (int logS = rem + 3; logS <= logL; logS += 3) dit_inv_stage<8, PAD>(buf, tw, logL, logS);
+// DIF transform (forward or inverse) of the natural-order input `ld_in`; the result stays in
+// `buf` in digit order.  Ends with a barrier.
+template <bool INV, typename T, class LdIn>
+__device__ __forceinline__ void dif_to_smem(c2_t<T> *buf, int logL, const Tw<T> &tw, LdIn &&ld_in) {
+    using V = c2_t<T>;
+    auto lds = [&](int p) -> V { return buf[ph(p)]; };
+    auto sts = [&](int p, V v) { buf[ph(p)] = v; };
+    const int P = fft_nstages(logL);
+    fft_stage<false, INV, T>(0, logL, tw, ld_in, sts);
+    __syncthreads();
+    for (int i = 1; i < P; ++i) {
+        fft_stage<false, INV, T>(i, logL, tw, lds, sts);
+        __syncthreads();
+    }
 }
 
 __device__ __forceinline__ int ilog2(int L) { return 31 - __clz(L); }
@@ -235,35 +351,34 @@ template <typename T> struct Trig2 {
 };
 
 // per-ring tables in shared memory (after the FFT buffer):
-//   untangle U(k) = exp(-2 pi i k / n), k <= N;  phase P(m) = exp(-i m phi0), m <= mmax;
-//   chirp C(q) = exp(-i pi q / N), q < 2N (Bluestein rings only)
+//   untangle U(k) = exp(-2 pi i k / n), k <= N;  phase P(m) = exp(-i m phi0), m <= mmax
 template <typename T> struct RingTrig {
-    Trig2<T> U, P, C;
+    Trig2<T> U, P;
 };
 
 template <typename T> __host__ __device__ __forceinline__ int trig_entries(int Nmax, int mmax) {
-    return 3 * 64 + (Nmax >> 6) + 2 + (mmax >> 6) + 2 + ((2 * Nmax) >> 6) + 2;
+    return 2 * 64 + (Nmax >> 6) + 2 + (mmax >> 6) + 2;
 }
 
-template <typename T>
-__device__ RingTrig<T> build_trig(c2_t<T> *tab, int n, int N, double phi0_pi, int mmax, bool chirp) {
-    using V = c2_t<T>;
-    V *u1 = tab, *p1 = u1 + 64, *c1 = p1 + 64;
-    V *u2 = c1 + 64;
-    const int nu2 = (N >> 6) + 1, np2 = (mmax >> 6) + 1, nc2 = chirp ? ((2 * N) >> 6) + 1 : 0;
-    V *p2 = u2 + nu2, *c2 = p2 + np2;
+template <typename T> __device__ __forceinline__ RingTrig<T> trig_layout(c2_t<T> *tab, int N) {
+    RingTrig<T> R;
+    c2_t<T> *u1 = tab, *p1 = u1 + 64, *u2 = p1 + 64, *p2 = u2 + (N >> 6) + 1;
+    R.U = {u1, u2};
+    R.P = {p1, p2};
+    return R;
+}
+
+template <typename T> __device__ RingTrig<T> build_trig(c2_t<T> *tab, int n, int N, double phi0_pi, int mmax) {
+    const RingTrig<T> R = trig_layout<T>(tab, N);
+    c2_t<T> *u1 = const_cast<c2_t<T> *>(R.U.fine), *u2 = const_cast<c2_t<T> *>(R.U.coarse);
+    c2_t<T> *p1 = const_cast<c2_t<T> *>(R.P.fine), *p2 = const_cast<c2_t<T> *>(R.P.coarse);
+    const int nu2 = (N >> 6) + 1, np2 = (mmax >> 6) + 1;
     for (int j = threadIdx.x; j < 64; j += blockDim.x) {
         u1[j] = expmipi<T>(2 * (int64_t)j, n);
         p1[j] = expmipi_real<T>((double)j * phi0_pi);
-        if (chirp) c1[j] = expmipi<T>(j, N);
     }
     for (int j = threadIdx.x; j < nu2; j += blockDim.x) u2[j] = expmipi<T>(128 * (int64_t)j, n);
     for (int j = threadIdx.x; j < np2; j += blockDim.x) p2[j] = expmipi_real<T>(64.0 * (double)j * phi0_pi);
-    for (int j = threadIdx.x; j < nc2; j += blockDim.x) c2[j] = expmipi<T>(64 * (int64_t)j, N);
-    RingTrig<T> R;
-    R.U = {u1, u2};
-    R.P = {p1, p2};
-    R.C = {c1, c2};
     return R;
 }
 
@@ -271,7 +386,7 @@ __device__ RingTrig<T> build_trig(c2_t<T> *tab, int n, int N, double phi0_pi, in
 // phi0 match (always on HEALPix grids).  Ends with a barrier.
 template <typename T>
 __device__ __forceinline__ RingTrig<T> trig_for_ring(const GeomDev &g, c2_t<T> *tab, int pair, int side, int n,
-                                                     int N, int mmax, bool chirp) {
+                                                     int N, int mmax) {
     bool rebuild = true;
     if (side == 1) {
         const int rn = g.pair_ring[2 * pair];
@@ -279,41 +394,48 @@ __device__ __forceinline__ RingTrig<T> trig_for_ring(const GeomDev &g, c2_t<T> *
         rebuild = g.nphi[rn] != g.nphi[rs] || g.phi0_pi[rn] != g.phi0_pi[rs];
     }
     if (rebuild) {
-        const RingTrig<T> R = build_trig<T>(tab, n, N, side ? g.phi0_pi[g.pair_ring[2 * pair + 1]] : g.phi0_pi[g.pair_ring[2 * pair]], mmax, chirp);
+        const RingTrig<T> R = build_trig<T>(tab, n, N, g.phi0_pi[g.pair_ring[2 * pair + side]], mmax);
         __syncthreads();
         return R;
     }
-    // same layout as build_trig produced for the north ring (same n, N, mmax, chirp)
-    RingTrig<T> R;
-    c2_t<T> *u1 = tab, *p1 = u1 + 64, *c1 = p1 + 64, *u2 = c1 + 64;
-    c2_t<T> *p2 = u2 + (N >> 6) + 1, *c2 = p2 + (mmax >> 6) + 1;
-    R.U = {u1, u2};
-    R.P = {p1, p2};
-    R.C = {c1, c2};
-    return R;
+    return trig_layout<T>(tab, N);
 }
 
-// chirp w_j = exp(-i pi j^2 / N)
-template <typename T> __device__ __forceinline__ c2_t<T> chirp(const RingTrig<T> &R, int64_t j, int N) {
-    return R.C((j * j) % (2 * (int64_t)N));
+// the chirp exp(-i pi j^2 / N), j < N, of a Bluestein ring: stored after its spectrum
+template <typename T> __device__ __forceinline__ const c2_t<T> *chirp_table(const GeomDev &g, int64_t bo, int L) {
+    return blu_table<T>(g) + bo + L;
 }
 
 // ------------------------------------------------------------------------------ analysis
+// F(m) of one ring lands in F[map][m][pair][side].  With `stage_n` the north ring's values wait
+// in shared memory until the south ring is done and each m is written as one (north, south)
+// vector store; otherwise (unpaired rings, or no room) each side is stored on its own.
+template <typename V> __device__ __forceinline__ void store_ns(V *dst, V n, V s);
+template <> __device__ __forceinline__ void store_ns<float2>(float2 *dst, float2 n, float2 s) {
+    *reinterpret_cast<float4 *>(dst) = make_float4(n.x, n.y, s.x, s.y);
+}
+template <> __device__ __forceinline__ void store_ns<double2>(double2 *dst, double2 n, double2 s) {
+    dst[0] = n;
+    dst[1] = s;
+}
+
 template <typename T>
-__global__ void __launch_bounds__(512, 2) ring_analysis_kernel(GeomDev g, const int32_t *__restrict__ pairs,
-                                                               const T *__restrict__ maps, int64_t map_stride,
-                                                               const double *__restrict__ w, c2_t<T> *__restrict__ Fm,
-                                                               int64_t fm_stride, int mmax, int flags, int unit_w,
-                                                               int mdouble, int Lcls) {
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1)
+    ring_analysis_kernel(GeomDev g, const int32_t *__restrict__ pairs, const T *__restrict__ maps, int64_t map_stride,
+                         const double *__restrict__ w, c2_t<T> *__restrict__ Fm, int64_t fm_stride, int mmax,
+                         int flags, int unit_w, int mdouble, int Lcls, int stage_n) {
     using V = c2_t<T>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V *buf = reinterpret_cast<V *>(smem_raw);
     V *tab = buf + padded_len(Lcls);
-    const int pair = pairs[blockIdx.y], b = blockIdx.x;  // maps fastest: a pair's tables stay in L2
+    V *stn = tab + trig_entries<T>(Lcls, mmax);  // north ring's F(m), m <= mmax (stage_n)
+    const int pair = pairs[blockIdx.x], b = blockIdx.y;  // pairs fastest: neighbours complete F's sectors
     const int64_t np = g.npairs;
     V *out = Fm + b * fm_stride;
     const Tw<T> tw = twiddles<T>(g);
     const double twopi = 6.283185307179586476925286766559;
+    const bool joint = stage_n && g.pair_ring[2 * pair + 1] >= 0;
+    auto sts = [&](int p, V v) { buf[ph(p)] = v; };
     for (int side = 0; side < 2; ++side) {
         const int r = g.pair_ring[2 * pair + side];
         if (r < 0) {  // unpaired ring: zero south half
@@ -324,26 +446,18 @@ __global__ void __launch_bounds__(512, 2) ring_analysis_kernel(GeomDev g, const 
         const int64_t bo = g.blu_ofs[r];
         const bool direct = bo < 0;
         __syncthreads();  // previous ring done with buf / tables
-        const RingTrig<T> R = trig_for_ring<T>(g, tab, pair, side, n, N, mmax, !direct);
+        const RingTrig<T> R = trig_for_ring<T>(g, tab, pair, side, n, N, mmax);
         const V *f2 = reinterpret_cast<const V *>(maps + b * map_stride + g.ofs[r]);  // ring offsets: multiples of 4
-        if (direct) {
-            for (int j = threadIdx.x; j < N; j += blockDim.x) buf[ph<true>(j)] = f2[j];
+        const V *ch = direct ? nullptr : chirp_table<T>(g, bo, L);
+        if (direct) {  // DIF from the ring itself: the spectrum stays in digit order
+            dif_to_smem<false, T>(buf, logL, tw, [&](int p) -> V { return f2[p]; });
         } else {
-            for (int j = threadIdx.x; j < L; j += blockDim.x)
-                buf[ph<true>(j)] = (j < N) ? cmul(f2[j], chirp(R, j, N)) : mk2((T)0, (T)0);
-        }
-        __syncthreads();
-        fft_fwd<true, T>(buf, tw, logL);
-        if (!direct) {
-            const V *Bt = blu_table<T>(g) + bo;
-            for (int i = threadIdx.x; i < L; i += blockDim.x) buf[ph<true>(i)] = cmul(buf[ph<true>(i)], Bt[i]);
+            bluestein<T>(buf, logL, tw, blu_table<T>(g) + bo,
+                         [&](int p) -> V { return p < N ? cmul(f2[p], ch[p]) : mk2((T)0, (T)0); }, sts);
             __syncthreads();
-            fft_inv<true, T>(buf, tw, logL);
         }
         // Z_k, 0 <= k < N
-        auto Z = [&](int k) -> V {
-            return direct ? buf[ph<true>(freq_to_pos(k, logL))] : cmul(buf[ph<true>(k)], chirp(R, k, N));
-        };
+        auto Z = [&](int k) -> V { return direct ? buf[ph(pos_of_freq(k, logL))] : cmul(buf[ph(k)], ch[k]); };
         const T scale = unit_w ? (T)1 : (T)(((flags & HB_F_NO2PI) ? 1.0 : twopi) * w[r] / (double)n);
         const int side_out = g.ring_side[r];
         auto emit = [&](int m, V X) {
@@ -351,13 +465,18 @@ __global__ void __launch_bounds__(512, 2) ring_analysis_kernel(GeomDev g, const 
             T sc = scale;
             if (mdouble && m > 0) sc *= (T)2;
             if ((flags & HB_F_NOFOLD) && m >= n) sc = (T)0;
-            out[((int64_t)m * np + pair) * 2 + side_out] = cscale(X, sc);
+            X = cscale(X, sc);
+            if (!joint)
+                out[((int64_t)m * np + pair) * 2 + side_out] = X;
+            else if (side == 0)
+                stn[m] = X;
+            else
+                store_ns(out + ((int64_t)m * np + pair) * 2, stn[m], X);
         };
         // F_k = (A - i U(k) D) / 2, A = Z_k + conj Z_{N-k}, D = Z_k - conj Z_{N-k}; harmonic m takes
-        // bin m mod n (conjugated above N).  Threads walk the buffer in storage order.
-        for (int p = threadIdx.x; p < N; p += blockDim.x) {
-            const int k = direct ? pos_to_freq(p, logL) : p;
-            const V zk = direct ? buf[ph<true>(p)] : cmul(buf[ph<true>(p)], chirp(R, p, N));
+        // bin m mod n (conjugated above N).
+        for (int k = threadIdx.x; k < N; k += blockDim.x) {
+            const V zk = Z(k);
             const V zc = cconj(k == 0 ? zk : Z(N - k));
             const V A = cadd(zk, zc), D = csub(zk, zc);
             auto bin = [&](int kk) -> V {
@@ -379,17 +498,16 @@ __global__ void __launch_bounds__(512, 2) ring_analysis_kernel(GeomDev g, const 
 
 // ------------------------------------------------------------------------------ synthesis
 template <typename T>
-__global__ void __launch_bounds__(512, 2) ring_synthesis_kernel(GeomDev g, const int32_t *__restrict__ pairs,
-                                                                const c2_t<T> *__restrict__ Gm, int64_t gm_stride,
-                                                                int mmax, T *__restrict__ maps, int64_t map_stride,
-                                                                const double *__restrict__ w, int apply_w, int mdouble,
-                                                                int flags, int Lcls, int stage_t) {
+__global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1)
+    ring_synthesis_kernel(GeomDev g, const int32_t *__restrict__ pairs, const c2_t<T> *__restrict__ Gm,
+                          int64_t gm_stride, int mmax, T *__restrict__ maps, int64_t map_stride,
+                          const double *__restrict__ w, int apply_w, int mdouble, int flags, int Lcls, int stage_t) {
     using V = c2_t<T>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V *buf = reinterpret_cast<V *>(smem_raw);
     V *tab = buf + padded_len(Lcls);
     V *ts = tab + trig_entries<T>(Lcls, mmax);  // staged T_m, m <= mmax (when stage_t)
-    const int pair = pairs[blockIdx.y], b = blockIdx.x;  // maps fastest: a pair's tables stay in L2
+    const int pair = pairs[blockIdx.x], b = blockIdx.y;  // pairs fastest: neighbours share G's sectors
     const int64_t np = g.npairs;
     const V *gin = Gm + b * gm_stride;
     const Tw<T> tw = twiddles<T>(g);
@@ -402,7 +520,8 @@ __global__ void __launch_bounds__(512, 2) ring_synthesis_kernel(GeomDev g, const
         const bool direct = bo < 0;
         const int side_in = g.ring_side[r];
         __syncthreads();
-        const RingTrig<T> R = trig_for_ring<T>(g, tab, pair, side, n, N, mmax, !direct);
+        const RingTrig<T> R = trig_for_ring<T>(g, tab, pair, side, n, N, mmax);
+        const V *ch = direct ? nullptr : chirp_table<T>(g, bo, L);
         // T_m = c_m G(m) exp(+i m phi0)
         auto Tm_global = [&](int m) -> V {
             V v = gin[((int64_t)m * np + pair) * 2 + side_in];
@@ -427,35 +546,28 @@ __global__ void __launch_bounds__(512, 2) ring_synthesis_kernel(GeomDev g, const
             }
             return acc;
         };
-        // Zv_k = (X_k + conj X_{N-k}) + i conj(U(k)) (X_k - conj X_{N-k}), k < N, written where the
-        // inverse transform expects it; threads walk the buffer in storage order.
-        if (!direct)
-            for (int j = N + threadIdx.x; j < L; j += blockDim.x) buf[ph<true>(j)] = mk2((T)0, (T)0);
-        for (int p = threadIdx.x; p < N; p += blockDim.x) {
-            const int k = direct ? pos_to_freq(p, logL) : p;
+        // Zv_k = (X_k + conj X_{N-k}) + i conj(U(k)) (X_k - conj X_{N-k}), 0 <= k < N
+        auto spec = [&](int k) -> V {
             const V xa = Xk(k), xb = cconj(Xk(N - k));
             const V S = cadd(xa, xb), D = csub(xa, xb);
             const V u = R.U(k);
-            const V z = mk2(S.x - u.x * D.y + u.y * D.x, S.y + u.x * D.x + u.y * D.y);  // S + i conj(u) D
-            // inverse DFT as conj(DFT(conj Z)) through the chirp-z convolution
-            buf[ph<true>(p)] = direct ? z : cmul(cconj(z), chirp(R, k, N));
-        }
-        __syncthreads();
-        if (direct) {
-            fft_inv<true, T>(buf, tw, logL);
-        } else {
-            fft_fwd<true, T>(buf, tw, logL);
-            const V *Bt = blu_table<T>(g) + bo;
-            for (int i = threadIdx.x; i < L; i += blockDim.x) buf[ph<true>(i)] = cmul(buf[ph<true>(i)], Bt[i]);
-            __syncthreads();
-            fft_inv<true, T>(buf, tw, logL);
-        }
+            return mk2(S.x - u.x * D.y + u.y * D.x, S.y + u.x * D.x + u.y * D.y);  // S + i conj(u) D
+        };
         const T pscale = apply_w ? (T)(((flags & HB_F_NO2PI) ? 1.0 : twopi) * w[r] / (double)n) : (T)1;
         V *out2 = reinterpret_cast<V *>(maps + b * map_stride + g.ofs[r]);
-        for (int j = threadIdx.x; j < N; j += blockDim.x) {
-            V z = buf[ph<true>(j)];
-            if (!direct) z = cconj(cmul(z, chirp(R, j, N)));
-            out2[j] = cscale(z, pscale);
+        // the spectrum in natural order (its folds loop over aliases, so it gets a pass of its own
+        // rather than sitting inside the unrolled first FFT pass); Bluestein: conj(Z_k) chirp_k
+        for (int k = threadIdx.x; k < L; k += blockDim.x)
+            buf[ph(k)] = direct ? spec(k) : (k < N ? cmul(cconj(spec(k)), ch[k]) : mk2((T)0, (T)0));
+        __syncthreads();
+        auto lds = [&](int p) -> V { return buf[ph(p)]; };
+        if (direct) {  // inverse DIF, then a digit-order read for the ring store
+            dif_to_smem<true, T>(buf, logL, tw, lds);
+            for (int j = threadIdx.x; j < N; j += blockDim.x) out2[j] = cscale(buf[ph(pos_of_freq(j, logL))], pscale);
+        } else {  // inverse DFT as conj(DFT(conj Z)) through the chirp-z convolution
+            bluestein<T>(buf, logL, tw, blu_table<T>(g) + bo, lds, [&](int p, V v) {
+                if (p < N) out2[p] = cscale(cconj(cmul(v, ch[p])), pscale);
+            });
         }
     }
 }
@@ -472,26 +584,37 @@ __global__ void twiddle_table_kernel(GeomDev g) {
     }
 }
 
-// Chirp spectra for Bluestein: Bt = FFT_L(b) / L in the forward transform's output order,
-// b_t = exp(+i pi t^2 / N) for |t| < N (circular); one CTA per distinct N, FP64, then rounded
-// to FP32 for the single-precision kernels.
-__global__ void __launch_bounds__(1024) bluestein_table_kernel(GeomDev g) {
+// Chirp spectra for Bluestein: Bt = FFT_L(b) / L in digit order (the order the fused middle
+// pass reads), b_t = exp(+i pi t^2 / N) for |t| < N (circular), and after it the chirp
+// exp(-i pi j^2 / N), j < N.  One CTA per distinct N; the transform runs in FP64 on the table
+// itself in global memory (barriers make each pass's stores visible to the block), then is
+// rounded to FP32 for the single-precision kernels.
+__global__ void __launch_bounds__(256) bluestein_table_kernel(GeomDev g) {
     const int r = g.blu_owner[blockIdx.x];
     const int64_t bo = g.blu_ofs[r];
-    const int N = g.nphi[r] >> 1, L = g.fft_len[r];
-    double2 *buf = g.blu_f64 + bo;  // global memory work buffer (the table itself)
+    const int N = g.nphi[r] >> 1, L = g.fft_len[r], logL = ilog2(L);
+    double2 *buf = g.blu_f64 + bo;
     for (int t = threadIdx.x; t < L; t += blockDim.x) {
         const int64_t j = (t < N) ? t : ((L - t < N) ? L - t : -1);
         double2 v = make_double2(0.0, 0.0);
         if (j >= 0) {
             const double2 e = expmipi<double>(j * j, N);  // exp(-i pi j^2/N)
             v = make_double2(e.x, -e.y);
+            if (t < N) {
+                g.blu_f64[bo + L + t] = e;
+                g.blu_f32[bo + L + t] = make_float2((float)e.x, (float)e.y);
+            }
         }
         buf[t] = v;
     }
     __syncthreads();
     const Tw<double> tw{g.tw64, g.log_tw};
-    fft_fwd<false, double>(buf, tw, ilog2(L));
+    auto ldg = [&](int p) -> double2 { return buf[p]; };
+    auto stg = [&](int p, double2 v) { buf[p] = v; };
+    for (int i = 0; i < fft_nstages(logL); ++i) {
+        fft_stage<false, false, double>(i, logL, tw, ldg, stg);
+        __syncthreads();
+    }
     const double inv = 1.0 / (double)L;
     for (int t = threadIdx.x; t < L; t += blockDim.x) {
         const double2 v = make_double2(buf[t].x * inv, buf[t].y * inv);
@@ -504,7 +627,7 @@ int build_fft_tables(GeomDev &g, cudaStream_t st) {
     twiddle_table_kernel<<<64, 256, 0, st>>>(g);
     HB_CHECK_LAUNCH();
     if (g.n_blu > 0) {
-        bluestein_table_kernel<<<(unsigned)g.n_blu, 1024, 0, st>>>(g);
+        bluestein_table_kernel<<<(unsigned)g.n_blu, 256, 0, st>>>(g);
         HB_CHECK_LAUNCH();
     }
     return HB_OK;
@@ -529,7 +652,20 @@ template <typename T> static size_t class_smem_syn(int L, int mmax, bool stage_t
     return class_smem<T>(L, mmax) + (stage_t ? sizeof(c2_t<T>) * (size_t)(mmax + 1) : 0);
 }
 
-static int class_threads(int L) { return L >= 4096 ? 512 : (L >= 512 ? 256 : (L >= 64 ? 128 : 64)); }
+static int smem_per_sm() {
+    static int v = -1;
+    if (v < 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess) v = 100 * 1024;
+    }
+    return v;
+}
+// CTAs of `bytes` dynamic shared memory that fit on one SM (1 KB reserved per CTA)
+static int ctas_by_smem(size_t bytes) { return (int)((size_t)smem_per_sm() / (bytes + 1024)); }
+
+// one radix-16 butterfly per thread where the class allows, 64 to 256 threads
+static int class_threads(int L) { return std::max(64, std::min(256, L / 16)); }
 
 template <typename T>
 static int check_smem(const GeomDev &g, int mmax) {
@@ -547,18 +683,24 @@ static int launch_analysis_t(const GeomDev &g, int nmaps, const T *maps, int64_t
                              c2_t<T> *Fm, int mmax, int flags, bool unit_w, bool mdouble, cudaStream_t st) {
     int rc = check_smem<T>(g, mmax);
     if (rc) return rc;
+    if (nmaps > 65535) return fail(HB_ERR_INVALID, "ring FFT: at most 65535 maps per call");
     const int64_t fm_stride = (int64_t)(mmax + 1) * g.npairs * 2;
     for (int c = 0; c < g.n_cls; ++c) {
         const int L = g.cls_L[c];
         const int64_t first = g.cls_first[c], cnt = g.cls_first[c + 1] - first;
-        const int smem = (int)class_smem<T>(L, mmax);
+        // stage the north ring's F(m) for joint (north, south) stores unless that costs CTAs per SM
+        const size_t base_smem = class_smem<T>(L, mmax), stage_bytes = sizeof(c2_t<T>) * (size_t)(mmax + 1);
+        const int ctas0 = ctas_by_smem(base_smem), ctas1 = ctas_by_smem(base_smem + stage_bytes);
+        const bool stage_n = base_smem + stage_bytes <= (size_t)max_smem_optin() && ctas1 >= std::min(2, ctas0);
+        const int smem = (int)(base_smem + (stage_n ? stage_bytes : 0));
         HB_CUDA_TRY(cudaFuncSetAttribute(ring_analysis_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         HB_CUDA_TRY(cudaFuncSetAttribute(ring_analysis_kernel<T>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                          cudaSharedmemCarveoutMaxShared));
-        dim3 grid((unsigned)nmaps, (unsigned)cnt);
+        dim3 grid((unsigned)cnt, (unsigned)nmaps);
         ring_analysis_kernel<T><<<grid, class_threads(L), smem, st>>>(g, g.cls_pairs + first, maps, map_stride,
                                                                        w ? w : g.w, Fm, fm_stride, mmax, flags,
-                                                                       unit_w ? 1 : 0, mdouble ? 1 : 0, L);
+                                                                       unit_w ? 1 : 0, mdouble ? 1 : 0, L,
+                                                                       stage_n ? 1 : 0);
         HB_CHECK_LAUNCH();
     }
     return HB_OK;
@@ -569,6 +711,7 @@ static int launch_synthesis_t(const GeomDev &g, int nmaps, const c2_t<T> *Gm, in
                               const double *w, bool apply_w, bool mdouble, int flags, cudaStream_t st) {
     int rc = check_smem<T>(g, mmax);
     if (rc) return rc;
+    if (nmaps > 65535) return fail(HB_ERR_INVALID, "ring FFT: at most 65535 maps per call");
     const int64_t gm_stride = (int64_t)(mmax + 1) * g.npairs * 2;
     for (int c = 0; c < g.n_cls; ++c) {
         const int L = g.cls_L[c];
@@ -578,7 +721,7 @@ static int launch_synthesis_t(const GeomDev &g, int nmaps, const c2_t<T> *Gm, in
         HB_CUDA_TRY(cudaFuncSetAttribute(ring_synthesis_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         HB_CUDA_TRY(cudaFuncSetAttribute(ring_synthesis_kernel<T>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                          cudaSharedmemCarveoutMaxShared));
-        dim3 grid((unsigned)nmaps, (unsigned)cnt);
+        dim3 grid((unsigned)cnt, (unsigned)nmaps);
         ring_synthesis_kernel<T><<<grid, class_threads(L), smem, st>>>(g, g.cls_pairs + first, Gm, gm_stride, mmax,
                                                                         maps, map_stride, w ? w : g.w,
                                                                         apply_w ? 1 : 0, mdouble ? 1 : 0, flags, L,

@@ -139,7 +139,7 @@ static int finish_geom(HostGeom &h, int64_t nside, const std::vector<double> &xn
                 blu_of_N[N] = h.blu_total;
                 h.blu_ofs[r] = h.blu_total;
                 h.blu_owner.push_back((int32_t)r);
-                h.blu_total += L;
+                h.blu_total += L + N;  // chirp spectrum (L entries), then the chirp itself (N entries)
             } else {
                 h.blu_ofs[r] = it->second;
             }

@@ -76,7 +76,9 @@ struct GeomDev {
     // direct FFT; otherwise Bluestein) and the offset of its chirp spectrum in blu_*.
     int32_t *fft_len;      // [nr]
     int64_t *blu_ofs;      // [nr] (-1 for direct)
-    double2 *blu_f64;      // concatenated chirp spectra, forward-transform output order, scaled by 1/L
+    // per distinct N: L entries of the chirp spectrum (forward-transform output order, scaled by
+    // 1/L), then N entries of the chirp exp(-i pi j^2 / N), j < N
+    double2 *blu_f64;
     float2 *blu_f32;
     int32_t *blu_owner;    // [n_blu] first ring using each distinct chirp table
     int64_t n_blu;

@@ -218,6 +218,14 @@ HB_API size_t hb_batched_plan_bytes(const hb_batched_plan *bp);
 HB_API int hb_batched_alm2map(hb_batched_plan *bp, const float *alm, float *maps, hb_stream_t stream);
 HB_API int hb_batched_map2alm(hb_batched_plan *bp, const float *maps, float *alm, hb_stream_t stream);
 HB_API int hb_batched_status(hb_batched_plan *bp, int *code);
+/* CUDA graph of a batched step: hb_batched_graph_capture records hb_batched_alm2map(alm -> maps)
+ * then hb_batched_map2alm(maps -> alm_out) (alm or alm_out may be null to keep one direction)
+ * on a private stream into an executable graph owned by the plan, replacing an earlier one; the
+ * buffer pointers are part of the graph.  hb_batched_graph_launch replays it on `stream`: one
+ * launch for the whole step, no host work per kernel.  (No counterpart in the reference, whose
+ * per-ring host loops cannot be captured.) */
+HB_API int hb_batched_graph_capture(hb_batched_plan *bp, const float *alm, float *maps, float *alm_out);
+HB_API int hb_batched_graph_launch(hb_batched_plan *bp, hb_stream_t stream);
 /* Profiling: with enable != 0 every exec records CUDA events between its kernels (do not enable
  * while capturing a CUDA graph); hb_batched_stage_ms then returns the last calls' stage times in
  * ms: [alm tile prep, tensor synthesis, ring synthesis, ring analysis, F tile prep, tensor
