@@ -103,17 +103,18 @@ __device__ __forceinline__ void store_rows8(uint4 *chunk, int N, int qh, int n, 
 // alm [map][nalm] complex64 -> per (m, 64-l chunk) the synthesis B tiles:
 // [q][h][N rows x 32 K (l = l0 + 2k + q)].
 template <int N, bool BF16>
-__global__ void __launch_bounds__(256) prep_alm_tiles_kernel(const TcGroup *groups, int gi, const float2 *__restrict__ alm,
+__global__ void __launch_bounds__(256, 4) prep_alm_tiles_kernel(const TcGroup *groups, int gi, const float2 *__restrict__ alm,
                                                              int64_t alm_stride) {
     extern __shared__ float2 sa[];  // l - m = i at i + i / 16
     const TcGroup &G = groups[gi];
-    const int m = blockIdx.x, b = blockIdx.y;
+    const int m = blockIdx.y, b = blockIdx.x;  // maps fastest: one m's tile rows are written together
     if (m > G.mmax) return;
     const int lmax = G.lmax;
     const int nch = (lmax - m + 64) / 64;
     const bool live = b < G.nmaps;
     const float2 *src = alm + (int64_t)b * alm_stride + alm_idx(lmax, m, m);
     float vmax = 0.f;
+#pragma unroll 8
     for (int i = threadIdx.x; i < nch * 64; i += blockDim.x) {
         const float2 v = (live && m + i <= lmax) ? src[i] : make_float2(0.f, 0.f);
         sa[i + (i >> 4)] = v;
@@ -144,17 +145,18 @@ __global__ void __launch_bounds__(256) prep_alm_tiles_kernel(const TcGroup *grou
 // F [map][m][pair][2] -> per (m, 32-pair chunk) the analysis B tiles [q][h][N x 32 pairs]
 // (E = F_N + F_S for q = 0, O = F_N - F_S for q = 1).
 template <int N, bool BF16>
-__global__ void __launch_bounds__(512) prep_g_tiles_kernel(const TcGroup *groups, int gi, const float2 *__restrict__ F,
+__global__ void __launch_bounds__(256, 3) prep_g_tiles_kernel(const TcGroup *groups, int gi, const float2 *__restrict__ F,
                                                            int64_t f_stride) {
     extern __shared__ float4 sf[];  // pair p (north, south) at p + p / 8
     const TcGroup &G = groups[gi];
-    const int m = blockIdx.x, b = blockIdx.y;
+    const int m = blockIdx.y, b = blockIdx.x;  // maps fastest: one m's tile rows are written together
     if (m > G.mmax) return;
     const int64_t np = G.g.npairs;
     const int npc = (int)G.npc;
     const bool live = b < G.nmaps;
     const float4 *src = reinterpret_cast<const float4 *>(F + (int64_t)b * f_stride + (int64_t)m * np * 2);
     float vmax = 0.f;
+#pragma unroll 8
     for (int p = threadIdx.x; p < npc * 32; p += blockDim.x) {
         const float4 f = (live && p < np) ? src[p] : make_float4(0.f, 0.f, 0.f, 0.f);
         sf[p + (p >> 3)] = f;
@@ -189,14 +191,13 @@ __global__ void __launch_bounds__(512) prep_g_tiles_kernel(const TcGroup *groups
 struct Rec {
     float l1, l2, xh, xl;
     int e;
-    // lambda_l = A x lambda_{l-1} + B lambda_{l-2}.  A x is formed off the dependency chain as an
-    // unevaluated sum ah + al (ah = fl(A xh), al = exact remainder + A xl): a single rounded A x
-    // would carry nearly the same relative error at every l (A_l -> 2 slowly), i.e. a systematic
-    // shift of x, which the hi + lo x exists to avoid.  The chain is two FMAs per step.
+    // lambda_l = A (x lambda_{l-1}) + B lambda_{l-2}, four FP32 operations.  x lambda_{l-1} is
+    // formed first from x = xh + xl (its rounding changes with lambda, so it does not accumulate);
+    // a rounded A x would carry nearly the same relative error at every l (A_l -> 2 slowly), i.e.
+    // a systematic shift of x, which the hi + lo x exists to avoid.
     __device__ __forceinline__ float step(float A, float B) {
-        const float ah = A * xh;
-        const float al = fmaf(A, xl, fmaf(A, xh, -ah));
-        const float v = fmaf(ah, l1, fmaf(al, l1, B * l2));
+        const float t = fmaf(xh, l1, xl * l1);
+        const float v = fmaf(A, t, B * l2);
         l2 = l1;
         l1 = v;
         return v;
@@ -253,6 +254,50 @@ __global__ void coef_table_kernel(int lmax, const int64_t *__restrict__ blk_ofs,
     const int m = blockIdx.x;
     const int64_t b0 = blk_ofs[m], nb = blk_ofs[m + 1] - b0;
     for (int64_t i = threadIdx.x; i < nb * 256; i += blockDim.x) coef_scalar(m + (int)i, m, lmax, tab[b0 * 256 + i]);
+}
+
+// Evanescent skip ranges.  Below its turning point the FP32 recursion state of a ring pair carries
+// an exponent e < 0 (|lambda| < 2^-32; its values are gated to exact zeros) and e never decreases
+// with l, so every value before a checkpoint at which all rows have e < 0 is an exact zero:
+//   syn[m * npb + pb] = leading 128-l half-blocks of (m, pair block pb) that end at such a
+//     checkpoint (checkpoint h at l = m + 128 h: h even ck, h odd the mid-block table; the
+//     half-block that reaches past lmax is never skipped);
+//   ana[blk_ofs[m] + jb] = leading 32-pair chunks whose rows all have e < 0 at the end of the
+//     256-l block jb (none when the block reaches past lmax; at least one chunk stays).
+// The kernels skip those chunks entirely (no recursion, no tile, no MMA): same results, less work.
+__global__ void __launch_bounds__(128) skip_table_kernel(GeomDev g, int lmax, const int64_t *__restrict__ blk_ofs,
+                                                         const float4 *__restrict__ ck, const float4 *__restrict__ ckh,
+                                                         int *__restrict__ syn, int *__restrict__ ana) {
+    const int m = blockIdx.x;
+    const int64_t np = g.npairs, b0 = blk_ofs[m], nb = blk_ofs[m + 1] - b0;
+    const int npb = (int)((np + 127) / 128), npc = (int)((np + 31) / 32);
+    auto dead_at = [&](const float4 *tab, int64_t blk, int64_t p) {
+        return p >= np || __float_as_int(tab[blk * np + p].z) < 0;
+    };
+    for (int pb = 0; pb < npb; ++pb) {
+        const int64_t p = (int64_t)pb * 128 + threadIdx.x;
+        int hb0 = 0;
+        for (int h = 1; m + 128 * h <= lmax; ++h) {
+            const bool dead = (h & 1) ? dead_at(ckh, b0 + (h - 1) / 2, p) : dead_at(ck, b0 + h / 2, p);
+            if (!__syncthreads_and(dead)) break;
+            hb0 = h;
+        }
+        if (threadIdx.x == 0) syn[(int64_t)m * npb + pb] = hb0;
+    }
+    __shared__ int first_live;
+    for (int64_t jb = 0; jb < nb; ++jb) {
+        if (threadIdx.x == 0) first_live = npc * 32;
+        __syncthreads();
+        if (jb + 1 < nb) {
+            for (int64_t p = threadIdx.x; p < np; p += blockDim.x)
+                if (!dead_at(ck, b0 + jb + 1, p)) atomicMin(&first_live, (int)p);
+        } else if (threadIdx.x == 0) {
+            first_live = 0;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) ana[b0 + jb] = min(first_live / 32, npc - 1);
+        __syncthreads();
+    }
 }
 
 // ------------------------------------------------------------------------------------ pipeline
@@ -401,6 +446,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             R.xh = live ? G.g.pair_xhi[p] : 0.f;
             R.xl = live ? G.g.pair_xlo[p] : 0.f;
             const int nch = (lmax - m + 64) / 64, nhb = (nch + 1) / 2;
+            const int c0 = U.w, hbs = c0 / 2 + (((c0 / 2) ^ wg) & 1);  // first live half-block of this group
             const int64_t b0 = G.blk_ofs[m];
             // the next half-block's coefficients and checkpoint are fetched one half-block ahead
             float2 cpre[4];
@@ -411,8 +457,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 for (int i = 0; i < 4; ++i) cpre[i] = G.coef[blk * 256 + (hb & 1) * 128 + lane + 32 * i];
                 kpre = live ? ((hb & 1) ? G.ckh : G.ck)[blk * np + p] : make_float4(0.f, 0.f, 0.f, 0.f);
             };
-            if (wg < nhb) fetch(wg);
-            for (int hb = wg; hb < nhb && ok; hb += 2) {
+            if (hbs < nhb) fetch(hbs);
+            for (int hb = hbs; hb < nhb && ok; hb += 2) {
                 __syncwarp();
 #pragma unroll
                 for (int i = 0; i < 4; ++i) L.coef[lane + 32 * i] = cpre[i];
@@ -452,7 +498,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             tc::fence_after();
             const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
             const float *scl = G.dscale + (int64_t)m * (N / 2);
-            const int nsets = nch < S ? nch : S;
+            const int nsets = nch - c0 < S ? nch - c0 : S;
 #pragma unroll 1
             for (int j = wg; j < N / 16; j += 2) {
                 float de[16], dd[16];
@@ -481,14 +527,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             int ui = 0;
             for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++ui) {
                 const int4 U = units[u];
-                const int nch = (groups[U.x].lmax - U.y + 64) / 64;
+                const int nch = (groups[U.x].lmax - U.y + 64) / 64, c0 = U.w;
                 if (ui > 0 && !tc::mbar_wait(L.tfree, (ui - 1) & 1, HB_TC_WAIT_NS)) {
                     set_err(err, 3);
                     ok = false;
                     break;
                 }
                 tc::fence_after();
-                for (int c = 0; c < nch; ++c) {
+                for (int c = c0; c < nch; ++c) {
                     const int g = (c >> 1) & 1;
                     uint32_t &itr = g ? itr1 : itr0;
                     const int s = g * SPR + (int)(itr % SPR);
@@ -499,7 +545,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     }
                     ++itr;
                     tc::fence_after();
-                    issue_stage<N>(tmem, tc::smem_u32(smem + s * STAGE), c % S, c < S, IDESC);
+                    issue_stage<N>(tmem, tc::smem_u32(smem + s * STAGE), (c - c0) % S, c - c0 < S, IDESC);
                     tc::mma_commit(&L.empty[s]);
                 }
                 if (!ok) break;
@@ -521,7 +567,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 const int m = U.y;
                 const int nch = (G.lmax - m + 64) / 64;
                 const uint4 *src = G.alm_tiles + G.alm_tile_ofs[m] * (16 * N);
-                for (int c = 0; c < nch; ++c) {
+                for (int c = U.w; c < nch; ++c) {
                     const int g = (c >> 1) & 1;
                     uint32_t &itr = g ? itr1 : itr0;
                     const int s = g * SPR + (int)(itr % SPR);
@@ -606,7 +652,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 xln = lv ? G.g.pair_xlo[pp] : 0.f;
             };
             bool first = true;
-            for (int c = 0; c < npc; ++c, ++it) {
+            for (int c = U.w; c < npc; ++c, ++it) {
                 const int s = it % ST;
                 if (s != owner) continue;
                 if (first) fetch(c);
@@ -650,7 +696,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             const int le = l0 + 2 * row;
             const uint32_t taddr = tmem + ((uint32_t)(owner * 32) << 16);
             const float *scl = G.dscale + (int64_t)m * (N / 2);
-            const int nsets = npc < S ? npc : S;
+            const int nsets = npc - U.w < S ? npc - U.w : S;
 #pragma unroll 1
             for (int j = half; j < N / 16; j += 2) {
                 float de[16], dd[16];
@@ -675,14 +721,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             uint32_t it = 0;
             int ui = 0;
             for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++ui) {
-                const int npc = (int)groups[units[u].x].npc;
+                const int npc = (int)groups[units[u].x].npc, c0 = units[u].w;
                 if (ui > 0 && !tc::mbar_wait(L.tfree, (ui - 1) & 1, HB_TC_WAIT_NS)) {
                     set_err(err, 13);
                     ok = false;
                     break;
                 }
                 tc::fence_after();
-                for (int c = 0; c < npc; ++c, ++it) {
+                for (int c = c0; c < npc; ++c, ++it) {
                     const int s = it % ST;
                     if (!tc::mbar_wait(&L.full[s], (it / ST) & 1, HB_TC_WAIT_NS)) {
                         set_err(err, 14);
@@ -690,7 +736,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         break;
                     }
                     tc::fence_after();
-                    issue_stage<N>(tmem, tc::smem_u32(smem + s * STAGE), c % S, c < S, IDESC);
+                    issue_stage<N>(tmem, tc::smem_u32(smem + s * STAGE), (c - c0) % S, c - c0 < S, IDESC);
                     tc::mma_commit(&L.empty[s]);
                 }
                 if (!ok) break;
@@ -712,7 +758,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 const int m = U.y;
                 const int npc = (int)G.npc;
                 const uint4 *src = G.g_tiles + (int64_t)m * npc * (16 * N);
-                for (int c = 0; c < npc; ++c, ++it) {
+                for (int c = U.w; c < npc; ++c, ++it) {
                     const int s = it % ST;
                     if (it >= ST && !tc::mbar_wait(&L.empty[s], ((it / ST) + 1) & 1, HB_TC_WAIT_NS)) {
                         set_err(err, 15);
@@ -808,7 +854,7 @@ static int launch_prep_alm(hb_batched_plan *bp, int gi, const float2 *alm, int64
     const TcGroup &G = bp->hgroups[gi];
     const int smem = (int)(sizeof(float2) * (size_t)(((G.lmax + 64) / 64) * 68));  // 64 l + 4 pads per chunk
     HB_CUDA_TRY(cudaFuncSetAttribute(prep_alm_tiles_kernel<N, BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    prep_alm_tiles_kernel<N, BF16><<<dim3(G.mmax + 1, N / 2), 256, smem, st>>>(bp->dgroups, gi, alm, stride);
+    prep_alm_tiles_kernel<N, BF16><<<dim3(N / 2, G.mmax + 1), 256, smem, st>>>(bp->dgroups, gi, alm, stride);
     HB_CHECK_LAUNCH();
     return HB_OK;
 }
@@ -817,7 +863,7 @@ static int launch_prep_g(hb_batched_plan *bp, int gi, const float2 *F, int64_t s
     const TcGroup &G = bp->hgroups[gi];
     const int smem = (int)(sizeof(float4) * (size_t)(G.npc * 36));  // 32 pairs + 4 pads per chunk
     HB_CUDA_TRY(cudaFuncSetAttribute(prep_g_tiles_kernel<N, BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    prep_g_tiles_kernel<N, BF16><<<dim3(G.mmax + 1, N / 2), 512, smem, st>>>(bp->dgroups, gi, F, stride);
+    prep_g_tiles_kernel<N, BF16><<<dim3(N / 2, G.mmax + 1), 256, smem, st>>>(bp->dgroups, gi, F, stride);
     HB_CHECK_LAUNCH();
     return HB_OK;
 }
@@ -905,22 +951,16 @@ int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int np
     }
     const int ngroups = (int)bp->hgroups.size();
     const size_t o_groups = carve(sizeof(TcGroup) * ngroups);
-    // units, sorted by decreasing work
-    std::vector<std::pair<double, int4>> su, au;
+    // work units (the skip counts in .w and the order by decreasing work follow once the
+    // recursion tables exist)
+    int64_t n_su = 0, n_au = 0;
     for (int gi = 0; gi < ngroups; ++gi) {
         const TcGroup &G = bp->hgroups[gi];
-        for (int m = 0; m <= G.mmax; ++m) {
-            for (int64_t pb = 0; pb < G.npb; ++pb)
-                su.push_back({-(double)(G.lmax - m + 1) * N, make_int4(gi, m, (int)pb, 0)});
-            for (int jb = 0; m + 256 * jb <= G.lmax; ++jb)
-                au.push_back({-(double)std::min(256, G.lmax - m - 256 * jb + 1) * G.npc * N, make_int4(gi, m, jb, 0)});
-        }
+        for (int m = 0; m <= G.mmax; ++m) n_su += G.npb, n_au += (G.lmax - m) / 256 + 1;
     }
-    std::stable_sort(su.begin(), su.end(), [](auto &a, auto &b) { return a.first < b.first; });
-    std::stable_sort(au.begin(), au.end(), [](auto &a, auto &b) { return a.first < b.first; });
-    bp->n_syn = (int)su.size();
-    bp->n_ana = (int)au.size();
-    const size_t o_su = carve(sizeof(int4) * su.size()), o_au = carve(sizeof(int4) * au.size());
+    bp->n_syn = (int)n_su;
+    bp->n_ana = (int)n_au;
+    const size_t o_su = carve(sizeof(int4) * n_su), o_au = carve(sizeof(int4) * n_au);
     char *base = nullptr;
     if (cudaMalloc(&base, total) != cudaSuccess) {
         cudaGetLastError();
@@ -962,9 +1002,6 @@ int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int np
             }
         }
     }
-    std::vector<int4> suv, auv;
-    for (auto &x : su) suv.push_back(x.second);
-    for (auto &x : au) auv.push_back(x.second);
     int rc = HB_OK;
     for (int i = 0; i < nplans && rc == HB_OK; ++i)
         if (cudaMemcpy(bp->parts[i].tile_ofs, tile_ofs[i].data(), 8 * tile_ofs[i].size(), cudaMemcpyHostToDevice) !=
@@ -972,16 +1009,67 @@ int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int np
             rc = fail(HB_ERR_CUDA, "hb_batched_plan_create: upload");
     if (rc == HB_OK &&
         (cudaMemcpy(bp->dgroups, bp->hgroups.data(), sizeof(TcGroup) * ngroups, cudaMemcpyHostToDevice) != cudaSuccess ||
-         cudaMemcpy(bp->syn_units, suv.data(), sizeof(int4) * suv.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
-         cudaMemcpy(bp->ana_units, auv.data(), sizeof(int4) * auv.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
          cudaMemset(bp->err, 0, sizeof(int)) != cudaSuccess))
         rc = fail(HB_ERR_CUDA, "hb_batched_plan_create: upload");
+    // recursion coefficient and mid-block tables, then the evanescent skip counts of every plan
+    std::vector<std::vector<int>> syn_skip(nplans), ana_skip(nplans);
     for (int i = 0; i < nplans && rc == HB_OK; ++i) {
         const hb_plan *p = plans[i];
         coef_table_kernel<<<p->mmax + 1, 256>>>(p->lmax, p->blk_ofs, bp->parts[i].coef);
         if (cudaGetLastError() != cudaSuccess || launch_ck_mid(p, bp->parts[i].ckh) != HB_OK ||
-            cudaDeviceSynchronize() != cudaSuccess)
+            cudaDeviceSynchronize() != cudaSuccess) {
             rc = fail(HB_ERR_CUDA, "hb_batched_plan_create: coefficient table");
+            break;
+        }
+        const int64_t np = p->g->d.npairs, npb = (np + 127) / 128;
+        int64_t nblocks = 0;
+        for (int m = 0; m <= p->mmax; ++m) nblocks += (p->lmax - m) / 256 + 1;
+        syn_skip[i].assign((size_t)(p->mmax + 1) * npb, 0);
+        ana_skip[i].assign((size_t)nblocks, 0);
+        int *dsk = nullptr;
+        if (cudaMalloc(&dsk, sizeof(int) * (syn_skip[i].size() + ana_skip[i].size())) != cudaSuccess) {
+            cudaGetLastError();
+            rc = fail(HB_ERR_ALLOC, "hb_batched_plan_create: skip tables");
+            break;
+        }
+        skip_table_kernel<<<p->mmax + 1, 128>>>(p->g->d, p->lmax, p->blk_ofs, p->ck, bp->parts[i].ckh, dsk,
+                                                  dsk + syn_skip[i].size());
+        if (cudaGetLastError() != cudaSuccess ||
+            cudaMemcpy(syn_skip[i].data(), dsk, sizeof(int) * syn_skip[i].size(), cudaMemcpyDeviceToHost) !=
+                cudaSuccess ||
+            cudaMemcpy(ana_skip[i].data(), dsk + syn_skip[i].size(), sizeof(int) * ana_skip[i].size(),
+                       cudaMemcpyDeviceToHost) != cudaSuccess)
+            rc = fail(HB_ERR_CUDA, "hb_batched_plan_create: skip tables");
+        cudaFree(dsk);
+    }
+    if (rc == HB_OK) {  // units with their skip counts, sorted by decreasing remaining work
+        std::vector<std::pair<double, int4>> su, au;
+        for (int gi = 0; gi < ngroups; ++gi) {
+            const TcGroup &G = bp->hgroups[gi];
+            const int pi = bp->group_part[gi];
+            std::vector<int64_t> bofs(G.mmax + 2, 0);
+            for (int m = 0; m <= G.mmax; ++m) bofs[m + 1] = bofs[m] + (G.lmax - m) / 256 + 1;
+            for (int m = 0; m <= G.mmax; ++m) {
+                const int nch = (G.lmax - m + 64) / 64;
+                for (int64_t pb = 0; pb < G.npb; ++pb) {
+                    const int c0 = 2 * syn_skip[pi][(size_t)m * G.npb + pb];
+                    su.push_back({-(double)(nch - c0) * N, make_int4(gi, m, (int)pb, c0)});
+                }
+                for (int jb = 0; m + 256 * jb <= G.lmax; ++jb) {
+                    const int c0 = ana_skip[pi][(size_t)(bofs[m] + jb)];
+                    au.push_back({-(double)std::min(256, G.lmax - m - 256 * jb + 1) * (G.npc - c0) * N,
+                                  make_int4(gi, m, jb, c0)});
+                }
+            }
+        }
+        std::stable_sort(su.begin(), su.end(), [](auto &a, auto &b) { return a.first < b.first; });
+        std::stable_sort(au.begin(), au.end(), [](auto &a, auto &b) { return a.first < b.first; });
+        std::vector<int4> suv, auv;
+        for (auto &x : su) suv.push_back(x.second);
+        for (auto &x : au) auv.push_back(x.second);
+        if (cudaMemcpy(bp->syn_units, suv.data(), sizeof(int4) * suv.size(), cudaMemcpyHostToDevice) != cudaSuccess ||
+            cudaMemcpy(bp->ana_units, auv.data(), sizeof(int4) * auv.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+            rc = fail(HB_ERR_CUDA, "hb_batched_plan_create: upload");
     }
     if (rc != HB_OK) {
         cudaFree(base);

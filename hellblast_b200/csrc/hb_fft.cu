@@ -473,25 +473,26 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1)
             else
                 store_ns(out + ((int64_t)m * np + pair) * 2, stn[m], X);
         };
-        // F_k = (A - i U(k) D) / 2, A = Z_k + conj Z_{N-k}, D = Z_k - conj Z_{N-k}; harmonic m takes
-        // bin m mod n (conjugated above N).
-        for (int k = threadIdx.x; k < N; k += blockDim.x) {
+        // Bins of the real ring: F_k = (A - i U(k) D) / 2 with A = Z_k + conj Z_{N-k},
+        // D = Z_k - conj Z_{N-k}, U(k) = exp(-2 pi i k / n); since U(N-k) = -conj U(k), the same
+        // A, D give F_{N-k} = conj(A + i U(k) D) / 2, so one thread takes the pair (k, N-k)
+        // (k = 0: bins 0 and N).  Harmonic m takes bin m mod n, conjugated above N.
+        auto emit_bin = [&](int kk, V X) {
+            for (int m = kk; m <= mmax; m += n) emit(m, X);
+            if (kk > 0 && kk < N)
+                for (int m = n - kk; m <= mmax; m += n) emit(m, cconj(X));
+        };
+        for (int k = threadIdx.x; 2 * k <= N; k += blockDim.x) {
             const V zk = Z(k);
             const V zc = cconj(k == 0 ? zk : Z(N - k));
             const V A = cadd(zk, zc), D = csub(zk, zc);
-            auto bin = [&](int kk) -> V {
-                const V u = R.U(kk);
-                const V iuD = mk2(-(u.x * D.y + u.y * D.x), u.x * D.x - u.y * D.y);  // i u D
-                return mk2((T)0.5 * (A.x - iuD.x), (T)0.5 * (A.y - iuD.y));
-            };
-            const V X = bin(k);
-            for (int m = k; m <= mmax; m += n) emit(m, X);
-            if (k > 0)
-                for (int m = n - k; m <= mmax; m += n) emit(m, cconj(X));
-            else {
-                const V XN = bin(N);
-                for (int m = N; m <= mmax; m += n) emit(m, XN);
-            }
+            const V u = R.U(k);
+            const V iuD = mk2(-(u.x * D.y + u.y * D.x), u.x * D.x - u.y * D.y);  // i u D
+            emit_bin(k, mk2((T)0.5 * (A.x - iuD.x), (T)0.5 * (A.y - iuD.y)));
+            if (k == 0)
+                emit_bin(N, mk2((T)0.5 * (A.x - D.y), (T)0.5 * (A.y + D.x)));  // U(N) = -1
+            else if (2 * k < N)
+                emit_bin(N - k, mk2((T)0.5 * (A.x + iuD.x), (T)(-0.5) * (A.y + iuD.y)));
         }
     }
 }
@@ -530,7 +531,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1)
             return v;
         };
         if (stage_t) {  // independent loads of every T_m of the ring, then the folds read shared memory
-#pragma unroll 4
+#pragma unroll 8
             for (int m = threadIdx.x; m <= mmax; m += blockDim.x) ts[m] = Tm_global(m);
             __syncthreads();
         }
