@@ -38,8 +38,10 @@ def parse():
     p.add_argument("--nside", type=int, default=2048)
     p.add_argument("--lmax", type=int, default=None)
     p.add_argument("--nmaps", type=int, default=None, help="maps per GPU (default 64 batched, 1 plain)")
-    p.add_argument("--split", default="f16", choices=["f16", "bf16"], help="16-bit type of the hi+lo split")
-    p.add_argument("--wide", action="store_true", help="groups of 64 maps (two accumulator sets)")
+    p.add_argument("--split", default=None, choices=["f16", "bf16"],
+                   help="16-bit type of the hi+lo split (default: chosen by the autotuner)")
+    p.add_argument("--wide", default=None, action="store_true",
+                   help="groups of 64 maps, MMA N = 128 (default: chosen by the autotuner)")
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--cpu-sample-m", type=int, default=12)
     return p.parse_args()
@@ -240,8 +242,13 @@ def main():
         def make_ev():
             return [torch.cuda.Event(enable_timing=True) for _ in range(5)]
     else:
-        bf16 = args.split == "bf16"
-        bp = hb.batched.plan(nside, lmax, B, bf16=bf16, wide=args.wide)
+        tune = None
+        if args.split is None and args.wide is None:  # measured choice: fastest within 1e-5 of FP64
+            tune = hb.batched.autotune(nside, lmax, B)
+            bf16, wide = tune["bf16"], tune["wide"]
+        else:
+            bf16, wide = args.split == "bf16", bool(args.wide)
+        bp = hb.batched.plan(nside, lmax, B, bf16=bf16, wide=wide)
         alm_flat, maps_flat, out_flat = alm.reshape(-1), maps.reshape(-1), alm_out.reshape(-1)
         # the whole step (both directions, every kernel) as one CUDA graph
         bp.capture(alm_flat, maps_flat, out_flat)
@@ -260,7 +267,7 @@ def main():
         def stage_times(evs):
             keys = stage_acc[0].keys()
             return {k: float(np.mean([s[k] for s in stage_acc])) for k in keys}
-        groups = (B + (63 if args.wide else 31)) // (64 if args.wide else 32)
+        groups = (B + (63 if wide else 31)) // (64 if wide else 32)
         n_launch = 2 * groups + 2 + 2 * fft_classes(nside)  # operand preps, tensor kernels, ring FFT classes
 
         def make_ev():
@@ -367,8 +374,9 @@ def main():
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic (Gaussian alm, C_l=(l+10)^-2)",
         "config": {"workload": (f"scalar map2alm+alm2map pair, nside {nside}, lmax {lmax}, float32 maps, "
-                                + (f"batched hi+lo split-{args.split.upper()} tcgen05 path"
-                                   f" ({'64' if args.wide else '32'} maps per group), " if args.mode == "batched"
+                                + (f"batched hi+lo split-{'BF16' if bf16 else 'F16'} tcgen05 path"
+                                   f" ({'64' if wide else '32'} maps per group"
+                                   f"{', autotuned' if tune else ''}), " if args.mode == "batched"
                                    else "plain per-map FP32 path, ") + f"{B} maps per GPU per step"),
                    "nside": nside, "lmax": lmax, "maps_per_gpu": B, "mode": args.mode,
                    "l2": "inputs larger than L2 (one map 201 MB, one alm 67 MB)",
@@ -381,6 +389,9 @@ def main():
         "gpu_launches": args.steps * n_launch,
         "clocks": clk.summary(),
     }
+    if args.mode == "batched" and tune is not None:
+        out["autotune"] = [{k: (round(v, 8) if isinstance(v, float) else v) for k, v in c.items()}
+                           for c in tune["candidates"]]
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         v, info = cpu_baseline(nside, lmax, args.cpu_sample_m)
         out["cpu_baseline"] = {"value": v, "unit": "pairs/s", "cores": info["cores"], "kind": info["kind"],

@@ -98,9 +98,13 @@ class BatchedPlan:
 
 
 def plan(nside: int, lmax: int, nmaps: int, mmax: int | None = None, weights: str = "dz",
-         bf16: bool = False, wide: bool = False) -> BatchedPlan:
+         bf16: bool = False, wide: bool = False, tuned: bool = False) -> BatchedPlan:
     """Cached single-geometry batched plan (HEALPix nside, lmax, nmaps maps).  ``bf16`` selects
-    the BF16 hi+lo split instead of the default IEEE-half hi+lo split, ``wide`` groups of 64 maps."""
+    the BF16 hi+lo split instead of the default IEEE-half hi+lo split, ``wide`` groups of 64 maps;
+    ``tuned`` takes both from ``autotune(nside, lmax, nmaps)`` (measured on first use)."""
+    if tuned:
+        t = autotune(nside, lmax, nmaps)
+        bf16, wide = t["bf16"], t["wide"]
     key = (int(nside), int(lmax), mmax, int(nmaps), weights, bool(bf16), bool(wide), torch.cuda.current_device())
     with _lock:
         bp = _cache.get(key)
@@ -178,3 +182,56 @@ class HostPipeline:
 
     def synchronize(self) -> None:
         self.s_out.synchronize()
+
+
+_tuned: dict[tuple, dict] = {}
+
+
+def autotune(nside: int, lmax: int, nmaps: int, tol: float = 1e-5, reps: int = 2, seed: int = 0,
+             candidates=((False, False), (False, True), (True, False), (True, True))) -> dict:
+    """Chooses the batched tile configuration for (nside, lmax, nmaps) on this GPU by measurement.
+
+    Each candidate (bf16, wide) is a 16-bit split type (IEEE half with power-of-two scaling, or
+    BF16) and an MMA tile width (N = 64: 32 maps per recursion pass, or N = 128: 64 maps per
+    pass).  For each, a plan is built, one alm2map + map2alm pair over `nmaps` synthetic maps is
+    timed with CUDA events (after a warm-up), and map 0's pair error against the FP64 transforms
+    is measured.  The fastest candidate with error <= tol wins; the result (with every
+    candidate's time and error) is cached per (nside, lmax, nmaps, device) and ``plan(...,
+    tuned=True)`` uses it.  The candidates' plans are released again (each holds its operand
+    tiles)."""
+    from .alm_ops import synalm
+    from . import hp_compat
+    dev = torch.device("cuda", torch.cuda.current_device())
+    key = (int(nside), int(lmax), int(nmaps), torch.cuda.get_device_name(dev))
+    if key in _tuned:
+        return _tuned[key]
+    cl = 1.0 / (torch.arange(lmax + 1, dtype=torch.float64) + 10.0) ** 2
+    a64 = synalm(cl.numpy(), lmax=lmax, seed=seed, device=dev)
+    m64 = hp_compat.alm2map(a64, nside, lmax=lmax)
+    ref = hp_compat.map2alm(m64, lmax=lmax)
+    alm = a64.to(torch.complex64).expand(nmaps, -1).contiguous().reshape(-1)
+    results = []
+    for bf16, wide in candidates:
+        bp = BatchedPlan([(G.healpix(nside), lmax, None, nmaps)], bf16=bf16, wide=wide)
+        maps = torch.empty(bp.total_pix, dtype=torch.float32, device=dev)
+        out = torch.empty_like(alm)
+        bp.alm2map(alm, out=maps)
+        bp.map2alm(maps, out=out)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            bp.alm2map(alm, out=maps)
+            bp.map2alm(maps, out=out)
+        e1.record()
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1) / reps
+        got = out[: ref.numel()].to(torch.complex128)
+        err = float(torch.linalg.norm(got - ref) / torch.linalg.norm(ref))
+        ok = bp.status() == 0 and err <= tol
+        results.append({"bf16": bf16, "wide": wide, "ms": ms, "rel_err": err, "ok": ok})
+        del bp, maps, out
+        torch.cuda.empty_cache()
+    good = [r for r in results if r["ok"]]
+    best = min(good, key=lambda r: r["ms"]) if good else min(results, key=lambda r: r["rel_err"])
+    _tuned[key] = {"bf16": best["bf16"], "wide": best["wide"], "candidates": results}
+    return _tuned[key]

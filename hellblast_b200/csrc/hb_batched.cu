@@ -359,22 +359,29 @@ __device__ __forceinline__ void store_split(uint8_t *A, int off, const float (&e
     *reinterpret_cast<uint4 *>(A + 3 * A_TILE + off) = lo;
 }
 
-// the 12 MMAs of one stage (2 parities x 2 K-steps x 3 split passes) into accumulator set `set`
+// The 12 MMAs of one stage (2 parities x 2 K-steps x 3 split passes).  The hi*hi products go to
+// accumulator set `hset`, the two cross products (about 2^-11 smaller) to set `lset`: the
+// tensor core's FP32 accumulation loses about one ulp of the accumulator per MMA, so keeping the
+// large products' set free of the cross products cuts the steps that round the result by 3x.
+// Live chunk i of a unit uses the set pair (hset, lset) = (2j, 2j+1), j = i mod (S/2); `first`
+// (the first S/2 live chunks) starts each set afresh.
 template <int N>
-__device__ __forceinline__ void issue_stage(uint32_t tmem, uint32_t a0, int set, bool first, uint32_t idesc) {
+__device__ __forceinline__ void issue_stage(uint32_t tmem, uint32_t a0, int hset, int lset, bool first,
+                                            uint32_t idesc) {
     const uint32_t b0 = a0 + A_STAGE;
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
-        const uint32_t d = tmem + set * 2 * N + q * N;
+        const uint32_t dh = tmem + hset * 2 * N + q * N, dl = tmem + lset * 2 * N + q * N;
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
             const uint64_t ah = tc::sdesc(a0 + (q * 2 + 0) * A_TILE + k * 256, 128, 512);
             const uint64_t al = tc::sdesc(a0 + (q * 2 + 1) * A_TILE + k * 256, 128, 512);
             const uint64_t bh = tc::sdesc(b0 + (q * 2 + 0) * (N * 64) + k * 256, 128, 512);
             const uint64_t bl = tc::sdesc(b0 + (q * 2 + 1) * (N * 64) + k * 256, 128, 512);
-            tc::mma_bf16(d, ah, bh, idesc, (!first || k > 0) ? 1u : 0u);
-            tc::mma_bf16(d, ah, bl, idesc, 1u);
-            tc::mma_bf16(d, al, bh, idesc, 1u);
+            const uint32_t acc = (!first || k > 0) ? 1u : 0u;
+            tc::mma_bf16(dh, ah, bh, idesc, acc);
+            tc::mma_bf16(dl, ah, bl, idesc, acc);
+            tc::mma_bf16(dl, al, bh, idesc, 1u);
         }
     }
 }
@@ -410,9 +417,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     constexpr int STAGE = A_STAGE + B_STAGE;
     constexpr uint32_t IDESC = tc::idesc_f16kind(128, N, 0, 0, BF16);
     constexpr float LS = BF16 ? 1.0f : 256.0f;  // lambda scale (|lambda| < 2^7 -> < 2^15 in half)
-    // S accumulator sets, chunk c accumulates into set c % S: the tensor core's FP32 accumulation
-    // error grows with the number of accumulate steps into one set; the epilogue sums the sets
-    // in IEEE FP32.
+    // S accumulator sets in S/2 (hi*hi, cross products) pairs, live chunk i using pair i mod S/2
+    // (issue_stage): the tensor core's FP32 accumulation error grows with the number of
+    // accumulate steps into one set; the epilogue sums the sets in IEEE FP32.
     constexpr int TCOLS = (2 * N * S < 32) ? 32 : 2 * N * S;
     static_assert(2 * N * S <= 512, "TMEM holds 512 columns");
     extern __shared__ __align__(1024) uint8_t smem[];
@@ -498,7 +505,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             tc::fence_after();
             const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
             const float *scl = G.dscale + (int64_t)m * (N / 2);
-            const int nsets = nch - c0 < S ? nch - c0 : S;
+            const int nsets = 2 * (nch - c0) < S ? 2 * (nch - c0) : S;
 #pragma unroll 1
             for (int j = wg; j < N / 16; j += 2) {
                 float de[16], dd[16];
@@ -545,7 +552,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     }
                     ++itr;
                     tc::fence_after();
-                    issue_stage<N>(tmem, tc::smem_u32(smem + s * STAGE), (c - c0) % S, c - c0 < S, IDESC);
+                    issue_stage<N>(tmem, tc::smem_u32(smem + s * STAGE), 2 * ((c - c0) % (S / 2)),
+                                   2 * ((c - c0) % (S / 2)) + 1, c - c0 < S / 2, IDESC);
                     tc::mma_commit(&L.empty[s]);
                 }
                 if (!ok) break;
@@ -696,7 +704,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             const int le = l0 + 2 * row;
             const uint32_t taddr = tmem + ((uint32_t)(owner * 32) << 16);
             const float *scl = G.dscale + (int64_t)m * (N / 2);
-            const int nsets = npc - U.w < S ? npc - U.w : S;
+            const int nsets = 2 * (npc - U.w) < S ? 2 * (npc - U.w) : S;
 #pragma unroll 1
             for (int j = half; j < N / 16; j += 2) {
                 float de[16], dd[16];
@@ -736,7 +744,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         break;
                     }
                     tc::fence_after();
-                    issue_stage<N>(tmem, tc::smem_u32(smem + s * STAGE), (c - c0) % S, c - c0 < S, IDESC);
+                    issue_stage<N>(tmem, tc::smem_u32(smem + s * STAGE), 2 * ((c - c0) % (S / 2)),
+                                   2 * ((c - c0) % (S / 2)) + 1, c - c0 < S / 2, IDESC);
                     tc::mma_commit(&L.empty[s]);
                 }
                 if (!ok) break;

@@ -99,21 +99,21 @@ def test_batched_vs_oracle_small(hb, oracle):
     assert np.linalg.norm(back - refa) / np.linalg.norm(refa) < TOL
 
 
-@pytest.mark.parametrize("nside", [1024, 2048])
-def test_batched_pair_accuracy_at_full_size(hb, nside):
-    """The north-star bar: the batched (IEEE-half hi+lo, default) pair within 1e-5 of FP64 at
-    lmax = 2 nside - 1, 8 maps."""
+@pytest.mark.parametrize("nside,wide", [(1024, False), (2048, False), (2048, True)])
+def test_batched_pair_accuracy_at_full_size(hb, nside, wide):
+    """The north-star bar: the batched pair (IEEE-half hi+lo; 32- or 64-map groups) within 1e-5
+    of FP64 at lmax = 2 nside - 1, 8 maps (first and last checked)."""
     lmax, nmaps = 2 * nside - 1, 8
     a64 = _batch(hb, lmax, nmaps, seed=7)
-    mb = hb.batched.alm2map(a64.to(torch.complex64), nside, lmax)
-    bb = hb.batched.map2alm(mb, nside, lmax)
+    mb = hb.batched.alm2map(a64.to(torch.complex64), nside, lmax, wide=wide)
+    bb = hb.batched.map2alm(mb, nside, lmax, wide=wide)
     errs = []
     for i in (0, nmaps - 1):
         m64 = hb.hp_compat.alm2map(a64[i], nside, lmax=lmax)
         b64 = hb.hp_compat.map2alm(m64, lmax=lmax)
         errs.append((rel(mb[i], m64), rel(bb[i], b64)))
         del m64, b64
-    assert hb.batched.plan(nside, lmax, nmaps).status() == 0
+    assert hb.batched.plan(nside, lmax, nmaps, wide=wide).status() == 0
     assert all(e[0] < TOL and e[1] < TOL for e in errs), errs
 
 
@@ -137,3 +137,17 @@ def test_batched_graph_replay_matches_direct_calls(hb):
         assert bp.status() == 0
         assert torch.equal(maps, ref_maps)
         assert torch.equal(out, ref_alm)
+
+
+def test_autotune_picks_a_measured_configuration_within_tolerance(hb):
+    nside, lmax, nmaps = 32, 63, 40
+    t = hb.batched.autotune(nside, lmax, nmaps)
+    assert len(t["candidates"]) == 4 and all(c["ms"] > 0 for c in t["candidates"])
+    chosen = [c for c in t["candidates"] if (c["bf16"], c["wide"]) == (t["bf16"], t["wide"])][0]
+    assert chosen["ok"] and chosen["rel_err"] <= TOL
+    assert chosen["ms"] == min(c["ms"] for c in t["candidates"] if c["ok"])
+    a = _batch(hb, lmax, nmaps, seed=5).to(torch.complex64)
+    bp = hb.batched.plan(nside, lmax, nmaps, tuned=True)
+    assert (bp.bf16, bp.wide) == (t["bf16"], t["wide"])
+    m = bp.alm2map(a).reshape(nmaps, -1)
+    assert rel(m, hb.hp_compat.alm2map(a.to(torch.complex128), nside, lmax=lmax)) < TOL
