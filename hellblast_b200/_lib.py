@@ -65,6 +65,7 @@ SIGNATURES = {
     "hb_batched_profile": (i32, [vp, i32]),
     "hb_batched_stage_ms": (i32, [vp, ctypes.POINTER(ctypes.c_float)]),
     "hb_batched_graph_capture": (i32, [vp, vp, vp, vp]),
+    "hb_batched_work": (i32, [vp, ctypes.POINTER(i64), ctypes.POINTER(i32)]),
     "hb_batched_graph_launch": (i32, [vp, vp]),
 }
 for _p in ("f32", "f64"):

@@ -83,6 +83,15 @@ class BatchedPlan:
         keys = ("prep_alm", "tensor_synthesis", "ring_synthesis", "ring_analysis", "prep_f", "tensor_analysis")
         return dict(zip(keys, [float(v) for v in ms]))
 
+    def executed_mma_flop(self) -> dict:
+        """Tensor-core FLOP one alm2map / one map2alm call executes (after the evanescent skip):
+        12 MMAs of 128 x N x 16 per live chunk."""
+        ch = (ctypes.c_int64 * 2)()
+        n = ctypes.c_int(0)
+        L.call("hb_batched_work", self.handle, ch, ctypes.byref(n))
+        per_chunk = 12 * 2 * 128 * n.value * 16
+        return {"synthesis": ch[0] * per_chunk, "analysis": ch[1] * per_chunk, "mma_n": n.value}
+
     def status(self) -> int:
         code = ctypes.c_int(0)
         L.call("hb_batched_status", self.handle, ctypes.byref(code))

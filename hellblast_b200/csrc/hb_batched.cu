@@ -311,7 +311,7 @@ __global__ void __launch_bounds__(128) skip_table_kernel(GeomDev g, int lmax, co
 constexpr int TC_THREADS = 320;
 constexpr int TC_PRODUCERS = 256;
 template <int N> constexpr int tc_b_stage() { return 4 * N * 64; }  // [q][h][N x 32] 16-bit
-template <int N> constexpr int syn_stages() { return N >= 128 ? 2 : 4; }  // two rings
+template <int N> constexpr int syn_stages() { return N >= 128 ? 3 : 4; }
 template <int N> constexpr int ana_stages() { return N >= 128 ? 3 : 4; }
 template <int ST, int N> constexpr int tc_smem() { return ST * (A_STAGE + tc_b_stage<N>()) + 8 * 128 * 8 + 128; }
 
@@ -407,12 +407,14 @@ __device__ __forceinline__ void load_sets(uint32_t taddr, int j, int nsets, floa
 
 // ------------------------------------------------------------------------------------ synthesis
 // Chunk c (64 l) of a unit belongs to half-block hb = c / 2 (128 l); half-blocks alternate
-// between the two producer warp groups (g = hb % 2), each with its own ring of SPR stages.  The
-// MMA thread and the loader walk the chunks in order, taking chunk c from ring (c / 2) % 2.
+// between the two producer warp groups (g = hb % 2).  All live chunks of the CTA's units share
+// one ring of ST stages in order: the i-th live chunk (counted across units) uses stage i % ST
+// for the (i / ST)-th time, so a producer group waits only for the chunk ST places earlier and
+// both groups keep stages filled while the MMA thread drains them.
 template <int N, bool BF16, int S>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     synth_tc_kernel(const TcGroup *__restrict__ groups, const int4 *__restrict__ units, int nunits, int *err) {
-    constexpr int ST = syn_stages<N>(), SPR = ST / 2;
+    constexpr int ST = syn_stages<N>();
     constexpr int B_STAGE = tc_b_stage<N>();
     constexpr int STAGE = A_STAGE + B_STAGE;
     constexpr uint32_t IDESC = tc::idesc_f16kind(128, N, 0, 0, BF16);
@@ -441,7 +443,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         // ---------------- producers + epilogue
         const int wg = warp >> 2;                   // half-blocks hb with hb % 2 == wg
         const int r = ((warp & 3) << 5) | lane;     // row = pair within the block
-        uint32_t itr = 0;                           // chunks of this warp group's ring so far
+        uint32_t base = 0;                          // live chunks of the earlier units
         int ui = 0;
         for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++ui) {
             const int4 U = units[u];
@@ -473,9 +475,10 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 R.load(kpre, LS);
                 const bool fast = __all_sync(0xffffffffu, R.e == 0);
                 if (hb + 2 < nhb) fetch(hb + 2);
-                for (int cc = 0; cc < 2 && 2 * hb + cc < nch; ++cc, ++itr) {
-                    const int s = wg * SPR + (int)(itr % SPR);
-                    if (itr >= SPR && !warp_wait(&L.empty[s], ((itr / SPR) + 1) & 1)) {
+                for (int cc = 0; cc < 2 && 2 * hb + cc < nch; ++cc) {
+                    const uint32_t it = base + (uint32_t)(2 * hb + cc - c0);
+                    const int s = (int)(it % ST);
+                    if (it >= ST && !warp_wait(&L.empty[s], ((it / ST) + 1) & 1)) {
                         if (lane == 0) set_err(err, 1);
                         ok = false;
                         break;
@@ -526,11 +529,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             }
             tc::fence_before();
             tc::mbar_arrive(L.tfree);
+            base += (uint32_t)(nch - c0);
         }
     } else if (warp == 8) {
         // ---------------- MMA issuer
         if (lane == 0) {
-            uint32_t itr0 = 0, itr1 = 0;  // per-ring chunk counters
+            uint32_t base = 0;  // live chunks of the earlier units
             int ui = 0;
             for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++ui) {
                 const int4 U = units[u];
@@ -542,15 +546,13 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 }
                 tc::fence_after();
                 for (int c = c0; c < nch; ++c) {
-                    const int g = (c >> 1) & 1;
-                    uint32_t &itr = g ? itr1 : itr0;
-                    const int s = g * SPR + (int)(itr % SPR);
-                    if (!tc::mbar_wait(&L.full[s], (itr / SPR) & 1, HB_TC_WAIT_NS)) {
+                    const uint32_t it = base + (uint32_t)(c - c0);
+                    const int s = (int)(it % ST);
+                    if (!tc::mbar_wait(&L.full[s], (it / ST) & 1, HB_TC_WAIT_NS)) {
                         set_err(err, 4);
                         ok = false;
                         break;
                     }
-                    ++itr;
                     tc::fence_after();
                     issue_stage<N>(tmem, tc::smem_u32(smem + s * STAGE), 2 * ((c - c0) % (S / 2)),
                                    2 * ((c - c0) % (S / 2)) + 1, c - c0 < S / 2, IDESC);
@@ -558,6 +560,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 }
                 if (!ok) break;
                 tc::mma_commit(L.accum);
+                base += (uint32_t)(nch - c0);
             }
             if (!ok) {  // let issued MMAs finish before the tensor memory is released
                 tc::mma_commit(L.drain);
@@ -568,7 +571,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     } else {
         // ---------------- loader of the pre-split alm tiles
         if (lane == 0) {
-            uint32_t itr0 = 0, itr1 = 0;  // per-ring chunk counters
+            uint32_t base = 0;  // live chunks of the earlier units
             for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
                 const int4 U = units[u];
                 const TcGroup &G = groups[U.x];
@@ -576,18 +579,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 const int nch = (G.lmax - m + 64) / 64;
                 const uint4 *src = G.alm_tiles + G.alm_tile_ofs[m] * (16 * N);
                 for (int c = U.w; c < nch; ++c) {
-                    const int g = (c >> 1) & 1;
-                    uint32_t &itr = g ? itr1 : itr0;
-                    const int s = g * SPR + (int)(itr % SPR);
-                    if (itr >= SPR && !tc::mbar_wait(&L.empty[s], ((itr / SPR) + 1) & 1, HB_TC_WAIT_NS)) {
+                    const uint32_t it = base + (uint32_t)(c - U.w);
+                    const int s = (int)(it % ST);
+                    if (it >= ST && !tc::mbar_wait(&L.empty[s], ((it / ST) + 1) & 1, HB_TC_WAIT_NS)) {
                         set_err(err, 5);
                         ok = false;
                         break;
                     }
-                    ++itr;
                     tc::mbar_arrive_expect_tx(&L.full[s], B_STAGE);
                     tc::bulk_g2s(smem + s * STAGE + A_STAGE, src + (int64_t)c * (16 * N), B_STAGE, &L.full[s]);
                 }
+                base += (uint32_t)(nch - U.w);
             }
         }
         __syncwarp();
@@ -819,6 +821,7 @@ struct hb_batched_plan {
     bool profile = false;
     cudaEvent_t ev[8] = {};  // synthesis: 0 prep 1 tensor 2 ring 3 end; analysis: 4 ring 5 prep 6 tensor 7 end
     cudaGraphExec_t graph = nullptr;  // hb_batched_graph_capture
+    int64_t live_syn = 0, live_ana = 0;  // chunks the tensor kernels run after the evanescent skip
     int64_t total_maps = 0, total_pix = 0, total_alm = 0;
 };
 
@@ -1073,6 +1076,11 @@ int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int np
         }
         std::stable_sort(su.begin(), su.end(), [](auto &a, auto &b) { return a.first < b.first; });
         std::stable_sort(au.begin(), au.end(), [](auto &a, auto &b) { return a.first < b.first; });
+        for (const auto &x : su) bp->live_syn += (int64_t)(-x.first / N + 0.5);
+        for (const auto &x : au) {
+            const TcGroup &G = bp->hgroups[x.second.x];
+            bp->live_ana += G.npc - x.second.w;
+        }
         std::vector<int4> suv, auv;
         for (auto &x : su) suv.push_back(x.second);
         for (auto &x : au) auv.push_back(x.second);
@@ -1199,6 +1207,14 @@ int hb_batched_stage_ms(hb_batched_plan *bp, float *ms) {
     HB_CUDA_TRY(cudaEventSynchronize(bp->ev[7]));
     const int pairs[6][2] = {{0, 1}, {1, 2}, {2, 3}, {4, 5}, {5, 6}, {6, 7}};
     for (int i = 0; i < 6; ++i) HB_CUDA_TRY(cudaEventElapsedTime(&ms[i], bp->ev[pairs[i][0]], bp->ev[pairs[i][1]]));
+    return HB_OK;
+}
+
+int hb_batched_work(const hb_batched_plan *bp, int64_t *chunks, int *mma_n) {
+    if (!bp || !chunks || !mma_n) return fail(HB_ERR_INVALID, "hb_batched_work: null argument");
+    chunks[0] = bp->live_syn;
+    chunks[1] = bp->live_ana;
+    *mma_n = bp->N;
     return HB_OK;
 }
 

@@ -347,6 +347,46 @@ void orc_spin2_analysis(int lmax, int mmax, int64_t nr, const double *x, const d
     }
 }
 
+/* Spin-2 analysis restricted to the nms harmonic orders ms[j]: Qf, Uf [j][r] weighted Fourier
+ * coefficients of those m; E, B [j][lmax + 1] complex (zero below max(m, 2)).  Same sums as
+ * orc_spin2_analysis, for spot checks of transforms too large to run in full here. */
+void orc_spin2_analysis_ms(int lmax, int nms, const int *ms, int64_t nr, const double *x, const double *theta,
+                           const double *Qf, const double *Uf, double *E, double *B) {
+    memset(E, 0, sizeof(double) * 2 * (size_t)nms * (lmax + 1));
+    memset(B, 0, sizeof(double) * 2 * (size_t)nms * (lmax + 1));
+    if (lmax < 2) return;
+#pragma omp parallel
+    {
+        double *a = (double *)calloc((size_t)lmax + 2, sizeof(double)), *b = (double *)calloc((size_t)lmax + 2, sizeof(double)),
+               *c = (double *)calloc((size_t)lmax + 2, sizeof(double)), *a2 = (double *)calloc((size_t)lmax + 2, sizeof(double)),
+               *b2 = (double *)calloc((size_t)lmax + 2, sizeof(double)), *c2 = (double *)calloc((size_t)lmax + 2, sizeof(double));
+        double *lp2 = (double *)calloc((size_t)lmax + 1, sizeof(double)), *lm2 = (double *)calloc((size_t)lmax + 1, sizeof(double));
+#pragma omp for schedule(dynamic, 1)
+        for (int j = 0; j < nms; ++j) {
+            const int m = ms[j], l0 = m > 2 ? m : 2;
+            double *e = E + 2 * (size_t)j * (lmax + 1), *bb = B + 2 * (size_t)j * (lmax + 1);
+            spin_coefs(lmax, m, -2, a, b, c);
+            spin_coefs(lmax, m, 2, a2, b2, c2);
+            for (int64_t r = 0; r < nr; ++r) {
+                long double th = theta[r];
+                long double lc = log2l(cosl(0.5L * th)), lsn = log2l(sinl(0.5L * th));
+                spin_lambda_point(lmax, m, -2, x[r], lc, lsn, a, b, c, lp2);
+                spin_lambda_point(lmax, m, 2, x[r], lc, lsn, a2, b2, c2, lm2);
+                const double qr = Qf[2 * ((int64_t)j * nr + r)], qi = Qf[2 * ((int64_t)j * nr + r) + 1];
+                const double ur = Uf[2 * ((int64_t)j * nr + r)], ui = Uf[2 * ((int64_t)j * nr + r) + 1];
+                for (int l = l0; l <= lmax; ++l) {
+                    double lp = 0.5 * (lp2[l] + lm2[l]), lm = 0.5 * (lp2[l] - lm2[l]);
+                    e[2 * l] -= lp * qr - lm * ui;
+                    e[2 * l + 1] -= lp * qi + lm * ur;
+                    bb[2 * l] -= lp * ur + lm * qi;
+                    bb[2 * l + 1] -= lp * ui - lm * qr;
+                }
+            }
+        }
+        free(a); free(b); free(c); free(a2); free(b2); free(c2); free(lp2); free(lm2);
+    }
+}
+
 /* Spin-2 synthesis.  Qg[m][r] = -sum_l (E lp + i B lm), Ug[m][r] = -sum_l (B lp - i E lm). */
 void orc_spin2_synthesis(int lmax, int mmax, int64_t nr, const double *x, const double *theta,
                          const double *E, const double *B, double *Qg, double *Ug) {

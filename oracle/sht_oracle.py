@@ -48,9 +48,11 @@ def _lib():
         lib.orc_spin2_analysis.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int64, D, D, D, D, D, D]
         lib.orc_spin2_synthesis.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int64, D, D, D, D, D, D]
         lib.orc_alm2cl.argtypes = [ctypes.c_int, ctypes.c_int, D, D, D]
+        lib.orc_spin2_analysis_ms.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int64,
+                                              D, D, D, D, D, D]
         for f in (lib.orc_ring_tables, lib.orc_lambda_lm, lib.orc_legendre_analysis,
                   lib.orc_legendre_synthesis, lib.orc_spin2_lambda, lib.orc_spin2_analysis,
-                  lib.orc_spin2_synthesis, lib.orc_alm2cl):
+                  lib.orc_spin2_synthesis, lib.orc_alm2cl, lib.orc_spin2_analysis_ms):
             f.restype = None
         _LIB = lib
     return _LIB
@@ -266,6 +268,35 @@ def map2alm_spin2(Q, U, geom: dict, lmax: int, mmax: int | None = None, weights=
     _lib().orc_spin2_analysis(lmax, mmax, geom["nr"], _p(_c(geom["x"])), _p(_c(geom["theta"])),
                               _p(Qf.view(np.float64)), _p(Uf.view(np.float64)),
                               _p(E.view(np.float64)), _p(B.view(np.float64)))
+    return E, B
+
+
+def ring_analysis_ms(maps: np.ndarray, geom: dict, ms, weights) -> np.ndarray:
+    """ring_analysis for the harmonic orders ``ms`` only: F[j, r] for m = ms[j] (with the
+    quadrature weights, phase and alias fold of ring_analysis)."""
+    ms = np.asarray(ms, dtype=np.int64)
+    nr = geom["nr"]
+    F = np.zeros((ms.size, nr), dtype=np.complex128)
+    for r in range(nr):
+        n = int(geom["nphi"][r]); s = int(geom["ring_start"][r])
+        R = np.fft.rfft(np.asarray(maps[s:s + n], dtype=np.float64))
+        k = ms % n
+        D = np.where(k <= n // 2, R[np.minimum(k, n // 2)], np.conj(R[np.minimum(n - k, n // 2)]))
+        F[:, r] = D * np.exp(-1j * ms * geom["phi0"][r]) * (2.0 * math.pi * weights[r] / n)
+    return F
+
+
+def map2alm_spin2_ms(Q, U, geom: dict, lmax: int, ms):
+    """(E, B) [len(ms), lmax + 1] of map2alm_spin2 at the harmonic orders ``ms`` only."""
+    ms = np.ascontiguousarray(ms, dtype=np.int32)
+    w = geom["weights_dz"]
+    Qf = _c(ring_analysis_ms(Q, geom, ms, w))
+    Uf = _c(ring_analysis_ms(U, geom, ms, w))
+    E = np.zeros((ms.size, lmax + 1), dtype=np.complex128)
+    B = np.zeros((ms.size, lmax + 1), dtype=np.complex128)
+    _lib().orc_spin2_analysis_ms(lmax, int(ms.size), ms.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), geom["nr"],
+                                 _p(_c(geom["x"])), _p(_c(geom["theta"])), _p(Qf.view(np.float64)),
+                                 _p(Uf.view(np.float64)), _p(E.view(np.float64)), _p(B.view(np.float64)))
     return E, B
 
 

@@ -165,3 +165,21 @@ def test_alias_fold_exact_for_band_limited_ring(oracle):
     # DFT of the sampled cosine at bins (11 mod 8) = 3 and 5; phase e^{-i m phi0}
     ref = np.array([np.sum(f * np.exp(-1j * k * phi)) for k in range(17)])
     assert np.allclose(F[:, 0], ref, atol=1e-12)
+
+
+def test_spin2_analysis_at_selected_m_matches_full(oracle):
+    """The m-subset spin-2 analysis (used to spot-check transforms too large for the full
+    oracle) reproduces the full analysis at those m."""
+    nside, lmax = 16, 40
+    g = oracle.ring_tables(nside)
+    cl = 1.0 / (np.arange(lmax + 1) + 10.0) ** 2
+    E = oracle.synalm(cl, seed=1)
+    B = oracle.synalm(0.1 * cl, seed=2)
+    Q, U = oracle.alm2map_spin2(E, B, g, lmax)
+    E1, B1 = oracle.map2alm_spin2(Q, U, g, lmax)
+    ms = [0, 1, 2, 3, 17, 40]
+    Es, Bs = oracle.map2alm_spin2_ms(Q, U, g, lmax, ms)
+    for j, m in enumerate(ms):
+        idx = oracle.alm_index(lmax, np.arange(m, lmax + 1), m)
+        np.testing.assert_allclose(Es[j, m:], E1[idx], rtol=0, atol=1e-13)
+        np.testing.assert_allclose(Bs[j, m:], B1[idx], rtol=0, atol=1e-13)
