@@ -84,13 +84,15 @@ __device__ __forceinline__ float block_pow2_scale(float vmax) {
     return res;
 }
 
-// Both prep kernels: one CTA per (m, map of the group).  The CTA reads the map's m-slice of the
-// batch operand once, coalesced, into shared memory (one pad entry per 8 or 16 so that the
-// per-thread runs below hit distinct banks), takes its maximum |value| for the power-of-two scale
-// of this (m, map), then each thread turns one run of 8 consecutive K positions into the hi/lo
-// rows of the K-major core matrices (row n = 2 map + re/im; element (n, k) at
-// (n%8)*8 + (n/8)*256 + (k/8)*64 + k%8), written as 16-byte stores; a thread's re and im rows
-// are adjacent and fill one 32-byte sector.  Map columns past the group's maps get zeros.
+// Both prep kernels: persistent CTAs walk the (m, map) slices of the batch operand (maps fastest,
+// so one m's tile rows are written together), two slices in flight: while the CTA splits slice
+// s out of one shared-memory buffer, cp.async copies slice s + gridDim.x into the other (one pad
+// entry per 8 or 16 so that the per-thread runs below hit distinct banks).  For each slice the
+// CTA takes the maximum |value| (the power-of-two scale of that (m, map)), then each thread
+// turns one run of 8 consecutive K positions into the hi/lo rows of the K-major core matrices
+// (row n = 2 map + re/im; element (n, k) at (n%8)*8 + (n/8)*256 + (k/8)*64 + k%8), written as
+// 16-byte stores; a thread's re and im rows are adjacent and fill one 32-byte sector.  Map
+// columns past the group's maps get zeros.
 template <bool BF16>
 __device__ __forceinline__ void store_rows8(uint4 *chunk, int N, int qh, int n, int g, const float (&v)[8]) {
     uint4 hi, lo;
@@ -100,89 +102,141 @@ __device__ __forceinline__ void store_rows8(uint4 *chunk, int N, int qh, int n, 
     chunk[(e + (int64_t)N * 32) / 8] = lo;
 }
 
+constexpr int PREP_THREADS = 512;
+template <int N> __host__ __device__ constexpr int prep_slices(int mmax) { return (mmax + 1) * (N / 2); }
+
 // alm [map][nalm] complex64 -> per (m, 64-l chunk) the synthesis B tiles:
-// [q][h][N rows x 32 K (l = l0 + 2k + q)].
+// [q][h][N rows x 32 K (l = l0 + 2k + q)].  Slice = (m, map): alm l = m .. lmax, padded to
+// whole 64-l chunks; l - m = i at i + i / 16 in the buffer (68 entries per chunk).  alm columns
+// start on 8-byte boundaries, so the copies are 8-byte cp.async.
 template <int N, bool BF16>
-__global__ void __launch_bounds__(256, 4) prep_alm_tiles_kernel(const TcGroup *groups, int gi, const float2 *__restrict__ alm,
-                                                             int64_t alm_stride) {
-    extern __shared__ float2 sa[];  // l - m = i at i + i / 16
+__global__ void __launch_bounds__(PREP_THREADS, 2) prep_alm_tiles_kernel(const TcGroup *groups, int gi,
+                                                                         const float2 *__restrict__ alm,
+                                                                         int64_t alm_stride, int dbl) {
+    extern __shared__ float2 sa[];
     const TcGroup &G = groups[gi];
-    const int m = blockIdx.y, b = blockIdx.x;  // maps fastest: one m's tile rows are written together
-    if (m > G.mmax) return;
-    const int lmax = G.lmax;
-    const int nch = (lmax - m + 64) / 64;
-    const bool live = b < G.nmaps;
-    const float2 *src = alm + (int64_t)b * alm_stride + alm_idx(lmax, m, m);
-    float vmax = 0.f;
-#pragma unroll 8
-    for (int i = threadIdx.x; i < nch * 64; i += blockDim.x) {
-        const float2 v = (live && m + i <= lmax) ? src[i] : make_float2(0.f, 0.f);
-        sa[i + (i >> 4)] = v;
-        vmax = fmaxf(vmax, fmaxf(fabsf(v.x), fabsf(v.y)));
-    }
-    const float s = block_pow2_scale(vmax);  // barriers: the slice is in shared memory after it
-    if (threadIdx.x == 0) G.dscale[(int64_t)m * (N / 2) + b] = s;
-    uint4 *base = const_cast<uint4 *>(G.alm_tiles) + G.alm_tile_ofs[m] * (16 * N);
-    for (int it = threadIdx.x; it < nch * 4; it += blockDim.x) {  // (chunk c, k8 group g): l = l0 + 16 g + 0..15
-        const int c = it >> 2, g = it & 3;
-        const float2 *run = sa + 17 * it;  // 16 (it) + it
-        uint4 *chunk = base + (int64_t)c * (16 * N);
-#pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            float re[8], im[8];
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-                const float2 v = run[2 * k + q];
-                re[k] = v.x * s;
-                im[k] = v.y * s;
-            }
-            store_rows8<BF16>(chunk, N, q, 2 * b, g, re);
-            store_rows8<BF16>(chunk, N, q, 2 * b + 1, g, im);
+    const int lmax = G.lmax, ns = prep_slices<N>(G.mmax);
+    const int per = ((lmax + 64) / 64) * 68;  // one buffer: the largest slice (m = 0)
+    auto issue = [&](int s, float2 *dst) {
+        const int m = s / (N / 2), b = s % (N / 2);
+        const int nch = (lmax - m + 64) / 64;
+        const bool live = b < G.nmaps;
+        const float2 *src = alm + (int64_t)b * alm_stride + alm_idx(lmax, m, m);
+        for (int i = threadIdx.x; i < nch * 64; i += blockDim.x) {
+            float2 *d = dst + i + (i >> 4);
+            if (live && m + i <= lmax)
+                tc::cp_async8(d, src + i);
+            else
+                *d = make_float2(0.f, 0.f);
         }
+    };
+    int s = blockIdx.x, buf = 0;
+    if (dbl && s < ns) issue(s, sa);
+    tc::cp_async_commit();
+    for (; s < ns; s += gridDim.x, buf ^= dbl) {
+        const int sn = s + gridDim.x;
+        if (!dbl) issue(s, sa);  // single buffer: this slice now
+        else if (sn < ns) issue(sn, sa + (buf ^ 1) * per);
+        tc::cp_async_commit();
+        if (dbl) tc::cp_async_wait<1>(); else tc::cp_async_wait<0>();
+        __syncthreads();
+        const int m = s / (N / 2), b = s % (N / 2);
+        const int nch = (lmax - m + 64) / 64;
+        const float2 *cur = sa + buf * per;
+        float vmax = 0.f;
+        for (int i = threadIdx.x; i < nch * 64; i += blockDim.x) {
+            const float2 v = cur[i + (i >> 4)];
+            vmax = fmaxf(vmax, fmaxf(fabsf(v.x), fabsf(v.y)));
+        }
+        const float sc = block_pow2_scale(vmax);
+        if (threadIdx.x == 0) G.dscale[(int64_t)m * (N / 2) + b] = sc;
+        uint4 *base = const_cast<uint4 *>(G.alm_tiles) + G.alm_tile_ofs[m] * (16 * N);
+        for (int it = threadIdx.x; it < nch * 4; it += blockDim.x) {  // (chunk c, k8 group g): l = l0 + 16 g + 0..15
+            const int c = it >> 2, g = it & 3;
+            const float2 *run = cur + 17 * it;  // 16 (it) + it
+            uint4 *chunk = base + (int64_t)c * (16 * N);
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                float re[8], im[8];
+#pragma unroll
+                for (int k = 0; k < 8; ++k) {
+                    const float2 v = run[2 * k + q];
+                    re[k] = v.x * sc;
+                    im[k] = v.y * sc;
+                }
+                store_rows8<BF16>(chunk, N, q, 2 * b, g, re);
+                store_rows8<BF16>(chunk, N, q, 2 * b + 1, g, im);
+            }
+        }
+        __syncthreads();  // every thread is done with this buffer before it is refilled
     }
+    tc::cp_async_wait<0>();
 }
 
 // F [map][m][pair][2] -> per (m, 32-pair chunk) the analysis B tiles [q][h][N x 32 pairs]
-// (E = F_N + F_S for q = 0, O = F_N - F_S for q = 1).
+// (E = F_N + F_S for q = 0, O = F_N - F_S for q = 1).  Slice = (m, map): npairs 16-byte
+// (north, south) entries, pair p at p + p / 8 in the buffer (36 entries per 32-pair chunk).
 template <int N, bool BF16>
-__global__ void __launch_bounds__(256, 3) prep_g_tiles_kernel(const TcGroup *groups, int gi, const float2 *__restrict__ F,
-                                                           int64_t f_stride) {
-    extern __shared__ float4 sf[];  // pair p (north, south) at p + p / 8
+__global__ void __launch_bounds__(PREP_THREADS, 1) prep_g_tiles_kernel(const TcGroup *groups, int gi,
+                                                                       const float2 *__restrict__ F, int64_t f_stride,
+                                                                       int dbl) {
+    extern __shared__ float4 sf[];
     const TcGroup &G = groups[gi];
-    const int m = blockIdx.y, b = blockIdx.x;  // maps fastest: one m's tile rows are written together
-    if (m > G.mmax) return;
     const int64_t np = G.g.npairs;
-    const int npc = (int)G.npc;
-    const bool live = b < G.nmaps;
-    const float4 *src = reinterpret_cast<const float4 *>(F + (int64_t)b * f_stride + (int64_t)m * np * 2);
-    float vmax = 0.f;
-#pragma unroll 8
-    for (int p = threadIdx.x; p < npc * 32; p += blockDim.x) {
-        const float4 f = (live && p < np) ? src[p] : make_float4(0.f, 0.f, 0.f, 0.f);
-        sf[p + (p >> 3)] = f;
-        vmax = fmaxf(vmax, fmaxf(fmaxf(fabsf(f.x + f.z), fabsf(f.y + f.w)), fmaxf(fabsf(f.x - f.z), fabsf(f.y - f.w))));
-    }
-    const float s = block_pow2_scale(vmax);
-    if (threadIdx.x == 0) G.dscale[(int64_t)m * (N / 2) + b] = s;
-    uint4 *base = const_cast<uint4 *>(G.g_tiles) + (int64_t)m * npc * (16 * N);
-    for (int it = threadIdx.x; it < npc * 4; it += blockDim.x) {  // (chunk c, k8 group g): pairs 8 it .. 8 it + 7
-        const int c = it >> 2, g = it & 3;
-        const float4 *run = sf + 9 * it;
-        uint4 *chunk = base + (int64_t)c * (16 * N);
-        float er[8], ei[8], orr[8], oi[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            const float4 f = run[j];
-            er[j] = (f.x + f.z) * s;
-            ei[j] = (f.y + f.w) * s;
-            orr[j] = (f.x - f.z) * s;
-            oi[j] = (f.y - f.w) * s;
+    const int npc = (int)G.npc, ns = prep_slices<N>(G.mmax), per = npc * 36;
+    auto issue = [&](int s, float4 *dst) {  // cp.async of slice s into dst, one commit group
+        const int m = s / (N / 2), b = s % (N / 2);
+        const bool live = b < G.nmaps;
+        const float4 *src = reinterpret_cast<const float4 *>(F + (int64_t)b * f_stride + (int64_t)m * np * 2);
+        for (int p = threadIdx.x; p < npc * 32; p += blockDim.x) {
+            float4 *d = dst + p + (p >> 3);
+            if (live && p < np)
+                tc::cp_async16(d, src + p);
+            else
+                *d = make_float4(0.f, 0.f, 0.f, 0.f);
         }
-        store_rows8<BF16>(chunk, N, 0, 2 * b, g, er);
-        store_rows8<BF16>(chunk, N, 0, 2 * b + 1, g, ei);
-        store_rows8<BF16>(chunk, N, 1, 2 * b, g, orr);
-        store_rows8<BF16>(chunk, N, 1, 2 * b + 1, g, oi);
+    };
+    int s = blockIdx.x, buf = 0;
+    if (dbl && s < ns) issue(s, sf);
+    tc::cp_async_commit();
+    for (; s < ns; s += gridDim.x, buf ^= dbl) {
+        const int sn = s + gridDim.x;
+        if (!dbl) issue(s, sf);  // single buffer (no room for two): this slice now
+        else if (sn < ns) issue(sn, sf + (buf ^ 1) * per);  // the buffer freed by the previous slice
+        tc::cp_async_commit();
+        if (dbl) tc::cp_async_wait<1>(); else tc::cp_async_wait<0>();  // this slice's copies are done
+        __syncthreads();
+        const int m = s / (N / 2), b = s % (N / 2);
+        const float4 *cur = sf + buf * per;
+        float vmax = 0.f;
+        for (int p = threadIdx.x; p < npc * 32; p += blockDim.x) {
+            const float4 f = cur[p + (p >> 3)];
+            vmax = fmaxf(vmax, fmaxf(fmaxf(fabsf(f.x + f.z), fabsf(f.y + f.w)), fmaxf(fabsf(f.x - f.z), fabsf(f.y - f.w))));
+        }
+        const float sc = block_pow2_scale(vmax);
+        if (threadIdx.x == 0) G.dscale[(int64_t)m * (N / 2) + b] = sc;
+        uint4 *base = const_cast<uint4 *>(G.g_tiles) + (int64_t)m * npc * (16 * N);
+        for (int it = threadIdx.x; it < npc * 4; it += blockDim.x) {  // (chunk c, k8 group g): pairs 8 it .. 8 it + 7
+            const int c = it >> 2, g = it & 3;
+            const float4 *run = cur + 9 * it;
+            uint4 *chunk = base + (int64_t)c * (16 * N);
+            float er[8], ei[8], orr[8], oi[8];
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const float4 f = run[j];
+                er[j] = (f.x + f.z) * sc;
+                ei[j] = (f.y + f.w) * sc;
+                orr[j] = (f.x - f.z) * sc;
+                oi[j] = (f.y - f.w) * sc;
+            }
+            store_rows8<BF16>(chunk, N, 0, 2 * b, g, er);
+            store_rows8<BF16>(chunk, N, 0, 2 * b + 1, g, ei);
+            store_rows8<BF16>(chunk, N, 1, 2 * b, g, orr);
+            store_rows8<BF16>(chunk, N, 1, 2 * b + 1, g, oi);
+        }
+        __syncthreads();  // every thread is done with this buffer before it is refilled
     }
+    tc::cp_async_wait<0>();
 }
 
 // ------------------------------------------------------------------------------------ recursion
@@ -861,21 +915,38 @@ static int launch_ana(hb_batched_plan *bp, float2 *alm_out, cudaStream_t st) {
     HB_CHECK_LAUNCH();
     return HB_OK;
 }
+// prep launch: persistent CTAs (one or two per SM), two slice buffers when they fit in shared
+// memory, else one
+static int max_smem_optin_b() {
+    static int v = -1;
+    if (v < 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) v = 48 * 1024;
+    }
+    return v;
+}
 template <int N, bool BF16>
 static int launch_prep_alm(hb_batched_plan *bp, int gi, const float2 *alm, int64_t stride, cudaStream_t st) {
     const TcGroup &G = bp->hgroups[gi];
-    const int smem = (int)(sizeof(float2) * (size_t)(((G.lmax + 64) / 64) * 68));  // 64 l + 4 pads per chunk
+    const size_t one = sizeof(float2) * (size_t)(((G.lmax + 64) / 64) * 68);  // 64 l + 4 pads per chunk
+    const int dbl = 2 * one <= (size_t)max_smem_optin_b() ? 1 : 0;
+    const int smem = (int)(one * (dbl ? 2 : 1));
     HB_CUDA_TRY(cudaFuncSetAttribute(prep_alm_tiles_kernel<N, BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    prep_alm_tiles_kernel<N, BF16><<<dim3(N / 2, G.mmax + 1), 256, smem, st>>>(bp->dgroups, gi, alm, stride);
+    const int grid = std::min(prep_slices<N>(G.mmax), sm_count() * 2);
+    prep_alm_tiles_kernel<N, BF16><<<grid, PREP_THREADS, smem, st>>>(bp->dgroups, gi, alm, stride, dbl);
     HB_CHECK_LAUNCH();
     return HB_OK;
 }
 template <int N, bool BF16>
 static int launch_prep_g(hb_batched_plan *bp, int gi, const float2 *F, int64_t stride, cudaStream_t st) {
     const TcGroup &G = bp->hgroups[gi];
-    const int smem = (int)(sizeof(float4) * (size_t)(G.npc * 36));  // 32 pairs + 4 pads per chunk
+    const size_t one = sizeof(float4) * (size_t)(G.npc * 36);  // 32 pairs + 4 pads per chunk
+    const int dbl = 2 * one <= (size_t)max_smem_optin_b() ? 1 : 0;
+    const int smem = (int)(one * (dbl ? 2 : 1));
     HB_CUDA_TRY(cudaFuncSetAttribute(prep_g_tiles_kernel<N, BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    prep_g_tiles_kernel<N, BF16><<<dim3(N / 2, G.mmax + 1), 256, smem, st>>>(bp->dgroups, gi, F, stride);
+    const int grid = std::min(prep_slices<N>(G.mmax), sm_count() * (dbl ? 1 : 2));
+    prep_g_tiles_kernel<N, BF16><<<grid, PREP_THREADS, smem, st>>>(bp->dgroups, gi, F, stride, dbl);
     HB_CHECK_LAUNCH();
     return HB_OK;
 }
@@ -1054,7 +1125,7 @@ int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int np
             rc = fail(HB_ERR_CUDA, "hb_batched_plan_create: skip tables");
         cudaFree(dsk);
     }
-    if (rc == HB_OK) {  // units with their skip counts, sorted by decreasing remaining work
+    if (rc == HB_OK) {  // units with their skip counts
         std::vector<std::pair<double, int4>> su, au;
         for (int gi = 0; gi < ngroups; ++gi) {
             const TcGroup &G = bp->hgroups[gi];
@@ -1074,8 +1145,17 @@ int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int np
                 }
             }
         }
-        std::stable_sort(su.begin(), su.end(), [](auto &a, auto &b) { return a.first < b.first; });
-        std::stable_sort(au.begin(), au.end(), [](auto &a, auto &b) { return a.first < b.first; });
+        // Order by (group, m), larger work first within an m: the CTAs take units round-robin,
+        // so all units of one m run at the same time on neighbouring CTAs and share that m's
+        // operand tiles through L2 (each analysis unit streams every pair chunk of its m, each
+        // synthesis unit every l chunk); the round-robin keeps the CTAs' totals balanced.
+        auto by_m = [](const std::pair<double, int4> &a, const std::pair<double, int4> &b) {
+            if (a.second.x != b.second.x) return a.second.x < b.second.x;
+            if (a.second.y != b.second.y) return a.second.y < b.second.y;
+            return a.first < b.first;
+        };
+        std::stable_sort(su.begin(), su.end(), by_m);
+        std::stable_sort(au.begin(), au.end(), by_m);
         for (const auto &x : su) bp->live_syn += (int64_t)(-x.first / N + 0.5);
         for (const auto &x : au) {
             const TcGroup &G = bp->hgroups[x.second.x];
