@@ -18,6 +18,7 @@ from .spin import eb_from_qu_gpu, map2alm_spin_gpu, qu_from_eb_gpu
 from . import hp_compat  # noqa: F401
 from . import autograd  # noqa: F401
 from . import batched  # noqa: F401
+from . import smoothing  # noqa: F401
 
 map2alm = map2alm_gpu
 alm2map = alm2map_gpu
@@ -27,4 +28,5 @@ __all__ = [
     "map2alm_gpu", "alm2map_gpu", "anafast_ring", "map2alm", "alm2map", "anafast",
     "almxfl", "alm2cl", "synalm", "alm_index", "alm_size", "getlmax", "healpy_to_ref", "ref_to_healpy",
     "HealpixRingTables", "map2alm_spin_gpu", "eb_from_qu_gpu", "qu_from_eb_gpu", "hp_compat", "autograd",
+    "batched", "smoothing",
 ]

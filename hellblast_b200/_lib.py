@@ -61,6 +61,7 @@ SIGNATURES = {
     "hb_batched_plan_bytes": (sz, [vp]),
     "hb_batched_alm2map": (i32, [vp, vp, vp, vp]),
     "hb_batched_map2alm": (i32, [vp, vp, vp, vp]),
+    "hb_batched_map2alm_fl": (i32, [vp, vp, vp, vp, vp]),
     "hb_batched_status": (i32, [vp, ctypes.POINTER(i32)]),
     "hb_batched_profile": (i32, [vp, i32]),
     "hb_batched_stage_ms": (i32, [vp, ctypes.POINTER(ctypes.c_float)]),

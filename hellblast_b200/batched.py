@@ -49,13 +49,19 @@ class BatchedPlan:
                torch.cuda.current_stream(alm.device).cuda_stream)
         return out
 
-    def map2alm(self, maps: torch.Tensor, out: torch.Tensor | None = None) -> torch.Tensor:
+    def map2alm(self, maps: torch.Tensor, out: torch.Tensor | None = None, fl: torch.Tensor | None = None) -> torch.Tensor:
+        """maps -> alm; with ``fl`` (a per-l filter, >= max lmax + 1 values) every alm(l, m) is
+        multiplied by fl[l] in the tensor-core kernel's store (almxfl fused)."""
         maps = maps.reshape(-1).contiguous()
         if maps.dtype != torch.float32 or maps.numel() != self.total_pix or not maps.is_cuda:
             raise ValueError(f"maps must be a CUDA float32 tensor of {self.total_pix} elements")
         out = torch.empty(self.total_alm, dtype=torch.complex64, device=maps.device) if out is None else out
-        L.call("hb_batched_map2alm", self.handle, maps.data_ptr(), out.data_ptr(),
-               torch.cuda.current_stream(maps.device).cuda_stream)
+        if fl is not None:
+            fl = torch.as_tensor(fl, dtype=torch.float32, device=maps.device).contiguous()
+            if fl.numel() < max(s[1] for s in self.specs) + 1:
+                raise ValueError("fl needs at least lmax + 1 entries")
+        L.call("hb_batched_map2alm_fl", self.handle, maps.data_ptr(), out.data_ptr(),
+               None if fl is None else fl.data_ptr(), torch.cuda.current_stream(maps.device).cuda_stream)
         return out
 
     def capture(self, alm: torch.Tensor | None, maps: torch.Tensor, out: torch.Tensor | None) -> None:

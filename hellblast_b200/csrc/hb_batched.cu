@@ -663,7 +663,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 template <int N, bool BF16, int S>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     anal_tc_kernel(const TcGroup *__restrict__ groups, const int4 *__restrict__ units, int nunits, float2 *alm_out,
-                   int *err) {
+                   int *err, const float *__restrict__ fl) {
     constexpr int ST = ana_stages<N>();
     constexpr int B_STAGE = tc_b_stage<N>();
     constexpr int STAGE = A_STAGE + B_STAGE;
@@ -771,8 +771,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     if (b < G.nmaps) {
                         float2 *dst = alm_out + G.alm_out_ofs + (int64_t)b * G.alm_stride + alm_idx(lmax, le, m);
                         const float inv = 1.0f / (LS * scl[b]);
-                        if (le <= lmax) dst[0] = make_float2(de[2 * h] * inv, de[2 * h + 1] * inv);
-                        if (le + 1 <= lmax) dst[1] = make_float2(dd[2 * h] * inv, dd[2 * h + 1] * inv);
+                        // optional per-l filter (almxfl fused into the store)
+                        const float f0 = fl && le <= lmax ? fl[le] * inv : inv;
+                        const float f1 = fl && le + 1 <= lmax ? fl[le + 1] * inv : inv;
+                        if (le <= lmax) dst[0] = make_float2(de[2 * h] * f0, de[2 * h + 1] * f0);
+                        if (le + 1 <= lmax) dst[1] = make_float2(dd[2 * h] * f1, dd[2 * h + 1] * f1);
                     }
                 }
             }
@@ -905,13 +908,13 @@ static int launch_syn(hb_batched_plan *bp, cudaStream_t st) {
     return HB_OK;
 }
 template <int N, bool BF16>
-static int launch_ana(hb_batched_plan *bp, float2 *alm_out, cudaStream_t st) {
+static int launch_ana(hb_batched_plan *bp, float2 *alm_out, const float *fl, cudaStream_t st) {
     const int smem = tc_smem<ana_stages<N>(), N>();
     constexpr int S = nsets<N>();
     HB_CUDA_TRY(cudaFuncSetAttribute(anal_tc_kernel<N, BF16, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     const int grid = std::min(bp->n_ana, sm_count());
     anal_tc_kernel<N, BF16, S><<<grid, TC_THREADS, smem, st>>>(bp->dgroups, bp->ana_units, bp->n_ana, alm_out,
-                                                                 bp->err);
+                                                                 bp->err, fl);
     HB_CHECK_LAUNCH();
     return HB_OK;
 }
@@ -1215,6 +1218,10 @@ int hb_batched_alm2map(hb_batched_plan *bp, const float *alm, float *maps, hb_st
 }
 
 int hb_batched_map2alm(hb_batched_plan *bp, const float *maps, float *alm, hb_stream_t stream) {
+    return hb_batched_map2alm_fl(bp, maps, alm, nullptr, stream);
+}
+
+int hb_batched_map2alm_fl(hb_batched_plan *bp, const float *maps, float *alm, const float *fl, hb_stream_t stream) {
     if (!bp || !alm || !maps) return fail(HB_ERR_INVALID, "hb_batched_map2alm: null argument");
     cudaStream_t st = (cudaStream_t)stream;
     int rc;
@@ -1232,7 +1239,7 @@ int hb_batched_map2alm(hb_batched_plan *bp, const float *maps, float *alm, hb_st
         if ((rc = HB_DISPATCH_N(bp, launch_prep_g)(bp, (int)gi, F, part.gf_stride, st))) return rc;
     }
     if (bp->profile) HB_CUDA_TRY(cudaEventRecord(bp->ev[6], st));
-    if ((rc = HB_DISPATCH_N(bp, launch_ana)(bp, (float2 *)alm, st))) return rc;
+    if ((rc = HB_DISPATCH_N(bp, launch_ana)(bp, (float2 *)alm, fl, st))) return rc;
     if (bp->profile) HB_CUDA_TRY(cudaEventRecord(bp->ev[7], st));
     return HB_OK;
 }

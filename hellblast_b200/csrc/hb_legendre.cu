@@ -94,6 +94,25 @@ template <> __device__ __forceinline__ double down_v<double>() { return 0x1p-512
 
 constexpr int COEF_CH = 256;  // l values per shared-memory coefficient chunk
 
+// Evanescent skip of the FP32 synthesis: a thread's K ring pairs are consecutive, so a warp
+// covers 32 K consecutive pairs.  Below its turning point a pair's recursion state has a negative
+// exponent (its values kept in units 2^-64 lower) and the exponent never decreases with l; if
+// every pair of the warp still has e < 0 at the checkpoint that ends the current 256-l block, the
+// warp skips the block (the next block re-anchors on its checkpoint anyway), dropping
+// contributions below 2^-64 of the result.  (The analysis kernel keeps its strided pair
+// mapping: its per-l block reduction runs for every warp, so skipping saved nothing there.)
+template <int K>
+__device__ __forceinline__ bool warp_block_dead(const float4 *__restrict__ ck, const int64_t *__restrict__ blk_ofs,
+                                                int m, int jnext, int64_t np, int64_t p0) {
+    if (blk_ofs[m] + jnext >= blk_ofs[m + 1]) return false;  // the block reaches lmax: no end checkpoint
+    const float4 *cb = ck + (blk_ofs[m] + jnext) * np;
+    bool dead = true;
+#pragma unroll
+    for (int k = 0; k < K; ++k)
+        if (p0 + k < np) dead &= __float_as_int(cb[p0 + k].z) < 0;
+    return __all_sync(0xffffffffu, dead);
+}
+
 template <typename T, int K, int NT>
 __global__ void __launch_bounds__(NT, 2) leg_analysis_kernel(GeomDev g, int lmax, int mmax, const c2_t<T> *__restrict__ Fm,
                                                              int64_t fm_stride, c2_t<T> *__restrict__ alm,
@@ -265,7 +284,7 @@ __global__ void __launch_bounds__(NT, 2) leg_synthesis_kernel(GeomDev g, int lma
     bool anyneg = false;
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-        const int64_t p = (int64_t)chunk * NT * K + (int64_t)k * NT + tid;
+        const int64_t p = (int64_t)chunk * NT * K + (int64_t)tid * K + k;
         l1[k] = (T)0;
         ae[k] = ao[k] = mk2((T)0, (T)0);
         if (p < np) {
@@ -280,6 +299,7 @@ __global__ void __launch_bounds__(NT, 2) leg_synthesis_kernel(GeomDev g, int lma
             e[k] = 0;
         }
     }
+    bool skip = false;  // this warp's rows are all evanescent through the current block
     for (int l0 = m; l0 <= lmax; l0 += 4) {
         const int lrel = l0 - m;
         if ((lrel % COEF_CH) == 0) {
@@ -297,7 +317,7 @@ __global__ void __launch_bounds__(NT, 2) leg_synthesis_kernel(GeomDev g, int lma
                     anyneg = false;
 #pragma unroll
                     for (int k = 0; k < K; ++k) {
-                        const int64_t p = (int64_t)chunk * NT * K + (int64_t)k * NT + tid;
+                        const int64_t p = (int64_t)chunk * NT * K + (int64_t)tid * K + k;
                         if (p < np) {
                             const float4 c = cb[p];
                             l1[k] = c.x;
@@ -313,8 +333,12 @@ __global__ void __launch_bounds__(NT, 2) leg_synthesis_kernel(GeomDev g, int lma
                         }
                     }
                 }
+                if (ck != nullptr)
+                    skip = warp_block_dead<K>(ck, blk_ofs, m, lrel / COEF_CH + 1, np,
+                                              (int64_t)chunk * NT * K + (int64_t)tid * K);
             }
         }
+        if (skip) continue;
         const int i0 = lrel % COEF_CH;
 #pragma unroll
         for (int s = 0; s < 4; ++s) {
@@ -352,7 +376,7 @@ __global__ void __launch_bounds__(NT, 2) leg_synthesis_kernel(GeomDev g, int lma
     }
 #pragma unroll
     for (int k = 0; k < K; ++k) {
-        const int64_t p = (int64_t)chunk * NT * K + (int64_t)k * NT + tid;
+        const int64_t p = (int64_t)chunk * NT * K + (int64_t)tid * K + k;
         if (p < np) {
             T f = (e[k] == 0) ? (T)1 : (T)ldexp(1.0, LegCfg<T>::SE * e[k]);
             V gn = cscale(cadd(ae[k], ao[k]), f), gs = cscale(csub(ae[k], ao[k]), f);

@@ -113,7 +113,7 @@ __device__ __forceinline__ void spin_weights(V qn, V qs, V un, V us, T eps, V &w
 }
 
 template <typename T, int K, int NT>
-__global__ void __launch_bounds__(NT) spin_analysis_kernel(GeomDev g, int lmax, int mmax, const c2_t<T> *__restrict__ QF,
+__global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 4 : 1) spin_analysis_kernel(GeomDev g, int lmax, int mmax, const c2_t<T> *__restrict__ QF,
                                                            const c2_t<T> *__restrict__ UF, int64_t fm_stride,
                                                            c2_t<T> *__restrict__ Eo, c2_t<T> *__restrict__ Bo,
                                                            int64_t alm_stride, int atomic,
@@ -283,7 +283,7 @@ __global__ void __launch_bounds__(NT) spin_analysis_kernel(GeomDev g, int lmax, 
 }
 
 template <typename T, int K, int NT>
-__global__ void __launch_bounds__(NT) spin_synthesis_kernel(GeomDev g, int lmax, int mmax, const c2_t<T> *__restrict__ E,
+__global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 4 : 1) spin_synthesis_kernel(GeomDev g, int lmax, int mmax, const c2_t<T> *__restrict__ E,
                                                             const c2_t<T> *__restrict__ B, int64_t alm_stride,
                                                             c2_t<T> *__restrict__ QG, c2_t<T> *__restrict__ UG,
                                                             int64_t gm_stride, const float4 *__restrict__ ckP,
@@ -475,7 +475,7 @@ template <typename T>
 static int spin_analysis_t(const GeomDev &g, int nmaps, int lmax, int mmax, const c2_t<T> *QF, const c2_t<T> *UF,
                            c2_t<T> *E, c2_t<T> *B, cudaStream_t st, const float4 *ckP, const float4 *ckM,
                            const int64_t *bo) {
-    if (g.npairs >= 512) return run_spin_analysis<T, 4, 128>(g, nmaps, lmax, mmax, QF, UF, E, B, st, ckP, ckM, bo);
+    if (g.npairs >= 256) return run_spin_analysis<T, 2, 128>(g, nmaps, lmax, mmax, QF, UF, E, B, st, ckP, ckM, bo);
     if (g.npairs >= 128) return run_spin_analysis<T, 2, 64>(g, nmaps, lmax, mmax, QF, UF, E, B, st, ckP, ckM, bo);
     return run_spin_analysis<T, 1, 64>(g, nmaps, lmax, mmax, QF, UF, E, B, st, ckP, ckM, bo);
 }
@@ -484,7 +484,7 @@ template <typename T>
 static int spin_synthesis_t(const GeomDev &g, int nmaps, int lmax, int mmax, const c2_t<T> *E, const c2_t<T> *B,
                             c2_t<T> *QG, c2_t<T> *UG, cudaStream_t st, const float4 *ckP, const float4 *ckM,
                             const int64_t *bo) {
-    if (g.npairs >= 512) return run_spin_synthesis<T, 4, 128>(g, nmaps, lmax, mmax, E, B, QG, UG, st, ckP, ckM, bo);
+    if (g.npairs >= 256) return run_spin_synthesis<T, 2, 128>(g, nmaps, lmax, mmax, E, B, QG, UG, st, ckP, ckM, bo);
     if (g.npairs >= 128) return run_spin_synthesis<T, 2, 64>(g, nmaps, lmax, mmax, E, B, QG, UG, st, ckP, ckM, bo);
     return run_spin_synthesis<T, 1, 64>(g, nmaps, lmax, mmax, E, B, QG, UG, st, ckP, ckM, bo);
 }

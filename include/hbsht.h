@@ -218,6 +218,11 @@ HB_API int hb_batched_plan_destroy(hb_batched_plan *bp);
 HB_API size_t hb_batched_plan_bytes(const hb_batched_plan *bp);
 HB_API int hb_batched_alm2map(hb_batched_plan *bp, const float *alm, float *maps, hb_stream_t stream);
 HB_API int hb_batched_map2alm(hb_batched_plan *bp, const float *maps, float *alm, hb_stream_t stream);
+/* hb_batched_map2alm with a per-l filter fused into the alm store: alm(l, m) *= fl[l] (device
+ * float array, at least max lmax + 1 entries over the plans; null = none).  The beam / pixel-window
+ * step of the smoothing pipeline (almxfl after map2alm; beams.py:38-47, smoothing.py:5-14). */
+HB_API int hb_batched_map2alm_fl(hb_batched_plan *bp, const float *maps, float *alm, const float *fl,
+                                 hb_stream_t stream);
 HB_API int hb_batched_status(hb_batched_plan *bp, int *code);
 /* Work the tensor-core kernels execute per call after the evanescent skip: chunks[0] synthesis
  * chunks (64 l x 128 ring pairs each), chunks[1] analysis chunks (32 ring pairs x 256 l each);
