@@ -28,9 +28,9 @@
 //     then inverse DIF and a digit-order read for the coalesced ring store;
 //   * synthesis, Bluestein ring: the same fused middle, and the last inverse DIT pass writes the
 //     ring to global memory.
-// Twiddles come from one table per geometry, W^j = exp(-2 pi i j/Lmax), j < Lmax/2
-// (FP64-computed, rounded for FP32): a radix-16 butterfly loads W^p, W^2p, W^4p, W^8p and forms
-// the others by at most three products.  The Bluestein chirp exp(-i pi j^2/N) is a stored table
+// Twiddles: a radix-16 butterfly takes W^p, W^2p, W^4p, W^8p and forms the others by at most
+// three products; FP32 computes the four with sincospif of exact arguments, FP64 reads them
+// from one table per geometry, W^j = exp(-2 pi i j/Lmax), j < Lmax/2 (FP64-computed).  The Bluestein chirp exp(-i pi j^2/N) is a stored table
 // per distinct N (after its spectrum).  The per-m factors of the untangling (exp(-2 pi i k/n))
 // and the ring phase (exp(-i m phi0)) are products of two entries of small per-ring tables
 // (64 fine steps x coarse steps), built per CTA with a few hundred FP64 sincospi.
@@ -74,8 +74,14 @@ template <typename T> struct Tw {
     using V = c2_t<T>;
     const V *tab;  // exp(-2 pi i j / 2^log_tw), j < 2^(log_tw - 1)
     int log_tw;
-    // exp(-2 pi i e / 2^logS), 0 <= e < 2^logS <= 2^log_tw
+    // exp(-2 pi i e / 2^logS), 0 <= e < 2^logS <= 2^log_tw.  FP32: sincospif of the exact
+    // argument 2e / 2^logS (no memory access on the butterflies' critical path); FP64: the table.
     __device__ __forceinline__ V w(int e, int logS) const {
+        if constexpr (sizeof(T) == 4) {
+            float sn, cs;
+            sincospif(__int2float_rn(e) * __int_as_float((127 - (logS - 1)) << 23), &sn, &cs);
+            return mk2(cs, -sn);
+        }
         const int j = e << (log_tw - logS);
         const int half = 1 << (log_tw - 1);
         const V v = tab[j & (half - 1)];
