@@ -326,6 +326,38 @@ __device__ __forceinline__ void dif_to_smem(c2_t<T> *buf, int logL, const Tw<T> 
 
 __device__ __forceinline__ int ilog2(int L) { return 31 - __clz(L); }
 
+// exp(+i n phi0) of a ring of n pixels when it is exactly +1 or -1 (HEALPix rings, where
+// n phi0 is 0 or pi), else 0
+__device__ __forceinline__ int alias_sign(double phi0_pi, int n) {
+    const double t = phi0_pi * (double)n, f = t - 2.0 * floor(0.5 * t);
+    if (fabs(f) < 1e-12 || fabs(f - 2.0) < 1e-12) return 1;
+    if (fabs(f - 1.0) < 1e-12) return -1;
+    return 0;
+}
+
+// Lanes per bin pair: a ring of n = 2N pixels has K = N/2 + 1 bin pairs (k, N - k).  When K is
+// small against the block, S = 2^j <= 32 neighbouring lanes share one k and each takes every
+// S-th alias m0 + q n of its residue classes, so the alias loops of the small polar rings
+// (up to mmax / n aliases per class) do not run on one thread each.
+__device__ __forceinline__ int lanes_per_bin(int K) {
+    int S = 1;
+    while (S < 32 && 2 * S * K <= (int)blockDim.x) S *= 2;
+    return S;
+}
+
+// asynchronous global -> shared copy of one complex value (cp.async), and its group bookkeeping
+template <typename V> __device__ __forceinline__ void cp_async_elem(V *dst, const V *src);
+template <> __device__ __forceinline__ void cp_async_elem<float2>(float2 *dst, const float2 *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+template <> __device__ __forceinline__ void cp_async_elem<double2>(double2 *dst, const double2 *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit_all() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_group 0;" ::: "memory"); }
+
 template <typename T> __device__ __forceinline__ Tw<T> twiddles(const GeomDev &g);
 template <> __device__ __forceinline__ Tw<float> twiddles<float>(const GeomDev &g) { return {g.tw32, g.log_tw}; }
 template <> __device__ __forceinline__ Tw<double> twiddles<double>(const GeomDev &g) { return {g.tw64, g.log_tw}; }
@@ -466,12 +498,10 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1)
         auto Z = [&](int k) -> V { return direct ? buf[ph(pos_of_freq(k, logL))] : cmul(buf[ph(k)], ch[k]); };
         const T scale = unit_w ? (T)1 : (T)(((flags & HB_F_NO2PI) ? 1.0 : twopi) * w[r] / (double)n);
         const int side_out = g.ring_side[r];
-        auto emit = [&](int m, V X) {
-            if (!(flags & HB_F_NOPHASE)) X = cmul(X, R.P(m));
-            T sc = scale;
-            if (mdouble && m > 0) sc *= (T)2;
-            if ((flags & HB_F_NOFOLD) && m >= n) sc = (T)0;
-            X = cscale(X, sc);
+        // F(m) = c_m scale X exp(-i m phi0), X the bin m mod n (conjugated above N)
+        auto put = [&](int m, V X) {  // X already carries scale exp(-i m phi0)
+            if (mdouble && m > 0) X = cscale(X, (T)2);
+            if ((flags & HB_F_NOFOLD) && m >= n) X = mk2((T)0, (T)0);
             if (!joint)
                 out[((int64_t)m * np + pair) * 2 + side_out] = X;
             else if (side == 0)
@@ -479,26 +509,44 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1)
             else
                 store_ns(out + ((int64_t)m * np + pair) * 2, stn[m], X);
         };
+        // When exp(-i n phi0) = s = +-1 (HEALPix rings), exp(-i (m0 + j n) phi0) =
+        // exp(-i m0 phi0) s^j: one phase product per residue class m0 instead of one per alias.
+        const bool nophase = flags & HB_F_NOPHASE;
+        const int s = nophase ? 1 : alias_sign(g.phi0_pi[r], n);
+        const int K = N / 2 + 1, SL = lanes_per_bin(K), q0 = threadIdx.x & (SL - 1), kstep = blockDim.x / SL;
+        auto emit_class = [&](int m0, V X) {  // aliases q = q0, q0 + S, ... of class m0
+            const V Y = cscale(nophase ? X : cmul(X, R.P(m0)), scale);
+            const V Yn = s > 0 ? Y : mk2(-Y.x, -Y.y);
+            for (int q = q0, m = m0 + q0 * n; m <= mmax; q += SL, m += SL * n)
+                put(m, s == 0 ? cscale(cmul(X, R.P(m)), scale) : (q & 1) ? Yn : Y);
+        };
         // Bins of the real ring: F_k = (A - i U(k) D) / 2 with A = Z_k + conj Z_{N-k},
         // D = Z_k - conj Z_{N-k}, U(k) = exp(-2 pi i k / n); since U(N-k) = -conj U(k), the same
         // A, D give F_{N-k} = conj(A + i U(k) D) / 2, so one thread takes the pair (k, N-k)
         // (k = 0: bins 0 and N).  Harmonic m takes bin m mod n, conjugated above N.
-        auto emit_bin = [&](int kk, V X) {
-            for (int m = kk; m <= mmax; m += n) emit(m, X);
-            if (kk > 0 && kk < N)
-                for (int m = n - kk; m <= mmax; m += n) emit(m, cconj(X));
-        };
-        for (int k = threadIdx.x; 2 * k <= N; k += blockDim.x) {
+        // The thread of k emits the residue classes k and n - k (bin k, the second conjugated) and
+        // N - k and N + k (bin N - k); k = 0: classes 0 and N.  One loop over the four keeps a
+        // single copy of the alias loop in the kernel (instruction-cache footprint).
+        const int cstep = N > mmax ? 2 : 1;  // classes n - k, N + k (c = 1, 3) exceed mmax
+        for (int k = threadIdx.x / SL; k < K; k += kstep) {
             const V zk = Z(k);
             const V zc = cconj(k == 0 ? zk : Z(N - k));
             const V A = cadd(zk, zc), D = csub(zk, zc);
             const V u = R.U(k);
             const V iuD = mk2(-(u.x * D.y + u.y * D.x), u.x * D.x - u.y * D.y);  // i u D
-            emit_bin(k, mk2((T)0.5 * (A.x - iuD.x), (T)0.5 * (A.y - iuD.y)));
-            if (k == 0)
-                emit_bin(N, mk2((T)0.5 * (A.x - D.y), (T)0.5 * (A.y + D.x)));  // U(N) = -1
-            else if (2 * k < N)
-                emit_bin(N - k, mk2((T)0.5 * (A.x + iuD.x), (T)(-0.5) * (A.y + iuD.y)));
+            const V Fk = mk2((T)0.5 * (A.x - iuD.x), (T)0.5 * (A.y - iuD.y));
+            const V Fb = k == 0 ? mk2((T)0.5 * (A.x - D.y), (T)0.5 * (A.y + D.x))  // bin N: U(N) = -1
+                                : mk2((T)0.5 * (A.x + iuD.x), (T)(-0.5) * (A.y + iuD.y));
+            const bool lo = k > 0, hi = k == 0 || 2 * k < N;
+#pragma unroll 1
+            for (int c = 0; c < 4; c += cstep) {
+                const bool on = c == 0 || (c == 1 && lo) || (c == 2 && hi) || (c == 3 && lo && hi);
+                if (!on) continue;
+                const int m0 = c == 0 ? k : c == 1 ? n - k : c == 2 ? N - k : N + k;
+                if (m0 > mmax) continue;
+                const V X = c < 2 ? Fk : Fb;
+                emit_class(m0, (c & 1) ? cconj(X) : X);
+            }
         }
     }
 }
@@ -519,8 +567,24 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1)
     const V *gin = Gm + b * gm_stride;
     const Tw<T> tw = twiddles<T>(g);
     const double twopi = 6.283185307179586476925286766559;
+    // stage_t = 1: a ring's G(m), m <= mmax, are loaded into ts when the ring starts.
+    // stage_t = 2 (grids too small to hide load latency with other CTAs): they are copied with
+    // cp.async, the north ring's before its trig tables are built, the south ring's as soon as
+    // the north ring's spectrum pass is done with ts, so that they land during the north FFT.
+    auto stage_issue = [&](int side_in) {
+        if (stage_t == 2) {
+            for (int m = threadIdx.x; m <= mmax; m += blockDim.x)
+                cp_async_elem(ts + m, gin + ((int64_t)m * np + pair) * 2 + side_in);
+            cp_async_commit_all();
+        } else {
+#pragma unroll 8
+            for (int m = threadIdx.x; m <= mmax; m += blockDim.x) ts[m] = gin[((int64_t)m * np + pair) * 2 + side_in];
+        }
+    };
+    const int rN = g.pair_ring[2 * pair], rS = g.pair_ring[2 * pair + 1];
+    if (stage_t == 2 && rN >= 0) stage_issue(g.ring_side[rN]);
     for (int side = 0; side < 2; ++side) {
-        const int r = g.pair_ring[2 * pair + side];
+        const int r = side ? rS : rN;
         if (r < 0) continue;
         const int n = g.nphi[r], N = n >> 1, L = g.fft_len[r], logL = ilog2(L);
         const int64_t bo = g.blu_ofs[r];
@@ -529,33 +593,36 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1)
         __syncthreads();
         const RingTrig<T> R = trig_for_ring<T>(g, tab, pair, side, n, N, mmax);
         const V *ch = direct ? nullptr : chirp_table<T>(g, bo, L);
-        // T_m = c_m G(m) exp(+i m phi0)
-        auto Tm_global = [&](int m) -> V {
-            V v = gin[((int64_t)m * np + pair) * 2 + side_in];
-            if (!(flags & HB_F_NOPHASE)) v = cmul(v, cconj(R.P(m)));
-            if (mdouble && m > 0) v = cscale(v, (T)2);
-            return v;
-        };
-        if (stage_t) {  // independent loads of every T_m of the ring, then the folds read shared memory
-#pragma unroll 8
-            for (int m = threadIdx.x; m <= mmax; m += blockDim.x) ts[m] = Tm_global(m);
+        if (stage_t) {  // this ring's G(m) in ts
+            if (stage_t == 1 || (side == 1 && rN < 0)) stage_issue(side_in);
+            cp_async_wait_all();
             __syncthreads();
         }
-        auto Tm = [&](int m) -> V { return stage_t ? ts[m] : Tm_global(m); };
-        // Hermitian half-spectrum bin X_k (0 <= k <= N) of the real ring, folded over m
-        auto Xk = [&](int k) -> V {
-            V acc = mk2((T)0, (T)0);
-            if (k == 0 || k == N) {
-                for (int m = k; m <= mmax; m += n) acc.x += Tm(m).x;
-            } else {
-                for (int m = k; m <= mmax; m += n) acc = cadd(acc, cscale(Tm(m), (T)0.5));
-                for (int m = n - k; m <= mmax; m += n) acc = cadd(acc, cscale(cconj(Tm(m)), (T)0.5));
+        auto G = [&](int m) -> V { return stage_t ? ts[m] : gin[((int64_t)m * np + pair) * 2 + side_in]; };
+        // T_m = c_m G(m) exp(+i m phi0).  The fold needs, per residue class m0 mod n,
+        // S(m0) = sum_j G(m0 + j n) exp(+i (m0 + j n) phi0).  When exp(i n phi0) = s = +-1
+        // (HEALPix rings) that is exp(i m0 phi0) sum_j s^j G(m0 + j n): one add per alias.
+        const bool nophase = flags & HB_F_NOPHASE;
+        const int s = nophase ? 1 : alias_sign(g.phi0_pi[r], n);
+        const int K = N / 2 + 1, SL = lanes_per_bin(K), q0 = threadIdx.x & (SL - 1), kstep = blockDim.x / SL;
+        // this lane's part of S(m0): aliases q = q0, q0 + SL, ..., before the factor exp(i m0 phi0)
+        // when s != 0
+        auto Ssum = [&](int m0) -> V {
+            V a = mk2((T)0, (T)0), c = a;  // even / odd q
+            for (int q = q0, m = m0 + q0 * n; m <= mmax; q += SL, m += SL * n) {
+                V v = G(m);
+                if (s == 0) v = cmul(v, cconj(R.P(m)));
+                if (q & 1)
+                    c = cadd(c, v);
+                else
+                    a = cadd(a, v);
             }
-            return acc;
+            return s < 0 ? csub(a, c) : cadd(a, c);
         };
+        const T dbl = mdouble ? (T)2 : (T)1, half = (T)0.5 * dbl;
         // Zv_k = (X_k + conj X_{N-k}) + i conj(U(k)) (X_k - conj X_{N-k}), 0 <= k < N
-        auto spec = [&](int k) -> V {
-            const V xa = Xk(k), xb = cconj(Xk(N - k));
+        auto spec = [&](V xa, V xb, int k) -> V {  // xa = X_k, xb = X_{N-k}
+            xb = cconj(xb);
             const V S = cadd(xa, xb), D = csub(xa, xb);
             const V u = R.U(k);
             return mk2(S.x - u.x * D.y + u.y * D.x, S.y + u.x * D.x + u.y * D.y);  // S + i conj(u) D
@@ -563,10 +630,53 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1)
         const T pscale = apply_w ? (T)(((flags & HB_F_NO2PI) ? 1.0 : twopi) * w[r] / (double)n) : (T)1;
         V *out2 = reinterpret_cast<V *>(maps + b * map_stride + g.ofs[r]);
         // the spectrum in natural order (its folds loop over aliases, so it gets a pass of its own
-        // rather than sitting inside the unrolled first FFT pass); Bluestein: conj(Z_k) chirp_k
-        for (int k = threadIdx.x; k < L; k += blockDim.x)
-            buf[ph(k)] = direct ? spec(k) : (k < N ? cmul(cconj(spec(k)), ch[k]) : mk2((T)0, (T)0));
+        // rather than sitting inside the unrolled first FFT pass); Bluestein: conj(Z_k) chirp_k.
+        // One thread takes the bins k and N - k of the Hermitian half-spectrum,
+        // X_k = c (S(k) + conj S(n - k)) / 2 and X_{N-k} = c (S(N - k) + conj S(N + k)) / 2, so
+        // every residue class of m mod n is folded once; k = 0 gives X_0 = c Re S(0) less the
+        // surplus weight of m = 0, and X_N = c Re S(N).  One loop over the four classes
+        // keeps a single copy of the alias loop in the kernel (instruction-cache footprint).
+        auto put = [&](int k, V z) { buf[ph(k)] = direct ? z : cmul(cconj(z), ch[k]); };
+        // The SL lanes of one k sum their parts with a butterfly (trip counts are uniform over the
+        // block, so every lane reaches each shuffle); lane q0 = 0 writes the bins.
+        const int iters = (K + kstep - 1) / kstep;
+        const int cstep = N > mmax ? 2 : 1;  // classes n - k, N + k (c = 1, 3) exceed mmax
+        for (int it = 0; it < iters; ++it) {
+            const int k = it * kstep + (int)threadIdx.x / SL;
+            const bool act = k < K;  // 2k <= N
+            const int nc = 2 * k == N ? 2 : 4;
+            V xa = mk2((T)0, (T)0), xb = xa;
+#pragma unroll 1
+            for (int c = 0; c < 4; c += cstep) {
+                const int m0 = c == 0 ? k : c == 1 ? n - k : c == 2 ? N - k : N + k;
+                const bool on = act && c < nc && m0 <= mmax && !(k == 0 && (c & 1));
+                V t = on ? Ssum(m0) : mk2((T)0, (T)0);
+                for (int o = 1; o < SL; o <<= 1) {
+                    t.x += __shfl_xor_sync(0xffffffffu, t.x, o);
+                    t.y += __shfl_xor_sync(0xffffffffu, t.y, o);
+                }
+                if (on && s != 0 && !nophase) t = cmul(t, cconj(R.P(m0)));
+                if (c & 1) t = cconj(t);
+                if (c < 2)
+                    xa = cadd(xa, t);
+                else
+                    xb = cadd(xb, t);
+            }
+            if (!act || q0 != 0) continue;
+            if (k == 0) {  // X_0 and X_N: S + conj S of the classes 0 and N
+                xa = mk2((T)2 * xa.x, (T)0);
+                xb = mk2((T)2 * xb.x, (T)0);
+            }
+            xa = cscale(xa, half);
+            xb = nc == 2 ? xa : cscale(xb, half);
+            if (k == 0) xa.x -= (dbl - (T)1) * G(0).x;
+            put(k, spec(xa, xb, k));
+            if (k > 0 && 2 * k < N) put(N - k, spec(xb, xa, N - k));
+        }
+        if (!direct)
+            for (int k = N + threadIdx.x; k < L; k += blockDim.x) buf[ph(k)] = mk2((T)0, (T)0);
         __syncthreads();
+        if (stage_t == 2 && side == 0 && rS >= 0) stage_issue(g.ring_side[rS]);  // lands during this ring's FFT
         auto lds = [&](int p) -> V { return buf[ph(p)]; };
         if (direct) {  // inverse DIF, then a digit-order read for the ring store
             dif_to_smem<true, T>(buf, logL, tw, lds);
@@ -668,6 +778,15 @@ static int smem_per_sm() {
     }
     return v;
 }
+static int sm_count() {
+    static int v = -1;
+    if (v < 0) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) v = 148;
+    }
+    return v;
+}
 // CTAs of `bytes` dynamic shared memory that fit on one SM (1 KB reserved per CTA)
 static int ctas_by_smem(size_t bytes) { return (int)((size_t)smem_per_sm() / (bytes + 1024)); }
 
@@ -724,15 +843,18 @@ static int launch_synthesis_t(const GeomDev &g, int nmaps, const c2_t<T> *Gm, in
         const int L = g.cls_L[c];
         const int64_t first = g.cls_first[c], cnt = g.cls_first[c + 1] - first;
         const bool stage_t = class_smem_syn<T>(L, mmax, true) <= (size_t)max_smem_optin();
-        const int smem = (int)class_smem_syn<T>(L, mmax, stage_t);
+        const int smem = (int)class_smem_syn<T>(L, mmax, stage_t), nt = class_threads(L);
         HB_CUDA_TRY(cudaFuncSetAttribute(ring_synthesis_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
         HB_CUDA_TRY(cudaFuncSetAttribute(ring_synthesis_kernel<T>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                          cudaSharedmemCarveoutMaxShared));
+        // asynchronous staging when the grid is under two waves of resident CTAs
+        int occ = 1;
+        HB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ring_synthesis_kernel<T>, nt, smem));
+        const bool async_t = stage_t && cnt * (int64_t)nmaps < 2 * (int64_t)sm_count() * std::max(occ, 1);
         dim3 grid((unsigned)cnt, (unsigned)nmaps);
-        ring_synthesis_kernel<T><<<grid, class_threads(L), smem, st>>>(g, g.cls_pairs + first, Gm, gm_stride, mmax,
-                                                                        maps, map_stride, w ? w : g.w,
-                                                                        apply_w ? 1 : 0, mdouble ? 1 : 0, flags, L,
-                                                                        stage_t ? 1 : 0);
+        ring_synthesis_kernel<T><<<grid, nt, smem, st>>>(g, g.cls_pairs + first, Gm, gm_stride, mmax, maps, map_stride,
+                                                         w ? w : g.w, apply_w ? 1 : 0, mdouble ? 1 : 0, flags, L,
+                                                         stage_t ? (async_t ? 2 : 1) : 0);
         HB_CHECK_LAUNCH();
     }
     return HB_OK;
