@@ -367,10 +367,11 @@ constexpr int TC_PRODUCERS = 256;
 template <int N> constexpr int tc_b_stage() { return 4 * N * 64; }  // [q][h][N x 32] 16-bit
 template <int N> constexpr int syn_stages() { return N >= 128 ? 3 : 4; }
 template <int N> constexpr int ana_stages() { return N >= 128 ? 3 : 4; }
-template <int ST, int N> constexpr int tc_smem() { return ST * (A_STAGE + tc_b_stage<N>()) + 8 * 128 * 8 + 128; }
+template <int ST, int N> constexpr int tc_smem() { return ST * (A_STAGE + tc_b_stage<N>()) + 8 * 128 * 8 + 8 * 64 * 4 + 128; }
 
 struct TcSmem {
     float2 *coef;  // this producer warp's 128 recursion coefficients
+    float *inv;    // this producer warp's inverse batch scales 1 / (ls s_b) of the unit's m, b < 64
     uint64_t *full, *empty, *accum, *tfree, *drain;
     uint32_t *tmem_slot;
 };
@@ -379,7 +380,8 @@ __device__ __forceinline__ TcSmem tc_smem_layout(uint8_t *smem, int warp) {
     constexpr int STAGE = A_STAGE + tc_b_stage<N>();
     TcSmem L;
     L.coef = reinterpret_cast<float2 *>(smem + ST * STAGE) + (warp & 7) * 128;
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + ST * STAGE + 8 * 128 * sizeof(float2));
+    L.inv = reinterpret_cast<float *>(smem + ST * STAGE + 8 * 128 * sizeof(float2)) + (warp & 7) * 64;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + ST * STAGE + 8 * 128 * sizeof(float2) + 8 * 64 * sizeof(float));
     L.full = bars;
     L.empty = bars + ST;
     L.accum = bars + 2 * ST;
@@ -399,6 +401,12 @@ __device__ __forceinline__ void tc_init_barriers(const TcSmem &L, int full_count
     tc::mbar_init(L.tfree, TC_PRODUCERS);
     tc::mbar_init(L.drain, 1);
     tc::fence_mbar_init();
+}
+
+// the epilogue's inverse batch scales 1 / (ls s_b) of one m into this warp's table (maps b < nmaps)
+__device__ __forceinline__ void load_inv_scales(float *inv, const float *scl, int nmaps, int nb, float ls) {
+    for (int b = threadIdx.x & 31; b < nb; b += 32) inv[b] = b < nmaps ? 1.0f / (ls * scl[b]) : 0.f;
+    __syncwarp();
 }
 
 // write 8 even + 8 odd split values of one A-tile row group: A + {0,1,2,3} * A_TILE + off
@@ -460,6 +468,17 @@ __device__ __forceinline__ void load_sets(uint32_t taddr, int j, int nsets, floa
 }
 
 // ------------------------------------------------------------------------------------ synthesis
+// one synthesis chunk of one row: 64 l in four groups of 8 even + 8 odd values
+template <bool CHECKED, bool BF16>
+__device__ __forceinline__ void gen_chunk_syn(Rec &R, const float2 *cf, uint8_t *A, int off) {
+#pragma unroll
+    for (int grp = 0; grp < 4; ++grp) {
+        float ev[8], od[8];
+        gen16<CHECKED>(R, cf + 16 * grp, ev, od);
+        store_split<BF16>(A, off + grp * 128, ev, od);
+    }
+}
+
 // Chunk c (64 l) of a unit belongs to half-block hb = c / 2 (128 l); half-blocks alternate
 // between the two producer warp groups (g = hb % 2).  All live chunks of the CTA's units share
 // one ring of ST stages in order: the i-th live chunk (counted across units) uses stage i % ST
@@ -539,21 +558,19 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     }
                     uint8_t *A = smem + s * STAGE;
                     const float2 *cf = L.coef + cc * 64;
-#pragma unroll
-                    for (int grp = 0; grp < 4; ++grp) {
-                        float ev[8], od[8];
-                        if (fast)
-                            gen16<false>(R, cf + 16 * grp, ev, od);
-                        else
-                            gen16<true>(R, cf + 16 * grp, ev, od);
-                        store_split<BF16>(A, (r & 7) * 16 + (r >> 3) * 512 + grp * 128, ev, od);
-                    }
+                    const int off = (r & 7) * 16 + (r >> 3) * 512;
+                    if (fast)  // one branch per chunk: straight-line code over its four row groups
+                        gen_chunk_syn<false, BF16>(R, cf, A, off);
+                    else
+                        gen_chunk_syn<true, BF16>(R, cf, A, off);
                     tc::fence_proxy_async_smem();
                     tc::mbar_arrive(&L.full[s]);
                 }
             }
             if (!ok) break;
-            // epilogue: this warp's lane quarter, column blocks j with j % 2 == wg
+            // epilogue: this warp's lane quarter, column blocks j with j % 2 == wg; the scales are
+            // fetched while the last MMAs drain
+            load_inv_scales(L.inv, G.dscale + (int64_t)m * (N / 2), G.nmaps, N / 2, LS);
             if (!warp_wait(L.accum, ui & 1)) {
                 if (lane == 0) set_err(err, 2);
                 ok = false;
@@ -561,7 +578,6 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             }
             tc::fence_after();
             const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
-            const float *scl = G.dscale + (int64_t)m * (N / 2);
             const int nsets = 2 * (nch - c0) < S ? 2 * (nch - c0) : S;
 #pragma unroll 1
             for (int j = wg; j < N / 16; j += 2) {
@@ -573,7 +589,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         const int b = j * 8 + h;
                         if (b < G.nmaps) {
                             float2 *dst = G.Gm + (int64_t)b * G.gm_stride + ((int64_t)m * np + p) * 2;
-                            const float inv = 1.0f / (LS * scl[b]);
+                            const float inv = L.inv[b];
                             const float re = de[2 * h] * inv, im = de[2 * h + 1] * inv, ro = dd[2 * h] * inv,
                                         io = dd[2 * h + 1] * inv;
                             *reinterpret_cast<float4 *>(dst) = make_float4(re + ro, im + io, re - ro, im - io);
@@ -657,6 +673,16 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 }
 
 // ------------------------------------------------------------------------------------ analysis
+// one analysis chunk of one pair: 128 l in eight groups of 8 even + 8 odd values
+template <bool CHECKED, bool BF16>
+__device__ __forceinline__ void gen_chunk_ana(Rec &R, const float2 *cf, uint8_t *A, int off0) {
+#pragma unroll 2
+    for (int grp = 0; grp < 8; ++grp) {
+        float ev[8], od[8];
+        gen16<CHECKED>(R, cf + 16 * grp, ev, od);
+        store_split<BF16>(A, off0 + grp * 512, ev, od);
+    }
+}
 // Chunk c (32 ring pairs) of a unit goes to stage c' % ST (c' = running chunk count); the two
 // warps w, w + 4 with w == c' % ST fill it, warp w the rows of l0 .. l0+127, warp w + 4 those of
 // l0+128 .. l0+255 (restarting from the mid-block checkpoint).
@@ -735,21 +761,17 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 uint8_t *A = smem + s * STAGE;
                 // MN-major: 8 consecutive rows (l of one parity) of pair `lane`
                 const int off0 = (lane & 7) * 16 + (lane >> 3) * 128 + half * 8 * 512;
-#pragma unroll 1
-                for (int grp = 0; grp < 8; ++grp) {
-                    float ev[8], od[8];
-                    if (fast)
-                        gen16<false>(R, L.coef + 16 * grp, ev, od);
-                    else
-                        gen16<true>(R, L.coef + 16 * grp, ev, od);
-                    store_split<BF16>(A, off0 + grp * 512, ev, od);
-                }
+                if (fast)
+                    gen_chunk_ana<false, BF16>(R, L.coef, A, off0);
+                else
+                    gen_chunk_ana<true, BF16>(R, L.coef, A, off0);
                 tc::fence_proxy_async_smem();
                 tc::mbar_arrive(&L.full[s]);
             }
             if (!ok) break;
             // epilogue: lane quarter warp % 4 = rows 32w'..32w'+31 (l = l0 + 2 row + parity),
-            // column blocks j with j % 2 == half
+            // column blocks j with j % 2 == half; the scales are fetched while the MMAs drain
+            load_inv_scales(L.inv, G.dscale + (int64_t)m * (N / 2), G.nmaps, N / 2, LS);
             if (!warp_wait(L.accum, ui & 1)) {
                 if (lane == 0) set_err(err, 12);
                 ok = false;
@@ -759,8 +781,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             const int row = owner * 32 + lane;
             const int le = l0 + 2 * row;
             const uint32_t taddr = tmem + ((uint32_t)(owner * 32) << 16);
-            const float *scl = G.dscale + (int64_t)m * (N / 2);
             const int nsets = 2 * (npc - U.w) < S ? 2 * (npc - U.w) : S;
+            // optional per-l filter (almxfl fused into the store)
+            const float fl0 = fl && le <= lmax ? fl[le] : 1.f, fl1 = fl && le + 1 <= lmax ? fl[le + 1] : 1.f;
 #pragma unroll 1
             for (int j = half; j < N / 16; j += 2) {
                 float de[16], dd[16];
@@ -770,10 +793,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     const int b = j * 8 + h;
                     if (b < G.nmaps) {
                         float2 *dst = alm_out + G.alm_out_ofs + (int64_t)b * G.alm_stride + alm_idx(lmax, le, m);
-                        const float inv = 1.0f / (LS * scl[b]);
-                        // optional per-l filter (almxfl fused into the store)
-                        const float f0 = fl && le <= lmax ? fl[le] * inv : inv;
-                        const float f1 = fl && le + 1 <= lmax ? fl[le + 1] * inv : inv;
+                        const float inv = L.inv[b];
+                        const float f0 = fl0 * inv, f1 = fl1 * inv;
                         if (le <= lmax) dst[0] = make_float2(de[2 * h] * f0, de[2 * h + 1] * f0);
                         if (le + 1 <= lmax) dst[1] = make_float2(dd[2 * h] * f1, dd[2 * h + 1] * f1);
                     }
