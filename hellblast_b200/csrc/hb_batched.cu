@@ -355,19 +355,25 @@ __global__ void __launch_bounds__(128) skip_table_kernel(GeomDev g, int lmax, co
 }
 
 // ------------------------------------------------------------------------------------ pipeline
-// Both kernels: warps 0-7 produce A tiles (recursion, one ring pair per thread) and run the
-// epilogue (TMEM lane quarter = warp % 4, columns split between warps w and w + 4); warp 8
-// allocates TMEM and one of its threads issues the MMAs; one thread of warp 9 streams the
-// pre-split batch tiles with bulk copies.  Two producer warps per SM sub-partition hide the
-// recursion's dependency latency.  The recursion restarts from the plan's FP64 checkpoints at
-// every 128 l (block starts and the mid-block table), which is what lets two warps share one
-// row's l range.
+// Both kernels: the producer warps (8 in analysis, 12 in synthesis) generate A tiles (recursion,
+// one ring pair or l row per thread) and run the epilogue (TMEM lane quarter = warp % 4, column
+// blocks split between the warps of one quarter); the next warp allocates TMEM and one of its
+// threads issues the MMAs; one thread of the last warp streams the pre-split batch tiles with
+// bulk copies.  Several producer warps per SM sub-partition hide the recursion's dependency
+// latency.  The recursion restarts from the plan's FP64 checkpoints at every 128 l (block
+// starts and the mid-block table), which is what lets several warps share one row's l range.
 constexpr int TC_THREADS = 320;
 constexpr int TC_PRODUCERS = 256;
 template <int N> constexpr int tc_b_stage() { return 4 * N * 64; }  // [q][h][N x 32] 16-bit
-template <int N> constexpr int syn_stages() { return N >= 128 ? 3 : 4; }
+// synthesis: SYN_GROUPS groups of four producer warps, group g owning stage g
+constexpr int SYN_GROUPS = 3;
+constexpr int SYN_PW = 4 * SYN_GROUPS;
+constexpr int SYN_THREADS = 32 * (SYN_PW + 2);
 template <int N> constexpr int ana_stages() { return N >= 128 ? 3 : 4; }
-template <int ST, int N> constexpr int tc_smem() { return ST * (A_STAGE + tc_b_stage<N>()) + 8 * 128 * 8 + 8 * 64 * 4 + 128; }
+// stages, then per producer warp 128 coefficients (float2) and 64 inverse scales, then barriers
+template <int ST, int N, int PW = 8> constexpr int tc_smem() {
+    return ST * (A_STAGE + tc_b_stage<N>()) + PW * (128 * 8 + 64 * 4) + 128;
+}
 
 struct TcSmem {
     float2 *coef;  // this producer warp's 128 recursion coefficients
@@ -375,13 +381,14 @@ struct TcSmem {
     uint64_t *full, *empty, *accum, *tfree, *drain;
     uint32_t *tmem_slot;
 };
-template <int ST, int N>
+template <int ST, int N, int PW = 8>
 __device__ __forceinline__ TcSmem tc_smem_layout(uint8_t *smem, int warp) {
     constexpr int STAGE = A_STAGE + tc_b_stage<N>();
+    const int pw = warp < PW ? warp : 0;
     TcSmem L;
-    L.coef = reinterpret_cast<float2 *>(smem + ST * STAGE) + (warp & 7) * 128;
-    L.inv = reinterpret_cast<float *>(smem + ST * STAGE + 8 * 128 * sizeof(float2)) + (warp & 7) * 64;
-    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + ST * STAGE + 8 * 128 * sizeof(float2) + 8 * 64 * sizeof(float));
+    L.coef = reinterpret_cast<float2 *>(smem + ST * STAGE) + pw * 128;
+    L.inv = reinterpret_cast<float *>(smem + ST * STAGE + PW * 128 * sizeof(float2)) + pw * 64;
+    uint64_t *bars = reinterpret_cast<uint64_t *>(smem + ST * STAGE + PW * 128 * sizeof(float2) + PW * 64 * sizeof(float));
     L.full = bars;
     L.empty = bars + ST;
     L.accum = bars + 2 * ST;
@@ -392,13 +399,13 @@ __device__ __forceinline__ TcSmem tc_smem_layout(uint8_t *smem, int warp) {
 }
 
 template <int ST>
-__device__ __forceinline__ void tc_init_barriers(const TcSmem &L, int full_count) {
+__device__ __forceinline__ void tc_init_barriers(const TcSmem &L, int full_count, int tfree_count = TC_PRODUCERS) {
     for (int s = 0; s < ST; ++s) {
         tc::mbar_init(&L.full[s], full_count);
         tc::mbar_init(&L.empty[s], 1);
     }
     tc::mbar_init(L.accum, 1);
-    tc::mbar_init(L.tfree, TC_PRODUCERS);
+    tc::mbar_init(L.tfree, tfree_count);
     tc::mbar_init(L.drain, 1);
     tc::fence_mbar_init();
 }
@@ -479,30 +486,32 @@ __device__ __forceinline__ void gen_chunk_syn(Rec &R, const float2 *cf, uint8_t 
     }
 }
 
-// Chunk c (64 l) of a unit belongs to half-block hb = c / 2 (128 l); half-blocks alternate
-// between the two producer warp groups (g = hb % 2).  All live chunks of the CTA's units share
-// one ring of ST stages in order: the i-th live chunk (counted across units) uses stage i % ST
-// for the (i / ST)-th time, so a producer group waits only for the chunk ST places earlier and
-// both groups keep stages filled while the MMA thread drains them.
+// Chunk c (64 l) of a unit belongs to half-block hb = c / 2 (128 l).  The unit's live half-blocks
+// hb0, hb0 + 1, ... go round-robin to SYN_GROUPS producer groups of four warps (three producer
+// warps per SM sub-partition hide the recursion's latency); group g fills only stage g, two
+// chunks per half-block, and waits only for the MMAs of its own previous chunk.  The MMA
+// thread (and the batch-tile loader) take the chunks in rounds: (group 0, 1, 2) for the first
+// chunk of their half-blocks, then for the second, then the next three half-blocks, so each
+// stage is consumed in the order its group fills it.
 template <int N, bool BF16, int S>
-__global__ void __launch_bounds__(TC_THREADS, 1)
+__global__ void __launch_bounds__(SYN_THREADS, 1)
     synth_tc_kernel(const TcGroup *__restrict__ groups, const int4 *__restrict__ units, int nunits, int *err) {
-    constexpr int ST = syn_stages<N>();
+    constexpr int ST = SYN_GROUPS;
     constexpr int B_STAGE = tc_b_stage<N>();
     constexpr int STAGE = A_STAGE + B_STAGE;
     constexpr uint32_t IDESC = tc::idesc_f16kind(128, N, 0, 0, BF16);
     constexpr float LS = BF16 ? 1.0f : 256.0f;  // lambda scale (|lambda| < 2^7 -> < 2^15 in half)
-    // S accumulator sets in S/2 (hi*hi, cross products) pairs, live chunk i using pair i mod S/2
-    // (issue_stage): the tensor core's FP32 accumulation error grows with the number of
-    // accumulate steps into one set; the epilogue sums the sets in IEEE FP32.
+    // S accumulator sets in S/2 (hi*hi, cross products) pairs, the k-th chunk of a unit (in MMA
+    // order) using pair k mod S/2 (issue_stage): the tensor core's FP32 accumulation error grows
+    // with the number of accumulate steps into one set; the epilogue sums the sets in IEEE FP32.
     constexpr int TCOLS = (2 * N * S < 32) ? 32 : 2 * N * S;
     static_assert(2 * N * S <= 512, "TMEM holds 512 columns");
     extern __shared__ __align__(1024) uint8_t smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const TcSmem L = tc_smem_layout<ST, N>(smem, warp);
+    const TcSmem L = tc_smem_layout<ST, N, SYN_PW>(smem, warp);
 
-    if (threadIdx.x == 0) tc_init_barriers<ST>(L, 128 + 1);
-    if (warp == 8) {
+    if (threadIdx.x == 0) tc_init_barriers<ST>(L, 128 + 1, 32 * SYN_PW);
+    if (warp == SYN_PW) {
         tc::tmem_alloc(L.tmem_slot, TCOLS);
         tc::tmem_relinquish();
     }
@@ -512,11 +521,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     const uint32_t tmem = *L.tmem_slot;
     bool ok = true;
 
-    if (warp < 8) {
+    if (warp < SYN_PW) {
         // ---------------- producers + epilogue
-        const int wg = warp >> 2;                   // half-blocks hb with hb % 2 == wg
-        const int r = ((warp & 3) << 5) | lane;     // row = pair within the block
-        uint32_t base = 0;                          // live chunks of the earlier units
+        const int wg = warp >> 2;                // producer group = stage
+        const int r = ((warp & 3) << 5) | lane;  // row = pair within the block
+        uint8_t *A = smem + wg * STAGE;
+        uint32_t gc = 0;  // chunks this group has filled (uses of its stage)
         int ui = 0;
         for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++ui) {
             const int4 U = units[u];
@@ -528,7 +538,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             R.xh = live ? G.g.pair_xhi[p] : 0.f;
             R.xl = live ? G.g.pair_xlo[p] : 0.f;
             const int nch = (lmax - m + 64) / 64, nhb = (nch + 1) / 2;
-            const int c0 = U.w, hbs = c0 / 2 + (((c0 / 2) ^ wg) & 1);  // first live half-block of this group
+            const int c0 = U.w, hbs = c0 / 2 + wg;  // c0 is even: skips are whole half-blocks
             const int64_t b0 = G.blk_ofs[m];
             // the next half-block's coefficients and checkpoint are fetched one half-block ahead
             float2 cpre[4];
@@ -540,23 +550,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 kpre = live ? ((hb & 1) ? G.ckh : G.ck)[blk * np + p] : make_float4(0.f, 0.f, 0.f, 0.f);
             };
             if (hbs < nhb) fetch(hbs);
-            for (int hb = hbs; hb < nhb && ok; hb += 2) {
+            for (int hb = hbs; hb < nhb && ok; hb += SYN_GROUPS) {
                 __syncwarp();
 #pragma unroll
                 for (int i = 0; i < 4; ++i) L.coef[lane + 32 * i] = cpre[i];
                 __syncwarp();
                 R.load(kpre, LS);
                 const bool fast = __all_sync(0xffffffffu, R.e == 0);
-                if (hb + 2 < nhb) fetch(hb + 2);
-                for (int cc = 0; cc < 2 && 2 * hb + cc < nch; ++cc) {
-                    const uint32_t it = base + (uint32_t)(2 * hb + cc - c0);
-                    const int s = (int)(it % ST);
-                    if (it >= ST && !warp_wait(&L.empty[s], ((it / ST) + 1) & 1)) {
+                if (hb + SYN_GROUPS < nhb) fetch(hb + SYN_GROUPS);
+                for (int cc = 0; cc < 2 && 2 * hb + cc < nch; ++cc, ++gc) {
+                    if (gc >= 1 && !warp_wait(&L.empty[wg], (gc + 1) & 1)) {
                         if (lane == 0) set_err(err, 1);
                         ok = false;
                         break;
                     }
-                    uint8_t *A = smem + s * STAGE;
                     const float2 *cf = L.coef + cc * 64;
                     const int off = (r & 7) * 16 + (r >> 3) * 512;
                     if (fast)  // one branch per chunk: straight-line code over its four row groups
@@ -564,12 +571,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     else
                         gen_chunk_syn<true, BF16>(R, cf, A, off);
                     tc::fence_proxy_async_smem();
-                    tc::mbar_arrive(&L.full[s]);
+                    tc::mbar_arrive(&L.full[wg]);
                 }
             }
             if (!ok) break;
-            // epilogue: this warp's lane quarter, column blocks j with j % 2 == wg; the scales are
-            // fetched while the last MMAs drain
+            // epilogue: this warp's lane quarter, column blocks j with j % SYN_GROUPS == wg; the
+            // scales are fetched while the last MMAs drain
             load_inv_scales(L.inv, G.dscale + (int64_t)m * (N / 2), G.nmaps, N / 2, LS);
             if (!warp_wait(L.accum, ui & 1)) {
                 if (lane == 0) set_err(err, 2);
@@ -580,7 +587,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             const uint32_t taddr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
             const int nsets = 2 * (nch - c0) < S ? 2 * (nch - c0) : S;
 #pragma unroll 1
-            for (int j = wg; j < N / 16; j += 2) {
+            for (int j = wg; j < N / 16; j += SYN_GROUPS) {
                 float de[16], dd[16];
                 load_sets<N>(taddr, j, nsets, de, dd);
                 if (live) {
@@ -599,38 +606,43 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             }
             tc::fence_before();
             tc::mbar_arrive(L.tfree);
-            base += (uint32_t)(nch - c0);
         }
-    } else if (warp == 8) {
+    } else if (warp == SYN_PW) {
         // ---------------- MMA issuer
         if (lane == 0) {
-            uint32_t base = 0;  // live chunks of the earlier units
+            uint32_t fbits = 0;  // bit g: parity of stage g's next fill
             int ui = 0;
             for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++ui) {
                 const int4 U = units[u];
-                const int nch = (groups[U.x].lmax - U.y + 64) / 64, c0 = U.w;
+                const int nch = (groups[U.x].lmax - U.y + 64) / 64, hb0 = U.w / 2, nhb = (nch + 1) / 2;
                 if (ui > 0 && !tc::mbar_wait(L.tfree, (ui - 1) & 1, HB_TC_WAIT_NS)) {
                     set_err(err, 3);
                     ok = false;
                     break;
                 }
                 tc::fence_after();
-                for (int c = c0; c < nch; ++c) {
-                    const uint32_t it = base + (uint32_t)(c - c0);
-                    const int s = (int)(it % ST);
-                    if (!tc::mbar_wait(&L.full[s], (it / ST) & 1, HB_TC_WAIT_NS)) {
-                        set_err(err, 4);
-                        ok = false;
-                        break;
+                int k = 0;  // chunk count of this unit in MMA order
+                for (int h3 = hb0; h3 < nhb && ok; h3 += SYN_GROUPS) {
+                    for (int cc = 0; cc < 2 && ok; ++cc) {
+                        for (int g = 0; g < SYN_GROUPS; ++g) {
+                            const int hb = h3 + g;
+                            if (hb >= nhb || 2 * hb + cc >= nch) continue;
+                            if (!tc::mbar_wait(&L.full[g], (fbits >> g) & 1u, HB_TC_WAIT_NS)) {
+                                set_err(err, 4);
+                                ok = false;
+                                break;
+                            }
+                            fbits ^= 1u << g;
+                            tc::fence_after();
+                            issue_stage<N>(tmem, tc::smem_u32(smem + g * STAGE), 2 * (k % (S / 2)),
+                                           2 * (k % (S / 2)) + 1, k < S / 2, IDESC);
+                            tc::mma_commit(&L.empty[g]);
+                            ++k;
+                        }
                     }
-                    tc::fence_after();
-                    issue_stage<N>(tmem, tc::smem_u32(smem + s * STAGE), 2 * ((c - c0) % (S / 2)),
-                                   2 * ((c - c0) % (S / 2)) + 1, c - c0 < S / 2, IDESC);
-                    tc::mma_commit(&L.empty[s]);
                 }
                 if (!ok) break;
                 tc::mma_commit(L.accum);
-                base += (uint32_t)(nch - c0);
             }
             if (!ok) {  // let issued MMAs finish before the tensor memory is released
                 tc::mma_commit(L.drain);
@@ -639,34 +651,42 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         }
         __syncwarp();
     } else {
-        // ---------------- loader of the pre-split alm tiles
+        // ---------------- loader of the pre-split alm tiles (same order as the MMA thread)
         if (lane == 0) {
-            uint32_t base = 0;  // live chunks of the earlier units
+            uint32_t ebits = 0, used = 0;  // bit g: parity of stage g's next drain / stage g used
             for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
                 const int4 U = units[u];
                 const TcGroup &G = groups[U.x];
                 const int m = U.y;
-                const int nch = (G.lmax - m + 64) / 64;
+                const int nch = (G.lmax - m + 64) / 64, hb0 = U.w / 2, nhb = (nch + 1) / 2;
                 const uint4 *src = G.alm_tiles + G.alm_tile_ofs[m] * (16 * N);
-                for (int c = U.w; c < nch; ++c) {
-                    const uint32_t it = base + (uint32_t)(c - U.w);
-                    const int s = (int)(it % ST);
-                    if (it >= ST && !tc::mbar_wait(&L.empty[s], ((it / ST) + 1) & 1, HB_TC_WAIT_NS)) {
-                        set_err(err, 5);
-                        ok = false;
-                        break;
+                for (int h3 = hb0; h3 < nhb && ok; h3 += SYN_GROUPS) {
+                    for (int cc = 0; cc < 2 && ok; ++cc) {
+                        for (int g = 0; g < SYN_GROUPS; ++g) {
+                            const int hb = h3 + g, c = 2 * hb + cc;
+                            if (hb >= nhb || c >= nch) continue;
+                            if (used & (1u << g)) {
+                                if (!tc::mbar_wait(&L.empty[g], (ebits >> g) & 1u, HB_TC_WAIT_NS)) {
+                                    set_err(err, 5);
+                                    ok = false;
+                                    break;
+                                }
+                                ebits ^= 1u << g;
+                            }
+                            used |= 1u << g;
+                            tc::mbar_arrive_expect_tx(&L.full[g], B_STAGE);
+                            tc::bulk_g2s(smem + g * STAGE + A_STAGE, src + (int64_t)c * (16 * N), B_STAGE,
+                                         &L.full[g]);
+                        }
                     }
-                    tc::mbar_arrive_expect_tx(&L.full[s], B_STAGE);
-                    tc::bulk_g2s(smem + s * STAGE + A_STAGE, src + (int64_t)c * (16 * N), B_STAGE, &L.full[s]);
                 }
-                base += (uint32_t)(nch - U.w);
             }
         }
         __syncwarp();
     }
     tc::fence_before();
     __syncthreads();
-    if (warp == 8) {
+    if (warp == SYN_PW) {
         tc::fence_after();
         tc::tmem_dealloc(tmem, TCOLS);
     }
@@ -920,11 +940,11 @@ template <int N> constexpr int nsets() { return 512 / (2 * N) > 4 ? 4 : 512 / (2
 
 template <int N, bool BF16>
 static int launch_syn(hb_batched_plan *bp, cudaStream_t st) {
-    const int smem = tc_smem<syn_stages<N>(), N>();
+    const int smem = tc_smem<SYN_GROUPS, N, SYN_PW>();
     constexpr int S = nsets<N>();
     HB_CUDA_TRY(cudaFuncSetAttribute(synth_tc_kernel<N, BF16, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     const int grid = std::min(bp->n_syn, sm_count());
-    synth_tc_kernel<N, BF16, S><<<grid, TC_THREADS, smem, st>>>(bp->dgroups, bp->syn_units, bp->n_syn, bp->err);
+    synth_tc_kernel<N, BF16, S><<<grid, SYN_THREADS, smem, st>>>(bp->dgroups, bp->syn_units, bp->n_syn, bp->err);
     HB_CHECK_LAUNCH();
     return HB_OK;
 }
