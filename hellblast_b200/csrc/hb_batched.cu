@@ -179,7 +179,7 @@ __global__ void __launch_bounds__(PREP_THREADS, 2) prep_alm_tiles_kernel(const T
 template <int N, bool BF16>
 __global__ void __launch_bounds__(PREP_THREADS, 1) prep_g_tiles_kernel(const TcGroup *groups, int gi,
                                                                        const float2 *__restrict__ F, int64_t f_stride,
-                                                                       int dbl) {
+                                                                       int nbuf) {
     extern __shared__ float4 sf[];
     const TcGroup &G = groups[gi];
     const int64_t np = G.g.npairs;
@@ -196,15 +196,20 @@ __global__ void __launch_bounds__(PREP_THREADS, 1) prep_g_tiles_kernel(const TcG
                 *d = make_float4(0.f, 0.f, 0.f, 0.f);
         }
     };
+    // nbuf slice buffers: nbuf - 1 slices in flight while one is converted
     int s = blockIdx.x, buf = 0;
-    if (dbl && s < ns) issue(s, sf);
-    tc::cp_async_commit();
-    for (; s < ns; s += gridDim.x, buf ^= dbl) {
-        const int sn = s + gridDim.x;
-        if (!dbl) issue(s, sf);  // single buffer (no room for two): this slice now
-        else if (sn < ns) issue(sn, sf + (buf ^ 1) * per);  // the buffer freed by the previous slice
+    for (int i = 0; i + 1 < nbuf; ++i) {
+        if (s + i * gridDim.x < ns) issue(s + i * gridDim.x, sf + i * per);
         tc::cp_async_commit();
-        if (dbl) tc::cp_async_wait<1>(); else tc::cp_async_wait<0>();  // this slice's copies are done
+    }
+    for (; s < ns; s += gridDim.x, buf = buf + 1 == nbuf ? 0 : buf + 1) {
+        const int sn = s + (nbuf - 1) * gridDim.x;
+        if (nbuf == 1) issue(s, sf);  // single buffer (no room for two): this slice now
+        else if (sn < ns) issue(sn, sf + (buf == 0 ? nbuf - 1 : buf - 1) * per);  // the buffer freed last
+        tc::cp_async_commit();
+        if (nbuf == 3) tc::cp_async_wait<2>();  // this slice's copies are done
+        else if (nbuf == 2) tc::cp_async_wait<1>();
+        else tc::cp_async_wait<0>();
         __syncthreads();
         const int m = s / (N / 2), b = s % (N / 2);
         const float4 *cur = sf + buf * per;
@@ -703,9 +708,9 @@ __device__ __forceinline__ void gen_chunk_ana(Rec &R, const float2 *cf, uint8_t 
         store_split<BF16>(A, off0 + grp * 512, ev, od);
     }
 }
-// Chunk c (32 ring pairs) of a unit goes to stage c' % ST (c' = running chunk count); the two
-// warps w, w + 4 with w == c' % ST fill it, warp w the rows of l0 .. l0+127, warp w + 4 those of
-// l0+128 .. l0+255 (restarting from the mid-block checkpoint).
+// Chunk c (32 ring pairs) of a unit goes to stage c' % ST (c' = running chunk count); two warps
+// fill it, one the rows of l0 .. l0+127, the other those of l0+128 .. l0+255 (restarting from the
+// mid-block checkpoint).
 template <int N, bool BF16, int S>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     anal_tc_kernel(const TcGroup *__restrict__ groups, const int4 *__restrict__ units, int nunits, float2 *alm_out,
@@ -734,7 +739,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
 
     if (warp < 8) {
         // ---------------- producers + epilogue
-        const int owner = warp & 3, half = warp >> 2;
+        // warp w < 4 fills the first l half of stage w, warp w >= 4 the second half of stage
+        // (w - 5) mod 4: the two halves of one stage run on different SM sub-partitions, and with
+        // three stages the six busy warps cover all four sub-partitions
+        const int quarter = warp & 3, half = warp >> 2;
+        const int owner = half ? ((warp - 5) & 3) : quarter;
         uint32_t it = 0;
         int ui = 0;
         for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++ui) {
@@ -798,9 +807,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 break;
             }
             tc::fence_after();
-            const int row = owner * 32 + lane;
+            const int row = quarter * 32 + lane;
             const int le = l0 + 2 * row;
-            const uint32_t taddr = tmem + ((uint32_t)(owner * 32) << 16);
+            const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16);
             const int nsets = 2 * (npc - U.w) < S ? 2 * (npc - U.w) : S;
             // optional per-l filter (almxfl fused into the store)
             const float fl0 = fl && le <= lmax ? fl[le] : 1.f, fl1 = fl && le + 1 <= lmax ? fl[le + 1] : 1.f;
@@ -986,11 +995,12 @@ template <int N, bool BF16>
 static int launch_prep_g(hb_batched_plan *bp, int gi, const float2 *F, int64_t stride, cudaStream_t st) {
     const TcGroup &G = bp->hgroups[gi];
     const size_t one = sizeof(float4) * (size_t)(G.npc * 36);  // 32 pairs + 4 pads per chunk
-    const int dbl = 2 * one <= (size_t)max_smem_optin_b() ? 1 : 0;
-    const int smem = (int)(one * (dbl ? 2 : 1));
+    const size_t room = (size_t)max_smem_optin_b() - 256;      // less the block reduction's table
+    const int nbuf = 3 * one <= room ? 3 : 2 * one <= room ? 2 : 1;
+    const int smem = (int)(one * nbuf);
     HB_CUDA_TRY(cudaFuncSetAttribute(prep_g_tiles_kernel<N, BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    const int grid = std::min(prep_slices<N>(G.mmax), sm_count() * (dbl ? 1 : 2));
-    prep_g_tiles_kernel<N, BF16><<<grid, PREP_THREADS, smem, st>>>(bp->dgroups, gi, F, stride, dbl);
+    const int grid = std::min(prep_slices<N>(G.mmax), sm_count() * (nbuf > 1 ? 1 : 2));
+    prep_g_tiles_kernel<N, BF16><<<grid, PREP_THREADS, smem, st>>>(bp->dgroups, gi, F, stride, nbuf);
     HB_CHECK_LAUNCH();
     return HB_OK;
 }
