@@ -161,6 +161,17 @@ template <> struct Half16<false> {
     static __device__ __forceinline__ float back(t a) { return __half2float(a); }
 };
 
+// (a - c, b - d) as one packed FP32x2 subtraction (IEEE round-to-nearest in each lane)
+__device__ __forceinline__ float2 sub2(float a, float b, float c, float d) {
+    unsigned long long p, q, r;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(p) : "f"(a), "f"(b));
+    asm("mov.b64 %0, {%1, %2};" : "=l"(q) : "f"(c), "f"(d));
+    asm("sub.rn.f32x2 %0, %1, %2;" : "=l"(r) : "l"(p), "l"(q));
+    float2 o;
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(o.x), "=f"(o.y) : "l"(r));
+    return o;
+}
+
 // 8 floats -> 8 "hi" = h(v) and 8 "lo" = h(v - hi), packed as two uint4
 template <bool BF16>
 __device__ __forceinline__ void split8(const float (&v)[8], uint4 &hi, uint4 &lo) {
@@ -170,8 +181,9 @@ __device__ __forceinline__ void split8(const float (&v)[8], uint4 &hi, uint4 &lo
     for (int i = 0; i < 4; ++i) {
         const float a = v[2 * i], b = v[2 * i + 1];
         typename H::t2 x = H::pack(a, b);
-        float2 f = H::unpack(x);
-        typename H::t2 y = H::pack(a - f.x, b - f.y);
+        const float2 f = H::unpack(x);
+        const float2 d = sub2(a, b, f.x, f.y);
+        typename H::t2 y = H::pack(d.x, d.y);
         h[i] = *reinterpret_cast<uint32_t *>(&x);
         l[i] = *reinterpret_cast<uint32_t *>(&y);
     }
