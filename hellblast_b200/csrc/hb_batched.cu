@@ -433,43 +433,45 @@ __device__ __forceinline__ void store_split(uint8_t *A, int off, const float (&e
     *reinterpret_cast<uint4 *>(A + 3 * A_TILE + off) = lo;
 }
 
-// The 12 MMAs of one stage (2 parities x 2 K-steps x 3 split passes).  The hi*hi products go to
-// accumulator set `hset`, the two cross products (about 2^-11 smaller) to set `lset`: the
+// The MMAs of one stage (2 parities x 2 K-steps x 3 split passes).  The hi*hi products go to
+// the "hi" set of a set pair, the two cross products (about 2^-11 smaller) to its "lo" set: the
 // tensor core's FP32 accumulation loses about one ulp of the accumulator per MMA, so keeping the
 // large products' set free of the cross products cuts the steps that round the result by 3x.
-// Live chunk i of a unit uses the set pair (hset, lset) = (2j, 2j+1), j = i mod (S/2); `first`
-// (the first S/2 live chunks) starts each set afresh.
+// TMEM columns of set pair j, parity q: hi at 4N j + 2N q, lo N further.  A_hi times the
+// batch tiles (hi | lo), which lie back to back in shared memory, is one MMA of width 2N into
+// (hi | lo); A_lo times B_hi is a second one into lo.  Live chunk i of a unit uses set pair
+// j = i mod (S/2); `first` (the first S/2 live chunks) starts each pair afresh.
 template <int N>
-__device__ __forceinline__ void issue_stage(uint32_t tmem, uint32_t a0, int hset, int lset, bool first,
-                                            uint32_t idesc) {
+__device__ __forceinline__ void issue_stage(uint32_t tmem, uint32_t a0, int pair, bool first, uint32_t idesc_n,
+                                            uint32_t idesc_2n) {
     const uint32_t b0 = a0 + A_STAGE;
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
-        const uint32_t dh = tmem + hset * 2 * N + q * N, dl = tmem + lset * 2 * N + q * N;
+        const uint32_t d = tmem + pair * 4 * N + q * 2 * N;
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
             const uint64_t ah = tc::sdesc(a0 + (q * 2 + 0) * A_TILE + k * 256, 128, 512);
             const uint64_t al = tc::sdesc(a0 + (q * 2 + 1) * A_TILE + k * 256, 128, 512);
             const uint64_t bh = tc::sdesc(b0 + (q * 2 + 0) * (N * 64) + k * 256, 128, 512);
-            const uint64_t bl = tc::sdesc(b0 + (q * 2 + 1) * (N * 64) + k * 256, 128, 512);
             const uint32_t acc = (!first || k > 0) ? 1u : 0u;
-            tc::mma_bf16(dh, ah, bh, idesc, acc);
-            tc::mma_bf16(dl, ah, bl, idesc, acc);
-            tc::mma_bf16(dl, al, bh, idesc, 1u);
+            tc::mma_bf16(d, ah, bh, idesc_2n, acc);  // B rows N .. 2N-1: the lo tile
+            tc::mma_bf16(d + N, al, bh, idesc_n, 1u);
         }
     }
 }
 
 // epilogue helper: columns [16j, 16j+16) of both parities, summed over the nsets accumulator sets
+// (set st: pair st / 2, hi or lo by st % 2; see issue_stage)
 template <int N>
 __device__ __forceinline__ void load_sets(uint32_t taddr, int j, int nsets, float (&de)[16], float (&dd)[16]) {
     tc::tmem_ld16(taddr + j * 16, de);
-    tc::tmem_ld16(taddr + N + j * 16, dd);
+    tc::tmem_ld16(taddr + 2 * N + j * 16, dd);
     tc::tmem_wait_ld();
     for (int st = 1; st < nsets; ++st) {
         float xe[16], xd[16];
-        tc::tmem_ld16(taddr + st * 2 * N + j * 16, xe);
-        tc::tmem_ld16(taddr + st * 2 * N + N + j * 16, xd);
+        const uint32_t col = (uint32_t)((st >> 1) * 4 * N + (st & 1) * N);
+        tc::tmem_ld16(taddr + col + j * 16, xe);
+        tc::tmem_ld16(taddr + col + 2 * N + j * 16, xd);
         tc::tmem_wait_ld();
 #pragma unroll
         for (int i = 0; i < 16; ++i) {
@@ -505,6 +507,7 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
     constexpr int B_STAGE = tc_b_stage<N>();
     constexpr int STAGE = A_STAGE + B_STAGE;
     constexpr uint32_t IDESC = tc::idesc_f16kind(128, N, 0, 0, BF16);
+    constexpr uint32_t IDESC2 = tc::idesc_f16kind(128, 2 * N, 0, 0, BF16);
     constexpr float LS = BF16 ? 1.0f : 256.0f;  // lambda scale (|lambda| < 2^7 -> < 2^15 in half)
     // S accumulator sets in S/2 (hi*hi, cross products) pairs, the k-th chunk of a unit (in MMA
     // order) using pair k mod S/2 (issue_stage): the tensor core's FP32 accumulation error grows
@@ -639,8 +642,8 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
                             }
                             fbits ^= 1u << g;
                             tc::fence_after();
-                            issue_stage<N>(tmem, tc::smem_u32(smem + g * STAGE), 2 * (k % (S / 2)),
-                                           2 * (k % (S / 2)) + 1, k < S / 2, IDESC);
+                            issue_stage<N>(tmem, tc::smem_u32(smem + g * STAGE), k % (S / 2), k < S / 2, IDESC,
+                                           IDESC2);
                             tc::mma_commit(&L.empty[g]);
                             ++k;
                         }
@@ -719,6 +722,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     constexpr int B_STAGE = tc_b_stage<N>();
     constexpr int STAGE = A_STAGE + B_STAGE;
     constexpr uint32_t IDESC = tc::idesc_f16kind(128, N, 1, 0, BF16);
+    constexpr uint32_t IDESC2 = tc::idesc_f16kind(128, 2 * N, 1, 0, BF16);
     constexpr float LS = BF16 ? 1.0f : 256.0f;
     constexpr int TCOLS = (2 * N * S < 32) ? 32 : 2 * N * S;  // S accumulator sets, see synth_tc_kernel
     static_assert(2 * N * S <= 512, "TMEM holds 512 columns");
@@ -853,8 +857,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         break;
                     }
                     tc::fence_after();
-                    issue_stage<N>(tmem, tc::smem_u32(smem + s * STAGE), 2 * ((c - c0) % (S / 2)),
-                                   2 * ((c - c0) % (S / 2)) + 1, c - c0 < S / 2, IDESC);
+                    issue_stage<N>(tmem, tc::smem_u32(smem + s * STAGE), (c - c0) % (S / 2), c - c0 < S / 2,
+                                   IDESC, IDESC2);
                     tc::mma_commit(&L.empty[s]);
                 }
                 if (!ok) break;
