@@ -91,7 +91,7 @@ class BatchedPlan:
 
     def executed_mma_flop(self) -> dict:
         """Tensor-core FLOP one alm2map / one map2alm call executes (after the evanescent skip):
-        12 MMAs of 128 x N x 16 per live chunk."""
+        the work of 12 MMAs of 128 x N x 16 per live chunk (issued as 4 of width 2N and 4 of width N)."""
         ch = (ctypes.c_int64 * 2)()
         n = ctypes.c_int(0)
         L.call("hb_batched_work", self.handle, ch, ctypes.byref(n))

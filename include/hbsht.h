@@ -226,7 +226,7 @@ HB_API int hb_batched_map2alm_fl(hb_batched_plan *bp, const float *maps, float *
 HB_API int hb_batched_status(hb_batched_plan *bp, int *code);
 /* Work the tensor-core kernels execute per call after the evanescent skip: chunks[0] synthesis
  * chunks (64 l x 128 ring pairs each), chunks[1] analysis chunks (32 ring pairs x 256 l each);
- * every chunk is 12 MMAs of 128 x mma_n x 16.  (No counterpart in the reference.) */
+ * every chunk is the work of 12 MMAs of 128 x mma_n x 16.  (No counterpart in the reference.) */
 HB_API int hb_batched_work(const hb_batched_plan *bp, int64_t *chunks, int *mma_n);
 /* CUDA graph of a batched step: hb_batched_graph_capture records hb_batched_alm2map(alm -> maps)
  * then hb_batched_map2alm(maps -> alm_out) (alm or alm_out may be null to keep one direction)
