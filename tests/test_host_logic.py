@@ -91,3 +91,21 @@ def test_precision_resolution():
     assert transforms.resolve_precision("fp32", torch.float64) == torch.float32
     with pytest.raises(ValueError):
         transforms.resolve_precision("bf16", torch.float32)
+
+
+def test_alias_phase_sign_is_exact_on_healpix_rings():
+    """The ring kernels fold the aliases m0 + j n of a residue class with one phase product
+    exp(i m0 phi0) when exp(i n phi0) is exactly +1 or -1 (else they take the per-alias phase).
+    Both phi0 conventions put every HEALPix ring on the +-1 path: n phi0 / pi is an integer
+    (0 or 1 mod 2) to within 1e-12, the tolerance of the device test."""
+    from hellblast_b200 import geometry
+    for phi0 in ("healpix", "reference"):
+        for nside in (1, 2, 8, 64, 2048):
+            t = geometry.host_ring_tables(nside, phi0)
+            x = t["phi0"] / np.pi * t["nphi"]
+            f = x - 2.0 * np.floor(0.5 * x)
+            plus = (np.abs(f) < 1e-12) | (np.abs(f - 2.0) < 1e-12)
+            minus = np.abs(f - 1.0) < 1e-12
+            assert np.all(plus | minus), (phi0, nside)
+            # the rings with a half-pixel shift (phi0 = pi / n) take s = -1
+            assert np.array_equal(minus, np.abs(t["phi0"] * t["nphi"] - np.pi) < 1e-9), (phi0, nside)
