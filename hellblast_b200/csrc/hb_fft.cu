@@ -561,7 +561,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1)
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V *buf = reinterpret_cast<V *>(smem_raw);
     V *tab = buf + padded_len(Lcls);
-    V *ts = tab + trig_entries<T>(Lcls, mmax);  // staged T_m, m <= mmax (when stage_t)
+    V *ts = tab + trig_entries<T>(Lcls, mmax);  // staged G(m) of the current ring, m <= mmax (when stage_t)
     const int pair = pairs[blockIdx.x], b = blockIdx.y;  // pairs fastest: neighbours share G's sectors
     const int64_t np = g.npairs;
     const V *gin = Gm + b * gm_stride;
@@ -764,7 +764,7 @@ static int max_smem_optin() {
 template <typename T> static size_t class_smem(int L, int mmax) {
     return sizeof(c2_t<T>) * ((size_t)padded_len(L) + (size_t)trig_entries<T>(L, mmax));
 }
-// synthesis: plus the staged T_m (mmax + 1 entries) when that fits
+// synthesis: plus the staged G(m) of one ring (mmax + 1 entries) when that fits
 template <typename T> static size_t class_smem_syn(int L, int mmax, bool stage_t) {
     return class_smem<T>(L, mmax) + (stage_t ? sizeof(c2_t<T>) * (size_t)(mmax + 1) : 0);
 }
