@@ -57,8 +57,8 @@ using namespace hb;
 extern "C" int hb_map2alm_f32_noalloc(const hb_plan *p, int nmaps, const float *maps, const double *weights,
                                       float *alm, int flags, hb_stream_t stream) {
     if (!p || !p->g) return fail(HB_ERR_INVALID, "hb_map2alm_f32_noalloc: null plan");
+    if (nmaps < 1 || nmaps > 65535) return fail(HB_ERR_INVALID, "hb_map2alm_f32_noalloc: nmaps must lie in [1, 65535]");
     const size_t need = hb_sht_workspace_size(p, 32, nmaps);
-    if (need == 0) return fail(HB_ERR_INVALID, "hb_map2alm_f32_noalloc: nmaps must lie in [1, 65535]");
     if (need > kScratchBytes)
         return fail(HB_ERR_INVALID, "hb_map2alm_f32_noalloc: this call needs " + std::to_string(need) +
                                         " bytes of scratch (nmaps * (mmax+1) * npairs * 16), the static scratch "

@@ -88,7 +88,15 @@ def alm2map(alm, g: G.Geometry, lmax: int, mmax: int | None = None, precision=No
     return out[0] if squeeze else out
 
 
-def map2alm_spin2(Q, U, g: G.Geometry, lmax: int, mmax: int | None = None, weights=None, precision=None):
+def map2alm_spin2(Q, U, g: G.Geometry, lmax: int, mmax: int | None = None, weights=None, precision=None,
+                  ref_compat=False):
+    """(Q, U) -> (E, B), healpy layout.  ``ref_compat=True`` reproduces the conventions of the
+    reference's map2alm_spin_gpu / eb_from_qu_gpu (spin.py:43-78) with the Wigner d it intends:
+    no phi0 phase, bins m >= nphi_r dropped instead of folded, orders above
+    max_r min(mmax, nphi_r // 2) zero (spin.py:53,57,65), and its spin functions
+    sqrt((2l+1)/4pi) d^l_{m,+-2} for a(+-2) (spin.py:29,58-59), where healpy's are d^l_{m,-+2}.
+    That last difference is the U -> -U (and B -> -B) change of polarisation convention:
+    E_ref(Q, U) = E(Q, -U), B_ref(Q, U) = -B(Q, -U)."""
     mmax = lmax if mmax is None else mmax
     q = flatten_rings(Q) if isinstance(Q, (list, tuple)) else as_tensor(Q)
     u = flatten_rings(U) if isinstance(U, (list, tuple)) else as_tensor(U)
@@ -97,11 +105,23 @@ def map2alm_spin2(Q, U, g: G.Geometry, lmax: int, mmax: int | None = None, weigh
     q = q.reshape(-1, g.npix).to(rt).contiguous()
     u = u.reshape(-1, g.npix).to(rt).contiguous()
     p = G.plan(g, lmax, mmax, precision=32 if rt == torch.float32 else 64, spin=True)
-    E, B = ops.map2alm_spin2(q, u, p.pid, device_weights(weights, g, q.device), 0)
+    flags = (L.HB_F_NOPHASE | L.HB_F_NOFOLD) if ref_compat else 0
+    E, B = ops.map2alm_spin2(q, -u if ref_compat else u, p.pid, device_weights(weights, g, q.device), flags)
+    if ref_compat:
+        B = -B
+        mcut = min(mmax, int(np.max(g.nphi)) // 2)  # spin.py:53 mmax_eff
+        if mcut < mmax:
+            E[:, ops.alm_size(lmax, mcut):] = 0
+            B[:, ops.alm_size(lmax, mcut):] = 0
     return (E[0], B[0]) if squeeze else (E, B)
 
 
-def alm2map_spin2(E, B, g: G.Geometry, lmax: int, mmax: int | None = None, precision=None):
+def alm2map_spin2(E, B, g: G.Geometry, lmax: int, mmax: int | None = None, precision=None, ref_compat=False):
+    """(E, B) -> (Q, U).  ``ref_compat=True`` follows the reference's qu_from_eb_gpu
+    (spin.py:80-115): no phi0 phase and its a(+2) = -(E - iB), which with its d^l_{m,+-2} spin
+    functions gives Q_ref = Q, U_ref = -U of the healpy convention.  (The reference's synthesis
+    is right for m = 0 input only: for m > 0 it fills the complex spin field's spectrum as if it
+    were real, spin.py:104,106.)"""
     mmax = lmax if mmax is None else mmax
     e = as_tensor(E)
     b = as_tensor(B)
@@ -111,7 +131,9 @@ def alm2map_spin2(E, B, g: G.Geometry, lmax: int, mmax: int | None = None, preci
     e = e.reshape(-1, e.shape[-1]).to(ct).contiguous()
     b = b.reshape(-1, b.shape[-1]).to(ct).contiguous()
     p = G.plan(g, lmax, mmax, precision=32 if rt == torch.float32 else 64, spin=True)
-    Q, U = ops.alm2map_spin2(e, b, p.pid, 0)
+    Q, U = ops.alm2map_spin2(e, b, p.pid, L.HB_F_NOPHASE if ref_compat else 0)
+    if ref_compat:
+        U = -U
     return (Q[0], U[0]) if squeeze else (Q, U)
 
 

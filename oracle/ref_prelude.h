@@ -5,6 +5,7 @@
 #include <cmath>
 #include <algorithm>
 using std::fmax; using std::fmin; using std::sqrt; using std::acos;
+using std::max; using std::min; using std::abs; using std::lgamma; using std::pow; using std::exp;
 #define __global__
 #define __device__
 #define __forceinline__ inline

@@ -258,17 +258,69 @@ def alm2map_adjoint(gmap, geom: dict, lmax: int, mmax: int | None = None, phase=
     return legendre_analysis(F, geom, lmax)
 
 
-def map2alm_spin2(Q, U, geom: dict, lmax: int, mmax: int | None = None, weights=None, phase=True):
+def map2alm_spin2(Q, U, geom: dict, lmax: int, mmax: int | None = None, weights=None, phase=True, fold=True):
     mmax = lmax if mmax is None else mmax
     w = geom["weights_dz"] if weights is None else weights
-    Qf = _c(ring_analysis(Q, geom, mmax, weights=w, phase=phase))
-    Uf = _c(ring_analysis(U, geom, mmax, weights=w, phase=phase))
+    Qf = _c(ring_analysis(Q, geom, mmax, weights=w, phase=phase, fold=fold))
+    Uf = _c(ring_analysis(U, geom, mmax, weights=w, phase=phase, fold=fold))
     n = alm_size(lmax, mmax)
     E = np.zeros(n, dtype=np.complex128); B = np.zeros(n, dtype=np.complex128)
     _lib().orc_spin2_analysis(lmax, mmax, geom["nr"], _p(_c(geom["x"])), _p(_c(geom["theta"])),
                               _p(Qf.view(np.float64)), _p(Uf.view(np.float64)),
                               _p(E.view(np.float64)), _p(B.view(np.float64)))
     return E, B
+
+
+def spin2_d_tables(geom: dict, lmax: int):
+    """Wigner d^l_{m,+2}(theta_r) and d^l_{m,-2}(theta_r), [m][ring][l] (zero for l < max(m, 2)), from
+    the oracle's own recursion (orc_spin2_lambda: _{-2}lambda = N_l d^l_{m,+2},
+    _{+2}lambda = N_l d^l_{m,-2}, N_l = sqrt((2l+1)/4pi))."""
+    th = _c(np.asarray(geom["theta"], dtype=np.float64))
+    nl = np.sqrt((2.0 * np.arange(lmax + 1) + 1.0) / (4.0 * math.pi))
+    dp2 = np.zeros((lmax + 1, th.size, lmax + 1)); dm2 = np.zeros_like(dp2)
+    for m in range(lmax + 1):
+        lp2, lm2 = spin2_lambda(lmax, m, th)
+        dp2[m] = lm2 / nl
+        dm2[m] = lp2 / nl
+    return dp2, dm2
+
+
+def map2alm_spin2_ref_compat(Q, U, geom: dict, lmax: int, mmax: int | None = None, weights=None, d_tables=None):
+    """The reference's spin-2 analysis, spin.py:43-78, restated with numpy.
+
+    Per ring: P = Q + iU and M = Q - iU (spin.py:43-44), PF = fft(P)/nphi and MF = fft(M)/nphi
+    (:50-51); the orders run to mmax_eff = max_r min(mmax, nphi_r // 2) (:53, :57) and ring r
+    contributes bin m only for m < nphi_r, with no phi0 phase and no alias fold (:65-66);
+    a_{+-2,lm} = 2 pi sqrt((2l+1)/4pi) sum_r w_r d^l_{m,+-2}(theta_r) PF/MF_r[m], l >= max(m, 2)
+    (:61, :67-68); E = -(a2 + a-2)/2, B = i (a2 - a-2)/2 (:76-77).  Outputs in the reference's
+    l(l+1)+m layout (:69-70): (a2, a-2, E, B).
+
+    ``d_tables`` = (d_p2, d_m2), each [m][ring][l], are the Wigner-d values to contract with:
+    the reference's own wigner_d_ms_sum tables reproduce its output exactly; the default is the
+    oracle's recursion (spin2_d_tables), i.e. the textbook d^l_{m,+-2} the reference's kernel
+    sets out to compute.
+    """
+    mmax = lmax if mmax is None else mmax
+    w = geom["weights_dz"] if weights is None else weights
+    dp2, dm2 = spin2_d_tables(geom, lmax) if d_tables is None else d_tables
+    nr = geom["nr"]
+    PF, MF = [], []
+    mmax_eff = 0
+    for r in range(nr):
+        n = int(geom["nphi"][r]); s = int(geom["ring_start"][r])
+        q = np.asarray(Q[s:s + n], dtype=np.float64); u = np.asarray(U[s:s + n], dtype=np.float64)
+        PF.append(np.fft.fft(q + 1j * u) / n)
+        MF.append(np.fft.fft(q - 1j * u) / n)
+        mmax_eff = max(mmax_eff, min(mmax, n // 2))
+    nl = np.sqrt((2.0 * np.arange(lmax + 1) + 1.0) / (4.0 * math.pi))
+    a2 = np.zeros((lmax + 1) ** 2, dtype=np.complex128); am2 = np.zeros_like(a2)
+    for m in range(mmax_eff + 1):
+        pf = np.array([PF[r][m] if m < int(geom["nphi"][r]) else 0.0 for r in range(nr)])
+        mf = np.array([MF[r][m] if m < int(geom["nphi"][r]) else 0.0 for r in range(nr)])
+        for l in range(max(m, 2), lmax + 1):
+            a2[l * (l + 1) + m] = np.sum(w * dp2[m][:, l] * pf) * nl[l] * (2.0 * math.pi)
+            am2[l * (l + 1) + m] = np.sum(w * dm2[m][:, l] * mf) * nl[l] * (2.0 * math.pi)
+    return a2, am2, -(a2 + am2) * 0.5, 1j * (a2 - am2) * 0.5
 
 
 def ring_analysis_ms(maps: np.ndarray, geom: dict, ms, weights) -> np.ndarray:

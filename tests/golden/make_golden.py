@@ -2,6 +2,7 @@
 
 Run in the build container (needs the reference tree; nothing at test time reads it):
     python tests/golden/make_golden.py [/path/to/reference]
+(default: $HB_REFERENCE_DIR, else the build container's reference mount)
 
 How the reference runs here (no CuPy, no GPU):
   * ``tests/golden/_cupy_shim`` provides a numpy-backed ``cupy`` module;
@@ -27,7 +28,8 @@ import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+_ARGS = [a for a in sys.argv[1:] if not a.startswith("--")]
+REF = _ARGS[0] if _ARGS else os.environ.get("HB_REFERENCE_DIR", "/root/reference")
 
 sys.path.insert(0, REPO)
 from oracle import sht_oracle as O  # noqa: E402
@@ -59,6 +61,54 @@ def host_legendre_block(x_cos, lmax, m):
     return P.view(cp.GArr)
 
 
+def host_wigner_d_ms(theta, lmax, m, s):
+    """The reference's wigner_d_ms_sum kernel (wigner_d_ms.cu:20-50) run as host code, in place
+    of spin._wigner_d_ms (spin.py:19-26)."""
+    th = np.ascontiguousarray(np.asarray(theta, dtype=np.float64))
+    out = np.zeros((th.size, lmax + 1))
+    lib.ref_wigner_d_ms_sum(th.ctypes.data_as(Dp), ctypes.c_int(th.size), ctypes.c_int(int(lmax)), ctypes.c_int(int(m)),
+                            ctypes.c_int(int(s)), out.ctypes.data_as(Dp))
+    return out.view(cp.GArr)
+
+
+def closed_form_d(l, m1, m2, theta):
+    """Wigner d^l_{m1 m2}(theta) from the textbook closed-form sum
+    sum_k (-1)^(m1-m2+k) sqrt((l+m1)!(l-m1)!(l+m2)!(l-m2)!) / ((l+m2-k)! k! (m1-m2+k)! (l-m1-k)!)
+    cos(theta/2)^(2l+m2-m1-2k) sin(theta/2)^(m1-m2+2k), evaluated with 40 significant digits.
+    This is the function wigner_d_ms_sum sets out to compute with (m1, m2) = (m, s): its
+    denominator is the one above, and the sign and the two powers are what the kernel gets wrong
+    (wigner_d_ms.cu:42-45)."""
+    import mpmath
+    mpmath.mp.dps = 40
+    t = mpmath.mpf(float(theta)) / 2
+    c, sn = mpmath.cos(t), mpmath.sin(t)
+    f = mpmath.factorial
+    pre = mpmath.sqrt(f(l + m1) * f(l - m1) * f(l + m2) * f(l - m2))
+    tot = mpmath.mpf(0)
+    for k in range(0, 2 * l + 1):
+        if l + m2 - k < 0 or m1 - m2 + k < 0 or l - m1 - k < 0:
+            continue
+        term = pre / (f(l + m2 - k) * f(k) * f(m1 - m2 + k) * f(l - m1 - k))
+        tot += (-1) ** (m1 - m2 + k) * term * c ** (2 * l + m2 - m1 - 2 * k) * sn ** (m1 - m2 + 2 * k)
+    return float(tot)
+
+
+_d_cache = {}
+
+
+def intended_wigner_d_ms(theta, lmax, m, s):
+    """spin._wigner_d_ms with the Wigner d the reference intends, d^l_{m,s}(theta), l >= max(|m|,|s|)."""
+    th = np.asarray(theta, dtype=np.float64)
+    key = (th.tobytes(), int(lmax), int(m), int(s))
+    if key not in _d_cache:
+        out = np.zeros((th.size, lmax + 1))
+        for l in range(max(abs(m), abs(s)), lmax + 1):
+            for i, t in enumerate(th):
+                out[i, l] = closed_form_d(l, int(m), int(s), t)
+        _d_cache[key] = out
+    return _d_cache[key].copy().view(cp.GArr)
+
+
 import hellblast.ring_tables as rt  # noqa: E402
 rt._get_fun = lambda src, fun: host_ring_tables
 import hellblast.sht_raw as sht_raw  # noqa: E402
@@ -72,6 +122,7 @@ import hellblast.alm_ops as alm_ops  # noqa: E402
 import hellblast.anafast  # noqa: E402,F401
 anafast = sys.modules["hellblast.anafast"]  # the package rebinds the name `anafast` (__init__.py:127)
 assert sht.map2alm_gpu is sht_raw.map2alm_gpu
+import hellblast.spin as spin  # noqa: E402  (imports isht, patched above)
 
 
 def rings_of(flat, tabs):
@@ -109,6 +160,44 @@ def case(name, nside, lmax, seed, m0_only=False):
     print("wrote", name, {k: getattr(v, "shape", v) for k, v in out.items()})
 
 
+def spin_case(name, nside, lmax, seed, stock):
+    """The reference's spin-2 analysis (map2alm_spin_gpu, eb_from_qu_gpu; spin.py:32-78) on Q/U
+    maps of a Gaussian E/B draw, and its synthesis (qu_from_eb_gpu, spin.py:80-115) of an m = 0
+    E/B input.  ``stock``: with the reference's own Wigner-d kernel, whose tables are stored
+    too; otherwise with the closed-form d^l_{m,+-2} that kernel sets out to compute."""
+    g = O.ring_tables(nside)
+    cl = 1.0 / (np.arange(lmax + 1) + 2.0) ** 2
+    cl[:2] = 0.0
+    E_in = O.synalm(cl, seed=seed)
+    B_in = O.synalm(0.3 * cl, seed=seed + 100)
+    Q, U = O.alm2map_spin2(E_in, B_in, g, lmax)
+    tabs = rt.HealpixRingTables(nside)
+    w = tabs.weights_dz()
+    th = np.asarray(tabs.theta_centers)
+    spin._wigner_d_ms = host_wigner_d_ms if stock else intended_wigner_d_ms
+    a2, am2 = spin.map2alm_spin_gpu(rings_of(Q, tabs), rings_of(U, tabs), tabs.theta_centers, tabs.nphi, w, lmax)
+    E, B = spin.eb_from_qu_gpu(rings_of(Q, tabs), rings_of(U, tabs), tabs.theta_centers, tabs.nphi, w, lmax)
+    out = dict(nside=nside, lmax=lmax, seed=seed, Q=Q, U=U, weights_dz=np.asarray(w), theta=th,
+               ref_a2=np.asarray(a2), ref_am2=np.asarray(am2), ref_E=np.asarray(E), ref_B=np.asarray(B))
+    if stock:
+        # the d tables the reference's kernel produced, [m][ring][l] for s = +2 and s = -2
+        out["ref_d_p2"] = np.stack([np.asarray(host_wigner_d_ms(th, lmax, m, 2)) for m in range(lmax + 1)])
+        out["ref_d_m2"] = np.stack([np.asarray(host_wigner_d_ms(th, lmax, m, -2)) for m in range(lmax + 1)])
+    else:
+        # synthesis of an m = 0 input (where the reference's real-field Hermitian fill is harmless)
+        keep = np.zeros(E_in.size, bool)
+        keep[O.alm_index(lmax, np.arange(lmax + 1), 0)] = True
+        E0 = np.where(keep, E_in, 0.0)
+        B0 = np.where(keep, B_in, 0.0)
+        cp.asrealarray = cp.real
+        Qr, Ur = spin.qu_from_eb_gpu(O.healpy_to_ref(E0, lmax).view(cp.GArr), O.healpy_to_ref(B0, lmax).view(cp.GArr),
+                                     tabs.theta_centers, tabs.nphi, lmax)
+        out.update(E0_in=E0, B0_in=B0, ref_Q_m0=np.concatenate([np.asarray(r) for r in Qr]),
+                   ref_U_m0=np.concatenate([np.asarray(r) for r in Ur]))
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **out)
+    print("wrote", name, {k: getattr(v, "shape", v) for k, v in out.items()})
+
+
 def tables():
     out = {}
     for nside in (1, 2, 4, 8, 16, 32, 64):
@@ -125,8 +214,13 @@ def tables():
 
 
 if __name__ == "__main__":
-    tables()
-    case("sht_nside8_lmax16", 8, 16, seed=0)
-    case("sht_nside32_lmax64", 32, 64, seed=1)
-    case("sht_nside32_lmax85", 32, 85, seed=2)
-    case("sht_nside16_lmax40_m0", 16, 40, seed=3, m0_only=True)
+    # --spin-only: regenerate the spin-2 fixtures alone
+    if "--spin-only" not in sys.argv:
+        tables()
+        case("sht_nside8_lmax16", 8, 16, seed=0)
+        case("sht_nside32_lmax64", 32, 64, seed=1)
+        case("sht_nside32_lmax85", 32, 85, seed=2)
+        case("sht_nside16_lmax40_m0", 16, 40, seed=3, m0_only=True)
+    spin_case("spin_stock_nside8_lmax20", 8, 20, seed=5, stock=True)
+    spin_case("spin_dexact_nside8_lmax20", 8, 20, seed=6, stock=False)
+    spin_case("spin_dexact_nside16_lmax40", 16, 40, seed=7, stock=False)

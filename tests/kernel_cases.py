@@ -2,7 +2,7 @@
 launching stream: the command line a user (or an ncu capture) runs to time or profile one part
 of the transform in isolation.
 
-    python -m hellblast_b200.kernel_cases CASE [--nside N] [--lmax L] [--nmaps B] [--reps R]
+    python tests/kernel_cases.py CASE [--nside N] [--lmax L] [--nmaps B] [--reps R]
 
 CASE is one of
   ring_tables  hb_ring_tables (HealpixRingTables, ring_tables.py:17-37 of the reference)
@@ -21,13 +21,17 @@ from __future__ import annotations
 import argparse
 import json
 
+import os
+import sys
+
 import numpy as np
 import torch
 
-from . import _lib as L
-from . import alm_ops, autograd, batched, ops
-from . import geometry as G
-from .ring_tables import HealpixRingTables
+sys.path.insert(0, os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+from hellblast_b200 import _lib as L  # noqa: E402
+from hellblast_b200 import alm_ops, autograd, batched, ops  # noqa: E402
+from hellblast_b200 import geometry as G  # noqa: E402
+from hellblast_b200.ring_tables import HealpixRingTables  # noqa: E402
 
 
 def _time(fn, reps, warmup, st):

@@ -80,6 +80,34 @@ def test_no_alloc_matches_workspace_entry_point_two_calls(lib):
     assert _rel(a3, r1) < TOL
 
 
+def test_no_alloc_unpaired_rings_after_a_larger_call(lib):
+    """A generic grid with an odd ring count and no mirror symmetry: every ring is unpaired, so
+    the south half of each F(m, pair) entry is the kernel's own zero, not a value left in the
+    shared scratch by the larger call made just before."""
+    L, G = lib
+    g1 = G.healpix(256)
+    p1 = G.plan(g1, 511, precision=32)
+    nalm1 = int(L.lib().hb_alm_size(511, 511))
+    a1 = _no_alloc(L, p1, _maps(16, g1.npix, 3), nalm1)
+    rng = np.random.default_rng(7)
+    nr = 37
+    theta = np.sort(rng.uniform(0.05, 3.0, nr))
+    nphi = 2 * rng.integers(8, 120, nr)
+    w = rng.uniform(0.01, 0.1, nr)
+    g2 = G.generic(theta, nphi, w, phi0=rng.uniform(0.0, 0.3, nr))
+    p2 = G.plan(g2, 90, precision=32)
+    nalm2 = int(L.lib().hb_alm_size(90, 90))
+    m2 = _maps(5, int(nphi.sum()), 4)
+    for _ in range(2):
+        a2 = _no_alloc(L, p2, m2, nalm2)
+        torch.cuda.synchronize()
+        r2 = _with_workspace(L, p2, m2, nalm2)
+        torch.cuda.synchronize()
+        assert np.isfinite(a1.abs().max().item())
+        assert _rel(a2, r2) < TOL
+        a1 = _no_alloc(L, p1, _maps(16, g1.npix, 5), nalm1)  # dirty the scratch again
+
+
 def test_no_alloc_rejects_calls_beyond_the_scratch(lib):
     L, G = lib
     g = G.healpix(256)
@@ -93,3 +121,8 @@ def test_no_alloc_rejects_calls_beyond_the_scratch(lib):
     assert "static scratch" in L.lib().hb_last_error_string().decode()
     with pytest.raises(ValueError):
         L.call("hb_map2alm_f32_noalloc", None, 1, maps.data_ptr(), None, alm.data_ptr(), 0, None)
+    small = G.plan(G.healpix(8), 8, precision=32)
+    rc = L.lib().hb_map2alm_f32_noalloc(small.handle, 65536, maps.data_ptr(), None, alm.data_ptr(), 0,
+                                        torch.cuda.current_stream().cuda_stream)
+    assert rc == L.HB_ERR_INVALID
+    assert "nmaps" in L.lib().hb_last_error_string().decode()
