@@ -43,6 +43,9 @@ def parse():
     p.add_argument("--wide", default=None, action="store_true",
                    help="groups of 64 maps, MMA N = 128 (default: chosen by the autotuner)")
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-extras", action="store_true",
+                   help="skip the plain-path and differentiable-path legs of the batched line")
+    p.add_argument("--plain-maps", type=int, default=4, help="maps timed one per call on the plain FP32 path")
     p.add_argument("--cpu-sample-m", type=int, default=12)
     return p.parse_args()
 
@@ -125,26 +128,110 @@ def cpu_baseline(nside, lmax, sample_m):
         "seconds": t4 - t0}
 
 
+def reference_pair_steps(nside, lmax, nsteps, seed=1):
+    """One full FP64 alm2map + map2alm pair of the oracle (the CPU restatement of the reference's
+    path: numpy ring FFTs, C + OpenMP Legendre work) cut into ``nsteps`` consecutive steps in
+    dependency order, so that the steps together do exactly one pair:
+      A: Legendre synthesis G(m, ring) for a set of orders m (sets balanced by l-range length);
+      B: ring synthesis and ring analysis of a block of rings (blocks balanced by pixel count;
+         the block's FFTs run on a thread pool);
+      D: Legendre analysis a_lm for a set of orders.
+    Returns (list of callables, the warm-up callables, a function returning the pair's result)."""
+    from concurrent.futures import ThreadPoolExecutor
+    from oracle import sht_oracle as O
+    g = O.ring_tables(nside)
+    nr, npix, mmax = g["nr"], int(g["npix"]), lmax
+    cl = 1.0 / (np.arange(lmax + 1) + 10.0) ** 2
+    alm = O.synalm(cl, lmax=lmax, seed=seed)
+    units = max(nsteps, 3)
+    na = max(1, int(round(0.4 * units)))
+    nb = max(1, units - 2 * na)
+    # orders: greedy balance of the l-range lengths over na sets
+    msets = [[] for _ in range(na)]
+    load = np.zeros(na)
+    for m in range(mmax + 1):  # descending cost
+        j = int(np.argmin(load))
+        msets[j].append(m)
+        load[j] += lmax - m + 1
+    msets = [np.array(sorted(x), dtype=np.int64) for x in msets]
+    rs = g["ring_start"]
+    cuts = [int(np.searchsorted(rs, npix * k / nb)) for k in range(nb)] + [nr]
+    rblocks = [(cuts[k], cuts[k + 1]) for k in range(nb) if cuts[k + 1] > cuts[k]]
+    G = np.zeros((mmax + 1, nr), dtype=np.complex128)
+    F = np.zeros((mmax + 1, nr), dtype=np.complex128)
+    mp = np.zeros(npix)
+    out = np.zeros((mmax + 1, lmax + 1), dtype=np.complex128)
+    w = g["weights_dz"]
+    threads = os.cpu_count() or 1
+
+    def A(ms):
+        return lambda: G.__setitem__(ms, O.legendre_synthesis_ms(O.alm_rows(alm, lmax, ms), g, lmax, ms))
+
+    def ring_block(r0, r1):
+        sg = O.ring_subset(g, r0, r1)
+        mp[rs[r0]:rs[r1]] = O.ring_synthesis(G[:, r0:r1], sg)
+        F[:, r0:r1] = O.ring_analysis(mp[rs[r0]:rs[r1]], sg, mmax, weights=w[r0:r1])
+
+    def B(r0, r1):
+        step = max(1, (r1 - r0 + 4 * threads - 1) // (4 * threads))
+        subs = [(a, min(a + step, r1)) for a in range(r0, r1, step)]
+
+        def run():
+            with ThreadPoolExecutor(threads) as ex:
+                list(ex.map(lambda ab: ring_block(*ab), subs))
+        return run
+
+    def D(ms):
+        return lambda: out.__setitem__(ms, O.legendre_analysis_ms(F[ms], g, lmax, ms))
+
+    work = [A(ms) for ms in msets] + [B(*rb) for rb in rblocks] + [D(ms) for ms in msets]
+    steps = [[] for _ in range(nsteps)]
+    for i, f in enumerate(work):  # consecutive units per step, in order
+        steps[i * nsteps // len(work)].append(f)
+    steps = [(lambda fs: (lambda: [f() for f in fs]))(fs) for fs in steps]
+
+    def result():
+        got = np.concatenate([out[m, m:] for m in range(mmax + 1)])
+        return float(np.linalg.norm(got - alm) / np.linalg.norm(alm))
+    return steps, [A(ms) for ms in msets], result
+
+
 def run_reference(args):
+    """The reference arm: the FP64 oracle (the CPU restatement of the reference's SHT path; the
+    reference's own path is CuPy-only and overflows above lmax 85) on the host cores.  The
+    --steps K steps together perform exactly one full alm2map + map2alm pair at the bench's
+    nside and lmax (reference_pair_steps); --warmup W runs W of the Legendre synthesis units
+    untimed first.  value = one pair / the K steps' total time."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     lmax = 2 * args.nside - 1 if args.lmax is None else args.lmax
-    vals = []
-    info = None
-    for _ in range(max(1, args.steps)):
-        v, info = cpu_baseline(args.nside, lmax, args.cpu_sample_m)
-        vals.append(v)
-    v = float(np.median(vals))
+    K = max(1, args.steps)
+    steps, warm, result = reference_pair_steps(args.nside, lmax, K)
+    for i in range(args.warmup):
+        warm[i % len(warm)]()
+    times = []
+    for f in steps:
+        t0 = time.perf_counter()
+        f()
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    v = 1.0 / total
+    cores = os.cpu_count()
+    sample = (f"one full FP64 pair (oracle: C + OpenMP Legendre on {cores} threads, numpy ring FFTs on a "
+              f"{cores}-thread pool) at nside {args.nside}, lmax {lmax}, cut into {K} steps in dependency "
+              f"order (Legendre synthesis by order sets, ring FFTs by ring blocks, Legendre analysis by "
+              f"order sets); {total:.1f} s in total")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": v, "unit": "pairs/s", "n_gpus": args.gpus,
-        "steps": args.steps, "warmup": 0, "ms_per_step": 1000.0 / v, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"scalar map2alm+alm2map pair, nside {args.nside}, lmax {lmax}, float64, CPU",
-                   "nside": args.nside, "lmax": lmax},
-        "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": info["cores"], "kind": "port",
-                         "sample": info["sample"]},
+        "steps": K, "warmup": args.warmup, "ms_per_step": 1000.0 * total / K, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (Gaussian alm, C_l=(l+10)^-2)",
+        "config": {"workload": f"scalar map2alm+alm2map pair, nside {args.nside}, lmax {lmax}, float64, CPU, "
+                               "one map per pair", "nside": args.nside, "lmax": lmax},
+        "cpu_baseline": {"value": v, "unit": "pairs/s", "cores": cores, "kind": "port", "sample": sample},
         "e2e": {"value": v, "unit": "pairs/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "round_trip_rel_err": result(),
+        "step_seconds": [round(t, 3) for t in times],
     }), flush=True)
 
 
@@ -160,6 +247,105 @@ def fft_classes(nside):
     nr = len(L)
     pair_L = np.maximum(L[: (nr + 1) // 2], L[::-1][: (nr + 1) // 2])
     return len(np.unique(pair_L))
+
+
+def hbm_bytes_ring_fft(nmaps, mmax, npairs, npix, itemsize=4):
+    """Algorithmic HBM bytes of one ring-FFT pass over `nmaps` maps (either direction): the
+    Fourier coefficients (mmax + 1) x npairs x (north, south) complex read or written once, and
+    every map pixel written or read once."""
+    return nmaps * ((mmax + 1) * npairs * 2 * 2 * itemsize + npix * itemsize)
+
+
+def load_traffic():
+    """DRAM bytes per launch measured by ncu (profiles/traffic_*.txt: `stage bytes` lines)."""
+    out = {}
+    d = os.path.join(ROOT, "profiles")
+    for name in sorted(os.listdir(d)) if os.path.isdir(d) else []:
+        if not (name.startswith("traffic_") and name.endswith(".txt")):
+            continue
+        with open(os.path.join(d, name)) as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) >= 2 and not line.startswith("#"):
+                    try:
+                        out[parts[0]] = float(parts[1])
+                    except ValueError:
+                        pass
+    return out
+
+
+def plain_leg(hb, L, G, nside, lmax, nmaps, alm_h, dev, st, reps=3):
+    """The plain FP32 per-map form (the comparison the metric names): alm2map + map2alm of one
+    map per call through the FP32 Legendre and ring-FFT kernels, `nmaps` maps, `reps` times."""
+    import torch
+    g = G.healpix(nside)
+    plan = G.plan(g, lmax, precision=32)
+    ws = torch.empty(plan.workspace_bytes(32, 1), dtype=torch.uint8, device=dev)
+    alm = alm_h[:nmaps].to(dev)
+    maps = torch.empty(nmaps, 12 * nside * nside, dtype=torch.float32, device=dev)
+    out = torch.empty_like(alm)
+    sp = st.cuda_stream
+
+    def run():
+        for i in range(nmaps):
+            L.call("hb_alm2map_f32", plan.handle, 1, alm[i].data_ptr(), maps[i].data_ptr(), ws.data_ptr(),
+                   ws.numel(), 0, sp)
+            L.call("hb_map2alm_f32", plan.handle, 1, maps[i].data_ptr(), None, out[i].data_ptr(), ws.data_ptr(),
+                   ws.numel(), 0, sp)
+    run()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    for _ in range(reps):
+        run()
+    e1.record(st)
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / (reps * nmaps)
+    del ws, maps, out
+    return 1000.0 / ms, ms
+
+
+def diff_leg(hb, nside, lmax, dev, st, reps=3):
+    """The differentiable path: the T + E/B power-spectrum loss sum_XX sum_l (C_l - 1.1 C_l^true)^2 /
+    (1.1 C_l^true)^2 of one float32 T, Q, U map set (TT (l+10)^-2, EE 0.1 TT, BB 0.01 TT), forward
+    alone and forward + backward through the adjoint kernels.  Returns (forward ms, ratio)."""
+    import torch
+    from hellblast_b200 import autograd
+    l = np.arange(lmax + 1, dtype=np.float64)
+    cl = 1.0 / (l + 10.0) ** 2
+    aT, aE, aB = (hb.synalm(c, lmax=lmax, seed=s, device=dev, dtype=torch.complex64)[None]
+                  for c, s in ((cl, 2), (0.1 * cl, 3), (0.01 * cl, 4)))
+    with torch.no_grad():
+        T = autograd.alm2map(aT, nside, lmax)
+        Q, U = autograd.alm2map_spin(aE, aB, nside, lmax)
+        tgt = [1.1 * autograd.alm2cl(x, lmax) for x in (aT, aE, aB)]
+
+    def loss_of(t, q, u):
+        e, b = autograd.map2alm_spin(q, u, nside, lmax)
+        cls = [autograd.alm2cl(autograd.map2alm(t, nside, lmax), lmax), autograd.alm2cl(e, lmax),
+               autograd.alm2cl(b, lmax)]
+        return sum((((c - ct) / ct)[:, 2:] ** 2).sum() for c, ct in zip(cls, tgt))
+
+    def fwd():
+        with torch.no_grad():
+            loss_of(T, Q, U)
+
+    def fwd_bwd():
+        t, q, u = (x.clone().requires_grad_(True) for x in (T, Q, U))
+        loss_of(t, q, u).backward()
+
+    res = []
+    for fn in (fwd, fwd_bwd):
+        fn()
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for _ in range(reps):
+            fn()
+        e1.record(st)
+        torch.cuda.synchronize(dev)
+        res.append(e0.elapsed_time(e1) / reps)
+    return res[0], res[1] / res[0]
 
 
 def main():
@@ -218,6 +404,7 @@ def main():
     except Exception:
         pass
     bf16_peak = float(peaks.get("bf16_tflops", 1590.0))
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
 
     if args.mode == "plain":
         plan = G.plan(g, lmax, mmax, precision=32)
@@ -367,13 +554,33 @@ def main():
         ex = bp.executed_mma_flop()               # MMAs actually issued (3 split passes, Re/Im columns,
         executed = 0.5 * (ex["synthesis"] + ex["analysis"])  # padding of the last group, evanescent skip)
         achieved = 2 * alg / t_dom / 1e12
-        roof = {"bound": "tensor", "kernel": "synth_tc_kernel + anal_tc_kernel", "achieved": achieved,
-                "peak": bf16_peak, "unit": "TFLOP/s", "frac": achieved / bf16_peak, "traffic": None,
-                "peak_source": "MEASURED_PEAKS.json bf16_tflops (burst)" if peaks else "fallback 1590 TFLOP/s",
-                "flop_per_launch": alg,
-                "tensor_flop_executed_per_launch": executed,
-                "tensor_achieved_executed": 2 * executed / t_dom / 1e12,
-                "tensor_frac_executed": 2 * executed / t_dom / 1e12 / bf16_peak}
+        tensor = {"bound": "tensor", "kernel": "synth_tc_kernel + anal_tc_kernel", "achieved": achieved,
+                  "peak": bf16_peak, "unit": "TFLOP/s", "frac": achieved / bf16_peak,
+                  "traffic": None,
+                  "peak_source": ("MEASURED_PEAKS.json bf16_tflops (burst), of measured" if peaks
+                                  else "fallback 1590 TFLOP/s, of fallback"),
+                  "flop_per_launch": alg,
+                  "tensor_flop_executed_per_launch": executed,
+                  "tensor_achieved_executed": 2 * executed / t_dom / 1e12,
+                  "tensor_frac_executed": 2 * executed / t_dom / 1e12 / bf16_peak}
+        # the ring FFTs (one launch per FFT-length class and direction; a "launch" below is the
+        # whole direction, all its class launches): HBM-bound
+        traffic = load_traffic()
+        fft_bytes = hbm_bytes_ring_fft(B, mmax, g.npairs, npix)
+        stage_roof = {"tensor_legendre": tensor}
+        for key, kern in (("ring_synthesis", "ring_synthesis_kernel<float>"),
+                          ("ring_analysis", "ring_analysis_kernel<float>")):
+            ach = fft_bytes / (stages[key] * 1e-3) / 1e9
+            stage_roof[key] = {"bound": "hbm", "kernel": kern + " (all FFT-length classes of one direction)",
+                               "achieved": ach, "peak": hbm_peak, "unit": "GB/s", "frac": ach / hbm_peak,
+                               "traffic": traffic.get(f"{key}_nside{nside}_maps{B}"),
+                               "peak_source": ("MEASURED_PEAKS.json hbm_gbs, of measured" if peaks
+                                               else "fallback 6650 GB/s, of fallback"),
+                               "bytes_per_launch": fft_bytes, "ms": stages[key]}
+        tensor["ms"] = stages["tensor_synthesis"] + stages["tensor_analysis"]
+        dom = max(stage_roof, key=lambda k: stage_roof[k]["ms"])
+        roof = dict(stage_roof[dom])
+        roof["stage"] = dom
     out = {
         "metric": METRIC, "value": value, "unit": "pairs/s", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -396,6 +603,20 @@ def main():
         "gpu_launches": args.steps * n_launch,
         "clocks": clk.summary(),
     }
+    if args.mode == "batched":
+        out["stages_roofline"] = stage_roof
+    if args.mode == "batched" and not args.no_extras:
+        del maps, alm_out
+        if args.mode == "batched":
+            del pipe
+        torch.cuda.empty_cache()
+        pv, pms = plain_leg(hb, L, G, nside, lmax, min(args.plain_maps, B), alm_h, dev, st)
+        out["plain_value"] = pv
+        out["plain_ms_per_map"] = pms
+        out["batched_over_plain"] = value / world / pv
+        f_ms, ratio = diff_leg(hb, nside, lmax, dev, st)
+        out["diff_forward_ms"] = f_ms
+        out["diff_fwd_bwd_over_fwd"] = ratio
     if args.mode == "batched" and tune is not None:
         out["autotune"] = [{k: (round(v, 8) if isinstance(v, float) else v) for k, v in c.items()}
                            for c in tune["candidates"]]

@@ -208,6 +208,76 @@ void orc_legendre_synthesis(int lmax, int mmax, int64_t nr, const double *x, con
     free(lc); free(ls);
 }
 
+/* Analysis restricted to the nms orders ms[j]: F [j][r] complex -> out [j][l] complex (l < ms[j]
+ * zero), for spot checks of transforms too large to run in full here. */
+void orc_legendre_analysis_ms(int lmax, int nms, const int *ms, int64_t nr, const double *x,
+                              const double *sin_theta, const double *F, double *out) {
+    int mx = 0;
+    for (int j = 0; j < nms; ++j) mx = ms[j] > mx ? ms[j] : mx;
+    long double *lc = (long double *)malloc(sizeof(long double) * (size_t)(mx + 1));
+    log2_sectoral_norm(mx, lc);
+    long double *ls = (long double *)malloc(sizeof(long double) * (size_t)nr);
+    for (int64_t r = 0; r < nr; ++r) ls[r] = log2l((long double)sin_theta[r]);
+    memset(out, 0, sizeof(double) * 2 * (size_t)nms * ((size_t)lmax + 1));
+#pragma omp parallel
+    {
+        double *A = (double *)calloc((size_t)lmax + 2, sizeof(double));
+        double *B = (double *)calloc((size_t)lmax + 2, sizeof(double));
+        double *lam = (double *)malloc(sizeof(double) * ((size_t)lmax + 1));
+#pragma omp for schedule(dynamic, 1)
+        for (int j = 0; j < nms; ++j) {
+            const int m = ms[j];
+            double *acc = out + 2 * (size_t)j * ((size_t)lmax + 1);
+            scalar_coefs(lmax, m, A, B);
+            for (int64_t r = 0; r < nr; ++r) {
+                const double fr = F[2 * ((int64_t)j * nr + r)], fi = F[2 * ((int64_t)j * nr + r) + 1];
+                scalar_lambda_point(lmax, m, x[r], ls[r], lc[m], A, B, lam);
+                for (int l = m; l <= lmax; ++l) {
+                    acc[2 * l] += lam[l] * fr;
+                    acc[2 * l + 1] += lam[l] * fi;
+                }
+            }
+        }
+        free(A); free(B); free(lam);
+    }
+    free(lc); free(ls);
+}
+
+/* Synthesis restricted to the nms orders ms[j]: a [j][l] complex -> G [j][r] complex. */
+void orc_legendre_synthesis_ms(int lmax, int nms, const int *ms, int64_t nr, const double *x,
+                               const double *sin_theta, const double *a, double *G) {
+    int mx = 0;
+    for (int j = 0; j < nms; ++j) mx = ms[j] > mx ? ms[j] : mx;
+    long double *lc = (long double *)malloc(sizeof(long double) * (size_t)(mx + 1));
+    log2_sectoral_norm(mx, lc);
+    long double *ls = (long double *)malloc(sizeof(long double) * (size_t)nr);
+    for (int64_t r = 0; r < nr; ++r) ls[r] = log2l((long double)sin_theta[r]);
+#pragma omp parallel
+    {
+        double *A = (double *)calloc((size_t)lmax + 2, sizeof(double));
+        double *B = (double *)calloc((size_t)lmax + 2, sizeof(double));
+        double *lam = (double *)malloc(sizeof(double) * ((size_t)lmax + 1));
+#pragma omp for schedule(dynamic, 1) collapse(2)
+        for (int j = 0; j < nms; ++j) {
+            for (int64_t r = 0; r < nr; ++r) {
+                const int m = ms[j];
+                const double *aj = a + 2 * (size_t)j * ((size_t)lmax + 1);
+                scalar_coefs(lmax, m, A, B);
+                scalar_lambda_point(lmax, m, x[r], ls[r], lc[m], A, B, lam);
+                double gr = 0.0, gi = 0.0;
+                for (int l = m; l <= lmax; ++l) {
+                    gr += lam[l] * aj[2 * l];
+                    gi += lam[l] * aj[2 * l + 1];
+                }
+                G[2 * ((int64_t)j * nr + r)] = gr;
+                G[2 * ((int64_t)j * nr + r) + 1] = gi;
+            }
+        }
+        free(A); free(B); free(lam);
+    }
+    free(lc); free(ls);
+}
+
 /* ------------------------------------------------------------------ spin-2 */
 /* Normalised spin functions N_l d^l_{m,s}(theta), N_l = sqrt((2l+1)/4pi), for l = l0..lmax,
  * l0 = max(m, 2), s = +2 or -2, by the three-term Wigner-d recursion in l

@@ -50,6 +50,12 @@ def _lib():
         lib.orc_alm2cl.argtypes = [ctypes.c_int, ctypes.c_int, D, D, D]
         lib.orc_spin2_analysis_ms.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.c_int64,
                                               D, D, D, D, D, D]
+        lib.orc_legendre_analysis_ms.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                                 ctypes.c_int64, D, D, D, D]
+        lib.orc_legendre_synthesis_ms.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                                  ctypes.c_int64, D, D, D, D]
+        for f in (lib.orc_legendre_analysis_ms, lib.orc_legendre_synthesis_ms):
+            f.restype = None
         for f in (lib.orc_ring_tables, lib.orc_lambda_lm, lib.orc_legendre_analysis,
                   lib.orc_legendre_synthesis, lib.orc_spin2_lambda, lib.orc_spin2_analysis,
                   lib.orc_spin2_synthesis, lib.orc_alm2cl, lib.orc_spin2_analysis_ms):
@@ -336,6 +342,69 @@ def ring_analysis_ms(maps: np.ndarray, geom: dict, ms, weights) -> np.ndarray:
         D = np.where(k <= n // 2, R[np.minimum(k, n // 2)], np.conj(R[np.minimum(n - k, n // 2)]))
         F[:, r] = D * np.exp(-1j * ms * geom["phi0"][r]) * (2.0 * math.pi * weights[r] / n)
     return F
+
+
+def legendre_analysis_ms(F, geom: dict, lmax: int, ms) -> np.ndarray:
+    """Legendre analysis of the orders ``ms`` only: F [len(ms), nr] -> [len(ms), lmax + 1]."""
+    ms = np.ascontiguousarray(ms, dtype=np.int32)
+    F = _c(np.asarray(F, dtype=np.complex128))
+    out = np.zeros((ms.size, lmax + 1), dtype=np.complex128)
+    _lib().orc_legendre_analysis_ms(lmax, int(ms.size), ms.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), geom["nr"],
+                                    _p(_c(geom["x"])), _p(_c(geom["sin_theta"])), _p(F.view(np.float64)),
+                                    _p(out.view(np.float64)))
+    return out
+
+
+def legendre_synthesis_ms(a, geom: dict, lmax: int, ms) -> np.ndarray:
+    """Legendre synthesis of the orders ``ms`` only: a [len(ms), lmax + 1] -> G [len(ms), nr]."""
+    ms = np.ascontiguousarray(ms, dtype=np.int32)
+    a = _c(np.asarray(a, dtype=np.complex128))
+    G = np.zeros((ms.size, geom["nr"]), dtype=np.complex128)
+    _lib().orc_legendre_synthesis_ms(lmax, int(ms.size), ms.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), geom["nr"],
+                                     _p(_c(geom["x"])), _p(_c(geom["sin_theta"])), _p(a.view(np.float64)),
+                                     _p(G.view(np.float64)))
+    return G
+
+
+def alm_rows(alm, lmax: int, ms, mmax: int | None = None) -> np.ndarray:
+    """healpy-layout alm -> [len(ms), lmax + 1] rows of the orders ``ms`` (l < m zero)."""
+    mmax = lmax if mmax is None else mmax
+    alm = np.asarray(alm, dtype=np.complex128)
+    out = np.zeros((len(ms), lmax + 1), dtype=np.complex128)
+    for j, m in enumerate(ms):
+        m = int(m)
+        out[j, m:] = alm[m * (2 * lmax + 1 - m) // 2 + np.arange(m, lmax + 1)]
+    return out
+
+
+def map2alm_ms(maps, geom: dict, lmax: int, ms, weights=None) -> np.ndarray:
+    """a_lm of map2alm at the harmonic orders ``ms`` only: [len(ms), lmax + 1] (l < m zero).
+    For spot checks of transforms too large for the full oracle."""
+    w = geom["weights_dz"] if weights is None else weights
+    return legendre_analysis_ms(ring_analysis_ms(maps, geom, ms, w), geom, lmax, ms)
+
+
+def alm2map_ms(alm, geom: dict, lmax: int, ms, mmax: int | None = None) -> np.ndarray:
+    """The map of alm2map when only the orders ``ms`` of ``alm`` (healpy layout) are kept."""
+    ms = np.unique(np.asarray(ms, dtype=np.int64))
+    Gj = legendre_synthesis_ms(alm_rows(alm, lmax, ms, mmax), geom, lmax, ms)
+    G = np.zeros((int(ms.max()) + 1, geom["nr"]), dtype=np.complex128)
+    G[ms] = Gj
+    return ring_synthesis(G, geom)
+
+
+def ring_subset(geom: dict, r0: int, r1: int) -> dict:
+    """The rings [r0, r1) of a geometry as a geometry of their own (ring offsets rebased), for
+    running the ring FFT steps of a transform over a block of rings."""
+    rs = geom["ring_start"]
+    sub = dict(geom)
+    sub["nr"] = r1 - r0
+    for k in ("nphi", "phi0", "theta", "x", "z", "sin_theta", "weights_dz"):
+        if k in geom:
+            sub[k] = geom[k][r0:r1]
+    sub["ring_start"] = rs[r0:r1 + 1] - rs[r0]
+    sub["npix"] = int(rs[r1] - rs[r0])
+    return sub
 
 
 def map2alm_spin2_ms(Q, U, geom: dict, lmax: int, ms):
