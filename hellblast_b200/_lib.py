@@ -55,6 +55,8 @@ SIGNATURES = {
     "hb_ring_synthesis": (i32, [vp, i32, i32, vp, vp, i32, vp]),
     "hb_legendre_analysis": (i32, [vp, i32, i32, vp, vp, vp]),
     "hb_legendre_synthesis": (i32, [vp, i32, i32, vp, vp, vp]),
+    "hb_legendre_analysis_ms": (i32, [vp, i32, i32, i32, vp, vp, vp, vp]),
+    "hb_legendre_synthesis_ms": (i32, [vp, i32, i32, i32, vp, vp, vp, vp]),
     "hb_probe_fp32": (i32, [i32, i32, i32, vp, vp]),
     "hb_batched_plan_create": (i32, [ctypes.POINTER(vp), ctypes.POINTER(i32), i32, i32, ctypes.POINTER(vp)]),
     "hb_batched_plan_destroy": (i32, [vp]),

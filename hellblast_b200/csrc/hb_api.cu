@@ -292,6 +292,22 @@ int hb_ring_synthesis(const hb_plan *p, int prec, int nmaps, const void *G, void
     return launch_ring_synthesis(p->g->d, prec, nmaps, G, p->mmax, maps, p->g->d.npix, nullptr, false, true, flags,
                                  ST(s));
 }
+int hb_legendre_analysis_ms(const hb_plan *p, int prec, int nmaps, int nm, const int32_t *mlist, const void *F,
+                            void *alm, hb_stream_t s) {
+    if ((prec != 32 && prec != 64) || !F || !alm || !mlist || nm < 1 || nm > 65535)
+        return fail(HB_ERR_INVALID, "hb_legendre_analysis_ms: bad args");
+    int rc = check_plan(p, nmaps, prec, false, "hb_legendre_analysis_ms");
+    if (rc) return rc;
+    return launch_leg_analysis(HB_PLAN_ARGS(p), F, alm, ST(s), ck_of(p, prec), p->blk_ofs, nm, mlist);
+}
+int hb_legendre_synthesis_ms(const hb_plan *p, int prec, int nmaps, int nm, const int32_t *mlist, const void *alm,
+                             void *G, hb_stream_t s) {
+    if ((prec != 32 && prec != 64) || !G || !alm || !mlist || nm < 1 || nm > 65535)
+        return fail(HB_ERR_INVALID, "hb_legendre_synthesis_ms: bad args");
+    int rc = check_plan(p, nmaps, prec, false, "hb_legendre_synthesis_ms");
+    if (rc) return rc;
+    return launch_leg_synthesis(HB_PLAN_ARGS(p), alm, G, ST(s), ck_of(p, prec), p->blk_ofs, nm, mlist);
+}
 int hb_legendre_analysis(const hb_plan *p, int prec, int nmaps, const void *F, void *alm, hb_stream_t s) {
     if ((prec != 32 && prec != 64) || !F || !alm) return fail(HB_ERR_INVALID, "hb_legendre_analysis: bad args");
     int rc = check_plan(p, nmaps, prec, false, "hb_legendre_analysis");

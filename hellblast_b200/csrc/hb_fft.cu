@@ -44,6 +44,7 @@
 #include <cmath>
 
 #include "hb_internal.cuh"
+#include "hb_fftcore.cuh"
 
 namespace hb {
 
@@ -87,107 +88,6 @@ template <typename T> struct Tw {
         const V v = tab[j & (half - 1)];
         return (j & half) ? mk2(-v.x, -v.y) : v;
     }
-};
-
-// multiply by -i (forward) or +i (inverse)
-template <bool INV, typename V> __device__ __forceinline__ V rot90(V a) {
-    return INV ? mk2(-a.y, a.x) : mk2(a.y, -a.x);
-}
-
-template <bool INV, typename V> __device__ __forceinline__ void dft2(V *x) {
-    const V a = x[0], b = x[1];
-    x[0] = cadd(a, b);
-    x[1] = csub(a, b);
-}
-
-template <bool INV, typename V> __device__ __forceinline__ void dft4(V &x0, V &x1, V &x2, V &x3) {
-    const V a0 = cadd(x0, x2), a1 = csub(x0, x2), a2 = cadd(x1, x3), a3 = rot90<INV>(csub(x1, x3));
-    x0 = cadd(a0, a2);
-    x2 = csub(a0, a2);
-    x1 = cadd(a1, a3);
-    x3 = csub(a1, a3);
-}
-
-template <bool INV, typename V> __device__ __forceinline__ void dft4(V *x) { dft4<INV>(x[0], x[1], x[2], x[3]); }
-
-template <bool INV, typename V> __device__ __forceinline__ void dft8(V *x) {
-    using T = decltype(x[0].x);
-    const T r = (T)0.70710678118654752440084436210484903928;
-    V e0 = x[0], e1 = x[2], e2 = x[4], e3 = x[6];
-    V o0 = x[1], o1 = x[3], o2 = x[5], o3 = x[7];
-    dft4<INV>(e0, e1, e2, e3);
-    dft4<INV>(o0, o1, o2, o3);
-    // o_q *= w8^q, w8 = exp(-+ 2 pi i / 8)
-    o1 = INV ? mk2(r * (o1.x - o1.y), r * (o1.x + o1.y)) : mk2(r * (o1.x + o1.y), r * (o1.y - o1.x));
-    o2 = rot90<INV>(o2);
-    o3 = INV ? mk2(-r * (o3.x + o3.y), r * (o3.x - o3.y)) : mk2(r * (o3.y - o3.x), -r * (o3.x + o3.y));
-    x[0] = cadd(e0, o0);
-    x[4] = csub(e0, o0);
-    x[1] = cadd(e1, o1);
-    x[5] = csub(e1, o1);
-    x[2] = cadd(e2, o2);
-    x[6] = csub(e2, o2);
-    x[3] = cadd(e3, o3);
-    x[7] = csub(e3, o3);
-}
-
-// x *= exp(-+ 2 pi i e / 16) for the constant exponents of the radix-16 butterfly
-template <int E, bool INV, typename V> __device__ __forceinline__ V w16(V a) {
-    using T = decltype(a.x);
-    constexpr double C[10] = {1.0, 0.92387953251128675612818318939678828682, 0.70710678118654752440084436210484903928,
-                              0.38268343236508977172845998403039886676, 0.0, -0.38268343236508977172845998403039886676,
-                              -0.70710678118654752440084436210484903928, -0.92387953251128675612818318939678828682, -1.0,
-                              -0.92387953251128675612818318939678828682};
-    constexpr double S[10] = {0.0, 0.38268343236508977172845998403039886676, 0.70710678118654752440084436210484903928,
-                              0.92387953251128675612818318939678828682, 1.0, 0.92387953251128675612818318939678828682,
-                              0.70710678118654752440084436210484903928, 0.38268343236508977172845998403039886676, 0.0,
-                              -0.38268343236508977172845998403039886676};
-    if constexpr (E == 0) return a;
-    else if constexpr (E == 4) return rot90<INV>(a);
-    else {
-        const T c = (T)C[E], s = INV ? (T)S[E] : (T)(-S[E]);  // (c, s) = cos - +i sin
-        return mk2(a.x * c - a.y * s, a.x * s + a.y * c);
-    }
-}
-
-// 16-point DFT as 4 x 4: inner DFT-4 over n2 (n = n1 + 4 n2), twiddles W16^(n1 k2), outer
-// DFT-4 over n1; X[4 k1 + k2] ends in register k1 + 4 k2 and is renamed into place.
-template <bool INV, typename V> __device__ __forceinline__ void dft16(V *x) {
-#pragma unroll
-    for (int n1 = 0; n1 < 4; ++n1) dft4<INV>(x[n1], x[n1 + 4], x[n1 + 8], x[n1 + 12]);
-    x[5] = w16<1, INV>(x[5]);
-    x[9] = w16<2, INV>(x[9]);
-    x[13] = w16<3, INV>(x[13]);
-    x[6] = w16<2, INV>(x[6]);
-    x[10] = w16<4, INV>(x[10]);
-    x[14] = w16<6, INV>(x[14]);
-    x[7] = w16<3, INV>(x[7]);
-    x[11] = w16<6, INV>(x[11]);
-    x[15] = w16<9, INV>(x[15]);
-#pragma unroll
-    for (int k2 = 0; k2 < 4; ++k2) dft4<INV>(x[4 * k2], x[4 * k2 + 1], x[4 * k2 + 2], x[4 * k2 + 3]);
-    V y[16];
-#pragma unroll
-    for (int k1 = 0; k1 < 4; ++k1)
-#pragma unroll
-        for (int k2 = 0; k2 < 4; ++k2) y[4 * k1 + k2] = x[k1 + 4 * k2];
-#pragma unroll
-    for (int i = 0; i < 16; ++i) x[i] = y[i];
-}
-
-template <int R, bool INV, typename V> __device__ __forceinline__ void dftR(V *x) {
-    if constexpr (R == 16)
-        dft16<INV>(x);
-    else if constexpr (R == 8)
-        dft8<INV>(x);
-    else if constexpr (R == 4)
-        dft4<INV>(x);
-    else
-        dft2<INV>(x);
-}
-
-template <int R> struct Log2R {
-    static constexpr int v = R == 16 ? 4 : (R == 8 ? 3 : (R == 4 ? 2 : 1));
 };
 
 // x[q] *= W_S^(pos q) (conjugated for INV), q = 1 .. R-1.  Radix 16 and 8 load W^pos, W^2pos,
@@ -740,6 +640,62 @@ __global__ void __launch_bounds__(256) bluestein_table_kernel(GeomDev g) {
     }
 }
 
+// Natural-order FP32 chirp spectra of the pair-packed Bluestein kernels (hb_ringpack.cu):
+// table e = FFT_L(b) / L, b_t = exp(+i pi t^2 / n) for |t| < n (circular), L = 2^logL >= 2n - 1,
+// n = ns[e].  One CTA per table; the FP64 transform runs in place in a global scratch slot
+// (DIF, digit order; barriers make each pass's stores visible to the block), and the result is
+// read back in natural order.
+__global__ void __launch_bounds__(256) pk_chirp_kernel(GeomDev g, const int32_t *__restrict__ ns,
+                                                       const int32_t *__restrict__ logLs,
+                                                       const int64_t *__restrict__ ofs, int first, double2 *scratch,
+                                                       int64_t slot, float2 *out) {
+    const int e = first + blockIdx.x, n = ns[e], logL = logLs[e], L = 1 << logL;
+    double2 *buf = scratch + (int64_t)blockIdx.x * slot;
+    for (int t = threadIdx.x; t < L; t += blockDim.x) {
+        const int64_t j = (t < n) ? t : ((L - t < n) ? L - t : -1);
+        double2 v = make_double2(0.0, 0.0);
+        if (j >= 0) {
+            const double2 c = expmipi<double>(j * j, n);  // exp(-i pi j^2 / n)
+            v = make_double2(c.x, -c.y);
+        }
+        buf[t] = v;
+    }
+    __syncthreads();
+    const Tw<double> tw{g.tw64, g.log_tw};
+    auto ldg = [&](int p) -> double2 { return buf[p]; };
+    auto stg = [&](int p, double2 v) { buf[p] = v; };
+    for (int i = 0; i < fft_nstages(logL); ++i) {
+        fft_stage<false, false, double>(i, logL, tw, ldg, stg);
+        __syncthreads();
+    }
+    const double inv = 1.0 / (double)L;
+    for (int k = threadIdx.x; k < L; k += blockDim.x) {
+        const double2 v = buf[pos_of_freq(k, logL)];
+        out[ofs[e] + k] = make_float2((float)(v.x * inv), (float)(v.y * inv));
+    }
+}
+
+int build_pk_chirp_tables(const GeomDev &g, int count, const int32_t *ns, const int32_t *logL, const int64_t *ofs,
+                          int max_logL, float2 *out, cudaStream_t st) {
+    const int64_t slot = int64_t(1) << max_logL;
+    const int chunk = 128;
+    double2 *scratch = nullptr;
+    if (cudaMalloc(&scratch, sizeof(double2) * slot * chunk) != cudaSuccess) {
+        cudaGetLastError();
+        return fail(HB_ERR_ALLOC, "hb_geom: chirp-spectrum scratch allocation failed");
+    }
+    int rc = HB_OK;
+    for (int first = 0; first < count && rc == HB_OK; first += chunk) {
+        const int cnt = std::min(chunk, count - first);
+        pk_chirp_kernel<<<cnt, 256, 0, st>>>(g, ns, logL, ofs, first, scratch, slot, out);
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) rc = fail(HB_ERR_CUDA, std::string("pk_chirp_kernel: ") + cudaGetErrorString(e));
+    }
+    if (cudaStreamSynchronize(st) != cudaSuccess && rc == HB_OK) rc = fail(HB_ERR_CUDA, "pk_chirp_kernel failed");
+    cudaFree(scratch);
+    return rc;
+}
+
 int build_fft_tables(GeomDev &g, cudaStream_t st) {
     twiddle_table_kernel<<<64, 256, 0, st>>>(g);
     HB_CHECK_LAUNCH();
@@ -811,9 +767,20 @@ static int launch_analysis_t(const GeomDev &g, int nmaps, const T *maps, int64_t
     if (rc) return rc;
     if (nmaps > 65535) return fail(HB_ERR_INVALID, "ring FFT: at most 65535 maps per call");
     const int64_t fm_stride = (int64_t)(mmax + 1) * g.npairs * 2;
-    for (int c = 0; c < g.n_cls; ++c) {
-        const int L = g.cls_L[c];
-        const int64_t first = g.cls_first[c], cnt = g.cls_first[c + 1] - first;
+    // FP32: the pair-packed kernels take the pairs they can (hb_ringpack.cu), this kernel the rest
+    const bool f32 = sizeof(T) == 4;
+    if (f32 && g.pk_n_cls > 0) {
+        rc = launch_pk_analysis(g, nmaps, reinterpret_cast<const float *>(maps), map_stride, w ? w : g.w,
+                                reinterpret_cast<float2 *>(Fm), mmax, flags, unit_w, mdouble, st);
+        if (rc) return rc;
+    }
+    const int ncls = f32 ? g.rest_n_cls : g.n_cls;
+    const int *clsL = f32 ? g.rest_L : g.cls_L;
+    const int64_t *clsF = f32 ? g.rest_first : g.cls_first;
+    const int32_t *clsP = f32 ? g.rest_pairs : g.cls_pairs;
+    for (int c = 0; c < ncls; ++c) {
+        const int L = clsL[c];
+        const int64_t first = clsF[c], cnt = clsF[c + 1] - first;
         // stage the north ring's F(m) for joint (north, south) stores unless that costs CTAs per SM
         const size_t base_smem = class_smem<T>(L, mmax), stage_bytes = sizeof(c2_t<T>) * (size_t)(mmax + 1);
         const int ctas0 = ctas_by_smem(base_smem), ctas1 = ctas_by_smem(base_smem + stage_bytes);
@@ -823,7 +790,7 @@ static int launch_analysis_t(const GeomDev &g, int nmaps, const T *maps, int64_t
         HB_CUDA_TRY(cudaFuncSetAttribute(ring_analysis_kernel<T>, cudaFuncAttributePreferredSharedMemoryCarveout,
                                          cudaSharedmemCarveoutMaxShared));
         dim3 grid((unsigned)cnt, (unsigned)nmaps);
-        ring_analysis_kernel<T><<<grid, class_threads(L), smem, st>>>(g, g.cls_pairs + first, maps, map_stride,
+        ring_analysis_kernel<T><<<grid, class_threads(L), smem, st>>>(g, clsP + first, maps, map_stride,
                                                                        w ? w : g.w, Fm, fm_stride, mmax, flags,
                                                                        unit_w ? 1 : 0, mdouble ? 1 : 0, L,
                                                                        stage_n ? 1 : 0);
@@ -839,9 +806,20 @@ static int launch_synthesis_t(const GeomDev &g, int nmaps, const c2_t<T> *Gm, in
     if (rc) return rc;
     if (nmaps > 65535) return fail(HB_ERR_INVALID, "ring FFT: at most 65535 maps per call");
     const int64_t gm_stride = (int64_t)(mmax + 1) * g.npairs * 2;
-    for (int c = 0; c < g.n_cls; ++c) {
-        const int L = g.cls_L[c];
-        const int64_t first = g.cls_first[c], cnt = g.cls_first[c + 1] - first;
+    // FP32: the pair-packed kernels take the pairs they can (hb_ringpack.cu), this kernel the rest
+    const bool f32 = sizeof(T) == 4;
+    if (f32 && g.pk_n_cls > 0) {
+        rc = launch_pk_synthesis(g, nmaps, reinterpret_cast<const float2 *>(Gm), mmax, reinterpret_cast<float *>(maps),
+                                 map_stride, w ? w : g.w, apply_w, mdouble, flags, st);
+        if (rc) return rc;
+    }
+    const int ncls = f32 ? g.rest_n_cls : g.n_cls;
+    const int *clsL = f32 ? g.rest_L : g.cls_L;
+    const int64_t *clsF = f32 ? g.rest_first : g.cls_first;
+    const int32_t *clsP = f32 ? g.rest_pairs : g.cls_pairs;
+    for (int c = 0; c < ncls; ++c) {
+        const int L = clsL[c];
+        const int64_t first = clsF[c], cnt = clsF[c + 1] - first;
         const bool stage_t = class_smem_syn<T>(L, mmax, true) <= (size_t)max_smem_optin();
         const int smem = (int)class_smem_syn<T>(L, mmax, stage_t), nt = class_threads(L);
         HB_CUDA_TRY(cudaFuncSetAttribute(ring_synthesis_kernel<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
@@ -852,7 +830,7 @@ static int launch_synthesis_t(const GeomDev &g, int nmaps, const c2_t<T> *Gm, in
         HB_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, ring_synthesis_kernel<T>, nt, smem));
         const bool async_t = stage_t && cnt * (int64_t)nmaps < 2 * (int64_t)sm_count() * std::max(occ, 1);
         dim3 grid((unsigned)cnt, (unsigned)nmaps);
-        ring_synthesis_kernel<T><<<grid, nt, smem, st>>>(g, g.cls_pairs + first, Gm, gm_stride, mmax, maps, map_stride,
+        ring_synthesis_kernel<T><<<grid, nt, smem, st>>>(g, clsP + first, Gm, gm_stride, mmax, maps, map_stride,
                                                          w ? w : g.w, apply_w ? 1 : 0, mdouble ? 1 : 0, flags, L,
                                                          stage_t ? (async_t ? 2 : 1) : 0);
         HB_CHECK_LAUNCH();

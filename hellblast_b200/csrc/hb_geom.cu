@@ -7,6 +7,7 @@
 // (no serial scan by thread 0), and phi0 in either the HEALPix convention (default) or the
 // reference's, which sits +1/2 pixel off on the equatorial belt (ring_tables_healpix.cu:25-27).
 #include <algorithm>
+#include <cstdlib>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -169,6 +170,62 @@ static int finish_geom(HostGeom &h, int64_t nside, const std::vector<double> &xn
     }
     cls_first.push_back(np);
     if (cls_L.size() > 32) return fail(HB_ERR_UNSUPPORTED, "hb_geom: more than 32 FFT length classes");
+    // FP32: the pairs of the pair-packed kernels by (log2 L, Bluestein), the rest as above
+    // (HB_NO_PAIR_PACK set in the environment keeps every pair on the general kernels,
+    // HB_NO_PAIR_PACK_BLU the Bluestein pairs)
+    const bool pack = std::getenv("HB_NO_PAIR_PACK") == nullptr;
+    const bool pack_blu = std::getenv("HB_NO_PAIR_PACK_BLU") == nullptr;
+    std::vector<std::pair<int32_t, int32_t>> pk, rest;
+    std::vector<int64_t> pkb_ofs(np, -1);
+    std::map<int, int64_t> bt_of_n;  // ring length -> offset of its chirp spectrum
+    std::vector<int32_t> bt_n, bt_logL;
+    std::vector<int64_t> bt_ofs;
+    int64_t bt_total = 0;
+    int pk_max_log = 0;
+    for (int64_t i = 0; i < np; ++i) {
+        const int32_t p = pl[i].second, rn = h.pair_ring[2 * p], rs = h.pair_ring[2 * p + 1];
+        int lg = 0;
+        bool blu = false;
+        if (pack && pk_pair_ok(h.nphi[rn], rs >= 0 ? h.nphi[rs] : -1, h.phi0_pi[rn], rs >= 0 ? h.phi0_pi[rs] : 0.0, &lg,
+                               &blu) && (pack_blu || !blu)) {
+            pk.push_back({lg | (blu ? 256 : 0), p});
+            pk_max_log = std::max(pk_max_log, lg);
+            if (blu) {
+                auto it = bt_of_n.find(h.nphi[rn]);
+                if (it == bt_of_n.end()) {
+                    it = bt_of_n.emplace(h.nphi[rn], bt_total).first;
+                    bt_n.push_back(h.nphi[rn]);
+                    bt_logL.push_back(lg);
+                    bt_ofs.push_back(bt_total);
+                    bt_total += int64_t(1) << lg;
+                }
+                pkb_ofs[p] = it->second;
+            }
+        } else {
+            rest.push_back(pl[i]);
+        }
+    }
+    if (pk_max_log > log_tw) log_tw = pk_max_log;  // the FP64 chirp-spectrum transforms use the table
+    std::sort(pk.begin(), pk.end());
+    std::vector<int32_t> pk_pairs(np, 0), rest_pairs(np, 0), pk_logn, rest_L;
+    std::vector<int64_t> pk_first, rest_first;
+    for (size_t i = 0; i < pk.size(); ++i) {
+        pk_pairs[i] = pk[i].second;
+        if (i == 0 || pk[i].first != pk[i - 1].first) {
+            pk_logn.push_back(pk[i].first);
+            pk_first.push_back((int64_t)i);
+        }
+    }
+    pk_first.push_back((int64_t)pk.size());
+    if (pk_logn.size() > 16) return fail(HB_ERR_UNSUPPORTED, "hb_geom: more than 16 pair-packed classes");
+    for (size_t i = 0; i < rest.size(); ++i) {
+        rest_pairs[i] = rest[i].second;
+        if (i == 0 || rest[i].first != rest[i - 1].first) {
+            rest_L.push_back(rest[i].first);
+            rest_first.push_back((int64_t)i);
+        }
+    }
+    rest_first.push_back((int64_t)rest.size());
 
     // one device allocation carved into 256-byte aligned pieces
     size_t total = 0;
@@ -183,7 +240,9 @@ static int finish_geom(HostGeom &h, int64_t nside, const std::vector<double> &xn
            o_plh = carve(8 * np), o_fl = carve(4 * nr), o_bo = carve(8 * nr), o_b64 = carve(16 * (h.blu_total + 1)),
            o_b32 = carve(8 * (h.blu_total + 1)), o_bw = carve(4 * (h.blu_owner.size() + 1)), o_cm = carve(8 * (HB_MAX_L + 1)), o_sp = carve(8 * (HB_MAX_L + 1)),
            o_t64 = carve(16 * ((size_t)1 << (log_tw - 1))), o_t32 = carve(8 * ((size_t)1 << (log_tw - 1))),
-           o_cp = carve(4 * (size_t)np);
+           o_cp = carve(4 * (size_t)np), o_pk = carve(4 * (size_t)np), o_rest = carve(4 * (size_t)np),
+           o_pkbo = carve(8 * (size_t)np), o_bt = carve(8 * (size_t)(bt_total + 1)),
+           o_btn = carve(4 * (bt_n.size() + 1)), o_btl = carve(4 * (bt_n.size() + 1)), o_bto = carve(8 * (bt_n.size() + 1));
     char *base = nullptr;
     if (cudaMalloc(&base, total) != cudaSuccess) {
         cudaGetLastError();
@@ -208,6 +267,13 @@ static int finish_geom(HostGeom &h, int64_t nside, const std::vector<double> &xn
     d.cls_pairs = (int32_t *)(base + o_cp); d.n_cls = (int)cls_L.size();
     for (size_t c = 0; c < cls_L.size(); ++c) { d.cls_L[c] = cls_L[c]; d.cls_first[c] = cls_first[c]; }
     d.cls_first[cls_L.size()] = np;
+    d.pk_pairs = (int32_t *)(base + o_pk); d.pk_n_cls = (int)pk_logn.size();
+    for (size_t c = 0; c < pk_logn.size(); ++c) { d.pk_logn[c] = pk_logn[c]; d.pk_first[c] = pk_first[c]; }
+    d.pk_first[pk_logn.size()] = pk_first.back();
+    d.pkb_bt = (float2 *)(base + o_bt); d.pkb_bt_ofs = (int64_t *)(base + o_pkbo);
+    d.rest_pairs = (int32_t *)(base + o_rest); d.rest_n_cls = (int)rest_L.size();
+    for (size_t c = 0; c < rest_L.size(); ++c) { d.rest_L[c] = rest_L[c]; d.rest_first[c] = rest_first[c]; }
+    d.rest_first[rest_L.size()] = rest_first.back();
     struct Up { void *dst; const void *src; size_t n; } ups[] = {
         {d.nphi, h.nphi.data(), 4 * (size_t)nr}, {d.ofs, h.ofs.data(), 8 * (size_t)nr},
         {d.phi0_pi, h.phi0_pi.data(), 8 * (size_t)nr}, {d.w, h.w.data(), 8 * (size_t)nr},
@@ -218,7 +284,10 @@ static int finish_geom(HostGeom &h, int64_t nside, const std::vector<double> &xn
         {d.pair_log2sh, h.pair_log2sh.data(), 8 * (size_t)np}, {d.fft_len, h.fft_len.data(), 4 * (size_t)nr},
         {d.blu_ofs, h.blu_ofs.data(), 8 * (size_t)nr},
         {d.blu_owner, h.blu_owner.data(), 4 * h.blu_owner.size()}, {d.log2cm, cm.data(), 8 * (size_t)(HB_MAX_L + 1)},
-        {d.log2spin, spin.data(), 8 * (size_t)(HB_MAX_L + 1)}, {d.cls_pairs, cls_pairs.data(), 4 * (size_t)np}};
+        {d.log2spin, spin.data(), 8 * (size_t)(HB_MAX_L + 1)}, {d.cls_pairs, cls_pairs.data(), 4 * (size_t)np},
+        {d.pk_pairs, pk_pairs.data(), 4 * (size_t)np}, {d.rest_pairs, rest_pairs.data(), 4 * (size_t)np},
+        {d.pkb_bt_ofs, pkb_ofs.data(), 8 * (size_t)np}, {base + o_btn, bt_n.data(), 4 * bt_n.size()},
+        {base + o_btl, bt_logL.data(), 4 * bt_n.size()}, {base + o_bto, bt_ofs.data(), 8 * bt_n.size()}};
     for (auto &u : ups) {
         if (cudaMemcpy(u.dst, u.src, u.n, cudaMemcpyHostToDevice) != cudaSuccess) {
             cudaGetLastError();
@@ -228,6 +297,9 @@ static int finish_geom(HostGeom &h, int64_t nside, const std::vector<double> &xn
         }
     }
     int rc = build_fft_tables(d, 0);
+    if (rc == HB_OK && !bt_n.empty())
+        rc = build_pk_chirp_tables(d, (int)bt_n.size(), (const int32_t *)(base + o_btn), (const int32_t *)(base + o_btl),
+                                   (const int64_t *)(base + o_bto), pk_max_log, d.pkb_bt, 0);
     if (rc == HB_OK && cudaStreamSynchronize(0) != cudaSuccess) rc = fail(HB_ERR_CUDA, "hb_geom: table build failed");
     if (rc != HB_OK) {
         cudaFree(base);

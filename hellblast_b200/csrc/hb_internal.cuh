@@ -7,6 +7,9 @@
 #include "../../include/hbsht.h"
 
 #define HB_MAX_L 16383
+// nphi range (log2) of the pair-packed FP32 ring FFT kernels
+#define PK_MIN_LOG 9
+#define PK_MAX_LOG 14
 
 namespace hb {
 
@@ -94,6 +97,19 @@ struct GeomDev {
     int cls_L[32];
     int64_t cls_first[33];
     int max_nphi;
+    // FP32 ring FFTs: pairs taken by the pair-packed kernels (hb_ringpack.cu), grouped by
+    // class key log2 L | (Bluestein << 8), and the remaining pairs in convolution-length
+    // classes as above
+    int32_t *pk_pairs;     // [npairs]
+    int pk_n_cls;
+    int pk_logn[16];
+    int64_t pk_first[17];
+    float2 *pkb_bt;        // natural-order chirp spectra of the pair-packed Bluestein pairs
+    int64_t *pkb_bt_ofs;   // [npairs] offset of the pair's table in pkb_bt (-1: not Bluestein)
+    int32_t *rest_pairs;   // [npairs]
+    int rest_n_cls;
+    int rest_L[32];
+    int64_t rest_first[33];
     double *log2cm;        // [HB_MAX_L+1] log2 sqrt((2m+1)!!/((2m)!! 4 pi)), scalar lambda_mm
     double *log2spin;      // [HB_MAX_L+1] log2 of the constant of N_l0 d^l0_{m,+-2}
 };
@@ -129,11 +145,16 @@ int launch_ring_analysis(const GeomDev &g, int precision, int nmaps, const void 
 int launch_ring_synthesis(const GeomDev &g, int precision, int nmaps, const void *Gm, int mmax, void *maps,
                           int64_t map_stride, const double *w, bool apply_weights, bool mdouble, int flags,
                           cudaStream_t st);
-// ck / blk_ofs: FP32 recursion checkpoints of a plan (null: no re-anchoring; FP64 ignores them)
+// ck / blk_ofs: FP32 recursion checkpoints of a plan (null: no re-anchoring; FP64 ignores them).
+// mlist (device, nm entries; null: all orders 0..mmax): the orders to transform, F / G holding
+// one row per listed order in list order; alm rows of the other orders are left untouched
+// (analysis over several pair chunks clears the whole alm first).
 int launch_leg_analysis(const GeomDev &g, int precision, int nmaps, int lmax, int mmax, const void *Fm,
-                        void *alm, cudaStream_t st, const float4 *ck, const int64_t *blk_ofs);
+                        void *alm, cudaStream_t st, const float4 *ck, const int64_t *blk_ofs, int nm = 0,
+                        const int32_t *mlist = nullptr);
 int launch_leg_synthesis(const GeomDev &g, int precision, int nmaps, int lmax, int mmax, const void *alm,
-                         void *Gm, cudaStream_t st, const float4 *ck, const int64_t *blk_ofs);
+                         void *Gm, cudaStream_t st, const float4 *ck, const int64_t *blk_ofs, int nm = 0,
+                         const int32_t *mlist = nullptr);
 int launch_spin_analysis(const GeomDev &g, int precision, int nmaps, int lmax, int mmax, const void *QFm,
                          const void *UFm, void *E, void *B, cudaStream_t st, const float4 *ckP, const float4 *ckM,
                          const int64_t *blk_ofs);
@@ -142,4 +163,14 @@ int launch_spin_synthesis(const GeomDev &g, int precision, int nmaps, int lmax, 
                           const float4 *ckM, const int64_t *blk_ofs);
 // FFT twiddle table and Bluestein chirp spectra of a geometry
 int build_fft_tables(GeomDev &g, cudaStream_t st);
+// pair-packed FP32 ring FFTs (hb_ringpack.cu) over the geometry's pk_* pairs
+bool pk_pair_ok(int nphiN, int nphiS, double phi0N_pi, double phi0S_pi, int *logL, bool *blu);
+// chirp spectra of the pair-packed Bluestein pairs: count tables, table e of length 2^logL[e]
+// for ring length ns[e] at out + ofs[e] (device arrays); FP64 computed, FP32 stored
+int build_pk_chirp_tables(const GeomDev &g, int count, const int32_t *ns, const int32_t *logL, const int64_t *ofs,
+                          int max_logL, float2 *out, cudaStream_t st);
+int launch_pk_synthesis(const GeomDev &g, int nmaps, const float2 *Gm, int mmax, float *maps, int64_t map_stride,
+                        const double *w, bool apply_w, bool mdouble, int flags, cudaStream_t st);
+int launch_pk_analysis(const GeomDev &g, int nmaps, const float *maps, int64_t map_stride, const double *w,
+                       float2 *Fm, int mmax, int flags, bool unit_w, bool mdouble, cudaStream_t st);
 }  // namespace hb

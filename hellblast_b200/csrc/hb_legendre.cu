@@ -118,7 +118,8 @@ __global__ void __launch_bounds__(NT, 2) leg_analysis_kernel(GeomDev g, int lmax
                                                              int64_t fm_stride, c2_t<T> *__restrict__ alm,
                                                              int64_t alm_stride, int atomic,
                                                              const float4 *__restrict__ ck,
-                                                             const int64_t *__restrict__ blk_ofs) {
+                                                             const int64_t *__restrict__ blk_ofs,
+                                                             const int32_t *__restrict__ mlist) {
     using V = c2_t<T>;
     constexpr int TL = LegCfg<T>::TL;
     constexpr int TPS = NT / TL;  // threads reducing one l slot
@@ -126,9 +127,11 @@ __global__ void __launch_bounds__(NT, 2) leg_analysis_kernel(GeomDev g, int lmax
     __shared__ V coef[COEF_CH];
     extern __shared__ __align__(16) unsigned char leg_dyn_smem[];
     V(*red)[TL][NT] = reinterpret_cast<V(*)[TL][NT]>(leg_dyn_smem);  // [2][TL][NT]
-    const int m = blockIdx.x, chunk = blockIdx.y, b = blockIdx.z, tid = threadIdx.x;
+    // F row blockIdx.x holds order m (all orders, or the orders of mlist in list order)
+    const int m = mlist ? mlist[blockIdx.x] : blockIdx.x, chunk = blockIdx.y, b = blockIdx.z, tid = threadIdx.x;
+    if (m < 0 || m > mmax) return;  // a listed order outside the plan: nothing read or written
     const int64_t np = g.npairs;
-    const V *F = Fm + b * fm_stride + (int64_t)m * np * 2;
+    const V *F = Fm + b * fm_stride + (int64_t)blockIdx.x * np * 2;
     V *out = alm + b * alm_stride;
 
     T l1[K], l2[K];
@@ -268,14 +271,17 @@ template <typename T, int K, int NT>
 __global__ void __launch_bounds__(NT, 2) leg_synthesis_kernel(GeomDev g, int lmax, int mmax, const c2_t<T> *__restrict__ alm,
                                                               int64_t alm_stride, c2_t<T> *__restrict__ Gm,
                                                               int64_t gm_stride, const float4 *__restrict__ ck,
-                                                              const int64_t *__restrict__ blk_ofs) {
+                                                              const int64_t *__restrict__ blk_ofs,
+                                                              const int32_t *__restrict__ mlist) {
     using V = c2_t<T>;
     __shared__ V coef[COEF_CH];
     __shared__ V acoef[COEF_CH];
-    const int m = blockIdx.x, chunk = blockIdx.y, b = blockIdx.z, tid = threadIdx.x;
+    // G row blockIdx.x holds order m (all orders, or the orders of mlist in list order)
+    const int m = mlist ? mlist[blockIdx.x] : blockIdx.x, chunk = blockIdx.y, b = blockIdx.z, tid = threadIdx.x;
+    if (m < 0 || m > mmax) return;  // a listed order outside the plan: nothing read or written
     const int64_t np = g.npairs;
     const V *a = alm + b * alm_stride;
-    V *G = Gm + b * gm_stride + (int64_t)m * np * 2;
+    V *G = Gm + b * gm_stride + (int64_t)blockIdx.x * np * 2;
 
     T l1[K], l2[K];
     XRep<T> x[K];
@@ -388,64 +394,68 @@ __global__ void __launch_bounds__(NT, 2) leg_synthesis_kernel(GeomDev g, int lma
 
 template <typename T, int K, int NT>
 static int run_analysis(const GeomDev &g, int nmaps, int lmax, int mmax, const c2_t<T> *Fm, c2_t<T> *alm,
-                        cudaStream_t st, const float4 *ck, const int64_t *bo) {
+                        cudaStream_t st, const float4 *ck, const int64_t *bo, int nm, const int32_t *mlist) {
     const int64_t per = (int64_t)K * NT;
     const int nchunks = (int)((g.npairs + per - 1) / per);
-    const int64_t fm_stride = (int64_t)(mmax + 1) * g.npairs * 2;
+    const int rows = mlist ? nm : mmax + 1;
+    const int64_t fm_stride = (int64_t)rows * g.npairs * 2;
     const int64_t alm_stride = alm_size(lmax, mmax);
     if (nchunks > 1) HB_CUDA_TRY(cudaMemsetAsync(alm, 0, sizeof(c2_t<T>) * alm_stride * nmaps, st));
     const int smem = 2 * LegCfg<T>::TL * NT * (int)sizeof(c2_t<T>);
     HB_CUDA_TRY(cudaFuncSetAttribute(leg_analysis_kernel<T, K, NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    dim3 grid((unsigned)(mmax + 1), (unsigned)nchunks, (unsigned)nmaps);
+    dim3 grid((unsigned)rows, (unsigned)nchunks, (unsigned)nmaps);
     leg_analysis_kernel<T, K, NT><<<grid, NT, smem, st>>>(g, lmax, mmax, Fm, fm_stride, alm, alm_stride, nchunks > 1,
-                                                           ck, bo);
+                                                           ck, bo, mlist);
     HB_CHECK_LAUNCH();
     return HB_OK;
 }
 
 template <typename T, int K, int NT>
 static int run_synthesis(const GeomDev &g, int nmaps, int lmax, int mmax, const c2_t<T> *alm, c2_t<T> *Gm,
-                         cudaStream_t st, const float4 *ck, const int64_t *bo) {
+                         cudaStream_t st, const float4 *ck, const int64_t *bo, int nm, const int32_t *mlist) {
     const int64_t per = (int64_t)K * NT;
     const int nchunks = (int)((g.npairs + per - 1) / per);
-    const int64_t gm_stride = (int64_t)(mmax + 1) * g.npairs * 2;
+    const int rows = mlist ? nm : mmax + 1;
+    const int64_t gm_stride = (int64_t)rows * g.npairs * 2;
     const int64_t alm_stride = alm_size(lmax, mmax);
-    dim3 grid((unsigned)(mmax + 1), (unsigned)nchunks, (unsigned)nmaps);
-    leg_synthesis_kernel<T, K, NT><<<grid, NT, 0, st>>>(g, lmax, mmax, alm, alm_stride, Gm, gm_stride, ck, bo);
+    dim3 grid((unsigned)rows, (unsigned)nchunks, (unsigned)nmaps);
+    leg_synthesis_kernel<T, K, NT><<<grid, NT, 0, st>>>(g, lmax, mmax, alm, alm_stride, Gm, gm_stride, ck, bo, mlist);
     HB_CHECK_LAUNCH();
     return HB_OK;
 }
 
 template <typename T>
-static int analysis_t(const GeomDev &g, int nmaps, int lmax, int mmax, const c2_t<T> *Fm, c2_t<T> *alm,
+static int analysis_t(const GeomDev &g, int nmaps, int lmax, int mmax, int nm, const int32_t *mlist, const c2_t<T> *Fm, c2_t<T> *alm,
                       cudaStream_t st, const float4 *ck, const int64_t *bo) {
-    if (g.npairs >= 1024) return run_analysis<T, 8, 256>(g, nmaps, lmax, mmax, Fm, alm, st, ck, bo);
-    if (g.npairs >= 256) return run_analysis<T, 4, 128>(g, nmaps, lmax, mmax, Fm, alm, st, ck, bo);
-    if (g.npairs >= 64) return run_analysis<T, 2, 64>(g, nmaps, lmax, mmax, Fm, alm, st, ck, bo);
-    return run_analysis<T, 1, 64>(g, nmaps, lmax, mmax, Fm, alm, st, ck, bo);
+    if (g.npairs >= 1024) return run_analysis<T, 8, 256>(g, nmaps, lmax, mmax, Fm, alm, st, ck, bo, nm, mlist);
+    if (g.npairs >= 256) return run_analysis<T, 4, 128>(g, nmaps, lmax, mmax, Fm, alm, st, ck, bo, nm, mlist);
+    if (g.npairs >= 64) return run_analysis<T, 2, 64>(g, nmaps, lmax, mmax, Fm, alm, st, ck, bo, nm, mlist);
+    return run_analysis<T, 1, 64>(g, nmaps, lmax, mmax, Fm, alm, st, ck, bo, nm, mlist);
 }
 
 template <typename T>
-static int synthesis_t(const GeomDev &g, int nmaps, int lmax, int mmax, const c2_t<T> *alm, c2_t<T> *Gm,
+static int synthesis_t(const GeomDev &g, int nmaps, int lmax, int mmax, int nm, const int32_t *mlist, const c2_t<T> *alm, c2_t<T> *Gm,
                        cudaStream_t st, const float4 *ck, const int64_t *bo) {
-    if (g.npairs >= 1024) return run_synthesis<T, 8, 256>(g, nmaps, lmax, mmax, alm, Gm, st, ck, bo);
-    if (g.npairs >= 256) return run_synthesis<T, 4, 128>(g, nmaps, lmax, mmax, alm, Gm, st, ck, bo);
-    if (g.npairs >= 64) return run_synthesis<T, 2, 64>(g, nmaps, lmax, mmax, alm, Gm, st, ck, bo);
-    return run_synthesis<T, 1, 64>(g, nmaps, lmax, mmax, alm, Gm, st, ck, bo);
+    if (g.npairs >= 1024) return run_synthesis<T, 8, 256>(g, nmaps, lmax, mmax, alm, Gm, st, ck, bo, nm, mlist);
+    if (g.npairs >= 256) return run_synthesis<T, 4, 128>(g, nmaps, lmax, mmax, alm, Gm, st, ck, bo, nm, mlist);
+    if (g.npairs >= 64) return run_synthesis<T, 2, 64>(g, nmaps, lmax, mmax, alm, Gm, st, ck, bo, nm, mlist);
+    return run_synthesis<T, 1, 64>(g, nmaps, lmax, mmax, alm, Gm, st, ck, bo, nm, mlist);
 }
 
 int launch_leg_analysis(const GeomDev &g, int precision, int nmaps, int lmax, int mmax, const void *Fm, void *alm,
-                        cudaStream_t st, const float4 *ck, const int64_t *bo) {
+                        cudaStream_t st, const float4 *ck, const int64_t *bo, int nm, const int32_t *mlist) {
     if (precision == 32)
-        return analysis_t<float>(g, nmaps, lmax, mmax, (const float2 *)Fm, (float2 *)alm, st, ck, bo);
-    return analysis_t<double>(g, nmaps, lmax, mmax, (const double2 *)Fm, (double2 *)alm, st, nullptr, nullptr);
+        return analysis_t<float>(g, nmaps, lmax, mmax, nm, mlist, (const float2 *)Fm, (float2 *)alm, st, ck, bo);
+    return analysis_t<double>(g, nmaps, lmax, mmax, nm, mlist, (const double2 *)Fm, (double2 *)alm, st, nullptr,
+                              nullptr);
 }
 
 int launch_leg_synthesis(const GeomDev &g, int precision, int nmaps, int lmax, int mmax, const void *alm, void *Gm,
-                         cudaStream_t st, const float4 *ck, const int64_t *bo) {
+                         cudaStream_t st, const float4 *ck, const int64_t *bo, int nm, const int32_t *mlist) {
     if (precision == 32)
-        return synthesis_t<float>(g, nmaps, lmax, mmax, (const float2 *)alm, (float2 *)Gm, st, ck, bo);
-    return synthesis_t<double>(g, nmaps, lmax, mmax, (const double2 *)alm, (double2 *)Gm, st, nullptr, nullptr);
+        return synthesis_t<float>(g, nmaps, lmax, mmax, nm, mlist, (const float2 *)alm, (float2 *)Gm, st, ck, bo);
+    return synthesis_t<double>(g, nmaps, lmax, mmax, nm, mlist, (const double2 *)alm, (double2 *)Gm, st, nullptr,
+                               nullptr);
 }
 
 }  // namespace hb

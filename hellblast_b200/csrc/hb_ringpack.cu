@@ -1,0 +1,510 @@
+// Pair-packed ring FFTs (FP32) for the ring pairs of HEALPix-type grids.
+//
+// Replaces, for these pairs, the per-ring cp.fft.fft / cp.fft.ifft loops of the reference
+// (sht_raw.py:38-43, sht_fallback.py:51-55, isht.py:16-24, spin.py:46-53,107-108).
+//
+// Which pairs: both rings (north r_N and its mirror r_S, or an unpaired ring alone) have the
+// same even nphi = n and the same phi0 = s pi / n for an integer s, and the transform length
+// L (n itself when n is a power of two, else the Bluestein length 2^ceil(log2(2n - 1))) lies in
+// [512, 16384].  On a HEALPix grid that is the whole equatorial belt (n = 4 nside, s = 0 or 1
+// alternating; with the reference's phi0 convention s = 1 or 2) and every polar ring from
+// ring index 64 on (n = 4i, s = 1).  Everything else (the smallest polar rings, generic grids,
+// FP64) runs in hb_fft.cu.
+//
+// Bluestein (n not a power of two): the length-n DFT X_j = c_j sum_k (x_k c_k) b_{j-k},
+// c_t = exp(-i pi t^2 / n), b_t = conj c_t, is a circular convolution of length L >= 2n - 1:
+// x c (zero-padded), forward FFT_L, times the chirp spectrum FFT_L(b) / L (natural order, one
+// FP32 table per distinct n in the geometry), inverse FFT_L, times c.  The synthesis runs the
+// inverse DFT as conj(DFT(conj Z)).  c_t comes from the phase table: t^2 mod 2n is exact.
+//
+// Packing: the two real rings of a pair form one complex sequence z_j = f_N[j] + i f_S[j],
+// j < n, transformed by one complex FFT of length n.  Synthesis builds the spectrum Z of z from
+// the two rings' folded Fourier coefficients and writes Re z to the north ring and Im z to the
+// south ring; analysis splits the spectrum of z into the two rings' spectra,
+// D_N[k] = (Z[k] + conj Z[n-k]) / 2 and D_S[k] = (Z[k] - conj Z[n-k]) / (2i).  No untangling
+// step and no per-ring second pass: one FFT per pair and map.
+//
+// phi0 phase and alias fold (the reference has neither, sht_raw.py:41,51): harmonic m lands on
+// bin m mod n and its conjugate on bin -m mod n; with phi0 = s pi / n,
+// exp(i m phi0) = exp(i pi s k / n) (-1)^(s j) for m = k + j n, so every residue class k of
+// m mod n takes one phase product and alternating signs over its aliases.
+//
+// FFT: Stockham autosort, compile-time length L = n = 2^LOGL, radix 16 for every pass but the
+// second, which takes the remaining 2^(LOGL mod 4).  Pass with radix R after sub-transforms of
+// length NS: butterfly b (j = b mod NS) reads points b + t L/R, multiplies point t by
+// W_L^(j t L/(NS R)), transforms, and writes point q to (b - j) R + j + q NS.  Every thread
+// holds 16 points per pass (one radix-16 butterfly, or 16/R small ones), so the transform runs
+// in place in one shared buffer: all loads of a pass, a barrier, then the stores.  Natural order
+// in and out: the analysis's first pass reads the two rings straight from global memory and the
+// synthesis's last pass writes them (both coalesced, lanes on consecutive pixels).  Twiddles and
+// the phi0 phases are products of two entries of small per-CTA tables (64 fine steps times
+// coarse steps, FP64-computed).
+#include <algorithm>
+#include <cmath>
+#include <type_traits>
+#include <vector>
+
+#include "hb_internal.cuh"
+#include "hb_fftcore.cuh"
+
+namespace hb {
+
+// shared-buffer index of FFT point i: one pad entry per 16 keeps the radix-R strided stores of
+// the first passes on distinct banks
+__device__ __forceinline__ int pk_pad(int i) { return i + (i >> 4); }
+
+template <int LOGL> struct PkCfg {
+    static constexpr int L = 1 << LOGL;
+    static constexpr int NT = L / 16;                                // threads: 16 points each
+    static constexpr int R1 = (LOGL & 3) ? (1 << (LOGL & 3)) : 16;   // radix of pass 1
+    static constexpr int NPASS = (LOGL >> 2) + ((LOGL & 3) ? 1 : 0);
+    static constexpr int BUF = L + (L >> 4);
+    static constexpr int TWC = L / 64;       // coarse twiddle entries W_L^(64 c)
+    static constexpr int PHC = 2 * L / 64;   // coarse phase entries exp(i pi 64 c / n), 2n <= 2L
+    static constexpr int SMEM = (BUF + 64 + TWC + 64 + PHC) * (int)sizeof(float2);
+    static constexpr int MINB = 65536 / (NT * 64) > 0 ? 65536 / (NT * 64) : 1;  // <= 64 registers
+};
+
+template <int LOGL, int P> struct PkPass {
+    static constexpr int R = P == 1 ? PkCfg<LOGL>::R1 : 16;
+    static constexpr int NS = P == 0 ? 1 : (P == 1 ? 16 : 16 * PkCfg<LOGL>::R1 * (1 << (4 * (P - 2))));
+};
+
+struct PkTab {
+    const float2 *twf, *twc;  // W_L^e = twf[e & 63] twc[e >> 6], e < L
+    const float2 *phf, *phc;  // exp(i pi e / n) = phf[e & 63] phc[e >> 6], e < 2n
+    __device__ __forceinline__ float2 w(int e) const { return cmul(twf[e & 63], twc[e >> 6]); }
+    __device__ __forceinline__ float2 ph(int e) const { return cmul(phf[e & 63], phc[e >> 6]); }
+};
+
+// per-CTA tables: twiddles of length L, phases exp(i pi e / n) for the ring length n
+template <int LOGL> __device__ __forceinline__ PkTab pk_tables(float2 *base, int n) {
+    using C = PkCfg<LOGL>;
+    float2 *twf = base, *twc = twf + 64, *phf = twc + C::TWC, *phc = phf + 64;
+    const double L = (double)C::L, dn = (double)n;
+    for (int i = threadIdx.x; i < 64 + C::TWC + 64 + C::PHC; i += C::NT) {
+        double sn, cs;
+        if (i < 64) {  // W_L^i
+            sincospi(-2.0 * (double)i / L, &sn, &cs);
+            twf[i] = make_float2((float)cs, (float)sn);
+        } else if (i < 64 + C::TWC) {  // W_L^(64 c)
+            sincospi(-2.0 * (double)(64 * (i - 64)) / L, &sn, &cs);
+            twc[i - 64] = make_float2((float)cs, (float)sn);
+        } else if (i < 128 + C::TWC) {  // exp(i pi e / n), e < 64
+            sincospi((double)(i - 64 - C::TWC) / dn, &sn, &cs);
+            phf[i - 64 - C::TWC] = make_float2((float)cs, (float)sn);
+        } else {  // exp(i pi 64 c / n), 64 c < 2n <= 2L
+            const int c = i - 128 - C::TWC;
+            sincospi((double)(64 * c) / dn, &sn, &cs);
+            phc[c] = make_float2((float)cs, (float)sn);
+        }
+    }
+    return {twf, twc, phf, phc};
+}
+
+// point t of a radix-R butterfly times W_L^(e t) (conjugate for INV), t = 1 .. R-1
+template <int R, bool INV>
+__device__ __forceinline__ void pk_twiddle(float2 *v, int e, const PkTab &T) {
+    auto app = [&](int q, float2 w) { v[q] = cmul(v[q], INV ? cconj(w) : w); };
+    if constexpr (R == 16) {
+        const float2 w1 = T.w(e), w2 = T.w(2 * e), w4 = T.w(4 * e), w8 = T.w(8 * e);
+        const float2 w3 = cmul(w1, w2), w5 = cmul(w4, w1), w6 = cmul(w4, w2), w7 = cmul(w4, w3);
+        app(1, w1); app(2, w2); app(3, w3); app(4, w4); app(5, w5); app(6, w6); app(7, w7); app(8, w8);
+        app(9, cmul(w8, w1)); app(10, cmul(w8, w2)); app(11, cmul(w8, w3)); app(12, cmul(w8, w4));
+        app(13, cmul(w8, w5)); app(14, cmul(w8, w6)); app(15, cmul(w8, w7));
+    } else if constexpr (R == 8) {
+        const float2 w1 = T.w(e), w2 = T.w(2 * e), w4 = T.w(4 * e), w3 = cmul(w1, w2);
+        app(1, w1); app(2, w2); app(3, w3); app(4, w4);
+        app(5, cmul(w4, w1)); app(6, cmul(w4, w2)); app(7, cmul(w4, w3));
+    } else if constexpr (R == 4) {
+        const float2 w1 = T.w(e), w2 = T.w(2 * e);
+        app(1, w1); app(2, w2); app(3, cmul(w1, w2));
+    } else {
+        app(1, T.w(e));
+    }
+}
+
+// One Stockham pass (see the file comment).  `ld(i)` / `st(i, v)` read and write point i of the
+// pass's input and output (shared or global memory).  The barrier between all loads and all
+// stores makes the in-place update over one shared buffer safe.
+template <int LOGL, int P, bool INV, class Ld, class St>
+__device__ __forceinline__ void pk_pass(const PkTab &T, Ld &&ld, St &&st) {
+    using C = PkCfg<LOGL>;
+    constexpr int L = C::L, NT = C::NT, R = PkPass<LOGL, P>::R, NS = PkPass<LOGL, P>::NS, G = 16 / R;
+    float2 x[16];
+#pragma unroll
+    for (int u = 0; u < G; ++u) {
+        const int b = threadIdx.x + u * NT;
+#pragma unroll
+        for (int t = 0; t < R; ++t) x[u * R + t] = ld(b + t * (L / R));
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < G; ++u) {
+        const int b = threadIdx.x + u * NT;
+        const int j = b & (NS - 1);
+        float2 *v = x + u * R;
+        if constexpr (NS > 1) pk_twiddle<R, INV>(v, j * (L / (NS * R)), T);
+        dftR<R, INV>(v);
+        const int base = (b - j) * R + j;
+#pragma unroll
+        for (int q = 0; q < R; ++q) st(base + q * NS, v[q]);
+    }
+}
+
+// passes P .. NPASS-1; pass 0 reads through ld0, the last pass writes through stl, the others
+// go through the shared buffer
+template <int LOGL, bool INV, int P, class Ld0, class StL>
+__device__ __forceinline__ void pk_run(float2 *buf, const PkTab &T, Ld0 &&ld0, StL &&stl) {
+    constexpr int NP = PkCfg<LOGL>::NPASS;
+    auto lds = [&](int i) -> float2 { return buf[pk_pad(i)]; };
+    auto sts = [&](int i, float2 v) { buf[pk_pad(i)] = v; };
+    if constexpr (P == NP - 1) {
+        pk_pass<LOGL, P, INV>(T, lds, stl);
+    } else {
+        if constexpr (P == 0)
+            pk_pass<LOGL, P, INV>(T, ld0, sts);
+        else
+            pk_pass<LOGL, P, INV>(T, lds, sts);
+        __syncthreads();
+        pk_run<LOGL, INV, P + 1>(buf, T, ld0, stl);
+    }
+}
+
+// phi0 / pi * n as the integer s mod 2n (the host admitted only pairs where it is an integer)
+__device__ __forceinline__ int pk_shift(double phi0_pi, int n) {
+    long long s = llrint(phi0_pi * (double)n) % (2LL * n);
+    return (int)(s < 0 ? s + 2LL * n : s);
+}
+
+__device__ __forceinline__ float2 f4lo(float4 v) { return make_float2(v.x, v.y); }
+__device__ __forceinline__ float2 f4hi(float4 v) { return make_float2(v.z, v.w); }
+
+// x mod m for 0 <= x < 2^31 and 256 <= m < 2^16: the float quotient estimate is off by at most
+// one either way (relative error 2^-23 of a quotient below 2^23 / 256), one correction each way
+struct PkMod {
+    int m;
+    float inv;
+    __device__ __forceinline__ int operator()(int x) const {
+        const int q = (int)((float)x * inv);
+        int r = x - q * m;
+        r += r < 0 ? m : 0;
+        r -= r >= m ? m : 0;
+        return r;
+    }
+};
+
+// ------------------------------------------------------------------------------ synthesis
+// G[map][m][pair][side] (FP32 complex; one float4 = (north, south) per (m, pair)) -> the two
+// rings of each pair.  c_m = 1 for m = 0 and `dbl` (2: real-field synthesis, 1: adjoint of the
+// weighted analysis) for m > 0; apply_w multiplies ring r by scale 2 pi w_r / n (no 2 pi with
+// HB_F_NO2PI).  BLU: n is not a power of two and L is its Bluestein length.
+template <int LOGL, bool BLU>
+__global__ void __launch_bounds__(PkCfg<LOGL>::NT, PkCfg<LOGL>::MINB)
+    ring_pair_synthesis_kernel(GeomDev g, const int32_t *__restrict__ pairs, const float4 *__restrict__ Gm,
+                               int64_t gm_stride4, int mmax, float *__restrict__ maps, int64_t map_stride,
+                               const double *__restrict__ w, int apply_w, int mdouble, int flags) {
+    using C = PkCfg<LOGL>;
+    constexpr int L = C::L, NT = C::NT;
+    extern __shared__ __align__(16) float2 pk_smem[];
+    float2 *buf = pk_smem;
+    const int pair = pairs[blockIdx.x], bm = blockIdx.y;
+    const int rN = g.pair_ring[2 * pair], rS = g.pair_ring[2 * pair + 1];
+    const int n = BLU ? g.nphi[rN] : L;
+    const PkTab T = pk_tables<LOGL>(pk_smem + C::BUF, n);
+    const int s = (flags & HB_F_NOPHASE) ? 0 : pk_shift(g.phi0_pi[rN], n);
+    const int64_t np = g.npairs;
+    const float4 *gin = Gm + bm * gm_stride4 + pair;  // (m, pair) entry at gin[m * np]
+    const float2 *bt = BLU ? g.pkb_bt + g.pkb_bt_ofs[pair] : nullptr;
+    const float dbl = mdouble ? 2.f : 1.f, chalf = 0.5f * dbl;
+    const float sg = (s & 1) ? -1.f : 1.f;
+    const bool hasS = rS >= 0;
+    const PkMod mod2n{2 * n, 1.f / (float)(2 * n)};
+    // phase-table index of exp(i pi s k / n): (s k) mod 2n (s k < 2^31: s < 2n <= 2^15, k <= n)
+    auto pidx = [&](int k) -> int { return BLU ? mod2n(s * k) : ((s * k) & (2 * n - 1)); };
+    __syncthreads();  // tables
+    // Bluestein chirp c_t = exp(-i pi t^2 / n), t < n <= 2^13
+    auto chirp = [&](int t) -> float2 { return cconj(T.ph(mod2n(t * t))); };
+    // spectrum point k of z: stored as is (direct) or as conj(Z[k]) c_k (Bluestein)
+    auto put = [&](int k, float2 z) { buf[pk_pad(k)] = BLU ? cmul(cconj(z), chirp(k)) : z; };
+    // an unpaired ring's south slot is not read as data: zeros keep the imaginary half finite
+    auto ld = [&](int m) -> float4 {
+        float4 v = __ldg(gin + (int64_t)m * np);
+        if (!hasS) v.z = v.w = 0.f;
+        return v;
+    };
+    // class sums S(k) = sum_j (-1)^(s j) c_m / 2 G(k + j n), north and south
+    auto csum = [&](int k, float2 &a, float2 &c) {
+        a = make_float2(0.f, 0.f);
+        c = a;
+        float sj = 1.f;
+        for (int m = k; m <= mmax; m += n) {
+            const float4 v = ld(m);
+            a.x += sj * v.x; a.y += sj * v.y;
+            c.x += sj * v.z; c.y += sj * v.w;
+            if (s & 1) sj = -sj;
+        }
+        a = cscale(a, chalf);
+        c = cscale(c, chalf);
+    };
+    auto put_pair = [&](int k, float2 SkN, float2 SkS, float2 SmN, float2 SmS) {
+        const float2 ph = T.ph(pidx(k));
+        // X(k) = ph (S(k) + (-1)^s conj S(n-k)), X(n-k) = conj(ph) ((-1)^s S(n-k) + conj S(k))
+        const float2 xkN = cmul(ph, make_float2(SkN.x + sg * SmN.x, SkN.y - sg * SmN.y));
+        const float2 xkS = cmul(ph, make_float2(SkS.x + sg * SmS.x, SkS.y - sg * SmS.y));
+        const float2 xcN = cmul(cconj(ph), make_float2(sg * SmN.x + SkN.x, sg * SmN.y - SkN.y));
+        const float2 xcS = cmul(cconj(ph), make_float2(sg * SmS.x + SkS.x, sg * SmS.y - SkS.y));
+        put(k, make_float2(xkN.x - xkS.y, xkN.y + xkS.x));  // X_N + i X_S
+        put(n - k, make_float2(xcN.x - xcS.y, xcN.y + xcS.x));
+    };
+    if (mmax < n) {  // at most one harmonic per residue class (the equatorial belt when mmax < 4 nside)
+#pragma unroll 4
+        for (int k = threadIdx.x + 1; k < n / 2; k += NT) {
+            const float4 a = k <= mmax ? ld(k) : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float4 c = n - k <= mmax ? ld(n - k) : make_float4(0.f, 0.f, 0.f, 0.f);
+            put_pair(k, cscale(f4lo(a), chalf), cscale(f4hi(a), chalf), cscale(f4lo(c), chalf),
+                     cscale(f4hi(c), chalf));
+        }
+    } else {
+        for (int k = threadIdx.x + 1; k < n / 2; k += NT) {
+            float2 SkN, SkS, SmN, SmS;
+            csum(k, SkN, SkS);
+            csum(n - k, SmN, SmS);
+            put_pair(k, SkN, SkS, SmN, SmS);
+        }
+    }
+    if (threadIdx.x == 0) {  // bins 0 and n/2: c_m Re(G(m) exp(i m phi0)) of their classes
+        float aN = 0.f, aS = 0.f, sj = 1.f;
+        for (int m = 0; m <= mmax; m += n) {
+            const float4 v = ld(m);
+            const float c = m == 0 ? 1.f : dbl;
+            aN += sj * c * v.x;
+            aS += sj * c * v.z;
+            if (s & 1) sj = -sj;
+        }
+        put(0, make_float2(aN, aS));
+        float2 hN, hS;
+        csum(n / 2, hN, hS);  // c/2 scaled: times 2 below
+        const float2 ph = T.ph(pidx(n / 2));
+        put(n / 2, make_float2(2.f * (ph.x * hN.x - ph.y * hN.y), 2.f * (ph.x * hS.x - ph.y * hS.y)));
+    }
+    if (BLU)  // zero padding of the convolution
+        for (int k = n + threadIdx.x; k < L; k += NT) buf[pk_pad(k)] = make_float2(0.f, 0.f);
+    __syncthreads();
+    const double sc2 = (flags & HB_F_NO2PI) ? 1.0 : 6.283185307179586476925286766559;
+    const float psN = apply_w ? (float)(sc2 * w[rN] / (double)n) : 1.f;
+    const float psS = (apply_w && hasS) ? (float)(sc2 * w[rS] / (double)n) : 1.f;
+    float *fN = maps + bm * map_stride + g.ofs[rN];
+    float *fS = hasS ? maps + bm * map_stride + g.ofs[rS] : nullptr;
+    auto lds = [&](int i) -> float2 { return buf[pk_pad(i)]; };
+    if constexpr (!BLU) {
+        pk_run<LOGL, true, 0>(buf, T, lds, [&](int i, float2 v) {
+            fN[i] = v.x * psN;
+            if (fS) fS[i] = v.y * psS;
+        });
+    } else {  // forward FFT_L, times the chirp spectrum, inverse FFT_L, times the chirp
+        auto sts = [&](int i, float2 v) { buf[pk_pad(i)] = v; };
+        pk_run<LOGL, false, 0>(buf, T, lds, sts);
+        __syncthreads();
+        for (int i = threadIdx.x; i < L; i += NT) buf[pk_pad(i)] = cmul(buf[pk_pad(i)], __ldg(bt + i));
+        __syncthreads();
+        pk_run<LOGL, true, 0>(buf, T, lds, sts);
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += NT) {
+            const float2 z = cconj(cmul(chirp(i), buf[pk_pad(i)]));
+            fN[i] = z.x * psN;
+            if (fS) fS[i] = z.y * psS;
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------ analysis
+// the two rings of each pair -> F[map][m][pair][side], F(m) = c_m scale exp(-i m phi0) D[m mod n]
+// (conjugated above n/2); scale = 2 pi w_r / n (1 with unit_w; no 2 pi with HB_F_NO2PI);
+// c_m = 2 for m > 0 with mdouble (adjoint of the synthesis), else 1; HB_F_NOFOLD keeps m < n.
+template <int LOGL, bool BLU>
+__global__ void __launch_bounds__(PkCfg<LOGL>::NT, PkCfg<LOGL>::MINB)
+    ring_pair_analysis_kernel(GeomDev g, const int32_t *__restrict__ pairs, const float *__restrict__ maps,
+                              int64_t map_stride, const double *__restrict__ w, float4 *__restrict__ Fm,
+                              int64_t fm_stride4, int mmax, int flags, int unit_w, int mdouble) {
+    using C = PkCfg<LOGL>;
+    constexpr int L = C::L, NT = C::NT;
+    extern __shared__ __align__(16) float2 pk_smem[];
+    float2 *buf = pk_smem;
+    const int pair = pairs[blockIdx.x], bm = blockIdx.y;
+    const int rN = g.pair_ring[2 * pair], rS = g.pair_ring[2 * pair + 1];
+    const int n = BLU ? g.nphi[rN] : L;
+    const PkTab T = pk_tables<LOGL>(pk_smem + C::BUF, n);
+    const int s = (flags & HB_F_NOPHASE) ? 0 : pk_shift(g.phi0_pi[rN], n);
+    const int64_t np = g.npairs;
+    const float *fN = maps + bm * map_stride + g.ofs[rN];
+    const float *fS = rS >= 0 ? maps + bm * map_stride + g.ofs[rS] : nullptr;
+    const float2 *bt = BLU ? g.pkb_bt + g.pkb_bt_ofs[pair] : nullptr;
+    const PkMod mod2n{2 * n, 1.f / (float)(2 * n)};
+    auto pidx = [&](int k) -> int { return BLU ? mod2n(s * k) : ((s * k) & (2 * n - 1)); };
+    auto chirp = [&](int t) -> float2 { return cconj(T.ph(mod2n(t * t))); };
+    auto sts = [&](int i, float2 v) { buf[pk_pad(i)] = v; };
+    auto ring = [&](int i) -> float2 { return make_float2(__ldg(fN + i), fS ? __ldg(fS + i) : 0.f); };
+    __syncthreads();  // tables
+    if constexpr (!BLU) {
+        pk_run<LOGL, false, 0>(buf, T, ring, sts);
+    } else {  // ring times the chirp (zero-padded), FFT_L, times the chirp spectrum, inverse FFT_L
+        auto lds = [&](int i) -> float2 { return buf[pk_pad(i)]; };
+        for (int i = threadIdx.x; i < L; i += NT)
+            buf[pk_pad(i)] = i < n ? cmul(ring(i), chirp(i)) : make_float2(0.f, 0.f);
+        __syncthreads();
+        pk_run<LOGL, false, 0>(buf, T, lds, sts);
+        __syncthreads();
+        for (int i = threadIdx.x; i < L; i += NT) buf[pk_pad(i)] = cmul(buf[pk_pad(i)], __ldg(bt + i));
+        __syncthreads();
+        pk_run<LOGL, true, 0>(buf, T, lds, sts);
+    }
+    __syncthreads();
+    auto Zf = [&](int k) -> float2 { return BLU ? cmul(chirp(k), buf[pk_pad(k)]) : buf[pk_pad(k)]; };
+    const double sc2 = (flags & HB_F_NO2PI) ? 1.0 : 6.283185307179586476925286766559;
+    const float scN = unit_w ? 1.f : (float)(sc2 * w[rN] / (double)n);
+    const float scS = rS < 0 ? 0.f : (unit_w ? 1.f : (float)(sc2 * w[rS] / (double)n));
+    const int mlim = (flags & HB_F_NOFOLD) ? min(mmax, n - 1) : mmax;
+    float4 *out = Fm + bm * fm_stride4 + pair;
+    for (int k = threadIdx.x; k <= n / 2; k += NT) {
+        const float2 zk = Zf(k), zc = k == 0 ? zk : Zf(n - k);
+        // D_N = (Z[k] + conj Z[n-k]) / 2, D_S = (Z[k] - conj Z[n-k]) / (2 i)
+        const float2 dN = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y - zc.y));
+        const float2 dS = make_float2(0.5f * (zk.y + zc.y), -0.5f * (zk.x - zc.x));
+        const float2 ph = cconj(T.ph(pidx(k)));
+        const float2 yN = cscale(cmul(ph, dN), scN), yS = cscale(cmul(ph, dS), scS);
+        float sj = 1.f;
+        for (int m = k; m <= mlim; m += n) {  // class k: (-1)^(s j) Y
+            const float c = (mdouble && m > 0) ? 2.f * sj : sj;
+            out[(int64_t)m * np] = make_float4(c * yN.x, c * yN.y, c * yS.x, c * yS.y);
+            if (s & 1) sj = -sj;
+        }
+        if (k > 0 && 2 * k < n) {  // class n - k: (-1)^(s (j + 1)) conj Y
+            sj = (s & 1) ? -1.f : 1.f;
+            for (int m = n - k; m <= mlim; m += n) {
+                const float c = mdouble ? 2.f * sj : sj;
+                out[(int64_t)m * np] = make_float4(c * yN.x, -c * yN.y, c * yS.x, -c * yS.y);
+                if (s & 1) sj = -sj;
+            }
+        }
+    }
+}
+
+// ------------------------------------------------------------------------------ host side
+static int pk_log2(int64_t v) {
+    int lg = 0;
+    while ((int64_t(1) << lg) < v) ++lg;
+    return lg;
+}
+
+// The pairs these kernels take (see the file comment).  *logL: log2 of the transform length;
+// *blu: whether it is a Bluestein pair.
+bool pk_pair_ok(int nphiN, int nphiS, double phi0N, double phi0S, int *logL, bool *blu) {
+    if (nphiN <= 0 || (nphiN & 1)) return false;
+    if (nphiS >= 0 && (nphiS != nphiN || phi0S != phi0N)) return false;
+    const double s = phi0N * (double)nphiN;  // phi0 / pi * n
+    if (std::fabs(s - std::nearbyint(s)) > 1e-9) return false;
+    const bool p2 = (nphiN & (nphiN - 1)) == 0;
+    const int lg = p2 ? pk_log2(nphiN) : pk_log2(2 * (int64_t)nphiN - 1);
+    if (lg < PK_MIN_LOG || lg > PK_MAX_LOG) return false;
+    *logL = lg;
+    *blu = !p2;
+    return true;
+}
+
+template <int LOGL, bool BLU> static int pk_prepare() {
+    static bool done = false;
+    if (!done) {
+        HB_CUDA_TRY(cudaFuncSetAttribute(ring_pair_synthesis_kernel<LOGL, BLU>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, PkCfg<LOGL>::SMEM));
+        HB_CUDA_TRY(cudaFuncSetAttribute(ring_pair_analysis_kernel<LOGL, BLU>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, PkCfg<LOGL>::SMEM));
+        done = true;
+    }
+    return HB_OK;
+}
+
+struct PkSynArgs {
+    int nmaps;
+    const float2 *Gm;
+    int mmax;
+    float *maps;
+    int64_t map_stride;
+    const double *w;
+    bool apply_w, mdouble;
+    int flags;
+};
+struct PkAnaArgs {
+    int nmaps;
+    const float *maps;
+    int64_t map_stride;
+    const double *w;
+    float2 *Fm;
+    int mmax, flags;
+    bool unit_w, mdouble;
+};
+
+template <int LOGL, bool BLU>
+static int pk_syn_one(const GeomDev &g, const int32_t *pairs, int64_t cnt, const PkSynArgs &a, cudaStream_t st) {
+    int rc = pk_prepare<LOGL, BLU>();
+    if (rc) return rc;
+    const int64_t gm4 = (int64_t)(a.mmax + 1) * g.npairs;
+    ring_pair_synthesis_kernel<LOGL, BLU>
+        <<<dim3((unsigned)cnt, (unsigned)a.nmaps), PkCfg<LOGL>::NT, PkCfg<LOGL>::SMEM, st>>>(
+            g, pairs, reinterpret_cast<const float4 *>(a.Gm), gm4, a.mmax, a.maps, a.map_stride, a.w,
+            a.apply_w ? 1 : 0, a.mdouble ? 1 : 0, a.flags);
+    HB_CHECK_LAUNCH();
+    return HB_OK;
+}
+
+template <int LOGL, bool BLU>
+static int pk_ana_one(const GeomDev &g, const int32_t *pairs, int64_t cnt, const PkAnaArgs &a, cudaStream_t st) {
+    int rc = pk_prepare<LOGL, BLU>();
+    if (rc) return rc;
+    const int64_t fm4 = (int64_t)(a.mmax + 1) * g.npairs;
+    ring_pair_analysis_kernel<LOGL, BLU>
+        <<<dim3((unsigned)cnt, (unsigned)a.nmaps), PkCfg<LOGL>::NT, PkCfg<LOGL>::SMEM, st>>>(
+            g, pairs, a.maps, a.map_stride, a.w, reinterpret_cast<float4 *>(a.Fm), fm4, a.mmax, a.flags,
+            a.unit_w ? 1 : 0, a.mdouble ? 1 : 0);
+    HB_CHECK_LAUNCH();
+    return HB_OK;
+}
+
+template <bool BLU, class A>
+static int pk_dispatch(const GeomDev &g, int logL, const int32_t *pp, int64_t cnt, const A &a, cudaStream_t st) {
+    constexpr bool SYN = std::is_same<A, PkSynArgs>::value;
+    switch (logL) {
+#define HB_PK_CASE(LG) \
+    case LG:           \
+        if constexpr (SYN) return pk_syn_one<LG, BLU>(g, pp, cnt, a, st); else return pk_ana_one<LG, BLU>(g, pp, cnt, a, st);
+        HB_PK_CASE(9) HB_PK_CASE(10) HB_PK_CASE(11) HB_PK_CASE(12) HB_PK_CASE(13) HB_PK_CASE(14)
+#undef HB_PK_CASE
+        default:
+            return fail(HB_ERR_UNSUPPORTED, "pair-packed ring FFT: unsupported length class");
+    }
+}
+
+template <class A> static int pk_all(const GeomDev &g, const A &a, cudaStream_t st) {
+    for (int c = 0; c < g.pk_n_cls; ++c) {
+        const int64_t first = g.pk_first[c], cnt = g.pk_first[c + 1] - first;
+        if (cnt <= 0) continue;
+        const int lg = g.pk_logn[c] & 0xff;
+        const bool blu = (g.pk_logn[c] >> 8) & 1;
+        int rc = blu ? pk_dispatch<true>(g, lg, g.pk_pairs + first, cnt, a, st)
+                     : pk_dispatch<false>(g, lg, g.pk_pairs + first, cnt, a, st);
+        if (rc) return rc;
+    }
+    return HB_OK;
+}
+
+int launch_pk_synthesis(const GeomDev &g, int nmaps, const float2 *Gm, int mmax, float *maps, int64_t map_stride,
+                        const double *w, bool apply_w, bool mdouble, int flags, cudaStream_t st) {
+    return pk_all(g, PkSynArgs{nmaps, Gm, mmax, maps, map_stride, w, apply_w, mdouble, flags}, st);
+}
+
+int launch_pk_analysis(const GeomDev &g, int nmaps, const float *maps, int64_t map_stride, const double *w,
+                       float2 *Fm, int mmax, int flags, bool unit_w, bool mdouble, cudaStream_t st) {
+    return pk_all(g, PkAnaArgs{nmaps, maps, map_stride, w, Fm, mmax, flags, unit_w, mdouble}, st);
+}
+
+}  // namespace hb

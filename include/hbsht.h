@@ -257,6 +257,17 @@ HB_API int hb_ring_synthesis(const hb_plan *p, int precision, int nmaps, const v
                              hb_stream_t stream);
 HB_API int hb_legendre_analysis(const hb_plan *p, int precision, int nmaps, const void *F, void *alm,
                                 hb_stream_t stream);
+/* The Legendre stages restricted to a list of orders, for a transform split over several GPUs by
+ * m (each rank transforms its own orders after the all-to-all exchange of the ring-FFT output).
+ * mlist: device array of nm orders (an order outside [0, mmax] is skipped); F / G hold one row
+ * [npairs][2] per listed order, in list order; alm is the full healpy-layout array of which only
+ * the listed orders' entries are written (the analysis may clear the others).  The reference
+ * has no multi-GPU path; these split sht_raw.py:46-56 (analysis) and isht.py:11-24 (synthesis)
+ * by order. */
+HB_API int hb_legendre_analysis_ms(const hb_plan *p, int precision, int nmaps, int nm, const int32_t *mlist,
+                                   const void *F, void *alm, hb_stream_t stream);
+HB_API int hb_legendre_synthesis_ms(const hb_plan *p, int precision, int nmaps, int nm, const int32_t *mlist,
+                                    const void *alm, void *G, hb_stream_t stream);
 HB_API int hb_legendre_synthesis(const hb_plan *p, int precision, int nmaps, const void *alm, void *G,
                                  hb_stream_t stream);
 

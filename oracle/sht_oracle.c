@@ -257,12 +257,12 @@ void orc_legendre_synthesis_ms(int lmax, int nms, const int *ms, int64_t nr, con
         double *A = (double *)calloc((size_t)lmax + 2, sizeof(double));
         double *B = (double *)calloc((size_t)lmax + 2, sizeof(double));
         double *lam = (double *)malloc(sizeof(double) * ((size_t)lmax + 1));
-#pragma omp for schedule(dynamic, 1) collapse(2)
+#pragma omp for schedule(dynamic, 1)
         for (int j = 0; j < nms; ++j) {
+            const int m = ms[j];
+            const double *aj = a + 2 * (size_t)j * ((size_t)lmax + 1);
+            scalar_coefs(lmax, m, A, B);
             for (int64_t r = 0; r < nr; ++r) {
-                const int m = ms[j];
-                const double *aj = a + 2 * (size_t)j * ((size_t)lmax + 1);
-                scalar_coefs(lmax, m, A, B);
                 scalar_lambda_point(lmax, m, x[r], ls[r], lc[m], A, B, lam);
                 double gr = 0.0, gi = 0.0;
                 for (int l = m; l <= lmax; ++l) {
