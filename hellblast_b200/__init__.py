@@ -19,6 +19,9 @@ from . import hp_compat  # noqa: F401
 from . import autograd  # noqa: F401
 from . import batched  # noqa: F401
 from . import smoothing  # noqa: F401
+from . import synfast  # noqa: F401
+from . import distributed  # noqa: F401
+from . import pixelfunc  # noqa: F401
 
 map2alm = map2alm_gpu
 alm2map = alm2map_gpu
@@ -28,5 +31,5 @@ __all__ = [
     "map2alm_gpu", "alm2map_gpu", "anafast_ring", "map2alm", "alm2map", "anafast",
     "almxfl", "alm2cl", "synalm", "alm_index", "alm_size", "getlmax", "healpy_to_ref", "ref_to_healpy",
     "HealpixRingTables", "map2alm_spin_gpu", "eb_from_qu_gpu", "qu_from_eb_gpu", "hp_compat", "autograd",
-    "batched", "smoothing",
+    "batched", "smoothing", "synfast", "distributed", "pixelfunc",
 ]

@@ -25,6 +25,8 @@ HB_WEIGHTS_UNIFORM = 1
 HB_F_NOPHASE = 1
 HB_F_NOFOLD = 2
 HB_F_NO2PI = 4
+HB_PIX_NEST = 1
+HB_PIX_REFERENCE = 2
 
 _lock = threading.Lock()
 _lib = None
@@ -56,6 +58,11 @@ SIGNATURES = {
     "hb_legendre_analysis": (i32, [vp, i32, i32, vp, vp, vp]),
     "hb_legendre_synthesis": (i32, [vp, i32, i32, vp, vp, vp]),
     "hb_legendre_analysis_ms": (i32, [vp, i32, i32, i32, vp, vp, vp, vp]),
+    "hb_ring2nest": (i32, [i64, i64, vp, vp, vp, vp]),
+    "hb_nest2ring": (i32, [i64, i64, vp, vp, vp, vp]),
+    "hb_pix2ang": (i32, [i64, i32, vp, i64, vp, vp, vp, vp, vp]),
+    "hb_ang2pix": (i32, [i64, i32, vp, vp, i64, vp, vp, vp, vp, vp]),
+    "hb_reorder": (i32, [i64, i32, i32, i32, vp, vp, vp]),
     "hb_legendre_synthesis_ms": (i32, [vp, i32, i32, i32, vp, vp, vp, vp]),
     "hb_probe_fp32": (i32, [i32, i32, i32, vp, vp]),
     "hb_batched_plan_create": (i32, [ctypes.POINTER(vp), ctypes.POINTER(i32), i32, i32, ctypes.POINTER(vp)]),

@@ -271,6 +271,29 @@ HB_API int hb_legendre_synthesis_ms(const hb_plan *p, int precision, int nmaps, 
 HB_API int hb_legendre_synthesis(const hb_plan *p, int precision, int nmaps, const void *alm, void *G,
                                  hb_stream_t stream);
 
+/* HEALPix pixel indexing (Gorski et al. 2005): every array is device memory, n points; bad is one
+ * device int that a kernel sets to 1 when an input is out of range (that output becomes -1 /
+ * NaN).  nside: a power of 2.
+ *   hb_ring2nest / hb_nest2ring: index conversion (replace order_convert.py:8-34, which goes
+ *     through angles; Ring2NestLUT in nested.py:19-41 needs healpy);
+ *   hb_pix2ang: pixel centres; HB_PIX_NEST for NESTED input (replaces nested_pix2ang.cu:16-85),
+ *     else RING (coords_ring.cu:30-54); HB_PIX_REFERENCE (RING only) uses the reference's phi0
+ *     table phi0_ref (nr entries, from hb_ring_tables with HB_PHI0_REFERENCE) and its wrap;
+ *   hb_ang2pix: the pixel holding (theta, phi): NESTED (what nested_gpu.cu:27-95 sets out to do)
+ *     or RING; HB_PIX_REFERENCE (RING only) reproduces coords_ring.py:18-24 + coords_ring.cu:9-29
+ *     (ring from the z_edges table, nr + 1 entries, then the nearest phi centre);
+ *   hb_reorder: map reordering RING -> NESTED (to_nest = 1) or back, nmaps maps of 12 nside^2
+ *     float (precision 32) or double (64) values, out of place. */
+enum { HB_PIX_NEST = 1, HB_PIX_REFERENCE = 2 };
+HB_API int hb_ring2nest(int64_t nside, int64_t n, const int64_t *ring, int64_t *nest, int *bad, hb_stream_t stream);
+HB_API int hb_nest2ring(int64_t nside, int64_t n, const int64_t *nest, int64_t *ring, int *bad, hb_stream_t stream);
+HB_API int hb_pix2ang(int64_t nside, int flags, const double *phi0_ref, int64_t n, const int64_t *pix, double *theta,
+                      double *phi, int *bad, hb_stream_t stream);
+HB_API int hb_ang2pix(int64_t nside, int flags, const double *z_edges, const double *phi0_ref, int64_t n,
+                      const double *theta, const double *phi, int64_t *pix, int *bad, hb_stream_t stream);
+HB_API int hb_reorder(int64_t nside, int to_nest, int precision, int nmaps, const void *in, void *out,
+                      hb_stream_t stream);
+
 /* Diagnostics (no reference counterpart): FP32 FMA throughput probe, blocks*threads threads
  * each running iters*8 FMAs; out holds blocks*threads floats.  Used by bench.py to measure the
  * FP32-pipe roofline on the running GPU. */

@@ -10,5 +10,8 @@ using std::max; using std::min; using std::abs; using std::lgamma; using std::po
 #define __device__
 #define __forceinline__ inline
 #define __restrict__
+/* block-shared tables become function statics (filled by emulated threads before use) */
+#define __shared__ static
+#define __syncthreads() ((void)0)
 struct hb_dim3 { long long x, y, z; };
 extern hb_dim3 blockIdx, threadIdx, blockDim, gridDim;

@@ -513,3 +513,190 @@ void orc_alm2cl(int lmax, int mmax, const double *alm1, const double *alm2, doub
         cl[l] = acc / (2.0 * l + 1.0);
     }
 }
+
+/* ------------------------------------------------------------------ pixel indexing */
+/* HEALPix pixelisation (Gorski et al. 2005, ApJ 622, 759, sections 4-5): 12 base faces, face f
+ * with corner ring jrll[f] * nside and corner longitude index jpll[f]; NESTED index
+ * f nside^2 + (ix, iy) bit-interleaved (ix in the even bits); RING index counted ring by ring
+ * from the north pole.  Restated for the parity tests of the reference's coordinate kernels
+ * (coords_ring.cu:9-54, nested_gpu.cu:27-95, nested_pix2ang.cu:16-85, order_convert.py:8-34). */
+static const int ORC_JRLL[12] = {2, 2, 2, 2, 3, 3, 3, 3, 4, 4, 4, 4};
+static const int ORC_JPLL[12] = {1, 3, 5, 7, 0, 2, 4, 6, 1, 3, 5, 7};
+
+static int64_t orc_spread(int64_t v) { /* bit i of v -> bit 2i */
+    int64_t r = 0;
+    for (int b = 0; b < 31; ++b) r |= ((v >> b) & 1LL) << (2 * b);
+    return r;
+}
+static int64_t orc_compress(int64_t v) { /* bit 2i of v -> bit i */
+    int64_t r = 0;
+    for (int b = 0; b < 31; ++b) r |= ((v >> (2 * b)) & 1LL) << b;
+    return r;
+}
+static int64_t orc_isqrt(int64_t v) {
+    int64_t r = (int64_t)sqrt((double)v);
+    while (r * r > v) --r;
+    while ((r + 1) * (r + 1) <= v) ++r;
+    return r;
+}
+
+static void orc_nest2xyf(int64_t nside, int64_t p, int64_t *ix, int64_t *iy, int *f) {
+    int64_t nn = nside * nside;
+    *f = (int)(p / nn);
+    p -= (int64_t)(*f) * nn;
+    *ix = orc_compress(p);
+    *iy = orc_compress(p >> 1);
+}
+static int64_t orc_xyf2nest(int64_t nside, int64_t ix, int64_t iy, int f) {
+    return (int64_t)f * nside * nside + orc_spread(ix) + 2 * orc_spread(iy);
+}
+static int64_t orc_xyf2ring(int64_t nside, int64_t ix, int64_t iy, int f) {
+    int64_t nl4 = 4 * nside, ncap = 2 * nside * (nside - 1), npix = 12 * nside * nside;
+    int64_t jr = (int64_t)ORC_JRLL[f] * nside - ix - iy - 1, nr, nbefore;
+    int kshift;
+    if (jr < nside) { nr = jr; nbefore = 2 * nr * (nr - 1); kshift = 0; }
+    else if (jr > 3 * nside) { nr = nl4 - jr; nbefore = npix - 2 * (nr + 1) * nr; kshift = 0; }
+    else { nr = nside; nbefore = ncap + (jr - nside) * nl4; kshift = (int)((jr - nside) & 1); }
+    int64_t jp = ((int64_t)ORC_JPLL[f] * nr + ix - iy + 1 + kshift) / 2;
+    if (jp > 4 * nr) jp -= 4 * nr;
+    else if (jp < 1) jp += 4 * nr;
+    return nbefore + jp - 1;
+}
+static void orc_ring2xyf(int64_t nside, int64_t p, int64_t *ix, int64_t *iy, int *f) {
+    int64_t nl2 = 2 * nside, ncap = 2 * nside * (nside - 1), npix = 12 * nside * nside;
+    int64_t iring, iphi, nr;
+    int kshift, face;
+    if (p < ncap) {
+        iring = (1 + orc_isqrt(1 + 2 * p)) >> 1;
+        iphi = p + 1 - 2 * iring * (iring - 1);
+        kshift = 0; nr = iring;
+        face = (int)((iphi - 1) / nr);
+    } else if (p < npix - ncap) {
+        int64_t ip = p - ncap, tmp = ip / (4 * nside);
+        iring = tmp + nside;
+        iphi = ip - tmp * 4 * nside + 1;
+        kshift = (int)((iring + nside) & 1);
+        nr = nside;
+        int64_t ire = tmp + 1, irm = nl2 + 2 - ire;
+        int64_t ifm = (iphi - ire / 2 + nside - 1) / nside, ifp = (iphi - irm / 2 + nside - 1) / nside;
+        face = (ifp == ifm) ? (int)(ifp | 4) : ((ifp < ifm) ? (int)ifp : (int)(ifm + 8));
+    } else {
+        int64_t ip = npix - p;
+        iring = (1 + orc_isqrt(2 * ip - 1)) >> 1;
+        iphi = 4 * iring + 1 - (ip - 2 * iring * (iring - 1));
+        kshift = 0; nr = iring;
+        iring = 2 * nl2 - iring;
+        face = 8 + (int)((iphi - 1) / nr);
+    }
+    int64_t irt = iring - (int64_t)ORC_JRLL[face] * nside + 1;
+    int64_t ipt = 2 * iphi - (int64_t)ORC_JPLL[face] * nr - kshift - 1;
+    if (ipt >= nl2) ipt -= 8 * nside;
+    *ix = (ipt - irt) >> 1;
+    *iy = (-ipt - irt) >> 1;
+    *f = face;
+}
+
+/* RING <-> NESTED index of n pixels */
+void orc_ring2nest(int64_t nside, int64_t n, const int64_t *in, int64_t *out) {
+#pragma omp parallel for
+    for (int64_t i = 0; i < n; ++i) {
+        int64_t ix, iy; int f;
+        orc_ring2xyf(nside, in[i], &ix, &iy, &f);
+        out[i] = orc_xyf2nest(nside, ix, iy, f);
+    }
+}
+void orc_nest2ring(int64_t nside, int64_t n, const int64_t *in, int64_t *out) {
+#pragma omp parallel for
+    for (int64_t i = 0; i < n; ++i) {
+        int64_t ix, iy; int f;
+        orc_nest2xyf(nside, in[i], &ix, &iy, &f);
+        out[i] = orc_xyf2ring(nside, ix, iy, f);
+    }
+}
+
+/* pixel centre (z = cos theta, phi) of RING pixel p */
+static void orc_ring_center(int64_t nside, int64_t p, double *z, double *phi) {
+    const double pi = 3.141592653589793238462643383279502884;
+    int64_t ncap = 2 * nside * (nside - 1), npix = 12 * nside * nside;
+    double fact2 = 4.0 / (double)npix;
+    if (p < ncap) {
+        int64_t iring = (1 + orc_isqrt(1 + 2 * p)) >> 1, iphi = p + 1 - 2 * iring * (iring - 1);
+        *z = 1.0 - (double)(iring * iring) * fact2;
+        *phi = ((double)iphi - 0.5) * (pi / (2.0 * (double)iring));
+    } else if (p < npix - ncap) {
+        int64_t ip = p - ncap, tmp = ip / (4 * nside), iring = tmp + nside, iphi = ip - tmp * 4 * nside + 1;
+        double fodd = ((iring + nside) & 1) ? 1.0 : 0.5;
+        *z = (double)(2 * nside - iring) * (2.0 / (3.0 * (double)nside));
+        *phi = ((double)iphi - fodd) * (pi / (2.0 * (double)nside));
+    } else {
+        int64_t ip = npix - p, iring = (1 + orc_isqrt(2 * ip - 1)) >> 1;
+        int64_t iphi = 4 * iring + 1 - (ip - 2 * iring * (iring - 1));
+        *z = -1.0 + (double)(iring * iring) * fact2;
+        *phi = ((double)iphi - 0.5) * (pi / (2.0 * (double)iring));
+    }
+}
+/* NESTED or RING pixel centres: theta, phi */
+void orc_pix2ang(int64_t nside, int nest, int64_t n, const int64_t *pix, double *theta, double *phi) {
+#pragma omp parallel for
+    for (int64_t i = 0; i < n; ++i) {
+        int64_t p = pix[i];
+        if (nest) {
+            int64_t ix, iy; int f;
+            orc_nest2xyf(nside, p, &ix, &iy, &f);
+            p = orc_xyf2ring(nside, ix, iy, f);
+        }
+        double z;
+        orc_ring_center(nside, p, &z, &phi[i]);
+        theta[i] = acos(z);
+    }
+}
+
+/* (z, phi) -> RING / NESTED pixel containing it */
+static void orc_zphi2xyf_or_ring(int64_t nside, double z, double phi, int nest, int64_t *out) {
+    const double pi = 3.141592653589793238462643383279502884;
+    double za = fabs(z);
+    double tt = fmod(phi, 2.0 * pi);
+    if (tt < 0.0) tt += 2.0 * pi;
+    tt *= 2.0 / pi; /* [0, 4) */
+    if (tt >= 4.0) tt = 0.0;
+    int64_t ncap = 2 * nside * (nside - 1), npix = 12 * nside * nside;
+    if (!nest) {
+        if (za <= 2.0 / 3.0) {
+            double t1 = (double)nside * (0.5 + tt), t2 = (double)nside * z * 0.75;
+            int64_t jp = (int64_t)(t1 - t2), jm = (int64_t)(t1 + t2);
+            int64_t ir = nside + 1 + jp - jm, kshift = 1 - (ir & 1);
+            int64_t ip = (jp + jm - nside + kshift + 1) / 2;
+            ip %= 4 * nside; if (ip < 0) ip += 4 * nside;
+            *out = ncap + (ir - 1) * 4 * nside + ip;
+        } else {
+            double tp = tt - (double)(int64_t)tt, tmp = (double)nside * sqrt(3.0 * (1.0 - za));
+            int64_t jp = (int64_t)(tp * tmp), jm = (int64_t)((1.0 - tp) * tmp);
+            int64_t ir = jp + jm + 1, ip = (int64_t)(tt * (double)ir);
+            ip %= 4 * ir; if (ip < 0) ip += 4 * ir;
+            *out = (z > 0.0) ? 2 * ir * (ir - 1) + ip : npix - 2 * ir * (ir + 1) + ip;
+        }
+        return;
+    }
+    int64_t ix, iy; int face;
+    if (za <= 2.0 / 3.0) {
+        double t1 = (double)nside * (0.5 + tt), t2 = (double)nside * z * 0.75;
+        int64_t jp = (int64_t)(t1 - t2), jm = (int64_t)(t1 + t2);
+        int64_t ifp = jp / nside, ifm = jm / nside;
+        face = (ifp == ifm) ? (int)(ifp | 4) : ((ifp < ifm) ? (int)ifp : (int)(ifm + 8));
+        ix = jm & (nside - 1);
+        iy = nside - (jp & (nside - 1)) - 1;
+    } else {
+        int ntt = (int)tt; if (ntt >= 4) ntt = 3;
+        double tp = tt - (double)ntt, tmp = (double)nside * sqrt(3.0 * (1.0 - za));
+        int64_t jp = (int64_t)(tp * tmp), jm = (int64_t)((1.0 - tp) * tmp);
+        if (jp > nside - 1) jp = nside - 1;
+        if (jm > nside - 1) jm = nside - 1;
+        if (z >= 0.0) { face = ntt; ix = nside - jm - 1; iy = nside - jp - 1; }
+        else { face = ntt + 8; ix = jp; iy = jm; }
+    }
+    *out = orc_xyf2nest(nside, ix, iy, face);
+}
+void orc_ang2pix(int64_t nside, int nest, int64_t n, const double *theta, const double *phi, int64_t *pix) {
+#pragma omp parallel for
+    for (int64_t i = 0; i < n; ++i) orc_zphi2xyf_or_ring(nside, cos(theta[i]), phi[i], nest, &pix[i]);
+}

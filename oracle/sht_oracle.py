@@ -56,6 +56,12 @@ def _lib():
                                                   ctypes.c_int64, D, D, D, D]
         for f in (lib.orc_legendre_analysis_ms, lib.orc_legendre_synthesis_ms):
             f.restype = None
+        lib.orc_ring2nest.argtypes = [ctypes.c_int64, ctypes.c_int64, I64, I64]
+        lib.orc_nest2ring.argtypes = [ctypes.c_int64, ctypes.c_int64, I64, I64]
+        lib.orc_pix2ang.argtypes = [ctypes.c_int64, ctypes.c_int, ctypes.c_int64, I64, D, D]
+        lib.orc_ang2pix.argtypes = [ctypes.c_int64, ctypes.c_int, ctypes.c_int64, D, D, I64]
+        for f in (lib.orc_ring2nest, lib.orc_nest2ring, lib.orc_pix2ang, lib.orc_ang2pix):
+            f.restype = None
         for f in (lib.orc_ring_tables, lib.orc_lambda_lm, lib.orc_legendre_analysis,
                   lib.orc_legendre_synthesis, lib.orc_spin2_lambda, lib.orc_spin2_analysis,
                   lib.orc_spin2_synthesis, lib.orc_alm2cl, lib.orc_spin2_analysis_ms):
@@ -474,3 +480,66 @@ def synalm(cl, lmax: int | None = None, seed: int = 0) -> np.ndarray:
             ms = np.arange(1, l + 1)
             alm[alm_index(lmax, l, ms)] = re + 1j * im
     return alm
+
+
+def synalm_te_from_normals(cltt, clee, clbb, clte, z1, z2, zb, lmax: int):
+    """The reference's correlated T/E/B draw (synfast_tqu.py:28-67) restated per l, with the unit
+    normals supplied (complex, healpy layout; Re of the m = 0 entries used): per l the Cholesky
+    factor of [[C_TT, C_TE], [C_TE, C_EE]] (:37-43; L21 = 0 when not positive definite),
+    aT = L11 z1, aE = L21 z1 + L22 z2, aB = sqrt(C_BB) zb, the m > 0 components scaled to
+    variance C/2 (:55, :60-64).  Returns (aT, aE, aB) in healpy layout."""
+    n = alm_size(lmax)
+    aT = np.zeros(n, dtype=np.complex128); aE = np.zeros_like(aT); aB = np.zeros_like(aT)
+    for l in range(lmax + 1):
+        Ctt, Cee, Cbb, Cte = float(cltt[l]), float(clee[l]), float(clbb[l]), float(clte[l])
+        if Ctt <= 0 or Cee <= 0 or (Ctt * Cee - Cte * Cte) <= 0:
+            L11, L21, L22 = math.sqrt(max(Ctt, 0.0)), 0.0, math.sqrt(max(Cee, 0.0))
+        else:
+            L11 = math.sqrt(Ctt)
+            L21 = Cte / L11
+            L22 = math.sqrt(Cee - L21 * L21)
+        sb = math.sqrt(max(Cbb, 0.0))
+        for m in range(l + 1):
+            k = alm_index(lmax, l, m)
+            if m == 0:
+                a, b, c = z1[k].real, z2[k].real, zb[k].real
+            else:
+                h = math.sqrt(0.5)
+                a, b, c = h * z1[k], h * z2[k], h * zb[k]
+            aT[k] = L11 * a
+            aE[k] = L21 * a + L22 * b
+            aB[k] = sb * c
+    return aT, aE, aB
+
+
+# ----------------------------------------------------------------------------- pixel indexing
+def _i64(a):
+    return np.ascontiguousarray(np.asarray(a, dtype=np.int64))
+
+
+def ring2nest(nside: int, ipix) -> np.ndarray:
+    """HEALPix RING -> NESTED index (Gorski et al. 2005), the C oracle."""
+    p = _i64(ipix); out = np.empty_like(p)
+    _lib().orc_ring2nest(nside, p.size, p.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                         out.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
+    return out
+
+
+def nest2ring(nside: int, ipix) -> np.ndarray:
+    p = _i64(ipix); out = np.empty_like(p)
+    _lib().orc_nest2ring(nside, p.size, p.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                         out.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
+    return out
+
+
+def pix2ang(nside: int, ipix, nest: bool = False):
+    p = _i64(ipix); th = np.empty(p.size); ph = np.empty(p.size)
+    _lib().orc_pix2ang(nside, int(nest), p.size, p.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)), _p(th), _p(ph))
+    return th, ph
+
+
+def ang2pix(nside: int, theta, phi, nest: bool = False) -> np.ndarray:
+    th = _c(np.asarray(theta, dtype=np.float64)).reshape(-1); ph = _c(np.asarray(phi, dtype=np.float64)).reshape(-1)
+    out = np.empty(th.size, dtype=np.int64)
+    _lib().orc_ang2pix(nside, int(nest), th.size, _p(th), _p(ph), out.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
+    return out

@@ -198,6 +198,76 @@ def spin_case(name, nside, lmax, seed, stock):
     print("wrote", name, {k: getattr(v, "shape", v) for k, v in out.items()})
 
 
+def pixel_case():
+    """The reference's pixel-coordinate drivers (coords_ring.py, nested_pix2ang.py, nested_gpu.py)
+    with their kernels (coords_ring.cu, nested_pix2ang.cu, nested_gpu.cu) run as host code."""
+    U64 = ctypes.POINTER(ctypes.c_ulonglong)
+    I32 = ctypes.POINTER(ctypes.c_int)
+    LLp = ctypes.POINTER(ctypes.c_longlong)
+
+    def arr(x):
+        return np.ascontiguousarray(np.asarray(x))
+
+    def k_ang2pix_ring(grid, block, args):
+        th, ph, ridx, N, rs, nphi, ph0, out = (arr(a) if hasattr(a, "shape") else a for a in args)
+        o = np.zeros(int(N), np.int64)
+        lib.ref_ang2pix_ring_with_rings(th.ctypes.data_as(Dp), ph.ctypes.data_as(Dp), ridx.astype(np.int32).ctypes.data_as(I32),
+                                        int(N), rs.astype(np.int64).ctypes.data_as(LLp),
+                                        nphi.astype(np.int32).ctypes.data_as(I32), ph0.ctypes.data_as(Dp),
+                                        o.ctypes.data_as(LLp))
+        args[7][...] = o
+
+    def k_pix2ang_ring(grid, block, args):
+        ip, N, thc, rs, nphi, ph0, oth, oph = (arr(a) if hasattr(a, "shape") else a for a in args)
+        t = np.zeros(int(N)); f = np.zeros(int(N))
+        lib.ref_pix2ang_ring_batch(ip.astype(np.int64).ctypes.data_as(LLp), int(N), thc.ctypes.data_as(Dp),
+                                   rs.astype(np.int64).ctypes.data_as(LLp), nphi.astype(np.int32).ctypes.data_as(I32),
+                                   ph0.ctypes.data_as(Dp), t.ctypes.data_as(Dp), f.ctypes.data_as(Dp))
+        args[6][...] = t
+        args[7][...] = f
+
+    def k_vec2pix_nest(grid, block, args):
+        th, ph, N, nside, out = args
+        o = np.zeros(int(N), np.uint64)
+        lib.ref_vec2pix_nest_batch(arr(th).ctypes.data_as(Dp), arr(ph).ctypes.data_as(Dp), int(N), int(nside),
+                                   o.ctypes.data_as(U64))
+        out[...] = o
+
+    def k_pix2ang_nest(grid, block, args):
+        ip, N, nside, oth, oph = args
+        t = np.zeros(int(N)); f = np.zeros(int(N))
+        lib.ref_pix2ang_nest_batch(arr(ip).astype(np.uint64).ctypes.data_as(U64), int(N), int(nside),
+                                   t.ctypes.data_as(Dp), f.ctypes.data_as(Dp))
+        oth[...] = t
+        oph[...] = f
+
+    import hellblast.coords_ring as cr
+    import hellblast.nested_gpu as ng
+    import hellblast.nested_pix2ang as npa
+    kern = {"ang2pix_ring_with_rings": k_ang2pix_ring, "pix2ang_ring_batch": k_pix2ang_ring,
+            "vec2pix_nest_batch": k_vec2pix_nest, "pix2ang_nest_batch": k_pix2ang_nest}
+    for mod in (cr, ng, npa):
+        mod._get_fun = lambda src, fun: kern[fun]
+    out = {}
+    rng = np.random.default_rng(11)
+    for nside in (1, 2, 4, 16, 1024):
+        npix = 12 * nside * nside
+        pix = np.arange(npix) if npix <= 3072 else np.sort(rng.choice(npix, 4000, replace=False))
+        th_n, ph_n = npa.pix2ang_nest_gpu(nside, pix)
+        mapper = cr.RingMapperGPU(nside)
+        th_r, ph_r = mapper.pix2ang(pix)
+        u = rng.uniform(-1.0, 1.0, 3000)
+        th = np.arccos(u)
+        ph = rng.uniform(0.0, 2.0 * np.pi, 3000)
+        out.update({f"n{nside}_pix": pix, f"n{nside}_nest_theta": np.asarray(th_n), f"n{nside}_nest_phi": np.asarray(ph_n),
+                    f"n{nside}_ring_theta": np.asarray(th_r), f"n{nside}_ring_phi": np.asarray(ph_r),
+                    f"n{nside}_dir_theta": th, f"n{nside}_dir_phi": ph,
+                    f"n{nside}_ref_ang2pix_ring": np.asarray(mapper.ang2pix(th, ph)),
+                    f"n{nside}_ref_ang2pix_nest": np.asarray(ng.ang2pix_nest_gpu(th, ph, nside))})
+    np.savez_compressed(os.path.join(HERE, "pixel_ref.npz"), **out)
+    print("wrote pixel_ref", len(out))
+
+
 def tables():
     out = {}
     for nside in (1, 2, 4, 8, 16, 32, 64):
@@ -214,6 +284,9 @@ def tables():
 
 
 if __name__ == "__main__":
+    if "--pixel-only" in sys.argv:
+        pixel_case()
+        sys.exit(0)
     # --spin-only: regenerate the spin-2 fixtures alone
     if "--spin-only" not in sys.argv:
         tables()
@@ -224,3 +297,4 @@ if __name__ == "__main__":
     spin_case("spin_stock_nside8_lmax20", 8, 20, seed=5, stock=True)
     spin_case("spin_dexact_nside8_lmax20", 8, 20, seed=6, stock=False)
     spin_case("spin_dexact_nside16_lmax40", 16, 40, seed=7, stock=False)
+    pixel_case()
