@@ -23,6 +23,7 @@ from . import synfast  # noqa: F401
 from . import distributed  # noqa: F401
 from . import pixelfunc  # noqa: F401
 from . import io_fits  # noqa: F401
+from . import rotate  # noqa: F401
 
 map2alm = map2alm_gpu
 alm2map = alm2map_gpu
@@ -32,5 +33,5 @@ __all__ = [
     "map2alm_gpu", "alm2map_gpu", "anafast_ring", "map2alm", "alm2map", "anafast",
     "almxfl", "alm2cl", "synalm", "alm_index", "alm_size", "getlmax", "healpy_to_ref", "ref_to_healpy",
     "HealpixRingTables", "map2alm_spin_gpu", "eb_from_qu_gpu", "qu_from_eb_gpu", "hp_compat", "autograd",
-    "batched", "smoothing", "synfast", "distributed", "pixelfunc", "io_fits",
+    "batched", "smoothing", "synfast", "distributed", "pixelfunc", "io_fits", "rotate",
 ]

@@ -63,6 +63,8 @@ SIGNATURES = {
     "hb_pix2ang": (i32, [i64, i32, vp, i64, vp, vp, vp, vp, vp]),
     "hb_ang2pix": (i32, [i64, i32, vp, vp, i64, vp, vp, vp, vp, vp]),
     "hb_reorder": (i32, [i64, i32, i32, i32, vp, vp, vp]),
+    "hb_wigner_d": (i32, [i32, i32, vp, vp, vp]),
+    "hb_rotate_alm": (i32, [i32, i32, vp, vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, vp]),
     "hb_legendre_synthesis_ms": (i32, [vp, i32, i32, i32, vp, vp, vp, vp]),
     "hb_probe_fp32": (i32, [i32, i32, i32, vp, vp]),
     "hb_batched_plan_create": (i32, [ctypes.POINTER(vp), ctypes.POINTER(i32), i32, i32, ctypes.POINTER(vp)]),

@@ -294,6 +294,17 @@ HB_API int hb_ang2pix(int64_t nside, int flags, const double *z_edges, const dou
 HB_API int hb_reorder(int64_t nside, int to_nest, int precision, int nmaps, const void *in, void *out,
                       hb_stream_t stream);
 
+/* Wigner d and alm rotation (FP64; device arrays).
+ *   hb_wigner_d: d^l_{m m'}(beta_b) for m, m' = -l..l into out[b][m + l][m' + l] (what
+ *     wigner_d_fast.cu:8-52 and wigner_full.py:12-40 compute by the closed-form sum; here by the
+ *     three-term recursion in l, stable to l = 16383);
+ *   hb_rotate_alm: a'_{lm} = sum_m' exp(-i m alpha) d^l_{mm'}(beta) exp(-i m' gamma) a_{lm'}
+ *     (Euler ZYZ, rotate_alm_euler.py:5-14 / wigner_full.py:79-96) for nmaps healpy-layout
+ *     complex128 alm vectors with mmax = lmax, out of place. */
+HB_API int hb_wigner_d(int l, int nbeta, const double *beta, double *out, hb_stream_t stream);
+HB_API int hb_rotate_alm(int lmax, int nmaps, const void *alm_in, void *alm_out, double alpha, double beta,
+                         double gamma, hb_stream_t stream);
+
 /* Diagnostics (no reference counterpart): FP32 FMA throughput probe, blocks*threads threads
  * each running iters*8 FMAs; out holds blocks*threads floats.  Used by bench.py to measure the
  * FP32-pipe roofline on the running GPU. */

@@ -700,3 +700,60 @@ void orc_ang2pix(int64_t nside, int nest, int64_t n, const double *theta, const 
 #pragma omp parallel for
     for (int64_t i = 0; i < n; ++i) orc_zphi2xyf_or_ring(nside, cos(theta[i]), phi[i], nest, &pix[i]);
 }
+
+/* ------------------------------------------------------------------ Wigner d */
+/* d^l_{m,m'}(beta) for m, m' = -l..l into out[(m+l)(2l+1) + m'+l], long double three-term
+ * recursion in l at fixed (m, m') from the edge element at l0 = max(|m|,|m'|)
+ * (d^j_{j,k} = sqrt((2j)!/((j+k)!(j-k)!)) cos(b/2)^{j+k} (-sin(b/2))^{j-k},
+ * d_{a,b} = (-1)^{a-b} d_{b,a} = d_{-b,-a}); beta reduced to [0, pi] first
+ * (d(2pi - b) = (-1)^{m-m'} d(b)).  For the parity tests of the alm rotation
+ * (rotate_alm_euler.py:5-14, wigner_full.py:12-96). */
+void orc_wigner_d(int l, double beta, double *out) {
+    const long double pi = 3.141592653589793238462643383279502884L;
+    long double b = fmodl((long double)beta, 2.0L * pi);
+    if (b < 0) b += 2.0L * pi;
+    int flip = b > pi;
+    if (flip) b = 2.0L * pi - b;
+    long double c = cosl(0.5L * b), s = sinl(0.5L * b), x = cosl(b);
+    int dim = 2 * l + 1;
+    for (int m = -l; m <= l; ++m) {
+        for (int mp = -l; mp <= l; ++mp) {
+            int j, k, sh;
+            if (abs(m) >= abs(mp)) {
+                if (m >= 0) { j = m; k = mp; sh = 0; }
+                else { j = -m; k = -mp; sh = (mp + j) & 1; }
+            } else {
+                if (mp > 0) { j = mp; k = m; sh = (m - j) & 1; }
+                else { j = -mp; k = -m; sh = 0; }
+            }
+            int l0 = j;
+            /* edge element, log-scaled like the spin-2 starts above */
+            long double L = 0.5L * (lfac2(2 * j) - lfac2(j + k) - lfac2(j - k));
+            int zero = 0;
+            if (j + k > 0) { if (c == 0) zero = 1; else L += (j + k) * log2l(c); }
+            if (j - k > 0) { if (s == 0) zero = 1; else L += (j - k) * log2l(s); }
+            int sign = (((j - k) & 1) ^ sh) ? -1 : 1;
+            long double d1 = 0, d0 = 0;
+            int e = 0;
+            if (!zero) {
+                e = (int)floorl((L + 128.0L) / 256.0L);
+                d1 = exp2l(L - 256.0L * e) * sign;
+            }
+            for (int ll = l0; ll < l; ++ll) {
+                long double v;
+                if (ll == 0) v = x * d1;
+                else {
+                    long double dl = ll, m2 = (long double)m * m, p2 = (long double)mp * mp;
+                    long double R1 = sqrtl(((dl + 1) * (dl + 1) - m2) * ((dl + 1) * (dl + 1) - p2));
+                    long double R0 = sqrtl((dl * dl - m2) * (dl * dl - p2));
+                    v = ((2 * dl + 1) * (dl * (dl + 1) * x - (long double)m * mp) * d1 - (dl + 1) * R0 * d0) / (dl * R1);
+                }
+                d0 = d1; d1 = v;
+                if (e < 0 && fabsl(d1) > 0x1p128L) { d1 = ldexpl(d1, -256); d0 = ldexpl(d0, -256); ++e; }
+            }
+            double v = (e == 0) ? (double)d1 : 0.0;
+            if (flip && ((m - mp) & 1)) v = -v;
+            out[(m + l) * dim + (mp + l)] = v;
+        }
+    }
+}

@@ -62,6 +62,8 @@ def _lib():
         lib.orc_ang2pix.argtypes = [ctypes.c_int64, ctypes.c_int, ctypes.c_int64, D, D, I64]
         for f in (lib.orc_ring2nest, lib.orc_nest2ring, lib.orc_pix2ang, lib.orc_ang2pix):
             f.restype = None
+        lib.orc_wigner_d.argtypes = [ctypes.c_int, ctypes.c_double, D]
+        lib.orc_wigner_d.restype = None
         for f in (lib.orc_ring_tables, lib.orc_lambda_lm, lib.orc_legendre_analysis,
                   lib.orc_legendre_synthesis, lib.orc_spin2_lambda, lib.orc_spin2_analysis,
                   lib.orc_spin2_synthesis, lib.orc_alm2cl, lib.orc_spin2_analysis_ms):
@@ -543,3 +545,38 @@ def ang2pix(nside: int, theta, phi, nest: bool = False) -> np.ndarray:
     out = np.empty(th.size, dtype=np.int64)
     _lib().orc_ang2pix(nside, int(nest), th.size, _p(th), _p(ph), out.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)))
     return out
+
+
+# ----------------------------------------------------------------------------- rotations
+def wigner_d(l: int, beta: float) -> np.ndarray:
+    """d^l_{mm'}(beta), [2l+1, 2l+1] with m, m' = -l..l (the C oracle's long double recursion)."""
+    out = np.zeros((2 * l + 1) * (2 * l + 1))
+    _lib().orc_wigner_d(int(l), float(beta), _p(out))
+    return out.reshape(2 * l + 1, 2 * l + 1)
+
+
+def rotate_alm_euler(alm, lmax: int, alpha: float, beta: float, gamma: float) -> np.ndarray:
+    """a'_{lm} = sum_m' exp(-i m alpha) d^l_{mm'}(beta) exp(-i m' gamma) a_{lm'} (wigner_full.py:79-96,
+    with the textbook d), healpy layout, a_{l,-m} = (-1)^m conj a_{lm}."""
+    a = np.asarray(alm, dtype=np.complex128)
+    out = np.zeros_like(a)
+    for l in range(lmax + 1):
+        m = np.arange(0, l + 1)
+        pos = a[alm_index(lmax, l, m)]
+        full = np.concatenate([((-1.0) ** m[:0:-1]) * np.conj(pos[:0:-1]), pos])  # m' = -l..l
+        mm = np.arange(-l, l + 1)
+        D = np.exp(-1j * mm[:, None] * alpha) * wigner_d(l, beta) * np.exp(-1j * mm[None, :] * gamma)
+        out[alm_index(lmax, l, m)] = (D @ full)[l:]
+    return out
+
+
+def eval_alm(alm, lmax: int, theta, phi) -> np.ndarray:
+    """f(theta, phi) = sum_lm a_lm Y_lm of a real field, at arbitrary points (direct sum)."""
+    th = np.asarray(theta, dtype=np.float64); ph = np.asarray(phi, dtype=np.float64)
+    a = np.asarray(alm, dtype=np.complex128)
+    f = np.zeros(th.size)
+    for m in range(lmax + 1):
+        lam = lambda_lm(lmax, m, np.cos(th), np.sin(th))  # [npts, lmax+1]
+        g = lam[:, m:] @ a[alm_index(lmax, np.arange(m, lmax + 1), m)]
+        f += (1.0 if m == 0 else 2.0) * np.real(g * np.exp(1j * m * ph))
+    return f

@@ -268,6 +268,19 @@ def pixel_case():
     print("wrote pixel_ref", len(out))
 
 
+def rotation_case():
+    """The reference's z rotation of ref-layout alm (rotate_alm.py:5-19), its one rotation that is
+    right as shipped (its Euler path's closed-form d is not a rotation matrix)."""
+    import hellblast.rotate_alm as ra
+    lmax = 20
+    cl = 1.0 / (np.arange(lmax + 1) + 2.0) ** 2
+    alm = O.synalm(cl, seed=9)
+    ref = O.healpy_to_ref(alm, lmax)
+    out = np.asarray(ra.rotate_alm_z(ref.view(cp.GArr), 0.7310, lmax))
+    np.savez_compressed(os.path.join(HERE, "rotate_z_ref.npz"), lmax=lmax, alpha=0.7310, alm=alm, ref_out=out)
+    print("wrote rotate_z_ref")
+
+
 def tables():
     out = {}
     for nside in (1, 2, 4, 8, 16, 32, 64):
@@ -286,6 +299,9 @@ def tables():
 if __name__ == "__main__":
     if "--pixel-only" in sys.argv:
         pixel_case()
+        sys.exit(0)
+    if "--rotation-only" in sys.argv:
+        rotation_case()
         sys.exit(0)
     # --spin-only: regenerate the spin-2 fixtures alone
     if "--spin-only" not in sys.argv:
