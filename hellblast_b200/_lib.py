@@ -74,6 +74,8 @@ SIGNATURES = {
     "hb_batched_map2alm": (i32, [vp, vp, vp, vp]),
     "hb_batched_map2alm_fl": (i32, [vp, vp, vp, vp, vp]),
     "hb_batched_status": (i32, [vp, ctypes.POINTER(i32)]),
+    "hb_batched_fault_test": (i32, [vp, ctypes.c_uint64, i32]),
+    "hb_batched_reset_status": (i32, [vp]),
     "hb_batched_profile": (i32, [vp, i32]),
     "hb_batched_stage_ms": (i32, [vp, ctypes.POINTER(ctypes.c_float)]),
     "hb_batched_graph_capture": (i32, [vp, vp, vp, vp]),

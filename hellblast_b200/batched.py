@@ -103,6 +103,14 @@ class BatchedPlan:
         L.call("hb_batched_status", self.handle, ctypes.byref(code))
         return code.value
 
+    def reset_status(self) -> None:
+        L.call("hb_batched_reset_status", self.handle)
+
+    def fault_test(self, wait_s: float = 2.0, withhold_copy: bool = False) -> None:
+        """Failure-detection test hook: bound of every tensor-core pipeline wait, and whether the
+        synthesis loader of CTA 0 withholds its first batch-tile copy (hb_batched_fault_test)."""
+        L.call("hb_batched_fault_test", self.handle, int(wait_s * 1e9), 1 if withhold_copy else 0)
+
     def __del__(self):  # pragma: no cover
         try:
             if self.handle:

@@ -18,7 +18,7 @@
 //   restarts at the block from the plan's FP64-computed checkpoint; three producer warps each
 //   own one pipeline stage (one pair per thread, 256 steps) and write MN-major A tiles.
 //
-// Every mbarrier wait is bounded (HB_TC_WAIT_NS); on expiry the kernel records an error code in
+// Every mbarrier wait is bounded (ctl.wait_ns, 2 s unless a plan sets it); on expiry the kernel records an error code in
 // *err and returns after releasing its tensor memory.
 #include <algorithm>
 #include <cmath>
@@ -56,10 +56,18 @@ struct TcGroup {
 
 __device__ __forceinline__ void set_err(int *err, int code) { atomicCAS(err, 0, code); }
 
+// Per-launch control of the tensor-core kernels: the bound of every mbarrier wait, and the
+// failure-detection test switch (inject = 1: the synthesis loader of CTA 0 withholds its first
+// batch-tile copy, so the waits on that stage run out and the kernel reports the error).
+struct TcCtl {
+    uint64_t wait_ns;
+    int inject;
+};
+
 // lane 0 waits (bounded), the result is broadcast so the whole warp takes the same path
-__device__ __forceinline__ bool warp_wait(uint64_t *bar, uint32_t parity) {
+__device__ __forceinline__ bool warp_wait(uint64_t *bar, uint32_t parity, uint64_t ns) {
     bool okw = true;
-    if ((threadIdx.x & 31) == 0) okw = tc::mbar_wait(bar, parity, HB_TC_WAIT_NS);
+    if ((threadIdx.x & 31) == 0) okw = tc::mbar_wait(bar, parity, ns);
     return __shfl_sync(0xffffffffu, (int)okw, 0) != 0;
 }
 
@@ -502,7 +510,8 @@ __device__ __forceinline__ void gen_chunk_syn(Rec &R, const float2 *cf, uint8_t 
 // stage is consumed in the order its group fills it.
 template <int N, bool BF16, int S>
 __global__ void __launch_bounds__(SYN_THREADS, 1)
-    synth_tc_kernel(const TcGroup *__restrict__ groups, const int4 *__restrict__ units, int nunits, int *err) {
+    synth_tc_kernel(const TcGroup *__restrict__ groups, const int4 *__restrict__ units, int nunits, int *err,
+                    TcCtl ctl) {
     constexpr int ST = SYN_GROUPS;
     constexpr int B_STAGE = tc_b_stage<N>();
     constexpr int STAGE = A_STAGE + B_STAGE;
@@ -567,7 +576,7 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
                 const bool fast = __all_sync(0xffffffffu, R.e == 0);
                 if (hb + SYN_GROUPS < nhb) fetch(hb + SYN_GROUPS);
                 for (int cc = 0; cc < 2 && 2 * hb + cc < nch; ++cc, ++gc) {
-                    if (gc >= 1 && !warp_wait(&L.empty[wg], (gc + 1) & 1)) {
+                    if (gc >= 1 && !warp_wait(&L.empty[wg], (gc + 1) & 1, ctl.wait_ns)) {
                         if (lane == 0) set_err(err, 1);
                         ok = false;
                         break;
@@ -586,7 +595,7 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
             // epilogue: this warp's lane quarter, column blocks j with j % SYN_GROUPS == wg; the
             // scales are fetched while the last MMAs drain
             load_inv_scales(L.inv, G.dscale + (int64_t)m * (N / 2), G.nmaps, N / 2, LS);
-            if (!warp_wait(L.accum, ui & 1)) {
+            if (!warp_wait(L.accum, ui & 1, ctl.wait_ns)) {
                 if (lane == 0) set_err(err, 2);
                 ok = false;
                 break;
@@ -623,7 +632,7 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
             for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++ui) {
                 const int4 U = units[u];
                 const int nch = (groups[U.x].lmax - U.y + 64) / 64, hb0 = U.w / 2, nhb = (nch + 1) / 2;
-                if (ui > 0 && !tc::mbar_wait(L.tfree, (ui - 1) & 1, HB_TC_WAIT_NS)) {
+                if (ui > 0 && !tc::mbar_wait(L.tfree, (ui - 1) & 1, ctl.wait_ns)) {
                     set_err(err, 3);
                     ok = false;
                     break;
@@ -635,7 +644,7 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
                         for (int g = 0; g < SYN_GROUPS; ++g) {
                             const int hb = h3 + g;
                             if (hb >= nhb || 2 * hb + cc >= nch) continue;
-                            if (!tc::mbar_wait(&L.full[g], (fbits >> g) & 1u, HB_TC_WAIT_NS)) {
+                            if (!tc::mbar_wait(&L.full[g], (fbits >> g) & 1u, ctl.wait_ns)) {
                                 set_err(err, 4);
                                 ok = false;
                                 break;
@@ -654,7 +663,7 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
             }
             if (!ok) {  // let issued MMAs finish before the tensor memory is released
                 tc::mma_commit(L.drain);
-                tc::mbar_wait(L.drain, 0, HB_TC_WAIT_NS);
+                tc::mbar_wait(L.drain, 0, ctl.wait_ns);
             }
         }
         __syncwarp();
@@ -662,6 +671,7 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
         // ---------------- loader of the pre-split alm tiles (same order as the MMA thread)
         if (lane == 0) {
             uint32_t ebits = 0, used = 0;  // bit g: parity of stage g's next drain / stage g used
+            bool withheld = false;
             for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
                 const int4 U = units[u];
                 const TcGroup &G = groups[U.x];
@@ -674,7 +684,7 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
                             const int hb = h3 + g, c = 2 * hb + cc;
                             if (hb >= nhb || c >= nch) continue;
                             if (used & (1u << g)) {
-                                if (!tc::mbar_wait(&L.empty[g], (ebits >> g) & 1u, HB_TC_WAIT_NS)) {
+                                if (!tc::mbar_wait(&L.empty[g], (ebits >> g) & 1u, ctl.wait_ns)) {
                                     set_err(err, 5);
                                     ok = false;
                                     break;
@@ -682,6 +692,10 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
                                 ebits ^= 1u << g;
                             }
                             used |= 1u << g;
+                            if (ctl.inject == 1 && blockIdx.x == 0 && !withheld) {  // failure-detection test
+                                withheld = true;
+                                continue;
+                            }
                             tc::mbar_arrive_expect_tx(&L.full[g], B_STAGE);
                             tc::bulk_g2s(smem + g * STAGE + A_STAGE, src + (int64_t)c * (16 * N), B_STAGE,
                                          &L.full[g]);
@@ -717,7 +731,7 @@ __device__ __forceinline__ void gen_chunk_ana(Rec &R, const float2 *cf, uint8_t 
 template <int N, bool BF16, int S>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     anal_tc_kernel(const TcGroup *__restrict__ groups, const int4 *__restrict__ units, int nunits, float2 *alm_out,
-                   int *err, const float *__restrict__ fl) {
+                   int *err, const float *__restrict__ fl, TcCtl ctl) {
     constexpr int ST = ana_stages<N>();
     constexpr int B_STAGE = tc_b_stage<N>();
     constexpr int STAGE = A_STAGE + B_STAGE;
@@ -786,7 +800,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 R.load(knext, LS);
                 fetch(c + ST);
                 const bool fast = __all_sync(0xffffffffu, R.e == 0);
-                if (it >= ST && !warp_wait(&L.empty[s], ((it / ST) + 1) & 1)) {
+                if (it >= ST && !warp_wait(&L.empty[s], ((it / ST) + 1) & 1, ctl.wait_ns)) {
                     if (lane == 0) set_err(err, 11);
                     ok = false;
                     break;
@@ -805,7 +819,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             // epilogue: lane quarter warp % 4 = rows 32w'..32w'+31 (l = l0 + 2 row + parity),
             // column blocks j with j % 2 == half; the scales are fetched while the MMAs drain
             load_inv_scales(L.inv, G.dscale + (int64_t)m * (N / 2), G.nmaps, N / 2, LS);
-            if (!warp_wait(L.accum, ui & 1)) {
+            if (!warp_wait(L.accum, ui & 1, ctl.wait_ns)) {
                 if (lane == 0) set_err(err, 12);
                 ok = false;
                 break;
@@ -843,7 +857,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             int ui = 0;
             for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++ui) {
                 const int npc = (int)groups[units[u].x].npc, c0 = units[u].w;
-                if (ui > 0 && !tc::mbar_wait(L.tfree, (ui - 1) & 1, HB_TC_WAIT_NS)) {
+                if (ui > 0 && !tc::mbar_wait(L.tfree, (ui - 1) & 1, ctl.wait_ns)) {
                     set_err(err, 13);
                     ok = false;
                     break;
@@ -851,7 +865,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 tc::fence_after();
                 for (int c = c0; c < npc; ++c, ++it) {
                     const int s = it % ST;
-                    if (!tc::mbar_wait(&L.full[s], (it / ST) & 1, HB_TC_WAIT_NS)) {
+                    if (!tc::mbar_wait(&L.full[s], (it / ST) & 1, ctl.wait_ns)) {
                         set_err(err, 14);
                         ok = false;
                         break;
@@ -866,7 +880,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             }
             if (!ok) {
                 tc::mma_commit(L.drain);
-                tc::mbar_wait(L.drain, 0, HB_TC_WAIT_NS);
+                tc::mbar_wait(L.drain, 0, ctl.wait_ns);
             }
         }
         __syncwarp();
@@ -882,7 +896,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 const uint4 *src = G.g_tiles + (int64_t)m * npc * (16 * N);
                 for (int c = U.w; c < npc; ++c, ++it) {
                     const int s = it % ST;
-                    if (it >= ST && !tc::mbar_wait(&L.empty[s], ((it / ST) + 1) & 1, HB_TC_WAIT_NS)) {
+                    if (it >= ST && !tc::mbar_wait(&L.empty[s], ((it / ST) + 1) & 1, ctl.wait_ns)) {
                         set_err(err, 15);
                         ok = false;
                         break;
@@ -927,6 +941,8 @@ struct hb_batched_plan {
     int4 *syn_units = nullptr, *ana_units = nullptr;
     int n_syn = 0, n_ana = 0, N = 128;
     int *err = nullptr;
+    uint64_t wait_ns = HB_TC_WAIT_NS;  // bound of every mbarrier wait of the tensor-core kernels
+    int inject = 0;                    // failure-detection test switch (hb_batched_fault_test)
     void *base = nullptr;
     size_t bytes = 0;
     bool profile = false;
@@ -957,7 +973,8 @@ static int launch_syn(hb_batched_plan *bp, cudaStream_t st) {
     constexpr int S = nsets<N>();
     HB_CUDA_TRY(cudaFuncSetAttribute(synth_tc_kernel<N, BF16, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     const int grid = std::min(bp->n_syn, sm_count());
-    synth_tc_kernel<N, BF16, S><<<grid, SYN_THREADS, smem, st>>>(bp->dgroups, bp->syn_units, bp->n_syn, bp->err);
+    synth_tc_kernel<N, BF16, S><<<grid, SYN_THREADS, smem, st>>>(bp->dgroups, bp->syn_units, bp->n_syn, bp->err,
+                                                                 TcCtl{bp->wait_ns, bp->inject});
     HB_CHECK_LAUNCH();
     return HB_OK;
 }
@@ -968,7 +985,7 @@ static int launch_ana(hb_batched_plan *bp, float2 *alm_out, const float *fl, cud
     HB_CUDA_TRY(cudaFuncSetAttribute(anal_tc_kernel<N, BF16, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     const int grid = std::min(bp->n_ana, sm_count());
     anal_tc_kernel<N, BF16, S><<<grid, TC_THREADS, smem, st>>>(bp->dgroups, bp->ana_units, bp->n_ana, alm_out,
-                                                                 bp->err, fl);
+                                                                 bp->err, fl, TcCtl{bp->wait_ns, 0});
     HB_CHECK_LAUNCH();
     return HB_OK;
 }
@@ -1357,6 +1374,20 @@ int hb_batched_work(const hb_batched_plan *bp, int64_t *chunks, int *mma_n) {
     chunks[0] = bp->live_syn;
     chunks[1] = bp->live_ana;
     *mma_n = bp->N;
+    return HB_OK;
+}
+
+int hb_batched_fault_test(hb_batched_plan *bp, uint64_t wait_ns, int withhold_copy) {
+    if (!bp || wait_ns < 1000000ull || wait_ns > 10000000000ull || withhold_copy < 0 || withhold_copy > 1)
+        return fail(HB_ERR_INVALID, "hb_batched_fault_test: wait_ns in [1 ms, 10 s], withhold_copy 0 or 1");
+    bp->wait_ns = wait_ns;
+    bp->inject = withhold_copy;
+    return HB_OK;
+}
+
+int hb_batched_reset_status(hb_batched_plan *bp) {
+    if (!bp) return fail(HB_ERR_INVALID, "hb_batched_reset_status: null plan");
+    HB_CUDA_TRY(cudaMemset(bp->err, 0, sizeof(int)));
     return HB_OK;
 }
 

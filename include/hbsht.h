@@ -224,6 +224,13 @@ HB_API int hb_batched_map2alm(hb_batched_plan *bp, const float *maps, float *alm
 HB_API int hb_batched_map2alm_fl(hb_batched_plan *bp, const float *maps, float *alm, const float *fl,
                                  hb_stream_t stream);
 HB_API int hb_batched_status(hb_batched_plan *bp, int *code);
+/* Failure-detection test hook (no reference counterpart): every mbarrier wait of the plan's
+ * tensor-core kernels gives up after wait_ns (default 2 s) and records an error code that
+ * hb_batched_status returns; with withhold_copy = 1 the synthesis kernel's loader in CTA 0
+ * skips its first batch-tile copy, so the waits on that stage run out, the kernel records the
+ * error and returns (the CUDA context stays usable).  hb_batched_reset_status clears the code. */
+HB_API int hb_batched_fault_test(hb_batched_plan *bp, uint64_t wait_ns, int withhold_copy);
+HB_API int hb_batched_reset_status(hb_batched_plan *bp);
 /* Work the tensor-core kernels execute per call after the evanescent skip: chunks[0] synthesis
  * chunks (64 l x 128 ring pairs each), chunks[1] analysis chunks (32 ring pairs x 256 l each);
  * every chunk is the work of 12 MMAs of 128 x mma_n x 16.  (No counterpart in the reference.) */

@@ -151,3 +151,27 @@ def test_autotune_picks_a_measured_configuration_within_tolerance(hb):
     assert (bp.bf16, bp.wide) == (t["bf16"], t["wide"])
     m = bp.alm2map(a).reshape(nmaps, -1)
     assert rel(m, hb.hp_compat.alm2map(a.to(torch.complex128), nside, lmax=lmax)) < TOL
+
+
+def test_bounded_wait_expires_and_context_stays_usable(hb):
+    """Failure detection without a GPU fault: with a 20 ms wait bound, the synthesis loader of
+    CTA 0 withholds its first batch-tile copy (hb_batched_fault_test); the waits on that stage
+    run out, the kernel records an error code and returns.  The host reads the code, clears it,
+    and the same plan then runs clean and correct."""
+    import time
+    nside, lmax, nmaps = 32, 63, 40
+    a = _batch(hb, lmax, nmaps, seed=9).to(torch.complex64)
+    bp = hb.batched.BatchedPlan([(hb.geometry.healpix(nside), lmax, None, nmaps)])
+    bp.fault_test(wait_s=0.02, withhold_copy=True)
+    t0 = time.perf_counter()
+    bp.alm2map(a.reshape(-1))
+    torch.cuda.synchronize()
+    assert time.perf_counter() - t0 < 5.0  # bounded: a few wait limits, not a hang
+    code = bp.status()
+    assert code != 0
+    bp.reset_status()
+    bp.fault_test(wait_s=2.0, withhold_copy=False)
+    m = bp.alm2map(a.reshape(-1)).reshape(nmaps, -1)
+    torch.cuda.synchronize()
+    assert bp.status() == 0
+    assert rel(m, hb.hp_compat.alm2map(a.to(torch.complex128), nside, lmax=lmax)) < TOL
