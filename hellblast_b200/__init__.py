@@ -5,7 +5,7 @@ the hp_compat scalar/spin-2 entry points), healpy m-major alm packing by default
 runs in the hand-written CUDA kernels of hellblast_b200/_lib/libhbsht.so (C ABI:
 include/hbsht.h), exposed as torch.ops.hb.*; there is no CPU fallback.
 """
-__version__ = "0.1.0"
+__version__ = "0.2.0"
 
 from . import _lib  # noqa: F401
 from . import ops  # noqa: F401  (registers torch.ops.hb.*)

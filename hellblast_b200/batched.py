@@ -210,8 +210,49 @@ class HostPipeline:
 _tuned: dict[tuple, dict] = {}
 
 
+def autotune_cache_path() -> str:
+    """JSON file that keeps autotune results across processes: $HB_AUTOTUNE_CACHE, else
+    ~/.cache/hellblast_b200/autotune.json."""
+    import os
+    return os.environ.get("HB_AUTOTUNE_CACHE",
+                          os.path.join(os.path.expanduser("~"), ".cache", "hellblast_b200", "autotune.json"))
+
+
+def _cache_key(key: tuple) -> str:
+    return "|".join(str(k) for k in key) + "|" + L.lib().hb_version().decode()
+
+
+def _cache_load() -> dict:
+    import json
+    try:
+        with open(autotune_cache_path()) as f:
+            d = json.load(f)
+        return d if isinstance(d, dict) else {}
+    except (OSError, ValueError):
+        return {}
+
+
+def _cache_store(key: tuple, result: dict) -> None:
+    """Add one result to the JSON cache (rewritten atomically; failures to write are ignored:
+    the cache only saves time)."""
+    import json
+    import os
+    import tempfile
+    path = autotune_cache_path()
+    try:
+        os.makedirs(os.path.dirname(path), exist_ok=True)
+        d = _cache_load()
+        d[_cache_key(key)] = result
+        fd, tmp = tempfile.mkstemp(dir=os.path.dirname(path), suffix=".tmp")
+        with os.fdopen(fd, "w") as f:
+            json.dump(d, f, indent=1, sort_keys=True)
+        os.replace(tmp, path)
+    except OSError:
+        pass
+
+
 def autotune(nside: int, lmax: int, nmaps: int, tol: float = 1e-5, reps: int = 2, seed: int = 0,
-             candidates=((False, False), (False, True), (True, False), (True, True))) -> dict:
+             candidates=((False, False), (False, True), (True, False), (True, True)), use_cache: bool = True) -> dict:
     """Chooses the batched tile configuration for (nside, lmax, nmaps) on this GPU by measurement.
 
     Each candidate (bf16, wide) is a 16-bit split type (IEEE half with power-of-two scaling, or
@@ -219,8 +260,9 @@ def autotune(nside: int, lmax: int, nmaps: int, tol: float = 1e-5, reps: int = 2
     pass).  For each, a plan is built, one alm2map + map2alm pair over `nmaps` synthetic maps is
     timed with CUDA events (after a warm-up), and map 0's pair error against the FP64 transforms
     is measured.  The fastest candidate with error <= tol wins; the result (with every
-    candidate's time and error) is cached per (nside, lmax, nmaps, device) and ``plan(...,
-    tuned=True)`` uses it.  The candidates' plans are released again (each holds its operand
+    candidate's time and error) is cached per (nside, lmax, nmaps, device) in the process and in
+    a JSON file (autotune_cache_path(), keyed also by the library version; ``use_cache=False``
+    measures afresh), and ``plan(..., tuned=True)`` uses it.  The candidates' plans are released again (each holds its operand
     tiles)."""
     from .alm_ops import synalm
     from . import hp_compat
@@ -228,6 +270,11 @@ def autotune(nside: int, lmax: int, nmaps: int, tol: float = 1e-5, reps: int = 2
     key = (int(nside), int(lmax), int(nmaps), torch.cuda.get_device_name(dev))
     if key in _tuned:
         return _tuned[key]
+    if use_cache:
+        hit = _cache_load().get(_cache_key(key))
+        if isinstance(hit, dict) and {"bf16", "wide", "candidates"} <= set(hit):
+            _tuned[key] = hit
+            return hit
     cl = 1.0 / (torch.arange(lmax + 1, dtype=torch.float64) + 10.0) ** 2
     a64 = synalm(cl.numpy(), lmax=lmax, seed=seed, device=dev)
     m64 = hp_compat.alm2map(a64, nside, lmax=lmax)
@@ -257,4 +304,6 @@ def autotune(nside: int, lmax: int, nmaps: int, tol: float = 1e-5, reps: int = 2
     good = [r for r in results if r["ok"]]
     best = min(good, key=lambda r: r["ms"]) if good else min(results, key=lambda r: r["rel_err"])
     _tuned[key] = {"bf16": best["bf16"], "wide": best["wide"], "candidates": results}
+    if use_cache:
+        _cache_store(key, _tuned[key])
     return _tuned[key]

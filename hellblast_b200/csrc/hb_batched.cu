@@ -1266,6 +1266,7 @@ size_t hb_batched_plan_bytes(const hb_batched_plan *bp) { return bp ? bp->bytes 
 
 int hb_batched_alm2map(hb_batched_plan *bp, const float *alm, float *maps, hb_stream_t stream) {
     if (!bp || !alm || !maps) return fail(HB_ERR_INVALID, "hb_batched_alm2map: null argument");
+    HB_NVTX("hb_batched_alm2map");
     cudaStream_t st = (cudaStream_t)stream;
     int rc;
     if (bp->profile) HB_CUDA_TRY(cudaEventRecord(bp->ev[0], st));
@@ -1295,6 +1296,7 @@ int hb_batched_map2alm(hb_batched_plan *bp, const float *maps, float *alm, hb_st
 
 int hb_batched_map2alm_fl(hb_batched_plan *bp, const float *maps, float *alm, const float *fl, hb_stream_t stream) {
     if (!bp || !alm || !maps) return fail(HB_ERR_INVALID, "hb_batched_map2alm: null argument");
+    HB_NVTX("hb_batched_map2alm");
     cudaStream_t st = (cudaStream_t)stream;
     int rc;
     if (bp->profile) HB_CUDA_TRY(cudaEventRecord(bp->ev[4], st));

@@ -841,6 +841,7 @@ static int launch_synthesis_t(const GeomDev &g, int nmaps, const c2_t<T> *Gm, in
 int launch_ring_analysis(const GeomDev &g, int precision, int nmaps, const void *maps, int64_t map_stride,
                          const double *w, void *Fm, int mmax, int flags, bool unit_weights, bool mdouble,
                          cudaStream_t st) {
+    HB_NVTX("ring_analysis");
     if (precision == 32)
         return launch_analysis_t<float>(g, nmaps, (const float *)maps, map_stride, w, (float2 *)Fm, mmax, flags,
                                         unit_weights, mdouble, st);
@@ -851,6 +852,7 @@ int launch_ring_analysis(const GeomDev &g, int precision, int nmaps, const void 
 int launch_ring_synthesis(const GeomDev &g, int precision, int nmaps, const void *Gm, int mmax, void *maps,
                           int64_t map_stride, const double *w, bool apply_weights, bool mdouble, int flags,
                           cudaStream_t st) {
+    HB_NVTX("ring_synthesis");
     if (precision == 32)
         return launch_synthesis_t<float>(g, nmaps, (const float2 *)Gm, mmax, (float *)maps, map_stride, w,
                                          apply_weights, mdouble, flags, st);

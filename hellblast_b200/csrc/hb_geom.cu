@@ -346,7 +346,7 @@ using namespace hb;
 extern "C" {
 
 const char *hb_last_error_string(void) { return g_last_error.c_str(); }
-const char *hb_version(void) { return "hbsht 0.1.0 (sm_100a)"; }
+const char *hb_version(void) { return "hbsht 0.2.0 (sm_100a)"; }
 int64_t hb_alm_size(int lmax, int mmax) {
     if (lmax < 0 || mmax < 0 || mmax > lmax) return -1;
     return alm_size(lmax, mmax);

@@ -1,6 +1,7 @@
 // Internal definitions shared by the hbsht CUDA sources (sm_100a).
 #pragma once
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
 #include <string>
 
@@ -28,6 +29,16 @@ int fail(int code, const std::string &msg);
         if (e_ != cudaSuccess)                                                                    \
             return ::hb::fail(HB_ERR_CUDA, std::string("kernel launch: ") + cudaGetErrorString(e_)); \
     } while (0)
+
+// NVTX range over a host-side launch sequence (header-only NVTX; inert unless a profiler is
+// attached), so timelines show which entry point and stage queued each kernel
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange &) = delete;
+    NvtxRange &operator=(const NvtxRange &) = delete;
+};
+#define HB_NVTX(name) ::hb::NvtxRange hb_nvtx_range_(name)
 
 // ----------------------------------------------------------------------------- complex helpers
 template <typename T> struct C2;

@@ -444,6 +444,7 @@ static int synthesis_t(const GeomDev &g, int nmaps, int lmax, int mmax, int nm, 
 
 int launch_leg_analysis(const GeomDev &g, int precision, int nmaps, int lmax, int mmax, const void *Fm, void *alm,
                         cudaStream_t st, const float4 *ck, const int64_t *bo, int nm, const int32_t *mlist) {
+    HB_NVTX("legendre_analysis");
     if (precision == 32)
         return analysis_t<float>(g, nmaps, lmax, mmax, nm, mlist, (const float2 *)Fm, (float2 *)alm, st, ck, bo);
     return analysis_t<double>(g, nmaps, lmax, mmax, nm, mlist, (const double2 *)Fm, (double2 *)alm, st, nullptr,
@@ -452,6 +453,7 @@ int launch_leg_analysis(const GeomDev &g, int precision, int nmaps, int lmax, in
 
 int launch_leg_synthesis(const GeomDev &g, int precision, int nmaps, int lmax, int mmax, const void *alm, void *Gm,
                          cudaStream_t st, const float4 *ck, const int64_t *bo, int nm, const int32_t *mlist) {
+    HB_NVTX("legendre_synthesis");
     if (precision == 32)
         return synthesis_t<float>(g, nmaps, lmax, mmax, nm, mlist, (const float2 *)alm, (float2 *)Gm, st, ck, bo);
     return synthesis_t<double>(g, nmaps, lmax, mmax, nm, mlist, (const double2 *)alm, (double2 *)Gm, st, nullptr,

@@ -109,3 +109,15 @@ def test_alias_phase_sign_is_exact_on_healpix_rings():
             assert np.all(plus | minus), (phi0, nside)
             # the rings with a half-pixel shift (phi0 = pi / n) take s = -1
             assert np.array_equal(minus, np.abs(t["phi0"] * t["nphi"] - np.pi) < 1e-9), (phi0, nside)
+
+
+def test_autotune_cache_round_trip(tmp_path, monkeypatch):
+    """The autotune JSON cache stores and returns a result under its key (no GPU involved)."""
+    from hellblast_b200 import batched
+    monkeypatch.setenv("HB_AUTOTUNE_CACHE", str(tmp_path / "sub" / "tune.json"))
+    key = (2048, 4095, 64, "NVIDIA B200")
+    res = {"bf16": False, "wide": True, "candidates": [{"bf16": False, "wide": True, "ms": 140.0}]}
+    batched._cache_store(key, res)
+    assert batched._cache_load()[batched._cache_key(key)] == res
+    batched._cache_store((1, 2, 3, "x"), {"bf16": True, "wide": False, "candidates": []})
+    assert len(batched._cache_load()) == 2
