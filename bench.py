@@ -34,7 +34,10 @@ def parse():
     p.add_argument("--steps", type=int, default=5)
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    p.add_argument("--mode", default="batched", choices=["plain", "batched"])
+    p.add_argument("--mode", default="batched", choices=["plain", "batched", "msharded"],
+                   help="batched: tensor-core batch per GPU (replicas); plain: FP32 per-map path; msharded: "
+                        "each map's transform split over the GPUs by ring pairs and orders m (one all-to-all "
+                        "per direction, strong scaling)")
     p.add_argument("--nside", type=int, default=2048)
     p.add_argument("--lmax", type=int, default=None)
     p.add_argument("--nmaps", type=int, default=None, help="maps per GPU (default 64 batched, 1 plain)")
@@ -236,19 +239,6 @@ def run_reference(args):
 
 
 # ----------------------------------------------------------------------------- GPU side
-def fft_classes(nside):
-    """Number of ring-FFT launches per direction: one per distinct convolution length of the
-    ring pairs (N = nphi/2 direct when a power of two, else Bluestein at 2^ceil(log2(2N-1)))."""
-    from hellblast_b200 import geometry as G
-    nphi = G.host_ring_tables(nside)["nphi"].astype(np.int64)
-    N = nphi // 2
-    pow2 = (N & (N - 1)) == 0
-    L = np.where(pow2, N, 1 << np.ceil(np.log2(2 * N - 1)).astype(np.int64))
-    nr = len(L)
-    pair_L = np.maximum(L[: (nr + 1) // 2], L[::-1][: (nr + 1) // 2])
-    return len(np.unique(pair_L))
-
-
 def hbm_bytes_ring_fft(nmaps, mmax, npairs, npix, itemsize=4):
     """Algorithmic HBM bytes of one ring-FFT pass over `nmaps` maps (either direction): the
     Fourier coefficients (mmax + 1) x npairs x (north, south) complex read or written once, and
@@ -348,10 +338,99 @@ def diff_leg(hb, nside, lmax, dev, st, reps=3):
     return res[0], res[1] / res[0]
 
 
+def run_msharded(args):
+    """--mode msharded: one FP32 alm2map + map2alm of B maps per step, every map split over the
+    ranks (distributed.MShardedSHT: ring-pair blocks for the FFTs, zig-zag order sets for the
+    Legendre work, one NCCL all-to-all per direction).  value = B pairs / step time (max over
+    ranks); e2e copies the alm in from pinned host memory and this rank's result out each step."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    import hellblast_b200 as hb
+    from hellblast_b200 import distributed as D
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=dev)
+    nside = args.nside
+    lmax = 2 * nside - 1 if args.lmax is None else args.lmax
+    B = args.nmaps if args.nmaps is not None else 4
+    st = torch.cuda.current_stream(dev)
+    cl = 1.0 / (np.arange(lmax + 1) + 10.0) ** 2
+    alm_h = torch.stack([hb.synalm(cl, lmax=lmax, seed=i, device="cpu", dtype=torch.complex64) for i in range(B)])
+    alm = alm_h.to(dev)
+    ms = D.MShardedSHT(nside, lmax, precision=32)
+    n_fft = ms.lg.fft_launches(32) if ms.lg is not None else 0
+
+    def step(a):
+        return ms.map2alm(ms.alm2map(a))
+
+    for _ in range(args.warmup):
+        out = step(alm)
+    torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    with Clocks(local) as clk:
+        t0 = torch.cuda.Event(enable_timing=True); t1 = torch.cuda.Event(enable_timing=True)
+        t0.record(st)
+        for _ in range(args.steps):
+            out = step(alm)
+        t1.record(st)
+        torch.cuda.synchronize(dev)
+    if world > 1:
+        dist.barrier()
+    ms_t = t0.elapsed_time(t1)
+    # accuracy: this rank's orders of map 0 against the single-GPU FP64 pair
+    a64 = alm_h[0].to(dev, torch.complex128)
+    b64 = hb.hp_compat.map2alm(hb.hp_compat.alm2map(a64, nside, lmax=lmax), lmax=lmax)
+    from hellblast_b200 import alm_ops
+    mine = torch.isin(alm_ops._m_of_index(lmax, lmax, str(dev)), torch.as_tensor(ms.layout.msets[rank], device=dev))
+    err = float(torch.linalg.norm((out[0].to(torch.complex128) - b64)[mine]) / torch.linalg.norm(b64[mine]))
+    pin_in = alm_h.pin_memory()
+    pin_out = torch.empty_like(pin_in).pin_memory()
+    e0 = torch.cuda.Event(enable_timing=True); e1 = torch.cuda.Event(enable_timing=True)
+    if world > 1:
+        dist.barrier()
+    e0.record(st)
+    for _ in range(args.steps):
+        r = step(pin_in.to(dev, non_blocking=True))
+        pin_out.copy_(r, non_blocking=True)
+    e1.record(st)
+    torch.cuda.synchronize(dev)
+    ms_e = e0.elapsed_time(e1)
+    if world > 1:
+        tt = torch.tensor([ms_t, ms_e], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms_t, ms_e = (float(x) for x in tt.tolist())
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    print(json.dumps({
+        "metric": METRIC, "value": args.steps * B / (ms_t * 1e-3), "unit": "pairs/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_t / args.steps, "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "f32", "data": "synthetic (Gaussian alm, C_l=(l+10)^-2)",
+        "config": {"workload": f"scalar map2alm+alm2map pair, nside {nside}, lmax {lmax}, float32, {B} maps per "
+                               f"step, each split over {world} GPUs by ring pairs and orders m", "nside": nside,
+                   "lmax": lmax, "maps_per_step": B, "mode": "msharded", "parallelism": f"m-sharded x{world}",
+                   "l2": "inputs larger than L2 (one map 201 MB at nside 2048)"},
+        "rel_err_vs_fp64_rank0_orders": err,
+        "e2e": {"value": args.steps * B / (ms_e * 1e-3), "unit": "pairs/s", "h2d_bytes_per_step": int(pin_in.numel() * 8),
+                "d2h_bytes_per_step": int(pin_out.numel() * 8), "api": "distributed.MShardedSHT from pinned host alm"},
+        "gpu_launches": args.steps * (2 + 2 * n_fft),
+        "clocks": clk.summary(),
+    }), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.mode == "msharded":
+        return run_msharded(args)
     import torch
     import torch.distributed as dist
     import hellblast_b200 as hb
@@ -408,7 +487,7 @@ def main():
 
     if args.mode == "plain":
         plan = G.plan(g, lmax, mmax, precision=32)
-        n_launch = 2 + 2 * fft_classes(nside)
+        n_launch = 2 + 2 * g.fft_launches(32)
         ws = torch.empty(plan.workspace_bytes(32, B), dtype=torch.uint8, device=dev)
 
         def step(ev=None):
@@ -455,7 +534,7 @@ def main():
             keys = stage_acc[0].keys()
             return {k: float(np.mean([s[k] for s in stage_acc])) for k in keys}
         groups = (B + (63 if wide else 31)) // (64 if wide else 32)
-        n_launch = 2 * groups + 2 + 2 * fft_classes(nside)  # operand preps, tensor kernels, ring FFT classes
+        n_launch = 2 * groups + 2 + 2 * g.fft_launches(32)  # operand preps, tensor kernels, ring FFT classes
 
         def make_ev():
             return True

@@ -45,6 +45,7 @@ SIGNATURES = {
     "hb_geom_create_healpix": (i32, [i64, i32, i32, ctypes.POINTER(vp)]),
     "hb_geom_create": (i32, [i64, vp, vp, vp, vp, ctypes.POINTER(vp)]),
     "hb_geom_destroy": (i32, [vp]),
+    "hb_geom_fft_launches": (i32, [vp, i32, ctypes.POINTER(i32)]),
     "hb_geom_info": (i32, [vp, ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.POINTER(i64), ctypes.POINTER(i64)]),
     "hb_plan_create": (i32, [vp, i32, i32, i32, ctypes.POINTER(vp)]),
     "hb_plan_destroy": (i32, [vp]),

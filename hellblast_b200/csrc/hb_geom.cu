@@ -455,4 +455,11 @@ int hb_geom_info(const hb_geom *g, int64_t *nr, int64_t *npix, int64_t *npairs, 
     return HB_OK;
 }
 
+int hb_geom_fft_launches(const hb_geom *g, int precision, int *n) {
+    if (!g || !n || (precision != 32 && precision != 64))
+        return fail(HB_ERR_INVALID, "hb_geom_fft_launches: bad arguments");
+    *n = precision == 32 ? g->d.pk_n_cls + g->d.rest_n_cls : g->d.n_cls;
+    return HB_OK;
+}
+
 }  // extern "C"

@@ -41,6 +41,12 @@ class Geometry:
             _next_id[0] += 1
             _registry[self.gid] = self
 
+    def fft_launches(self, precision: int = 32) -> int:
+        """Ring-FFT kernel launches per direction (one per transform-length class)."""
+        n = ctypes.c_int(0)
+        L.call("hb_geom_fft_launches", self.handle, int(precision), ctypes.byref(n))
+        return n.value
+
     def __del__(self):  # pragma: no cover - interpreter shutdown order
         try:
             if self.handle:

@@ -97,6 +97,10 @@ HB_API int hb_geom_create(int64_t nr, const double *theta, const int32_t *nphi, 
 HB_API int hb_geom_destroy(hb_geom *g);
 /* nr, npix, ring pairs used by the Legendre kernels, nside (0 if not HEALPix) */
 HB_API int hb_geom_info(const hb_geom *g, int64_t *nr, int64_t *npix, int64_t *npairs, int64_t *nside);
+/* Kernel launches one ring-FFT stage of the geometry makes per direction in the given
+ * precision (one per transform-length class; no reference counterpart: its FFT is one cuFFT
+ * call per ring, sht_raw.py:38-43). */
+HB_API int hb_geom_fft_launches(const hb_geom *g, int precision, int *n);
 
 /* Transform plans: a geometry plus (lmax, mmax) plus the FP64-computed checkpoints that
  * re-anchor the FP32 Legendre recursions every 256 l (FP32 transforms need them to stay within
