@@ -366,6 +366,8 @@ __global__ void __launch_bounds__(PkCfg<LOGL>::NT, PkCfg<LOGL>::MINB)
     const float scS = rS < 0 ? 0.f : (unit_w ? 1.f : (float)(sc2 * w[rS] / (double)n));
     const int mlim = (flags & HB_F_NOFOLD) ? min(mmax, n - 1) : mmax;
     float4 *out = Fm + bm * fm_stride4 + pair;
+    // HB_F_NOFOLD: the orders the ring does not resolve (m >= n) are zero, not left unwritten
+    for (int m = mlim + 1 + threadIdx.x; m <= mmax; m += NT) out[(int64_t)m * np] = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int k = threadIdx.x; k <= n / 2; k += NT) {
         const float2 zk = Zf(k), zc = k == 0 ? zk : Zf(n - k);
         // D_N = (Z[k] + conj Z[n-k]) / 2, D_S = (Z[k] - conj Z[n-k]) / (2 i)
