@@ -452,6 +452,10 @@ __device__ __forceinline__ void store_split(uint8_t *A, int off, const float (&e
 template <int N>
 __device__ __forceinline__ void issue_stage(uint32_t tmem, uint32_t a0, int pair, bool first, uint32_t idesc_n,
                                             uint32_t idesc_2n) {
+    // one cta_group::1 MMA is at most 256 wide and N a multiple of 16; the 2N-wide MMA reads the
+    // lo batch tile as B rows N .. 2N-1, so it must follow the hi tile directly (N * 64 bytes)
+    static_assert(2 * N <= 256 && N % 16 == 0, "the hi x (hi | lo) MMA needs 2N <= 256, N % 16 == 0");
+    static_assert(tc_b_stage<N>() == 4 * N * 64, "batch stage = [parity][hi | lo][N x 32], tiles back to back");
     const uint32_t b0 = a0 + A_STAGE;
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
@@ -523,6 +527,7 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
     // with the number of accumulate steps into one set; the epilogue sums the sets in IEEE FP32.
     constexpr int TCOLS = (2 * N * S < 32) ? 32 : 2 * N * S;
     static_assert(2 * N * S <= 512, "TMEM holds 512 columns");
+    static_assert(S >= 2 && S % 2 == 0, "accumulator sets come in (hi, cross) pairs");
     extern __shared__ __align__(1024) uint8_t smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const TcSmem L = tc_smem_layout<ST, N, SYN_PW>(smem, warp);
