@@ -256,8 +256,10 @@ __global__ void pix2ang_kernel(int64_t nside, int log2n, int nest, int ref, cons
             int64_t iring, iphi;
             ring_pos(nside, p, iring, iphi);
             const int64_t nphi = iring < nside ? 4 * iring : (iring <= 3 * nside ? 4 * nside : 4 * (4 * nside - iring));
-            ph = phi0_ref[iring - 1] + (double)(iphi - 1) * (twopi / (double)nphi);
-            if (ph >= twopi) ph -= twopi * floor(ph / twopi);
+            // separate rounded multiply and add (no FMA contraction), as the reference's host-side
+            // arithmetic rounds them
+            ph = __dadd_rn(phi0_ref[iring - 1], __dmul_rn((double)(iphi - 1), twopi / (double)nphi));
+            if (ph >= twopi) ph = __dsub_rn(ph, __dmul_rn(twopi, floor(ph / twopi)));
         }
         theta[i] = acos(z);
         phi[i] = ph;

@@ -236,8 +236,8 @@ class MShardedSHT:
                                            if self.local_rings.size else np.zeros(0, np.int64), device=self.device)
         if self.local_rings.size:
             lr = self.local_rings
-            self.lg = G.generic(t["theta_centers"][lr], nphi[lr].astype(np.int32), t["weights_dz"][lr],
-                                phi0=t["phi_center0"][lr])
+            self.lg = G.generic(t["theta"][lr], nphi[lr].astype(np.int32), t["weights_dz"][lr],
+                                phi0=t["phi0"][lr])
             if self.lg.npairs != p1 - p0:
                 raise RuntimeError("local ring block did not pair up like the global grid")
             self.lplan = G.plan(self.lg, self.lmax, self.mmax, precision=self.prec)
