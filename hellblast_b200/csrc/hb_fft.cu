@@ -640,9 +640,10 @@ __global__ void __launch_bounds__(256) bluestein_table_kernel(GeomDev g) {
     }
 }
 
-// Natural-order FP32 chirp spectra of the pair-packed Bluestein kernels (hb_ringpack.cu):
-// table e = FFT_L(b) / L, b_t = exp(+i pi t^2 / n) for |t| < n (circular), L = 2^logL >= 2n - 1,
-// n = ns[e].  One CTA per table; the FP64 transform runs in place in a global scratch slot
+// FP32 tables of the pair-packed Bluestein kernels (hb_ringpack.cu), 3L/2 entries each: the
+// natural-order chirp spectrum FFT_L(b) / L, b_t = exp(+i pi t^2 / n) for |t| < n (circular),
+// L = 2^logL >= 2n - 1, n = ns[e], then the chirp c_t = exp(-i pi t^2 / n) for t < L/2 (zero
+// from n on).  One CTA per table; the FP64 transform runs in place in a global scratch slot
 // (DIF, digit order; barriers make each pass's stores visible to the block), and the result is
 // read back in natural order.
 __global__ void __launch_bounds__(256) pk_chirp_kernel(GeomDev g, const int32_t *__restrict__ ns,
@@ -672,6 +673,11 @@ __global__ void __launch_bounds__(256) pk_chirp_kernel(GeomDev g, const int32_t 
     for (int k = threadIdx.x; k < L; k += blockDim.x) {
         const double2 v = buf[pos_of_freq(k, logL)];
         out[ofs[e] + k] = make_float2((float)(v.x * inv), (float)(v.y * inv));
+    }
+    for (int t = threadIdx.x; t < L / 2; t += blockDim.x) {
+        double2 c = make_double2(0.0, 0.0);
+        if (t < n) c = expmipi<double>((int64_t)t * t, n);
+        out[ofs[e] + L + t] = make_float2((float)c.x, (float)c.y);
     }
 }
 

@@ -67,11 +67,27 @@ template <int E, bool INV, typename V> __device__ __forceinline__ V w16(V a) {
     }
 }
 
+// DFT-4 of (x0, x1, 0, 0): the two zero inputs are not added (x + 0 is not x for x = -0, so the
+// compiler cannot drop those additions by itself)
+template <bool INV, typename V> __device__ __forceinline__ void dft4_h(V &x0, V &x1, V &x2, V &x3) {
+    const V a = x0, b = x1, rb = rot90<INV>(x1);
+    x0 = cadd(a, b);
+    x2 = csub(a, b);
+    x1 = cadd(a, rb);
+    x3 = csub(a, rb);
+}
+
 // 16-point DFT as 4 x 4: inner DFT-4 over n2 (n = n1 + 4 n2), twiddles W16^(n1 k2), outer
 // DFT-4 over n1; X[4 k1 + k2] ends in register k1 + 4 k2 and is renamed into place.
-template <bool INV, typename V> __device__ __forceinline__ void dft16(V *x) {
+// HALF: inputs 8 .. 15 are zero and are not read.
+template <bool INV, bool HALF = false, typename V> __device__ __forceinline__ void dft16(V *x) {
 #pragma unroll
-    for (int n1 = 0; n1 < 4; ++n1) dft4<INV>(x[n1], x[n1 + 4], x[n1 + 8], x[n1 + 12]);
+    for (int n1 = 0; n1 < 4; ++n1) {
+        if constexpr (HALF)
+            dft4_h<INV>(x[n1], x[n1 + 4], x[n1 + 8], x[n1 + 12]);
+        else
+            dft4<INV>(x[n1], x[n1 + 4], x[n1 + 8], x[n1 + 12]);
+    }
     x[5] = w16<1, INV>(x[5]);
     x[9] = w16<2, INV>(x[9]);
     x[13] = w16<3, INV>(x[13]);

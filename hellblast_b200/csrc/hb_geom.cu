@@ -197,7 +197,7 @@ static int finish_geom(HostGeom &h, int64_t nside, const std::vector<double> &xn
                     bt_n.push_back(h.nphi[rn]);
                     bt_logL.push_back(lg);
                     bt_ofs.push_back(bt_total);
-                    bt_total += int64_t(1) << lg;
+                    bt_total += (int64_t(3) << lg) / 2;  // chirp spectrum (L) and chirp (L/2)
                 }
                 pkb_ofs[p] = it->second;
             }

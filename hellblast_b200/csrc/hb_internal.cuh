@@ -115,7 +115,7 @@ struct GeomDev {
     int pk_n_cls;
     int pk_logn[16];
     int64_t pk_first[17];
-    float2 *pkb_bt;        // natural-order chirp spectra of the pair-packed Bluestein pairs
+    float2 *pkb_bt;        // pair-packed Bluestein tables: chirp spectrum (L) then chirp (L/2) per n
     int64_t *pkb_bt_ofs;   // [npairs] offset of the pair's table in pkb_bt (-1: not Bluestein)
     int32_t *rest_pairs;   // [npairs]
     int rest_n_cls;

@@ -13,9 +13,21 @@
 //
 // Bluestein (n not a power of two): the length-n DFT X_j = c_j sum_k (x_k c_k) b_{j-k},
 // c_t = exp(-i pi t^2 / n), b_t = conj c_t, is a circular convolution of length L >= 2n - 1:
-// x c (zero-padded), forward FFT_L, times the chirp spectrum FFT_L(b) / L (natural order, one
-// FP32 table per distinct n in the geometry), inverse FFT_L, times c.  The synthesis runs the
-// inverse DFT as conj(DFT(conj Z)).  c_t comes from the phase table: t^2 mod 2n is exact.
+// x c (zero-padded), forward FFT_L, times the chirp spectrum FFT_L(b) / L (natural order), inverse
+// FFT_L, times c.  The synthesis runs the inverse DFT as conj(DFT(conj Z)).  One FP32 table per
+// distinct n in the geometry holds the chirp spectrum (L entries) followed by c_t (t < L/2,
+// FP64-computed from t^2 mod 2n, zero from n on).  n <= L/2 (n is even and 2n - 1 <= L), so the
+// forward FFT's input is zero from L/2 on and only the inverse FFT's outputs below L/2 are used:
+// its first pass reads 8 of the 16 points of each butterfly and its last pass computes and
+// writes 8.  The chirp products ride in the analysis's first pass (ring times c) and in the
+// synthesis's last pass (output times c); the chirp-spectrum product is a separate step over
+// the shared buffer (fused into a pass, its 16 global loads per thread spill registers).
+//
+// Grid: (pair, map), so the CTAs in flight work on runs of neighbouring pairs of one map and
+// their strided 16-byte coefficient accesses fill whole sectors, except for the Bluestein
+// synthesis: (map, pair), so all maps of a pair run together and read that pair's tables once
+// from DRAM (measured at nside 2048, 64 maps: the synthesis 2.5 ms faster per direction this way,
+// the analysis 2.1 ms slower).
 //
 // Packing: the two real rings of a pair form one complex sequence z_j = f_N[j] + i f_S[j],
 // j < n, transformed by one complex FFT of length n.  Synthesis builds the spectrum Z of z from
@@ -126,17 +138,22 @@ __device__ __forceinline__ void pk_twiddle(float2 *v, int e, const PkTab &T) {
 
 // One Stockham pass (see the file comment).  `ld(i)` / `st(i, v)` read and write point i of the
 // pass's input and output (shared or global memory).  The barrier between all loads and all
-// stores makes the in-place update over one shared buffer safe.
-template <int LOGL, int P, bool INV, class Ld, class St>
+// stores makes the in-place update over one shared buffer safe.  HIN (first pass only): input
+// points from L/2 on are zero and are not read.  HOUT (last pass only): output points from L/2
+// on are neither computed nor written.
+template <int LOGL, int P, bool INV, bool HIN, bool HOUT, class Ld, class St>
 __device__ __forceinline__ void pk_pass(const PkTab &T, Ld &&ld, St &&st) {
     using C = PkCfg<LOGL>;
     constexpr int L = C::L, NT = C::NT, R = PkPass<LOGL, P>::R, NS = PkPass<LOGL, P>::NS, G = 16 / R;
+    static_assert(!HIN || (P == 0 && R == 16), "half input: the first pass, radix 16");
+    static_assert(!HOUT || (P == C::NPASS - 1 && R == 16 && NS == L / 16), "half output: the last pass, radix 16");
     float2 x[16];
 #pragma unroll
     for (int u = 0; u < G; ++u) {
         const int b = threadIdx.x + u * NT;
 #pragma unroll
-        for (int t = 0; t < R; ++t) x[u * R + t] = ld(b + t * (L / R));
+        for (int t = 0; t < R; ++t)
+            if (!HIN || t < R / 2) x[u * R + t] = ld(b + t * (L / R));
     }
     __syncthreads();
 #pragma unroll
@@ -145,29 +162,34 @@ __device__ __forceinline__ void pk_pass(const PkTab &T, Ld &&ld, St &&st) {
         const int j = b & (NS - 1);
         float2 *v = x + u * R;
         if constexpr (NS > 1) pk_twiddle<R, INV>(v, j * (L / (NS * R)), T);
-        dftR<R, INV>(v);
+        if constexpr (HIN)
+            dft16<INV, true>(v);
+        else
+            dftR<R, INV>(v);
         const int base = (b - j) * R + j;
 #pragma unroll
-        for (int q = 0; q < R; ++q) st(base + q * NS, v[q]);
+        for (int q = 0; q < R; ++q)
+            if (!HOUT || q < R / 2) st(base + q * NS, v[q]);
     }
 }
 
-// passes P .. NPASS-1; pass 0 reads through ld0, the last pass writes through stl, the others
-// go through the shared buffer
-template <int LOGL, bool INV, int P, class Ld0, class StL>
+// passes P .. NPASS-1; pass 0 reads through ld0 (HIN: half input), the last pass writes through
+// stl (HOUT: half output), the others go through the shared buffer
+template <int LOGL, bool INV, bool HIN, bool HOUT, int P = 0, class Ld0, class StL>
 __device__ __forceinline__ void pk_run(float2 *buf, const PkTab &T, Ld0 &&ld0, StL &&stl) {
     constexpr int NP = PkCfg<LOGL>::NPASS;
+    static_assert(NP >= 3, "pair-packed lengths have at least three passes");
     auto lds = [&](int i) -> float2 { return buf[pk_pad(i)]; };
     auto sts = [&](int i, float2 v) { buf[pk_pad(i)] = v; };
     if constexpr (P == NP - 1) {
-        pk_pass<LOGL, P, INV>(T, lds, stl);
+        pk_pass<LOGL, P, INV, false, HOUT>(T, lds, stl);
     } else {
         if constexpr (P == 0)
-            pk_pass<LOGL, P, INV>(T, ld0, sts);
+            pk_pass<LOGL, P, INV, HIN, false>(T, ld0, sts);
         else
-            pk_pass<LOGL, P, INV>(T, lds, sts);
+            pk_pass<LOGL, P, INV, false, false>(T, lds, sts);
         __syncthreads();
-        pk_run<LOGL, INV, P + 1>(buf, T, ld0, stl);
+        pk_run<LOGL, INV, HIN, HOUT, P + 1>(buf, T, ld0, stl);
     }
 }
 
@@ -208,14 +230,15 @@ __global__ void __launch_bounds__(PkCfg<LOGL>::NT, PkCfg<LOGL>::MINB)
     constexpr int L = C::L, NT = C::NT;
     extern __shared__ __align__(16) float2 pk_smem[];
     float2 *buf = pk_smem;
-    const int pair = pairs[blockIdx.x], bm = blockIdx.y;
+    const int pair = pairs[BLU ? blockIdx.y : blockIdx.x], bm = BLU ? blockIdx.x : blockIdx.y;
     const int rN = g.pair_ring[2 * pair], rS = g.pair_ring[2 * pair + 1];
     const int n = BLU ? g.nphi[rN] : L;
     const PkTab T = pk_tables<LOGL>(pk_smem + C::BUF, n);
     const int s = (flags & HB_F_NOPHASE) ? 0 : pk_shift(g.phi0_pi[rN], n);
     const int64_t np = g.npairs;
     const float4 *gin = Gm + bm * gm_stride4 + pair;  // (m, pair) entry at gin[m * np]
-    const float2 *bt = BLU ? g.pkb_bt + g.pkb_bt_ofs[pair] : nullptr;
+    // Bluestein tables: chirp spectrum bt[0, L), chirp ch[t] = exp(-i pi t^2 / n) for t < n
+    const float2 *bt = BLU ? g.pkb_bt + g.pkb_bt_ofs[pair] : nullptr, *ch = BLU ? bt + L : nullptr;
     const float dbl = mdouble ? 2.f : 1.f, chalf = 0.5f * dbl;
     const float sg = (s & 1) ? -1.f : 1.f;
     const bool hasS = rS >= 0;
@@ -223,10 +246,8 @@ __global__ void __launch_bounds__(PkCfg<LOGL>::NT, PkCfg<LOGL>::MINB)
     // phase-table index of exp(i pi s k / n): (s k) mod 2n (s k < 2^31: s < 2n <= 2^15, k <= n)
     auto pidx = [&](int k) -> int { return BLU ? mod2n(s * k) : ((s * k) & (2 * n - 1)); };
     __syncthreads();  // tables
-    // Bluestein chirp c_t = exp(-i pi t^2 / n), t < n <= 2^13
-    auto chirp = [&](int t) -> float2 { return cconj(T.ph(mod2n(t * t))); };
     // spectrum point k of z: stored as is (direct) or as conj(Z[k]) c_k (Bluestein)
-    auto put = [&](int k, float2 z) { buf[pk_pad(k)] = BLU ? cmul(cconj(z), chirp(k)) : z; };
+    auto put = [&](int k, float2 z) { buf[pk_pad(k)] = BLU ? cmul(cconj(z), __ldg(ch + k)) : z; };
     // an unpaired ring's south slot is not read as data: zeros keep the imaginary half finite
     auto ld = [&](int m) -> float4 {
         float4 v = __ldg(gin + (int64_t)m * np);
@@ -288,8 +309,8 @@ __global__ void __launch_bounds__(PkCfg<LOGL>::NT, PkCfg<LOGL>::MINB)
         const float2 ph = T.ph(pidx(n / 2));
         put(n / 2, make_float2(2.f * (ph.x * hN.x - ph.y * hN.y), 2.f * (ph.x * hS.x - ph.y * hS.y)));
     }
-    if (BLU)  // zero padding of the convolution
-        for (int k = n + threadIdx.x; k < L; k += NT) buf[pk_pad(k)] = make_float2(0.f, 0.f);
+    if (BLU)  // zero padding of the convolution (the first pass reads points below L/2 only)
+        for (int k = n + threadIdx.x; k < L / 2; k += NT) buf[pk_pad(k)] = make_float2(0.f, 0.f);
     __syncthreads();
     const double sc2 = (flags & HB_F_NO2PI) ? 1.0 : 6.283185307179586476925286766559;
     const float psN = apply_w ? (float)(sc2 * w[rN] / (double)n) : 1.f;
@@ -298,23 +319,24 @@ __global__ void __launch_bounds__(PkCfg<LOGL>::NT, PkCfg<LOGL>::MINB)
     float *fS = hasS ? maps + bm * map_stride + g.ofs[rS] : nullptr;
     auto lds = [&](int i) -> float2 { return buf[pk_pad(i)]; };
     if constexpr (!BLU) {
-        pk_run<LOGL, true, 0>(buf, T, lds, [&](int i, float2 v) {
+        pk_run<LOGL, true, false, false>(buf, T, lds, [&](int i, float2 v) {
             fN[i] = v.x * psN;
             if (fS) fS[i] = v.y * psS;
         });
-    } else {  // forward FFT_L, times the chirp spectrum, inverse FFT_L, times the chirp
-        auto sts = [&](int i, float2 v) { buf[pk_pad(i)] = v; };
-        pk_run<LOGL, false, 0>(buf, T, lds, sts);
+    } else {
+        // forward FFT_L (input zero from L/2 on), times the chirp spectrum
+        pk_run<LOGL, false, true, false>(buf, T, lds, [&](int i, float2 v) { buf[pk_pad(i)] = v; });
         __syncthreads();
         for (int i = threadIdx.x; i < L; i += NT) buf[pk_pad(i)] = cmul(buf[pk_pad(i)], __ldg(bt + i));
         __syncthreads();
-        pk_run<LOGL, true, 0>(buf, T, lds, sts);
-        __syncthreads();
-        for (int i = threadIdx.x; i < n; i += NT) {
-            const float2 z = cconj(cmul(chirp(i), buf[pk_pad(i)]));
-            fN[i] = z.x * psN;
-            if (fS) fS[i] = z.y * psS;
-        }
+        // inverse FFT_L, points below L/2 only; times the chirp, conjugated, to the two rings
+        pk_run<LOGL, true, false, true>(buf, T, lds, [&](int i, float2 v) {
+            if (i < n) {
+                const float2 z = cconj(cmul(__ldg(ch + i), v));
+                fN[i] = z.x * psN;
+                if (fS) fS[i] = z.y * psS;
+            }
+        });
     }
 }
 
@@ -339,28 +361,28 @@ __global__ void __launch_bounds__(PkCfg<LOGL>::NT, PkCfg<LOGL>::MINB)
     const int64_t np = g.npairs;
     const float *fN = maps + bm * map_stride + g.ofs[rN];
     const float *fS = rS >= 0 ? maps + bm * map_stride + g.ofs[rS] : nullptr;
-    const float2 *bt = BLU ? g.pkb_bt + g.pkb_bt_ofs[pair] : nullptr;
+    // Bluestein tables: chirp spectrum bt[0, L), chirp ch[t] = exp(-i pi t^2 / n) for t < n
+    const float2 *bt = BLU ? g.pkb_bt + g.pkb_bt_ofs[pair] : nullptr, *ch = BLU ? bt + L : nullptr;
     const PkMod mod2n{2 * n, 1.f / (float)(2 * n)};
     auto pidx = [&](int k) -> int { return BLU ? mod2n(s * k) : ((s * k) & (2 * n - 1)); };
-    auto chirp = [&](int t) -> float2 { return cconj(T.ph(mod2n(t * t))); };
     auto sts = [&](int i, float2 v) { buf[pk_pad(i)] = v; };
     auto ring = [&](int i) -> float2 { return make_float2(__ldg(fN + i), fS ? __ldg(fS + i) : 0.f); };
     __syncthreads();  // tables
     if constexpr (!BLU) {
-        pk_run<LOGL, false, 0>(buf, T, ring, sts);
-    } else {  // ring times the chirp (zero-padded), FFT_L, times the chirp spectrum, inverse FFT_L
+        pk_run<LOGL, false, false, false>(buf, T, ring, sts);
+    } else {
+        // forward FFT_L of the chirped ring (zero from n on; read below L/2 only), times the chirp
+        // spectrum; inverse FFT_L, points below L/2 only
         auto lds = [&](int i) -> float2 { return buf[pk_pad(i)]; };
-        for (int i = threadIdx.x; i < L; i += NT)
-            buf[pk_pad(i)] = i < n ? cmul(ring(i), chirp(i)) : make_float2(0.f, 0.f);
-        __syncthreads();
-        pk_run<LOGL, false, 0>(buf, T, lds, sts);
+        auto ld0 = [&](int i) -> float2 { return i < n ? cmul(ring(i), __ldg(ch + i)) : make_float2(0.f, 0.f); };
+        pk_run<LOGL, false, true, false>(buf, T, ld0, sts);
         __syncthreads();
         for (int i = threadIdx.x; i < L; i += NT) buf[pk_pad(i)] = cmul(buf[pk_pad(i)], __ldg(bt + i));
         __syncthreads();
-        pk_run<LOGL, true, 0>(buf, T, lds, sts);
+        pk_run<LOGL, true, false, true>(buf, T, lds, sts);
     }
     __syncthreads();
-    auto Zf = [&](int k) -> float2 { return BLU ? cmul(chirp(k), buf[pk_pad(k)]) : buf[pk_pad(k)]; };
+    auto Zf = [&](int k) -> float2 { return BLU ? cmul(__ldg(ch + k), buf[pk_pad(k)]) : buf[pk_pad(k)]; };
     const double sc2 = (flags & HB_F_NO2PI) ? 1.0 : 6.283185307179586476925286766559;
     const float scN = unit_w ? 1.f : (float)(sc2 * w[rN] / (double)n);
     const float scS = rS < 0 ? 0.f : (unit_w ? 1.f : (float)(sc2 * w[rS] / (double)n));
@@ -446,15 +468,25 @@ struct PkAnaArgs {
     bool unit_w, mdouble;
 };
 
+// (pair, map) grid, or (map, pair) with MAP_FAST (the Bluestein synthesis; see the file comment)
+template <bool MAP_FAST> static int pk_grid(int64_t cnt, int nmaps, dim3 *grid) {
+    const int64_t y = MAP_FAST ? cnt : nmaps;
+    if (y > 65535 || cnt > INT32_MAX || nmaps <= 0)
+        return fail(HB_ERR_UNSUPPORTED, "pair-packed ring FFT: more than 65535 pairs in a class or maps in a batch");
+    *grid = MAP_FAST ? dim3((unsigned)nmaps, (unsigned)cnt) : dim3((unsigned)cnt, (unsigned)nmaps);
+    return HB_OK;
+}
+
 template <int LOGL, bool BLU>
 static int pk_syn_one(const GeomDev &g, const int32_t *pairs, int64_t cnt, const PkSynArgs &a, cudaStream_t st) {
     int rc = pk_prepare<LOGL, BLU>();
+    dim3 grid;
+    if (!rc) rc = pk_grid<BLU>(cnt, a.nmaps, &grid);
     if (rc) return rc;
     const int64_t gm4 = (int64_t)(a.mmax + 1) * g.npairs;
-    ring_pair_synthesis_kernel<LOGL, BLU>
-        <<<dim3((unsigned)cnt, (unsigned)a.nmaps), PkCfg<LOGL>::NT, PkCfg<LOGL>::SMEM, st>>>(
-            g, pairs, reinterpret_cast<const float4 *>(a.Gm), gm4, a.mmax, a.maps, a.map_stride, a.w,
-            a.apply_w ? 1 : 0, a.mdouble ? 1 : 0, a.flags);
+    ring_pair_synthesis_kernel<LOGL, BLU><<<grid, PkCfg<LOGL>::NT, PkCfg<LOGL>::SMEM, st>>>(
+        g, pairs, reinterpret_cast<const float4 *>(a.Gm), gm4, a.mmax, a.maps, a.map_stride, a.w, a.apply_w ? 1 : 0,
+        a.mdouble ? 1 : 0, a.flags);
     HB_CHECK_LAUNCH();
     return HB_OK;
 }
@@ -462,10 +494,11 @@ static int pk_syn_one(const GeomDev &g, const int32_t *pairs, int64_t cnt, const
 template <int LOGL, bool BLU>
 static int pk_ana_one(const GeomDev &g, const int32_t *pairs, int64_t cnt, const PkAnaArgs &a, cudaStream_t st) {
     int rc = pk_prepare<LOGL, BLU>();
+    dim3 grid;
+    if (!rc) rc = pk_grid<false>(cnt, a.nmaps, &grid);
     if (rc) return rc;
     const int64_t fm4 = (int64_t)(a.mmax + 1) * g.npairs;
-    ring_pair_analysis_kernel<LOGL, BLU>
-        <<<dim3((unsigned)cnt, (unsigned)a.nmaps), PkCfg<LOGL>::NT, PkCfg<LOGL>::SMEM, st>>>(
+    ring_pair_analysis_kernel<LOGL, BLU><<<grid, PkCfg<LOGL>::NT, PkCfg<LOGL>::SMEM, st>>>(
             g, pairs, a.maps, a.map_stride, a.w, reinterpret_cast<float4 *>(a.Fm), fm4, a.mmax, a.flags,
             a.unit_w ? 1 : 0, a.mdouble ? 1 : 0);
     HB_CHECK_LAUNCH();
