@@ -92,14 +92,14 @@ __device__ __forceinline__ float block_pow2_scale(float vmax) {
     return res;
 }
 
-// Both prep kernels: persistent CTAs walk the (m, map) slices of the batch operand (maps fastest,
-// so one m's tile rows are written together), two slices in flight: while the CTA splits slice
-// s out of one shared-memory buffer, cp.async copies slice s + gridDim.x into the other (one pad
-// entry per 8 or 16 so that the per-thread runs below hit distinct banks).  For each slice the
-// CTA takes the maximum |value| (the power-of-two scale of that (m, map)), then each thread
-// turns one run of 8 consecutive K positions into the hi/lo rows of the K-major core matrices
-// (row n = 2 map + re/im; element (n, k) at (n%8)*8 + (n/8)*256 + (k/8)*64 + k%8), written as
-// 16-byte stores; a thread's re and im rows are adjacent and fill one 32-byte sector.  Map
+// The prep kernels turn runs of 8 consecutive K positions into the hi/lo rows of the K-major
+// core matrices (row n = 2 map + re/im; element (n, k) at (n%8)*8 + (n/8)*256 + (k/8)*64 + k%8),
+// written as 16-byte stores; a thread's re and im rows are adjacent and fill one 32-byte sector.
+// prep_alm_tiles_kernel: persistent CTAs walk the (m, map) slices of the batch operand (maps
+// fastest, so one m's tile rows are written together), two slices in flight: while the CTA
+// splits slice s out of one shared-memory buffer, cp.async copies slice s + gridDim.x into the
+// other (one pad entry per 16 so that the per-thread runs below hit distinct banks).  For each
+// slice the CTA takes the maximum |value| (the power-of-two scale of that (m, map)).  Map
 // columns past the group's maps get zeros.
 template <bool BF16>
 __device__ __forceinline__ void store_rows8(uint4 *chunk, int N, int qh, int n, int g, const float (&v)[8]) {
@@ -181,73 +181,117 @@ __global__ void __launch_bounds__(PREP_THREADS, 2) prep_alm_tiles_kernel(const T
     tc::cp_async_wait<0>();
 }
 
-// F [map][m][pair][2] -> per (m, 32-pair chunk) the analysis B tiles [q][h][N x 32 pairs]
-// (E = F_N + F_S for q = 0, O = F_N - F_S for q = 1).  Slice = (m, map): npairs 16-byte
-// (north, south) entries, pair p at p + p / 8 in the buffer (36 entries per 32-pair chunk).
+// F [map][m/8][pair][m%8][north, south] (the m-blocked F the batched ring analysis writes, see
+// fg_off) -> per (m, 32-pair chunk) the analysis B tiles [q][h][N x 32 pairs] (E = F_N + F_S
+// for q = 0, O = F_N - F_S for q = 1).  Work item = (block of 8 orders, quad of 4 maps): the 8
+// orders of one pair and map are one 128-byte line of F, and the 4 maps' rows of one
+// (m, chunk, k8 group, q, h) are one 128-byte segment of the tile.  F16: a first sweep over the
+// item's lines takes the maxima of |E|, |O| per (m, map) (the power-of-two scale, as
+// block_pow2_scale); BF16 has FP32's exponent range and uses scale 1 (a power-of-two scale
+// would change no bit of the result).  Then the item streams through shared memory in stages
+// of PF_PAIRS pairs of its 4 maps (cp.async, two stages in flight).  Warp w converts order w;
+// lane (k8 group, map) turns its 8 pairs into the hi/lo rows 2 map, 2 map + 1 of E and O, so
+// the 4 lanes of one k8 group write the interleaved rows of one tile segment in the same
+// instruction.  Shared-memory slot of (map, pair p, order j): map * PF_MS + 9 p + p / 8 + j
+// (the 8 lanes of a quarter-warp, 4 maps x 2 k8 groups, land on distinct bank groups).  Map
+// columns past the group's maps get zeros.
+constexpr int PF_THREADS = 256, PF_PAIRS = 64, PF_MAPS = 4;
+constexpr int PF_MS = 586;  // >= 9 * 63 + 7 + 8 entries per map, = 2 mod 8
+constexpr int PF_STAGE = PF_MAPS * PF_MS;
+constexpr int PF_SMEM = 2 * PF_STAGE * (int)sizeof(float4);
+__device__ __forceinline__ int pf_slot(int map, int p, int j) { return map * PF_MS + 9 * p + (p >> 3) + j; }
 template <int N, bool BF16>
-__global__ void __launch_bounds__(PREP_THREADS, 1) prep_g_tiles_kernel(const TcGroup *groups, int gi,
-                                                                       const float2 *__restrict__ F, int64_t f_stride,
-                                                                       int nbuf) {
+__global__ void __launch_bounds__(PF_THREADS, 3) prep_f_tiles_kernel(const TcGroup *groups, int gi,
+                                                                     const float4 *__restrict__ F, int64_t f_stride4) {
+    static_assert(PF_THREADS == 32 * 8 && PF_PAIRS == 8 * 8 && PF_MAPS == 4, "warp = order, lane = (k8 group, map)");
+    static_assert(PF_MS >= 9 * (PF_PAIRS - 1) + (PF_PAIRS - 1) / 8 + 8 && PF_MS % 8 == 2, "map stride");
+    static_assert((N / 2) % PF_MAPS == 0, "whole map quads");
     extern __shared__ float4 sf[];
+    __shared__ float red[PF_THREADS / 32][PF_MAPS * 8];
+    __shared__ float scl[PF_MAPS * 8];
     const TcGroup &G = groups[gi];
     const int64_t np = G.g.npairs;
-    const int npc = (int)G.npc, ns = prep_slices<N>(G.mmax), per = npc * 36;
-    auto issue = [&](int s, float4 *dst) {  // cp.async of slice s into dst, one commit group
-        const int m = s / (N / 2), b = s % (N / 2);
-        const bool live = b < G.nmaps;
-        const float4 *src = reinterpret_cast<const float4 *>(F + (int64_t)b * f_stride + (int64_t)m * np * 2);
-        for (int p = threadIdx.x; p < npc * 32; p += blockDim.x) {
-            float4 *d = dst + p + (p >> 3);
-            if (live && p < np)
-                tc::cp_async16(d, src + p);
-            else
-                *d = make_float4(0.f, 0.f, 0.f, 0.f);
-        }
-    };
-    // nbuf slice buffers: nbuf - 1 slices in flight while one is converted
-    int s = blockIdx.x, buf = 0;
-    for (int i = 0; i + 1 < nbuf; ++i) {
-        if (s + i * gridDim.x < ns) issue(s + i * gridDim.x, sf + i * per);
-        tc::cp_async_commit();
-    }
-    for (; s < ns; s += gridDim.x, buf = buf + 1 == nbuf ? 0 : buf + 1) {
-        const int sn = s + (nbuf - 1) * gridDim.x;
-        if (nbuf == 1) issue(s, sf);  // single buffer (no room for two): this slice now
-        else if (sn < ns) issue(sn, sf + (buf == 0 ? nbuf - 1 : buf - 1) * per);  // the buffer freed last
-        tc::cp_async_commit();
-        if (nbuf == 3) tc::cp_async_wait<2>();  // this slice's copies are done
-        else if (nbuf == 2) tc::cp_async_wait<1>();
-        else tc::cp_async_wait<0>();
-        __syncthreads();
-        const int m = s / (N / 2), b = s % (N / 2);
-        const float4 *cur = sf + buf * per;
-        float vmax = 0.f;
-        for (int p = threadIdx.x; p < npc * 32; p += blockDim.x) {
-            const float4 f = cur[p + (p >> 3)];
-            vmax = fmaxf(vmax, fmaxf(fmaxf(fabsf(f.x + f.z), fabsf(f.y + f.w)), fmaxf(fabsf(f.x - f.z), fabsf(f.y - f.w))));
-        }
-        const float sc = block_pow2_scale(vmax);
-        if (threadIdx.x == 0) G.dscale[(int64_t)m * (N / 2) + b] = sc;
-        uint4 *base = const_cast<uint4 *>(G.g_tiles) + (int64_t)m * npc * (16 * N);
-        for (int it = threadIdx.x; it < npc * 4; it += blockDim.x) {  // (chunk c, k8 group g): pairs 8 it .. 8 it + 7
-            const int c = it >> 2, g = it & 3;
-            const float4 *run = cur + 9 * it;
-            uint4 *chunk = base + (int64_t)c * (16 * N);
-            float er[8], ei[8], orr[8], oi[8];
+    const int npc = (int)G.npc, npad = npc * 32, nq = (N / 2) / PF_MAPS, items = (G.mmax / 8 + 1) * nq;
+    const int nstage = (npad + PF_PAIRS - 1) / PF_PAIRS;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int j = warp, bl = lane & 3, g8 = lane >> 2;  // order, map in the quad, k8 group in the stage
+    for (int item = blockIdx.x; item < items; item += gridDim.x) {
+        const int mb = item / nq, b0 = (item % nq) * PF_MAPS, m = 8 * mb + j;
+        const float4 *src = F + (int64_t)b0 * f_stride4 + (int64_t)mb * np * 8;  // map bb at + bb f_stride4
+        float sc = 1.f;
+        if constexpr (!BF16) {  // u = 8 p + jj: the stride keeps every thread on order jj = threadIdx.x % 8
+            const int jj = threadIdx.x & 7;
+            float vmax[PF_MAPS];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const float4 f = run[j];
-                er[j] = (f.x + f.z) * sc;
-                ei[j] = (f.y + f.w) * sc;
-                orr[j] = (f.x - f.z) * sc;
-                oi[j] = (f.y - f.w) * sc;
+            for (int bb = 0; bb < PF_MAPS; ++bb) {
+                vmax[bb] = 0.f;
+                if (b0 + bb < G.nmaps && 8 * mb + jj <= G.mmax) {
+                    const float4 *s4 = src + (int64_t)bb * f_stride4;
+#pragma unroll 8
+                    for (int64_t u = threadIdx.x; u < np * 8; u += PF_THREADS) {
+                        const float4 f = __ldg(s4 + u);
+                        vmax[bb] = fmaxf(vmax[bb], fmaxf(fmaxf(fabsf(f.x + f.z), fabsf(f.y + f.w)),
+                                                         fmaxf(fabsf(f.x - f.z), fabsf(f.y - f.w))));
+                    }
+                }
+                vmax[bb] = fmaxf(vmax[bb], __shfl_xor_sync(0xffffffffu, vmax[bb], 8));
+                vmax[bb] = fmaxf(vmax[bb], __shfl_xor_sync(0xffffffffu, vmax[bb], 16));
+                if (lane < 8) red[warp][bb * 8 + lane] = vmax[bb];
             }
-            store_rows8<BF16>(chunk, N, 0, 2 * b, g, er);
-            store_rows8<BF16>(chunk, N, 0, 2 * b + 1, g, ei);
-            store_rows8<BF16>(chunk, N, 1, 2 * b, g, orr);
-            store_rows8<BF16>(chunk, N, 1, 2 * b + 1, g, oi);
+            __syncthreads();
+            if (threadIdx.x < PF_MAPS * 8) {
+                float v = 0.f;
+                for (int w = 0; w < PF_THREADS / 32; ++w) v = fmaxf(v, red[w][threadIdx.x]);
+                int e = 0;
+                if (v > 0.f) frexpf(v, &e);  // v in [2^(e-1), 2^e): scaled to [2^13, 2^14)
+                scl[threadIdx.x] = v > 0.f ? ldexpf(1.0f, 14 - e) : 1.0f;
+            }
+            __syncthreads();
+            sc = scl[bl * 8 + j];
         }
-        __syncthreads();  // every thread is done with this buffer before it is refilled
+        if (threadIdx.x < PF_MAPS * 8) {  // (map b0 + t / 8, order t % 8)
+            const int mm = 8 * mb + (threadIdx.x & 7);
+            if (mm <= G.mmax) G.dscale[(int64_t)mm * (N / 2) + b0 + (threadIdx.x >> 3)] = BF16 ? 1.f : scl[threadIdx.x];
+        }
+        auto issue = [&](int stg, float4 *dst) {  // one commit group: t = (map, pair, order)
+            for (int t = threadIdx.x; t < PF_MAPS * PF_PAIRS * 8; t += PF_THREADS) {
+                const int jj = t & 7, pl = (t >> 3) % PF_PAIRS, bb = t / (8 * PF_PAIRS);
+                const int64_t p = (int64_t)stg * PF_PAIRS + pl;
+                float4 *d = dst + pf_slot(bb, pl, jj);
+                if (b0 + bb < G.nmaps && p < np && 8 * mb + jj <= G.mmax)
+                    tc::cp_async16(d, src + (int64_t)bb * f_stride4 + p * 8 + jj);
+                else
+                    *d = make_float4(0.f, 0.f, 0.f, 0.f);
+            }
+        };
+        issue(0, sf);
+        tc::cp_async_commit();
+        for (int stg = 0; stg < nstage; ++stg) {
+            const float4 *cur = sf + (stg & 1) * PF_STAGE;
+            if (stg + 1 < nstage) issue(stg + 1, sf + ((stg + 1) & 1) * PF_STAGE);
+            tc::cp_async_commit();
+            tc::cp_async_wait<1>();  // all groups but the one just committed: stage stg is in
+            __syncthreads();
+            const int p0 = stg * PF_PAIRS + 8 * g8;
+            if (m <= G.mmax && p0 < npad) {
+                const int c = p0 >> 5, g = (p0 >> 3) & 3, b = b0 + bl;
+                uint4 *chunk = const_cast<uint4 *>(G.g_tiles) + ((int64_t)m * npc + c) * (16 * N);
+                float er[8], ei[8], orr[8], oi[8];
+#pragma unroll
+                for (int i = 0; i < 8; ++i) {
+                    const float4 f = cur[pf_slot(bl, 8 * g8 + i, j)];
+                    er[i] = (f.x + f.z) * sc;
+                    ei[i] = (f.y + f.w) * sc;
+                    orr[i] = (f.x - f.z) * sc;
+                    oi[i] = (f.y - f.w) * sc;
+                }
+                store_rows8<BF16>(chunk, N, 0, 2 * b, g, er);
+                store_rows8<BF16>(chunk, N, 0, 2 * b + 1, g, ei);
+                store_rows8<BF16>(chunk, N, 1, 2 * b, g, orr);
+                store_rows8<BF16>(chunk, N, 1, 2 * b + 1, g, oi);
+            }
+            __syncthreads();  // every thread is done with this stage's buffer before it is refilled
+        }
     }
     tc::cp_async_wait<0>();
 }
@@ -932,8 +976,10 @@ struct hb_batched_plan {
         const hb_plan *p;
         int nmaps;
         int64_t map_ofs, alm_ofs;     // offsets of this plan's maps / alm in the caller's buffers (elements)
-        float2 *GF;                   // G (synthesis) / F (analysis) buffer [nmaps][mmax+1][np][2]
-        int64_t gf_stride;
+        // G (synthesis, m-major [nmaps][mmax+1][np][2]) / F (analysis, m-blocked [nmaps][rows/8][np][8][2],
+        // rows = mmax+1 padded to a multiple of 8: fg_off) buffer; complex elements per map of each
+        float2 *GF;
+        int64_t gf_stride, ff_stride;
         int64_t *tile_ofs;            // device [mmax+1] alm chunk offsets
         float2 *coef;                 // recursion coefficient table (coef_table_kernel)
         float4 *ckh;                  // mid-block recursion checkpoints (launch_ck_mid)
@@ -1017,16 +1063,14 @@ static int launch_prep_alm(hb_batched_plan *bp, int gi, const float2 *alm, int64
     HB_CHECK_LAUNCH();
     return HB_OK;
 }
+// F: the group's first map in the m-blocked F (stride: complex elements per map)
 template <int N, bool BF16>
-static int launch_prep_g(hb_batched_plan *bp, int gi, const float2 *F, int64_t stride, cudaStream_t st) {
+static int launch_prep_f(hb_batched_plan *bp, int gi, const float2 *F, int64_t stride, cudaStream_t st) {
     const TcGroup &G = bp->hgroups[gi];
-    const size_t one = sizeof(float4) * (size_t)(G.npc * 36);  // 32 pairs + 4 pads per chunk
-    const size_t room = (size_t)max_smem_optin_b() - 256;      // less the block reduction's table
-    const int nbuf = 3 * one <= room ? 3 : 2 * one <= room ? 2 : 1;
-    const int smem = (int)(one * nbuf);
-    HB_CUDA_TRY(cudaFuncSetAttribute(prep_g_tiles_kernel<N, BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    const int grid = std::min(prep_slices<N>(G.mmax), sm_count() * (nbuf > 1 ? 1 : 2));
-    prep_g_tiles_kernel<N, BF16><<<grid, PREP_THREADS, smem, st>>>(bp->dgroups, gi, F, stride, nbuf);
+    HB_CUDA_TRY(cudaFuncSetAttribute(prep_f_tiles_kernel<N, BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, PF_SMEM));
+    const int grid = std::min((G.mmax / 8 + 1) * (N / 2 / PF_MAPS), sm_count() * 3);
+    prep_f_tiles_kernel<N, BF16><<<grid, PF_THREADS, PF_SMEM, st>>>(bp->dgroups, gi,
+                                                                     reinterpret_cast<const float4 *>(F), stride / 2);
     HB_CHECK_LAUNCH();
     return HB_OK;
 }
@@ -1072,7 +1116,7 @@ int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int np
         for (int m = 0; m <= p->mmax; ++m) to[m + 1] = to[m] + (p->lmax - m + 64) / 64;
         chunks_a[i] = to[p->mmax + 1];
         const int ng = (nmaps[i] + GM - 1) / GM;
-        offs[i].gf = carve((size_t)nmaps[i] * (p->mmax + 1) * np * 2 * sizeof(float2));
+        offs[i].gf = carve((size_t)nmaps[i] * fg_rows(p->mmax, true) * np * 2 * sizeof(float2));
         offs[i].tofs = carve(8 * (size_t)(p->mmax + 2));
         offs[i].tiles_a = carve((size_t)ng * chunks_a[i] * 256 * N);
         offs[i].tiles_g = carve((size_t)ng * (p->mmax + 1) * ((np + 31) / 32) * 256 * N);
@@ -1139,7 +1183,8 @@ int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int np
     for (int i = 0; i < nplans; ++i) {
         auto &part = bp->parts[i];
         part.GF = (float2 *)(base + offs[i].gf);
-        part.gf_stride = (int64_t)(part.p->mmax + 1) * part.p->g->d.npairs * 2;
+        part.gf_stride = fg_rows(part.p->mmax, false) * part.p->g->d.npairs * 2;
+        part.ff_stride = fg_rows(part.p->mmax, true) * part.p->g->d.npairs * 2;
         part.tile_ofs = (int64_t *)(base + offs[i].tofs);
         part.coef = (float2 *)(base + offs[i].coef);
         part.ckh = (float4 *)(base + offs[i].ckh);
@@ -1308,14 +1353,14 @@ int hb_batched_map2alm_fl(hb_batched_plan *bp, const float *maps, float *alm, co
     for (const auto &part : bp->parts) {
         const GeomDev &d = part.p->g->d;
         if ((rc = launch_ring_analysis(d, 32, part.nmaps, maps + part.map_ofs, d.npix, nullptr, part.GF, part.p->mmax, 0,
-                                       false, false, st)))
+                                       false, false, st, /*mblk=*/true)))
             return rc;
     }
     if (bp->profile) HB_CUDA_TRY(cudaEventRecord(bp->ev[5], st));
     for (size_t gi = 0; gi < bp->hgroups.size(); ++gi) {
         const auto &part = bp->parts[bp->group_part[gi]];
-        const float2 *F = part.GF + (int64_t)bp->group_first_map[gi] * part.gf_stride;
-        if ((rc = HB_DISPATCH_N(bp, launch_prep_g)(bp, (int)gi, F, part.gf_stride, st))) return rc;
+        const float2 *F = part.GF + (int64_t)bp->group_first_map[gi] * part.ff_stride;
+        if ((rc = HB_DISPATCH_N(bp, launch_prep_f)(bp, (int)gi, F, part.ff_stride, st))) return rc;
     }
     if (bp->profile) HB_CUDA_TRY(cudaEventRecord(bp->ev[6], st));
     if ((rc = HB_DISPATCH_N(bp, launch_ana)(bp, (float2 *)alm, fl, st))) return rc;

@@ -361,7 +361,7 @@ template <typename T>
 __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1)
     ring_analysis_kernel(GeomDev g, const int32_t *__restrict__ pairs, const T *__restrict__ maps, int64_t map_stride,
                          const double *__restrict__ w, c2_t<T> *__restrict__ Fm, int64_t fm_stride, int mmax,
-                         int flags, int unit_w, int mdouble, int Lcls, int stage_n) {
+                         int flags, int unit_w, int mdouble, int Lcls, int stage_n, int mblk) {
     using V = c2_t<T>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     V *buf = reinterpret_cast<V *>(smem_raw);
@@ -370,6 +370,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1)
     const int pair = pairs[blockIdx.x], b = blockIdx.y;  // pairs fastest: neighbours complete F's sectors
     const int64_t np = g.npairs;
     V *out = Fm + b * fm_stride;
+    auto slot = [&](int m) -> int64_t { return fg_off(m, pair, np, mblk != 0) * 2; };  // (north, south) of m
     const Tw<T> tw = twiddles<T>(g);
     const double twopi = 6.283185307179586476925286766559;
     const bool joint = stage_n && g.pair_ring[2 * pair + 1] >= 0;
@@ -377,7 +378,7 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1)
     for (int side = 0; side < 2; ++side) {
         const int r = g.pair_ring[2 * pair + side];
         if (r < 0) {  // unpaired ring: zero south half
-            for (int m = threadIdx.x; m <= mmax; m += blockDim.x) out[((int64_t)m * np + pair) * 2 + 1] = mk2((T)0, (T)0);
+            for (int m = threadIdx.x; m <= mmax; m += blockDim.x) out[slot(m) + 1] = mk2((T)0, (T)0);
             continue;
         }
         const int n = g.nphi[r], N = n >> 1, L = g.fft_len[r], logL = ilog2(L);
@@ -403,11 +404,11 @@ __global__ void __launch_bounds__(256, sizeof(T) == 4 ? 3 : 1)
             if (mdouble && m > 0) X = cscale(X, (T)2);
             if ((flags & HB_F_NOFOLD) && m >= n) X = mk2((T)0, (T)0);
             if (!joint)
-                out[((int64_t)m * np + pair) * 2 + side_out] = X;
+                out[slot(m) + side_out] = X;
             else if (side == 0)
                 stn[m] = X;
             else
-                store_ns(out + ((int64_t)m * np + pair) * 2, stn[m], X);
+                store_ns(out + slot(m), stn[m], X);
         };
         // When exp(-i n phi0) = s = +-1 (HEALPix rings), exp(-i (m0 + j n) phi0) =
         // exp(-i m0 phi0) s^j: one phase product per residue class m0 instead of one per alias.
@@ -768,16 +769,17 @@ static int check_smem(const GeomDev &g, int mmax) {
 
 template <typename T>
 static int launch_analysis_t(const GeomDev &g, int nmaps, const T *maps, int64_t map_stride, const double *w,
-                             c2_t<T> *Fm, int mmax, int flags, bool unit_w, bool mdouble, cudaStream_t st) {
+                             c2_t<T> *Fm, int mmax, int flags, bool unit_w, bool mdouble, cudaStream_t st,
+                             bool mblk) {
     int rc = check_smem<T>(g, mmax);
     if (rc) return rc;
     if (nmaps > 65535) return fail(HB_ERR_INVALID, "ring FFT: at most 65535 maps per call");
-    const int64_t fm_stride = (int64_t)(mmax + 1) * g.npairs * 2;
+    const int64_t fm_stride = fg_rows(mmax, mblk) * g.npairs * 2;
     // FP32: the pair-packed kernels take the pairs they can (hb_ringpack.cu), this kernel the rest
     const bool f32 = sizeof(T) == 4;
     if (f32 && g.pk_n_cls > 0) {
         rc = launch_pk_analysis(g, nmaps, reinterpret_cast<const float *>(maps), map_stride, w ? w : g.w,
-                                reinterpret_cast<float2 *>(Fm), mmax, flags, unit_w, mdouble, st);
+                                reinterpret_cast<float2 *>(Fm), mmax, flags, unit_w, mdouble, st, mblk);
         if (rc) return rc;
     }
     const int ncls = f32 ? g.rest_n_cls : g.n_cls;
@@ -799,7 +801,7 @@ static int launch_analysis_t(const GeomDev &g, int nmaps, const T *maps, int64_t
         ring_analysis_kernel<T><<<grid, class_threads(L), smem, st>>>(g, clsP + first, maps, map_stride,
                                                                        w ? w : g.w, Fm, fm_stride, mmax, flags,
                                                                        unit_w ? 1 : 0, mdouble ? 1 : 0, L,
-                                                                       stage_n ? 1 : 0);
+                                                                       stage_n ? 1 : 0, mblk ? 1 : 0);
         HB_CHECK_LAUNCH();
     }
     return HB_OK;
@@ -846,13 +848,13 @@ static int launch_synthesis_t(const GeomDev &g, int nmaps, const c2_t<T> *Gm, in
 
 int launch_ring_analysis(const GeomDev &g, int precision, int nmaps, const void *maps, int64_t map_stride,
                          const double *w, void *Fm, int mmax, int flags, bool unit_weights, bool mdouble,
-                         cudaStream_t st) {
+                         cudaStream_t st, bool mblk) {
     HB_NVTX("ring_analysis");
     if (precision == 32)
         return launch_analysis_t<float>(g, nmaps, (const float *)maps, map_stride, w, (float2 *)Fm, mmax, flags,
-                                        unit_weights, mdouble, st);
+                                        unit_weights, mdouble, st, mblk);
     return launch_analysis_t<double>(g, nmaps, (const double *)maps, map_stride, w, (double2 *)Fm, mmax, flags,
-                                     unit_weights, mdouble, st);
+                                     unit_weights, mdouble, st, mblk);
 }
 
 int launch_ring_synthesis(const GeomDev &g, int precision, int nmaps, const void *Gm, int mmax, void *maps,

@@ -150,9 +150,19 @@ namespace hb {
 // the plan's scalar recursion states at l0 + 128 of every 256-l block (same indexing as ck);
 // default stream, asynchronous
 int launch_ck_mid(const hb_plan *p, float4 *ck_mid);
+// F(m, ring pair) workspaces: m-major [m][pair][north, south], or with mblk (the batched FP32
+// analysis) blocked by 8 orders, [m/8][pair][m%8][north, south], so that one ring pair's
+// consecutive orders share 128-byte lines; rows = orders padded to a multiple of 8
+__host__ __device__ __forceinline__ int64_t fg_rows(int mmax, bool mblk) {
+    return mblk ? (int64_t)((mmax + 8) / 8) * 8 : (int64_t)mmax + 1;
+}
+// offset of (m, pair p) in (north, south) complex pairs
+__device__ __forceinline__ int64_t fg_off(int m, int64_t p, int64_t np, bool mblk) {
+    return mblk ? (((int64_t)(m >> 3) * np + p) << 3) + (m & 7) : (int64_t)m * np + p;
+}
 int launch_ring_analysis(const GeomDev &g, int precision, int nmaps, const void *maps, int64_t map_stride,
                          const double *w, void *Fm, int mmax, int flags, bool unit_weights, bool mdouble,
-                         cudaStream_t st);
+                         cudaStream_t st, bool mblk = false);
 int launch_ring_synthesis(const GeomDev &g, int precision, int nmaps, const void *Gm, int mmax, void *maps,
                           int64_t map_stride, const double *w, bool apply_weights, bool mdouble, int flags,
                           cudaStream_t st);
@@ -183,5 +193,5 @@ int build_pk_chirp_tables(const GeomDev &g, int count, const int32_t *ns, const 
 int launch_pk_synthesis(const GeomDev &g, int nmaps, const float2 *Gm, int mmax, float *maps, int64_t map_stride,
                         const double *w, bool apply_w, bool mdouble, int flags, cudaStream_t st);
 int launch_pk_analysis(const GeomDev &g, int nmaps, const float *maps, int64_t map_stride, const double *w,
-                       float2 *Fm, int mmax, int flags, bool unit_w, bool mdouble, cudaStream_t st);
+                       float2 *Fm, int mmax, int flags, bool unit_w, bool mdouble, cudaStream_t st, bool mblk);
 }  // namespace hb

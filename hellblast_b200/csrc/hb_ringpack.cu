@@ -71,9 +71,11 @@ template <int LOGL> struct PkCfg {
     static constexpr int R1 = (LOGL & 3) ? (1 << (LOGL & 3)) : 16;   // radix of pass 1
     static constexpr int NPASS = (LOGL >> 2) + ((LOGL & 3) ? 1 : 0);
     static constexpr int BUF = L + (L >> 4);
-    static constexpr int TWC = L / 64;       // coarse twiddle entries W_L^(64 c)
+    static constexpr int TW = L / 16;        // twiddle entries W_L^e and W_L^(4e), e < L/16
+    static constexpr int TWP = TW + TW / 16; // ... stored at e + e/16 (pk_pad), see PkTab
+    static constexpr int TWS = R1 < 16 ? 16 * R1 : 0;  // pass-1 twiddles W_(16 R1)^(j t), j < 16, t < R1
     static constexpr int PHC = 2 * L / 64;   // coarse phase entries exp(i pi 64 c / n), 2n <= 2L
-    static constexpr int SMEM = (BUF + 64 + TWC + 64 + PHC) * (int)sizeof(float2);
+    static constexpr int SMEM = (BUF + 2 * TWP + TWS + 64 + PHC) * (int)sizeof(float2);
     static constexpr int MINB = 65536 / (NT * 64) > 0 ? 65536 / (NT * 64) : 1;  // <= 64 registers
 };
 
@@ -83,61 +85,67 @@ template <int LOGL, int P> struct PkPass {
 };
 
 struct PkTab {
-    const float2 *twf, *twc;  // W_L^e = twf[e & 63] twc[e >> 6], e < L
+    // radix-16 passes: the butterfly exponent e = j L / (16 NS) < L/16 indexes tw1 = W_L^e and
+    // tw4 = W_L^(4e) directly (entry e at pk_pad(e): the middle passes' exponents step by 16,
+    // which would put a half-warp on one bank); the other powers are their products (at most
+    // three products deep)
+    const float2 *tw1, *tw4;
+    const float2 *tws;        // pass 1 of radix R1 < 16 (NS = 16): W_(16 R1)^(j t) at tws[j R1 + t]
     const float2 *phf, *phc;  // exp(i pi e / n) = phf[e & 63] phc[e >> 6], e < 2n
-    __device__ __forceinline__ float2 w(int e) const { return cmul(twf[e & 63], twc[e >> 6]); }
     __device__ __forceinline__ float2 ph(int e) const { return cmul(phf[e & 63], phc[e >> 6]); }
 };
 
-// per-CTA tables: twiddles of length L, phases exp(i pi e / n) for the ring length n
+// per-CTA tables (FP64-computed, rounded to FP32): twiddles of length L, phases
+// exp(i pi e / n) for the ring length n
 template <int LOGL> __device__ __forceinline__ PkTab pk_tables(float2 *base, int n) {
     using C = PkCfg<LOGL>;
-    float2 *twf = base, *twc = twf + 64, *phf = twc + C::TWC, *phc = phf + 64;
+    float2 *tw1 = base, *tw4 = tw1 + C::TWP, *tws = tw4 + C::TWP, *phf = tws + C::TWS, *phc = phf + 64;
     const double L = (double)C::L, dn = (double)n;
-    for (int i = threadIdx.x; i < 64 + C::TWC + 64 + C::PHC; i += C::NT) {
+    constexpr int E1 = 2 * C::TW, E2 = E1 + C::TWS, E3 = E2 + 64, E4 = E3 + C::PHC;
+    for (int i = threadIdx.x; i < E4; i += C::NT) {
         double sn, cs;
-        if (i < 64) {  // W_L^i
-            sincospi(-2.0 * (double)i / L, &sn, &cs);
-            twf[i] = make_float2((float)cs, (float)sn);
-        } else if (i < 64 + C::TWC) {  // W_L^(64 c)
-            sincospi(-2.0 * (double)(64 * (i - 64)) / L, &sn, &cs);
-            twc[i - 64] = make_float2((float)cs, (float)sn);
-        } else if (i < 128 + C::TWC) {  // exp(i pi e / n), e < 64
-            sincospi((double)(i - 64 - C::TWC) / dn, &sn, &cs);
-            phf[i - 64 - C::TWC] = make_float2((float)cs, (float)sn);
+        float2 *dst;
+        if (i < E1) {  // W_L^e, W_L^(4e)
+            const int e = i < C::TW ? i : i - C::TW;
+            sincospi(-2.0 * (double)(i < C::TW ? e : 4 * e) / L, &sn, &cs);
+            dst = (i < C::TW ? tw1 : tw4) + pk_pad(e);
+        } else if (i < E2) {  // W_(16 R1)^(j t)
+            const int j = (i - E1) / C::R1, t = (i - E1) % C::R1;
+            sincospi(-2.0 * (double)(j * t) / (double)(16 * C::R1), &sn, &cs);
+            dst = tws + (i - E1);
+        } else if (i < E3) {  // exp(i pi e / n), e < 64
+            sincospi((double)(i - E2) / dn, &sn, &cs);
+            dst = phf + (i - E2);
         } else {  // exp(i pi 64 c / n), 64 c < 2n <= 2L
-            const int c = i - 128 - C::TWC;
-            sincospi((double)(64 * c) / dn, &sn, &cs);
-            phc[c] = make_float2((float)cs, (float)sn);
+            sincospi((double)(64 * (i - E3)) / dn, &sn, &cs);
+            dst = phc + (i - E3);
         }
+        *dst = make_float2((float)cs, (float)sn);
     }
-    return {twf, twc, phf, phc};
+    return {tw1, tw4, tws, phf, phc};
 }
 
-// point t of a radix-R butterfly times W_L^(e t) (conjugate for INV), t = 1 .. R-1
+// points t = 1 .. R-1 of a radix-R butterfly with exponent e (radix 16) or pass-1 row j (R < 16)
+// times W_L^(e t) (conjugate for INV)
 template <int R, bool INV>
-__device__ __forceinline__ void pk_twiddle(float2 *v, int e, const PkTab &T) {
+__device__ __forceinline__ void pk_twiddle(float2 *v, int e, int j, const PkTab &T) {
     auto app = [&](int q, float2 w) { v[q] = cmul(v[q], INV ? cconj(w) : w); };
     if constexpr (R == 16) {
-        const float2 w1 = T.w(e), w2 = T.w(2 * e), w4 = T.w(4 * e), w8 = T.w(8 * e);
+        const float2 w1 = T.tw1[pk_pad(e)], w4 = T.tw4[pk_pad(e)];
+        const float2 w2 = cmul(w1, w1), w8 = cmul(w4, w4);
         const float2 w3 = cmul(w1, w2), w5 = cmul(w4, w1), w6 = cmul(w4, w2), w7 = cmul(w4, w3);
         app(1, w1); app(2, w2); app(3, w3); app(4, w4); app(5, w5); app(6, w6); app(7, w7); app(8, w8);
         app(9, cmul(w8, w1)); app(10, cmul(w8, w2)); app(11, cmul(w8, w3)); app(12, cmul(w8, w4));
         app(13, cmul(w8, w5)); app(14, cmul(w8, w6)); app(15, cmul(w8, w7));
-    } else if constexpr (R == 8) {
-        const float2 w1 = T.w(e), w2 = T.w(2 * e), w4 = T.w(4 * e), w3 = cmul(w1, w2);
-        app(1, w1); app(2, w2); app(3, w3); app(4, w4);
-        app(5, cmul(w4, w1)); app(6, cmul(w4, w2)); app(7, cmul(w4, w3));
-    } else if constexpr (R == 4) {
-        const float2 w1 = T.w(e), w2 = T.w(2 * e);
-        app(1, w1); app(2, w2); app(3, cmul(w1, w2));
     } else {
-        app(1, T.w(e));
+#pragma unroll
+        for (int t = 1; t < R; ++t) app(t, T.tws[j * R + t]);
     }
 }
 
-// One Stockham pass (see the file comment).  `ld(i)` / `st(i, v)` read and write point i of the
-// pass's input and output (shared or global memory).  The barrier between all loads and all
+// One Stockham pass (see the file comment).  `ld(i, ip)` / `st(i, ip, v)` read and write point i
+// of the pass's input and output, ip = pk_pad(i) its shared-buffer slot (base plus compile-time
+// offsets: every stride here is a multiple of 16).  The barrier between all loads and all
 // stores makes the in-place update over one shared buffer safe.  HIN (first pass only): input
 // points from L/2 on are zero and are not read.  HOUT (last pass only): output points from L/2
 // on are neither computed nor written.
@@ -147,13 +155,17 @@ __device__ __forceinline__ void pk_pass(const PkTab &T, Ld &&ld, St &&st) {
     constexpr int L = C::L, NT = C::NT, R = PkPass<LOGL, P>::R, NS = PkPass<LOGL, P>::NS, G = 16 / R;
     static_assert(!HIN || (P == 0 && R == 16), "half input: the first pass, radix 16");
     static_assert(!HOUT || (P == C::NPASS - 1 && R == 16 && NS == L / 16), "half output: the last pass, radix 16");
+    static_assert((L / R) % 16 == 0 && NT % 16 == 0 && (NS == 1 || NS % 16 == 0) && (NS > 1 || R == 16),
+                  "padded offsets are base plus constants");
+    constexpr int LS = L / R + L / R / 16, US = NT + NT / 16, QS = NS == 1 ? 1 : NS + NS / 16;
+    const int tp = pk_pad(threadIdx.x);
     float2 x[16];
 #pragma unroll
     for (int u = 0; u < G; ++u) {
-        const int b = threadIdx.x + u * NT;
+        const int b = threadIdx.x + u * NT, bp = tp + u * US;
 #pragma unroll
         for (int t = 0; t < R; ++t)
-            if (!HIN || t < R / 2) x[u * R + t] = ld(b + t * (L / R));
+            if (!HIN || t < R / 2) x[u * R + t] = ld(b + t * (L / R), bp + t * LS);
     }
     __syncthreads();
 #pragma unroll
@@ -161,15 +173,16 @@ __device__ __forceinline__ void pk_pass(const PkTab &T, Ld &&ld, St &&st) {
         const int b = threadIdx.x + u * NT;
         const int j = b & (NS - 1);
         float2 *v = x + u * R;
-        if constexpr (NS > 1) pk_twiddle<R, INV>(v, j * (L / (NS * R)), T);
+        if constexpr (NS > 1) pk_twiddle<R, INV>(v, j * (L / (NS * R)), j, T);
         if constexpr (HIN)
             dft16<INV, true>(v);
         else
             dftR<R, INV>(v);
         const int base = (b - j) * R + j;
+        const int basep = NS == 1 ? 17 * b : pk_pad(base);  // NS == 1: base = 16 b, slot 17 b
 #pragma unroll
         for (int q = 0; q < R; ++q)
-            if (!HOUT || q < R / 2) st(base + q * NS, v[q]);
+            if (!HOUT || q < R / 2) st(base + q * NS, basep + q * QS, v[q]);
     }
 }
 
@@ -179,8 +192,8 @@ template <int LOGL, bool INV, bool HIN, bool HOUT, int P = 0, class Ld0, class S
 __device__ __forceinline__ void pk_run(float2 *buf, const PkTab &T, Ld0 &&ld0, StL &&stl) {
     constexpr int NP = PkCfg<LOGL>::NPASS;
     static_assert(NP >= 3, "pair-packed lengths have at least three passes");
-    auto lds = [&](int i) -> float2 { return buf[pk_pad(i)]; };
-    auto sts = [&](int i, float2 v) { buf[pk_pad(i)] = v; };
+    auto lds = [&](int, int ip) -> float2 { return buf[ip]; };
+    auto sts = [&](int, int ip, float2 v) { buf[ip] = v; };
     if constexpr (P == NP - 1) {
         pk_pass<LOGL, P, INV, false, HOUT>(T, lds, stl);
     } else {
@@ -317,20 +330,20 @@ __global__ void __launch_bounds__(PkCfg<LOGL>::NT, PkCfg<LOGL>::MINB)
     const float psS = (apply_w && hasS) ? (float)(sc2 * w[rS] / (double)n) : 1.f;
     float *fN = maps + bm * map_stride + g.ofs[rN];
     float *fS = hasS ? maps + bm * map_stride + g.ofs[rS] : nullptr;
-    auto lds = [&](int i) -> float2 { return buf[pk_pad(i)]; };
+    auto lds = [&](int, int ip) -> float2 { return buf[ip]; };
     if constexpr (!BLU) {
-        pk_run<LOGL, true, false, false>(buf, T, lds, [&](int i, float2 v) {
+        pk_run<LOGL, true, false, false>(buf, T, lds, [&](int i, int, float2 v) {
             fN[i] = v.x * psN;
             if (fS) fS[i] = v.y * psS;
         });
     } else {
         // forward FFT_L (input zero from L/2 on), times the chirp spectrum
-        pk_run<LOGL, false, true, false>(buf, T, lds, [&](int i, float2 v) { buf[pk_pad(i)] = v; });
+        pk_run<LOGL, false, true, false>(buf, T, lds, [&](int, int ip, float2 v) { buf[ip] = v; });
         __syncthreads();
         for (int i = threadIdx.x; i < L; i += NT) buf[pk_pad(i)] = cmul(buf[pk_pad(i)], __ldg(bt + i));
         __syncthreads();
         // inverse FFT_L, points below L/2 only; times the chirp, conjugated, to the two rings
-        pk_run<LOGL, true, false, true>(buf, T, lds, [&](int i, float2 v) {
+        pk_run<LOGL, true, false, true>(buf, T, lds, [&](int i, int, float2 v) {
             if (i < n) {
                 const float2 z = cconj(cmul(__ldg(ch + i), v));
                 fN[i] = z.x * psN;
@@ -341,14 +354,16 @@ __global__ void __launch_bounds__(PkCfg<LOGL>::NT, PkCfg<LOGL>::MINB)
 }
 
 // ------------------------------------------------------------------------------ analysis
-// the two rings of each pair -> F[map][m][pair][side], F(m) = c_m scale exp(-i m phi0) D[m mod n]
-// (conjugated above n/2); scale = 2 pi w_r / n (1 with unit_w; no 2 pi with HB_F_NO2PI);
-// c_m = 2 for m > 0 with mdouble (adjoint of the synthesis), else 1; HB_F_NOFOLD keeps m < n.
+// the two rings of each pair -> F[map][m][pair][side] (m-major, or blocked by 8 orders with
+// mblk: fg_off), F(m) = c_m scale exp(-i m phi0) D[m mod n] (conjugated above n/2);
+// scale = 2 pi w_r / n (1 with unit_w; no 2 pi with HB_F_NO2PI); c_m = 2 for m > 0 with mdouble
+// (adjoint of the synthesis), else 1; HB_F_NOFOLD keeps m < n.  Lanes take consecutive orders, so
+// in the blocked layout 8 lanes fill one 128-byte line.
 template <int LOGL, bool BLU>
 __global__ void __launch_bounds__(PkCfg<LOGL>::NT, PkCfg<LOGL>::MINB)
     ring_pair_analysis_kernel(GeomDev g, const int32_t *__restrict__ pairs, const float *__restrict__ maps,
                               int64_t map_stride, const double *__restrict__ w, float4 *__restrict__ Fm,
-                              int64_t fm_stride4, int mmax, int flags, int unit_w, int mdouble) {
+                              int64_t fm_stride4, int mmax, int flags, int unit_w, int mdouble, int mblk) {
     using C = PkCfg<LOGL>;
     constexpr int L = C::L, NT = C::NT;
     extern __shared__ __align__(16) float2 pk_smem[];
@@ -365,16 +380,16 @@ __global__ void __launch_bounds__(PkCfg<LOGL>::NT, PkCfg<LOGL>::MINB)
     const float2 *bt = BLU ? g.pkb_bt + g.pkb_bt_ofs[pair] : nullptr, *ch = BLU ? bt + L : nullptr;
     const PkMod mod2n{2 * n, 1.f / (float)(2 * n)};
     auto pidx = [&](int k) -> int { return BLU ? mod2n(s * k) : ((s * k) & (2 * n - 1)); };
-    auto sts = [&](int i, float2 v) { buf[pk_pad(i)] = v; };
-    auto ring = [&](int i) -> float2 { return make_float2(__ldg(fN + i), fS ? __ldg(fS + i) : 0.f); };
+    auto sts = [&](int, int ip, float2 v) { buf[ip] = v; };
+    auto ring = [&](int i, int = 0) -> float2 { return make_float2(__ldg(fN + i), fS ? __ldg(fS + i) : 0.f); };
     __syncthreads();  // tables
     if constexpr (!BLU) {
         pk_run<LOGL, false, false, false>(buf, T, ring, sts);
     } else {
         // forward FFT_L of the chirped ring (zero from n on; read below L/2 only), times the chirp
         // spectrum; inverse FFT_L, points below L/2 only
-        auto lds = [&](int i) -> float2 { return buf[pk_pad(i)]; };
-        auto ld0 = [&](int i) -> float2 { return i < n ? cmul(ring(i), __ldg(ch + i)) : make_float2(0.f, 0.f); };
+        auto lds = [&](int, int ip) -> float2 { return buf[ip]; };
+        auto ld0 = [&](int i, int) -> float2 { return i < n ? cmul(ring(i), __ldg(ch + i)) : make_float2(0.f, 0.f); };
         pk_run<LOGL, false, true, false>(buf, T, ld0, sts);
         __syncthreads();
         for (int i = threadIdx.x; i < L; i += NT) buf[pk_pad(i)] = cmul(buf[pk_pad(i)], __ldg(bt + i));
@@ -387,9 +402,10 @@ __global__ void __launch_bounds__(PkCfg<LOGL>::NT, PkCfg<LOGL>::MINB)
     const float scN = unit_w ? 1.f : (float)(sc2 * w[rN] / (double)n);
     const float scS = rS < 0 ? 0.f : (unit_w ? 1.f : (float)(sc2 * w[rS] / (double)n));
     const int mlim = (flags & HB_F_NOFOLD) ? min(mmax, n - 1) : mmax;
-    float4 *out = Fm + bm * fm_stride4 + pair;
+    float4 *out = Fm + bm * fm_stride4;
+    auto at = [&](int m) -> float4 & { return out[fg_off(m, pair, np, mblk != 0)]; };
     // HB_F_NOFOLD: the orders the ring does not resolve (m >= n) are zero, not left unwritten
-    for (int m = mlim + 1 + threadIdx.x; m <= mmax; m += NT) out[(int64_t)m * np] = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int m = mlim + 1 + threadIdx.x; m <= mmax; m += NT) at(m) = make_float4(0.f, 0.f, 0.f, 0.f);
     for (int k = threadIdx.x; k <= n / 2; k += NT) {
         const float2 zk = Zf(k), zc = k == 0 ? zk : Zf(n - k);
         // D_N = (Z[k] + conj Z[n-k]) / 2, D_S = (Z[k] - conj Z[n-k]) / (2 i)
@@ -400,14 +416,14 @@ __global__ void __launch_bounds__(PkCfg<LOGL>::NT, PkCfg<LOGL>::MINB)
         float sj = 1.f;
         for (int m = k; m <= mlim; m += n) {  // class k: (-1)^(s j) Y
             const float c = (mdouble && m > 0) ? 2.f * sj : sj;
-            out[(int64_t)m * np] = make_float4(c * yN.x, c * yN.y, c * yS.x, c * yS.y);
+            at(m) = make_float4(c * yN.x, c * yN.y, c * yS.x, c * yS.y);
             if (s & 1) sj = -sj;
         }
         if (k > 0 && 2 * k < n) {  // class n - k: (-1)^(s (j + 1)) conj Y
             sj = (s & 1) ? -1.f : 1.f;
             for (int m = n - k; m <= mlim; m += n) {
                 const float c = mdouble ? 2.f * sj : sj;
-                out[(int64_t)m * np] = make_float4(c * yN.x, -c * yN.y, c * yS.x, -c * yS.y);
+                at(m) = make_float4(c * yN.x, -c * yN.y, c * yS.x, -c * yS.y);
                 if (s & 1) sj = -sj;
             }
         }
@@ -465,7 +481,7 @@ struct PkAnaArgs {
     const double *w;
     float2 *Fm;
     int mmax, flags;
-    bool unit_w, mdouble;
+    bool unit_w, mdouble, mblk;
 };
 
 // (pair, map) grid, or (map, pair) with MAP_FAST (the Bluestein synthesis; see the file comment)
@@ -497,10 +513,10 @@ static int pk_ana_one(const GeomDev &g, const int32_t *pairs, int64_t cnt, const
     dim3 grid;
     if (!rc) rc = pk_grid<false>(cnt, a.nmaps, &grid);
     if (rc) return rc;
-    const int64_t fm4 = (int64_t)(a.mmax + 1) * g.npairs;
+    const int64_t fm4 = fg_rows(a.mmax, a.mblk) * g.npairs;
     ring_pair_analysis_kernel<LOGL, BLU><<<grid, PkCfg<LOGL>::NT, PkCfg<LOGL>::SMEM, st>>>(
-            g, pairs, a.maps, a.map_stride, a.w, reinterpret_cast<float4 *>(a.Fm), fm4, a.mmax, a.flags,
-            a.unit_w ? 1 : 0, a.mdouble ? 1 : 0);
+        g, pairs, a.maps, a.map_stride, a.w, reinterpret_cast<float4 *>(a.Fm), fm4, a.mmax, a.flags, a.unit_w ? 1 : 0,
+        a.mdouble ? 1 : 0, a.mblk ? 1 : 0);
     HB_CHECK_LAUNCH();
     return HB_OK;
 }
@@ -538,8 +554,8 @@ int launch_pk_synthesis(const GeomDev &g, int nmaps, const float2 *Gm, int mmax,
 }
 
 int launch_pk_analysis(const GeomDev &g, int nmaps, const float *maps, int64_t map_stride, const double *w,
-                       float2 *Fm, int mmax, int flags, bool unit_w, bool mdouble, cudaStream_t st) {
-    return pk_all(g, PkAnaArgs{nmaps, maps, map_stride, w, Fm, mmax, flags, unit_w, mdouble}, st);
+                       float2 *Fm, int mmax, int flags, bool unit_w, bool mdouble, cudaStream_t st, bool mblk) {
+    return pk_all(g, PkAnaArgs{nmaps, maps, map_stride, w, Fm, mmax, flags, unit_w, mdouble, mblk}, st);
 }
 
 }  // namespace hb
