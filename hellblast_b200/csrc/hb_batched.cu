@@ -92,15 +92,12 @@ __device__ __forceinline__ float block_pow2_scale(float vmax) {
     return res;
 }
 
-// The prep kernels turn runs of 8 consecutive K positions into the hi/lo rows of the K-major
-// core matrices (row n = 2 map + re/im; element (n, k) at (n%8)*8 + (n/8)*256 + (k/8)*64 + k%8),
-// written as 16-byte stores; a thread's re and im rows are adjacent and fill one 32-byte sector.
-// prep_alm_tiles_kernel: persistent CTAs walk the (m, map) slices of the batch operand (maps
-// fastest, so one m's tile rows are written together), two slices in flight: while the CTA
-// splits slice s out of one shared-memory buffer, cp.async copies slice s + gridDim.x into the
-// other (one pad entry per 16 so that the per-thread runs below hit distinct banks).  For each
-// slice the CTA takes the maximum |value| (the power-of-two scale of that (m, map)).  Map
-// columns past the group's maps get zeros.
+// The prep kernels (prep_alm_tiles_kernel, prep_f_tiles_kernel) turn runs of 8 consecutive K
+// positions into the hi/lo rows of the K-major core matrices (row n = 2 map + re/im; element
+// (n, k) at (n%8)*8 + (n/8)*256 + (k/8)*64 + k%8), written as 16-byte stores.  Rows 8j .. 8j+7
+// (maps 4j .. 4j+3) of one k8 group are one 128-byte segment, so both kernels work on quads of
+// maps and let 4 lanes write one segment's interleaved rows in the same instruction (scattered
+// 16-byte stores from separate instructions cost one L2 request each and ran at half the rate).
 template <bool BF16>
 __device__ __forceinline__ void store_rows8(uint4 *chunk, int N, int qh, int n, int g, const float (&v)[8]) {
     uint4 hi, lo;
@@ -110,73 +107,103 @@ __device__ __forceinline__ void store_rows8(uint4 *chunk, int N, int qh, int n, 
     chunk[(e + (int64_t)N * 32) / 8] = lo;
 }
 
-constexpr int PREP_THREADS = 512;
-template <int N> __host__ __device__ constexpr int prep_slices(int mmax) { return (mmax + 1) * (N / 2); }
-
-// alm [map][nalm] complex64 -> per (m, 64-l chunk) the synthesis B tiles:
-// [q][h][N rows x 32 K (l = l0 + 2k + q)].  Slice = (m, map): alm l = m .. lmax, padded to
-// whole 64-l chunks; l - m = i at i + i / 16 in the buffer (68 entries per chunk).  alm columns
-// start on 8-byte boundaries, so the copies are 8-byte cp.async.
+// alm [map][nalm] complex64 -> per (m, 64-l chunk) the synthesis B tiles
+// [q][h][N rows x 32 K (l = l0 + 2k + q)], chunks of m covering l = m .. lmax (zero past lmax).
+// Work item = (m, quad of 4 maps): the 4 maps' rows of one (chunk, k8 group, q, h) are one
+// 128-byte segment of the tile.  F16: a first sweep over the item's alm takes the maximum |value|
+// per (m, map) (the power-of-two scale, as block_pow2_scale); BF16 uses scale 1 (a power-of-two
+// scale would change no bit of the result).  Then the item's l range streams through shared
+// memory in stages of PA_L values of its 4 maps (8-byte cp.async, alm rows start on 8-byte
+// boundaries; two stages in flight).  Thread (k8 group, parity q, map) turns its 8 values of one
+// parity into the hi/lo rows 2 map (re) and 2 map + 1 (im), so the 4 lanes of one (k8 group, q)
+// write the interleaved rows of one tile segment in the same instruction.  Shared-memory slot of
+// (map, i = l - m - stage start): map * PA_MS + i + 2 (i / 16), which puts the 16 lanes of a
+// half-warp (4 maps x 2 parities x 2 k8 groups) on distinct banks.  Map columns past the group's
+// maps get zeros.
+constexpr int PA_THREADS = 256, PA_L = 512, PA_MAPS = 4;
+constexpr int PA_MS = 580;  // >= PA_L + 2 * (PA_L / 16) entries per map, = 4 mod 16
+constexpr int PA_STAGE = PA_MAPS * PA_MS;
+constexpr int PA_SMEM = 2 * PA_STAGE * (int)sizeof(float2);
+__device__ __forceinline__ int pa_slot(int map, int i) { return map * PA_MS + i + 2 * (i >> 4); }
 template <int N, bool BF16>
-__global__ void __launch_bounds__(PREP_THREADS, 2) prep_alm_tiles_kernel(const TcGroup *groups, int gi,
-                                                                         const float2 *__restrict__ alm,
-                                                                         int64_t alm_stride, int dbl) {
+__global__ void __launch_bounds__(PA_THREADS, 4) prep_alm_tiles_kernel(const TcGroup *groups, int gi,
+                                                                       const float2 *__restrict__ alm,
+                                                                       int64_t alm_stride) {
+    static_assert(PA_THREADS == 8 * 32 && PA_L == 32 * 16 && PA_MAPS == 4, "lane = (k8 group, parity, map)");
+    static_assert(PA_MS >= PA_L + 2 * (PA_L / 16) && PA_MS % 16 == 4, "map stride");
+    static_assert((N / 2) % PA_MAPS == 0, "whole map quads");
     extern __shared__ float2 sa[];
+    __shared__ float red[PA_THREADS / 32][PA_MAPS];
+    __shared__ float scl[PA_MAPS];
     const TcGroup &G = groups[gi];
-    const int lmax = G.lmax, ns = prep_slices<N>(G.mmax);
-    const int per = ((lmax + 64) / 64) * 68;  // one buffer: the largest slice (m = 0)
-    auto issue = [&](int s, float2 *dst) {
-        const int m = s / (N / 2), b = s % (N / 2);
-        const int nch = (lmax - m + 64) / 64;
-        const bool live = b < G.nmaps;
-        const float2 *src = alm + (int64_t)b * alm_stride + alm_idx(lmax, m, m);
-        for (int i = threadIdx.x; i < nch * 64; i += blockDim.x) {
-            float2 *d = dst + i + (i >> 4);
-            if (live && m + i <= lmax)
-                tc::cp_async8(d, src + i);
-            else
-                *d = make_float2(0.f, 0.f);
-        }
-    };
-    int s = blockIdx.x, buf = 0;
-    if (dbl && s < ns) issue(s, sa);
-    tc::cp_async_commit();
-    for (; s < ns; s += gridDim.x, buf ^= dbl) {
-        const int sn = s + gridDim.x;
-        if (!dbl) issue(s, sa);  // single buffer: this slice now
-        else if (sn < ns) issue(sn, sa + (buf ^ 1) * per);
-        tc::cp_async_commit();
-        if (dbl) tc::cp_async_wait<1>(); else tc::cp_async_wait<0>();
-        __syncthreads();
-        const int m = s / (N / 2), b = s % (N / 2);
-        const int nch = (lmax - m + 64) / 64;
-        const float2 *cur = sa + buf * per;
-        float vmax = 0.f;
-        for (int i = threadIdx.x; i < nch * 64; i += blockDim.x) {
-            const float2 v = cur[i + (i >> 4)];
-            vmax = fmaxf(vmax, fmaxf(fabsf(v.x), fabsf(v.y)));
-        }
-        const float sc = block_pow2_scale(vmax);
-        if (threadIdx.x == 0) G.dscale[(int64_t)m * (N / 2) + b] = sc;
-        uint4 *base = const_cast<uint4 *>(G.alm_tiles) + G.alm_tile_ofs[m] * (16 * N);
-        for (int it = threadIdx.x; it < nch * 4; it += blockDim.x) {  // (chunk c, k8 group g): l = l0 + 16 g + 0..15
-            const int c = it >> 2, g = it & 3;
-            const float2 *run = cur + 17 * it;  // 16 (it) + it
-            uint4 *chunk = base + (int64_t)c * (16 * N);
+    const int lmax = G.lmax, nq = (N / 2) / PA_MAPS, items = (G.mmax + 1) * nq;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int bl = lane & 3, q = (lane >> 2) & 1, gl = 4 * warp + (lane >> 3);  // map, parity, k8 group
+    for (int item = blockIdx.x; item < items; item += gridDim.x) {
+        const int m = item / nq, b0 = (item % nq) * PA_MAPS, b = b0 + bl;
+        const int nl = lmax - m + 1, nch = (lmax - m + 64) / 64, nstage = (nch * 64 + PA_L - 1) / PA_L;
+        const float2 *src = alm + (int64_t)b0 * alm_stride + alm_idx(lmax, m, m);  // map bb at + bb alm_stride
+        float sc = 1.f;
+        if constexpr (!BF16) {
+            float vmax[PA_MAPS];
 #pragma unroll
-            for (int q = 0; q < 2; ++q) {
+            for (int bb = 0; bb < PA_MAPS; ++bb) {
+                vmax[bb] = 0.f;
+                if (b0 + bb < G.nmaps)
+                    for (int i = threadIdx.x; i < nl; i += PA_THREADS) {
+                        const float2 v = __ldg(src + (int64_t)bb * alm_stride + i);
+                        vmax[bb] = fmaxf(vmax[bb], fmaxf(fabsf(v.x), fabsf(v.y)));
+                    }
+                for (int o = 16; o >= 1; o >>= 1) vmax[bb] = fmaxf(vmax[bb], __shfl_xor_sync(0xffffffffu, vmax[bb], o));
+                if (lane == 0) red[warp][bb] = vmax[bb];
+            }
+            __syncthreads();
+            if (threadIdx.x < PA_MAPS) {
+                float v = 0.f;
+                for (int w = 0; w < PA_THREADS / 32; ++w) v = fmaxf(v, red[w][threadIdx.x]);
+                int e = 0;
+                if (v > 0.f) frexpf(v, &e);  // v in [2^(e-1), 2^e): scaled to [2^13, 2^14)
+                scl[threadIdx.x] = v > 0.f ? ldexpf(1.0f, 14 - e) : 1.0f;
+            }
+            __syncthreads();
+            sc = scl[bl];
+        }
+        if (threadIdx.x < PA_MAPS) G.dscale[(int64_t)m * (N / 2) + b0 + threadIdx.x] = BF16 ? 1.f : scl[threadIdx.x];
+        uint4 *base = const_cast<uint4 *>(G.alm_tiles) + G.alm_tile_ofs[m] * (16 * N);
+        auto issue = [&](int stg, float2 *dst) {  // one commit group: t = (map, i)
+            for (int t = threadIdx.x; t < PA_MAPS * PA_L; t += PA_THREADS) {
+                const int bb = t / PA_L, il = t % PA_L, i = stg * PA_L + il;
+                float2 *d = dst + pa_slot(bb, il);
+                if (b0 + bb < G.nmaps && i < nl)
+                    tc::cp_async8(d, src + (int64_t)bb * alm_stride + i);
+                else
+                    *d = make_float2(0.f, 0.f);
+            }
+        };
+        issue(0, sa);
+        tc::cp_async_commit();
+        for (int stg = 0; stg < nstage; ++stg) {
+            const float2 *cur = sa + (stg & 1) * PA_STAGE;
+            if (stg + 1 < nstage) issue(stg + 1, sa + ((stg + 1) & 1) * PA_STAGE);
+            tc::cp_async_commit();
+            tc::cp_async_wait<1>();  // all groups but the one just committed: stage stg is in
+            __syncthreads();
+            const int i0 = stg * PA_L + 16 * gl;  // l - m of this k8 group's first value
+            if (i0 < nch * 64) {
+                const int c = i0 >> 6, g = (i0 >> 4) & 3;
+                uint4 *chunk = base + (int64_t)c * (16 * N);
                 float re[8], im[8];
 #pragma unroll
                 for (int k = 0; k < 8; ++k) {
-                    const float2 v = run[2 * k + q];
+                    const float2 v = cur[pa_slot(bl, 16 * gl + 2 * k + q)];
                     re[k] = v.x * sc;
                     im[k] = v.y * sc;
                 }
                 store_rows8<BF16>(chunk, N, q, 2 * b, g, re);
                 store_rows8<BF16>(chunk, N, q, 2 * b + 1, g, im);
             }
+            __syncthreads();  // every thread is done with this stage's buffer before it is refilled
         }
-        __syncthreads();  // every thread is done with this buffer before it is refilled
     }
     tc::cp_async_wait<0>();
 }
@@ -1054,12 +1081,9 @@ static int max_smem_optin_b() {
 template <int N, bool BF16>
 static int launch_prep_alm(hb_batched_plan *bp, int gi, const float2 *alm, int64_t stride, cudaStream_t st) {
     const TcGroup &G = bp->hgroups[gi];
-    const size_t one = sizeof(float2) * (size_t)(((G.lmax + 64) / 64) * 68);  // 64 l + 4 pads per chunk
-    const int dbl = 2 * one <= (size_t)max_smem_optin_b() ? 1 : 0;
-    const int smem = (int)(one * (dbl ? 2 : 1));
-    HB_CUDA_TRY(cudaFuncSetAttribute(prep_alm_tiles_kernel<N, BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
-    const int grid = std::min(prep_slices<N>(G.mmax), sm_count() * 2);
-    prep_alm_tiles_kernel<N, BF16><<<grid, PREP_THREADS, smem, st>>>(bp->dgroups, gi, alm, stride, dbl);
+    HB_CUDA_TRY(cudaFuncSetAttribute(prep_alm_tiles_kernel<N, BF16>, cudaFuncAttributeMaxDynamicSharedMemorySize, PA_SMEM));
+    const int grid = std::min((G.mmax + 1) * (N / 2 / PA_MAPS), sm_count() * 4);
+    prep_alm_tiles_kernel<N, BF16><<<grid, PA_THREADS, PA_SMEM, st>>>(bp->dgroups, gi, alm, stride);
     HB_CHECK_LAUNCH();
     return HB_OK;
 }
