@@ -24,10 +24,11 @@
 // the shared buffer (fused into a pass, its 16 global loads per thread spill registers).
 //
 // Grid: (pair, map), so the CTAs in flight work on runs of neighbouring pairs of one map and
-// their strided 16-byte coefficient accesses fill whole sectors, except for the Bluestein
-// synthesis: (map, pair), so all maps of a pair run together and read that pair's tables once
-// from DRAM (measured at nside 2048, 64 maps: the synthesis 2.5 ms faster per direction this way,
-// the analysis 2.1 ms slower).
+// their strided 16-byte coefficient accesses fill whole sectors of the m-major G / F, except for
+// the Bluestein pairs of the synthesis and of the m-blocked analysis (fg_off; one CTA fills each
+// 128-byte line there): (map, pair), so all maps of a pair run together and read that pair's
+// tables once from DRAM.  Measured at nside 2048, 64 maps: the Bluestein synthesis 2.5 ms faster
+// per direction this way; the m-major analysis 2.1 ms slower, the m-blocked one 2.5 ms faster.
 //
 // Packing: the two real rings of a pair form one complex sequence z_j = f_N[j] + i f_S[j],
 // j < n, transformed by one complex FFT of length n.  Synthesis builds the spectrum Z of z from
@@ -368,7 +369,8 @@ __global__ void __launch_bounds__(PkCfg<LOGL>::NT, PkCfg<LOGL>::MINB)
     constexpr int L = C::L, NT = C::NT;
     extern __shared__ __align__(16) float2 pk_smem[];
     float2 *buf = pk_smem;
-    const int pair = pairs[blockIdx.x], bm = blockIdx.y;
+    const bool mf = BLU && mblk;
+    const int pair = pairs[mf ? blockIdx.y : blockIdx.x], bm = mf ? blockIdx.x : blockIdx.y;
     const int rN = g.pair_ring[2 * pair], rS = g.pair_ring[2 * pair + 1];
     const int n = BLU ? g.nphi[rN] : L;
     const PkTab T = pk_tables<LOGL>(pk_smem + C::BUF, n);
@@ -484,7 +486,8 @@ struct PkAnaArgs {
     bool unit_w, mdouble, mblk;
 };
 
-// (pair, map) grid, or (map, pair) with MAP_FAST (the Bluestein synthesis; see the file comment)
+// (pair, map) grid, or (map, pair) with MAP_FAST (Bluestein pairs: the synthesis and the m-blocked
+// analysis; see the file comment)
 template <bool MAP_FAST> static int pk_grid(int64_t cnt, int nmaps, dim3 *grid) {
     const int64_t y = MAP_FAST ? cnt : nmaps;
     if (y > 65535 || cnt > INT32_MAX || nmaps <= 0)
@@ -511,7 +514,7 @@ template <int LOGL, bool BLU>
 static int pk_ana_one(const GeomDev &g, const int32_t *pairs, int64_t cnt, const PkAnaArgs &a, cudaStream_t st) {
     int rc = pk_prepare<LOGL, BLU>();
     dim3 grid;
-    if (!rc) rc = pk_grid<false>(cnt, a.nmaps, &grid);
+    if (!rc) rc = (BLU && a.mblk) ? pk_grid<true>(cnt, a.nmaps, &grid) : pk_grid<false>(cnt, a.nmaps, &grid);
     if (rc) return rc;
     const int64_t fm4 = fg_rows(a.mmax, a.mblk) * g.npairs;
     ring_pair_analysis_kernel<LOGL, BLU><<<grid, PkCfg<LOGL>::NT, PkCfg<LOGL>::SMEM, st>>>(
