@@ -1069,15 +1069,6 @@ static int launch_ana(hb_batched_plan *bp, float2 *alm_out, const float *fl, cud
 }
 // prep launch: persistent CTAs (one or two per SM), two slice buffers when they fit in shared
 // memory, else one
-static int max_smem_optin_b() {
-    static int v = -1;
-    if (v < 0) {
-        int dev = 0;
-        cudaGetDevice(&dev);
-        if (cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) v = 48 * 1024;
-    }
-    return v;
-}
 template <int N, bool BF16>
 static int launch_prep_alm(hb_batched_plan *bp, int gi, const float2 *alm, int64_t stride, cudaStream_t st) {
     const TcGroup &G = bp->hgroups[gi];

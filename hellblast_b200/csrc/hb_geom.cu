@@ -197,7 +197,8 @@ static int finish_geom(HostGeom &h, int64_t nside, const std::vector<double> &xn
                     bt_n.push_back(h.nphi[rn]);
                     bt_logL.push_back(lg);
                     bt_ofs.push_back(bt_total);
-                    bt_total += (int64_t(3) << lg) / 2;  // chirp spectrum (L) and chirp (L/2)
+                    // chirp spectrum (L), chirp (L/2), phase block; offsets stay even (16-byte aligned)
+                    bt_total += ((int64_t(3) << lg) / 2 + pk_phase_entries(lg) + 1) & ~int64_t(1);
                 }
                 pkb_ofs[p] = it->second;
             }
@@ -243,6 +244,12 @@ static int finish_geom(HostGeom &h, int64_t nside, const std::vector<double> &xn
            o_cp = carve(4 * (size_t)np), o_pk = carve(4 * (size_t)np), o_rest = carve(4 * (size_t)np),
            o_pkbo = carve(8 * (size_t)np), o_bt = carve(8 * (size_t)(bt_total + 1)),
            o_btn = carve(4 * (bt_n.size() + 1)), o_btl = carve(4 * (bt_n.size() + 1)), o_bto = carve(8 * (bt_n.size() + 1));
+    int64_t tw_ofs[PK_MAX_LOG + 1] = {}, tw_total = 0;  // pair-packed table blocks per length class
+    for (int lg = PK_MIN_LOG; lg <= PK_MAX_LOG; ++lg) {
+        tw_ofs[lg] = tw_total;
+        tw_total += (pk_tab_entries(lg) + 1) & ~int64_t(1);
+    }
+    const size_t o_ptw = carve(8 * (size_t)tw_total);
     char *base = nullptr;
     if (cudaMalloc(&base, total) != cudaSuccess) {
         cudaGetLastError();
@@ -271,6 +278,8 @@ static int finish_geom(HostGeom &h, int64_t nside, const std::vector<double> &xn
     for (size_t c = 0; c < pk_logn.size(); ++c) { d.pk_logn[c] = pk_logn[c]; d.pk_first[c] = pk_first[c]; }
     d.pk_first[pk_logn.size()] = pk_first.back();
     d.pkb_bt = (float2 *)(base + o_bt); d.pkb_bt_ofs = (int64_t *)(base + o_pkbo);
+    d.pk_tw = (float2 *)(base + o_ptw);
+    for (int lg = 0; lg <= PK_MAX_LOG; ++lg) d.pk_tw_ofs[lg] = tw_ofs[lg];
     d.rest_pairs = (int32_t *)(base + o_rest); d.rest_n_cls = (int)rest_L.size();
     for (size_t c = 0; c < rest_L.size(); ++c) { d.rest_L[c] = rest_L[c]; d.rest_first[c] = rest_first[c]; }
     d.rest_first[rest_L.size()] = rest_first.back();
@@ -300,6 +309,9 @@ static int finish_geom(HostGeom &h, int64_t nside, const std::vector<double> &xn
     if (rc == HB_OK && !bt_n.empty())
         rc = build_pk_chirp_tables(d, (int)bt_n.size(), (const int32_t *)(base + o_btn), (const int32_t *)(base + o_btl),
                                    (const int64_t *)(base + o_bto), pk_max_log, d.pkb_bt, 0);
+    if (rc == HB_OK)
+        rc = build_pk_tables(d, (int)bt_n.size(), (const int32_t *)(base + o_btn), (const int32_t *)(base + o_btl),
+                             (const int64_t *)(base + o_bto), 0);
     if (rc == HB_OK && cudaStreamSynchronize(0) != cudaSuccess) rc = fail(HB_ERR_CUDA, "hb_geom: table build failed");
     if (rc != HB_OK) {
         cudaFree(base);

@@ -115,8 +115,14 @@ struct GeomDev {
     int pk_n_cls;
     int pk_logn[16];
     int64_t pk_first[17];
-    float2 *pkb_bt;        // pair-packed Bluestein tables: chirp spectrum (L) then chirp (L/2) per n
+    // pair-packed Bluestein tables per distinct n: chirp spectrum (L), chirp (L/2), then the
+    // phase block of the CTA table (pk_phase_entries)
+    float2 *pkb_bt;
     int64_t *pkb_bt_ofs;   // [npairs] offset of the pair's table in pkb_bt (-1: not Bluestein)
+    // per transform length 2^k, k in [PK_MIN_LOG, PK_MAX_LOG]: the pair-packed kernels' shared
+    // table block (twiddles, then the phases for n = 2^k), copied by every CTA (pk_tab_entries)
+    float2 *pk_tw;
+    int64_t pk_tw_ofs[PK_MAX_LOG + 1];
     int32_t *rest_pairs;   // [npairs]
     int rest_n_cls;
     int rest_L[32];
@@ -190,6 +196,14 @@ bool pk_pair_ok(int nphiN, int nphiS, double phi0N_pi, double phi0S_pi, int *log
 // for ring length ns[e] at out + ofs[e] (device arrays); FP64 computed, FP32 stored
 int build_pk_chirp_tables(const GeomDev &g, int count, const int32_t *ns, const int32_t *logL, const int64_t *ofs,
                           int max_logL, float2 *out, cudaStream_t st);
+// the pair-packed kernels' table blocks: entries of the block for transform length 2^logL
+// (twiddles and phases) and of its phase part (one per Bluestein ring length)
+int64_t pk_tab_entries(int logL);
+int64_t pk_phase_entries(int logL);
+// fills g.pk_tw (every length class) and the phase part of each Bluestein table (count tables as
+// for build_pk_chirp_tables, phase block at ofs[e] + 3 L / 2)
+int build_pk_tables(const GeomDev &g, int count, const int32_t *ns, const int32_t *logL, const int64_t *ofs,
+                    cudaStream_t st);
 int launch_pk_synthesis(const GeomDev &g, int nmaps, const float2 *Gm, int mmax, float *maps, int64_t map_stride,
                         const double *w, bool apply_w, bool mdouble, int flags, cudaStream_t st);
 int launch_pk_analysis(const GeomDev &g, int nmaps, const float *maps, int64_t map_stride, const double *w,

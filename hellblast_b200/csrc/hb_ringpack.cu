@@ -49,9 +49,10 @@
 // holds 16 points per pass (one radix-16 butterfly, or 16/R small ones), so the transform runs
 // in place in one shared buffer: all loads of a pass, a barrier, then the stores.  Natural order
 // in and out: the analysis's first pass reads the two rings straight from global memory and the
-// synthesis's last pass writes them (both coalesced, lanes on consecutive pixels).  Twiddles and
-// the phi0 phases are products of two entries of small per-CTA tables (64 fine steps times
-// coarse steps, FP64-computed).
+// synthesis's last pass writes them (both coalesced, lanes on consecutive pixels).  Twiddles come
+// from direct tables of W_L^e and W_L^(4e), the phi0 phases from products of two entries of a
+// fine and a coarse table; both are FP64-computed once per geometry and copied into every CTA's
+// shared memory (PkTab).
 #include <algorithm>
 #include <cmath>
 #include <type_traits>
@@ -76,7 +77,9 @@ template <int LOGL> struct PkCfg {
     static constexpr int TWP = TW + TW / 16; // ... stored at e + e/16 (pk_pad), see PkTab
     static constexpr int TWS = R1 < 16 ? 16 * R1 : 0;  // pass-1 twiddles W_(16 R1)^(j t), j < 16, t < R1
     static constexpr int PHC = 2 * L / 64;   // coarse phase entries exp(i pi 64 c / n), 2n <= 2L
-    static constexpr int SMEM = (BUF + 2 * TWP + TWS + 64 + PHC) * (int)sizeof(float2);
+    static constexpr int TWB = 2 * TWP + TWS;  // twiddle part of the table block
+    static constexpr int TAB = TWB + 64 + PHC; // table block: twiddles, then phases
+    static constexpr int SMEM = (BUF + TAB) * (int)sizeof(float2);
     static constexpr int MINB = 65536 / (NT * 64) > 0 ? 65536 / (NT * 64) : 1;  // <= 64 registers
 };
 
@@ -96,33 +99,40 @@ struct PkTab {
     __device__ __forceinline__ float2 ph(int e) const { return cmul(phf[e & 63], phc[e >> 6]); }
 };
 
-// per-CTA tables (FP64-computed, rounded to FP32): twiddles of length L, phases
-// exp(i pi e / n) for the ring length n
-template <int LOGL> __device__ __forceinline__ PkTab pk_tables(float2 *base, int n) {
+// Entry i of the table block of transform length L = 2^LOGL (FP64-computed, rounded to FP32):
+// tw1 and tw4 (entry e at pk_pad(e); slot 16 of every 17, which pk_pad skips, holds zero), the
+// pass-1 table, then the phase block for ring length n (pk_phase_entry).  Built once per geometry
+// (build_pk_tables); every CTA copies its block into shared memory (pk_tables).
+__device__ __forceinline__ float2 pk_phase_entry(int i, int n) {  // exp(i pi e / n): e = i < 64, or 64 (i - 64)
+    double sn, cs;
+    sincospi((double)(i < 64 ? i : 64 * (i - 64)) / (double)n, &sn, &cs);
+    return make_float2((float)cs, (float)sn);
+}
+template <int LOGL> __device__ __forceinline__ float2 pk_table_entry(int i, int n) {
+    using C = PkCfg<LOGL>;
+    double sn = 0.0, cs = 0.0;
+    if (i < 2 * C::TWP) {  // W_L^e (first block), W_L^(4e) (second)
+        const int slot = i % C::TWP, r = slot % 17;
+        if (r == 16) return make_float2(0.f, 0.f);
+        const int e = 16 * (slot / 17) + r;
+        sincospi(-2.0 * (double)(i < C::TWP ? e : 4 * e) / (double)C::L, &sn, &cs);
+    } else if (i < C::TWB) {  // W_(16 R1)^(j t)
+        const int j = (i - 2 * C::TWP) / C::R1, t = (i - 2 * C::TWP) % C::R1;
+        sincospi(-2.0 * (double)(j * t) / (double)(16 * C::R1), &sn, &cs);
+    } else {
+        return pk_phase_entry(i - C::TWB, n);
+    }
+    return make_float2((float)cs, (float)sn);
+}
+
+// the CTA's table block: the twiddles of length L from gtw (the geometry's block for L), the
+// phases exp(i pi e / n) from gph (a Bluestein ring's phase block) or, for n = L, from gtw
+__device__ __forceinline__ float2 pk_ld(const float2 *p) { return __ldg(p); }
+template <int LOGL>
+__device__ __forceinline__ PkTab pk_tables(float2 *base, const float2 *__restrict__ gtw, const float2 *__restrict__ gph) {
     using C = PkCfg<LOGL>;
     float2 *tw1 = base, *tw4 = tw1 + C::TWP, *tws = tw4 + C::TWP, *phf = tws + C::TWS, *phc = phf + 64;
-    const double L = (double)C::L, dn = (double)n;
-    constexpr int E1 = 2 * C::TW, E2 = E1 + C::TWS, E3 = E2 + 64, E4 = E3 + C::PHC;
-    for (int i = threadIdx.x; i < E4; i += C::NT) {
-        double sn, cs;
-        float2 *dst;
-        if (i < E1) {  // W_L^e, W_L^(4e)
-            const int e = i < C::TW ? i : i - C::TW;
-            sincospi(-2.0 * (double)(i < C::TW ? e : 4 * e) / L, &sn, &cs);
-            dst = (i < C::TW ? tw1 : tw4) + pk_pad(e);
-        } else if (i < E2) {  // W_(16 R1)^(j t)
-            const int j = (i - E1) / C::R1, t = (i - E1) % C::R1;
-            sincospi(-2.0 * (double)(j * t) / (double)(16 * C::R1), &sn, &cs);
-            dst = tws + (i - E1);
-        } else if (i < E3) {  // exp(i pi e / n), e < 64
-            sincospi((double)(i - E2) / dn, &sn, &cs);
-            dst = phf + (i - E2);
-        } else {  // exp(i pi 64 c / n), 64 c < 2n <= 2L
-            sincospi((double)(64 * (i - E3)) / dn, &sn, &cs);
-            dst = phc + (i - E3);
-        }
-        *dst = make_float2((float)cs, (float)sn);
-    }
+    for (int i = threadIdx.x; i < C::TAB; i += C::NT) base[i] = pk_ld((gph && i >= C::TWB) ? gph + (i - C::TWB) : gtw + i);
     return {tw1, tw4, tws, phf, phc};
 }
 
@@ -247,12 +257,13 @@ __global__ void __launch_bounds__(PkCfg<LOGL>::NT, PkCfg<LOGL>::MINB)
     const int pair = pairs[BLU ? blockIdx.y : blockIdx.x], bm = BLU ? blockIdx.x : blockIdx.y;
     const int rN = g.pair_ring[2 * pair], rS = g.pair_ring[2 * pair + 1];
     const int n = BLU ? g.nphi[rN] : L;
-    const PkTab T = pk_tables<LOGL>(pk_smem + C::BUF, n);
+    // Bluestein tables: chirp spectrum bt[0, L), chirp ch[t] = exp(-i pi t^2 / n) for t < n, then
+    // the ring's phase block
+    const float2 *bt = BLU ? g.pkb_bt + g.pkb_bt_ofs[pair] : nullptr, *ch = BLU ? bt + L : nullptr;
+    const PkTab T = pk_tables<LOGL>(pk_smem + C::BUF, g.pk_tw + g.pk_tw_ofs[LOGL], BLU ? bt + L + L / 2 : nullptr);
     const int s = (flags & HB_F_NOPHASE) ? 0 : pk_shift(g.phi0_pi[rN], n);
     const int64_t np = g.npairs;
     const float4 *gin = Gm + bm * gm_stride4 + pair;  // (m, pair) entry at gin[m * np]
-    // Bluestein tables: chirp spectrum bt[0, L), chirp ch[t] = exp(-i pi t^2 / n) for t < n
-    const float2 *bt = BLU ? g.pkb_bt + g.pkb_bt_ofs[pair] : nullptr, *ch = BLU ? bt + L : nullptr;
     const float dbl = mdouble ? 2.f : 1.f, chalf = 0.5f * dbl;
     const float sg = (s & 1) ? -1.f : 1.f;
     const bool hasS = rS >= 0;
@@ -373,13 +384,14 @@ __global__ void __launch_bounds__(PkCfg<LOGL>::NT, PkCfg<LOGL>::MINB)
     const int pair = pairs[mf ? blockIdx.y : blockIdx.x], bm = mf ? blockIdx.x : blockIdx.y;
     const int rN = g.pair_ring[2 * pair], rS = g.pair_ring[2 * pair + 1];
     const int n = BLU ? g.nphi[rN] : L;
-    const PkTab T = pk_tables<LOGL>(pk_smem + C::BUF, n);
+    // Bluestein tables: chirp spectrum bt[0, L), chirp ch[t] = exp(-i pi t^2 / n) for t < n, then
+    // the ring's phase block
+    const float2 *bt = BLU ? g.pkb_bt + g.pkb_bt_ofs[pair] : nullptr, *ch = BLU ? bt + L : nullptr;
+    const PkTab T = pk_tables<LOGL>(pk_smem + C::BUF, g.pk_tw + g.pk_tw_ofs[LOGL], BLU ? bt + L + L / 2 : nullptr);
     const int s = (flags & HB_F_NOPHASE) ? 0 : pk_shift(g.phi0_pi[rN], n);
     const int64_t np = g.npairs;
     const float *fN = maps + bm * map_stride + g.ofs[rN];
     const float *fS = rS >= 0 ? maps + bm * map_stride + g.ofs[rS] : nullptr;
-    // Bluestein tables: chirp spectrum bt[0, L), chirp ch[t] = exp(-i pi t^2 / n) for t < n
-    const float2 *bt = BLU ? g.pkb_bt + g.pkb_bt_ofs[pair] : nullptr, *ch = BLU ? bt + L : nullptr;
     const PkMod mod2n{2 * n, 1.f / (float)(2 * n)};
     auto pidx = [&](int k) -> int { return BLU ? mod2n(s * k) : ((s * k) & (2 * n - 1)); };
     auto sts = [&](int, int ip, float2 v) { buf[ip] = v; };
@@ -559,6 +571,48 @@ int launch_pk_synthesis(const GeomDev &g, int nmaps, const float2 *Gm, int mmax,
 int launch_pk_analysis(const GeomDev &g, int nmaps, const float *maps, int64_t map_stride, const double *w,
                        float2 *Fm, int mmax, int flags, bool unit_w, bool mdouble, cudaStream_t st, bool mblk) {
     return pk_all(g, PkAnaArgs{nmaps, maps, map_stride, w, Fm, mmax, flags, unit_w, mdouble, mblk}, st);
+}
+
+
+// ------------------------------------------------------------------------------ table blocks
+int64_t pk_tab_entries(int logL) {
+    switch (logL) {
+#define HB_PK_TAB(LG) \
+    case LG:          \
+        return PkCfg<LG>::TAB;
+        HB_PK_TAB(9) HB_PK_TAB(10) HB_PK_TAB(11) HB_PK_TAB(12) HB_PK_TAB(13) HB_PK_TAB(14)
+#undef HB_PK_TAB
+        default:
+            return 0;
+    }
+}
+int64_t pk_phase_entries(int logL) { return 64 + 2 * (int64_t(1) << logL) / 64; }
+
+template <int LOGL> __global__ void __launch_bounds__(256) pk_twtab_kernel(float2 *out) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < PkCfg<LOGL>::TAB; i += gridDim.x * blockDim.x)
+        out[i] = pk_table_entry<LOGL>(i, PkCfg<LOGL>::L);
+}
+// one CTA per Bluestein table: its ring's phase block at ofs[e] + 3 L / 2
+__global__ void __launch_bounds__(256) pk_phtab_kernel(const int32_t *__restrict__ ns, const int32_t *__restrict__ logLs,
+                                                       const int64_t *__restrict__ ofs, float2 *out) {
+    const int e = blockIdx.x, n = ns[e], L = 1 << logLs[e];
+    const int cnt = 64 + 2 * L / 64;
+    float2 *dst = out + ofs[e] + 3 * (int64_t)L / 2;
+    for (int i = threadIdx.x; i < cnt; i += blockDim.x) dst[i] = pk_phase_entry(i, n);
+}
+
+int build_pk_tables(const GeomDev &g, int count, const int32_t *ns, const int32_t *logL, const int64_t *ofs,
+                    cudaStream_t st) {
+#define HB_PK_TW(LG)                                                                                   \
+    pk_twtab_kernel<LG><<<(PkCfg<LG>::TAB + 255) / 256, 256, 0, st>>>(g.pk_tw + g.pk_tw_ofs[LG]); \
+    HB_CHECK_LAUNCH();
+    HB_PK_TW(9) HB_PK_TW(10) HB_PK_TW(11) HB_PK_TW(12) HB_PK_TW(13) HB_PK_TW(14)
+#undef HB_PK_TW
+    if (count > 0) {
+        pk_phtab_kernel<<<count, 256, 0, st>>>(ns, logL, ofs, g.pkb_bt);
+        HB_CHECK_LAUNCH();
+    }
+    return HB_OK;
 }
 
 }  // namespace hb
