@@ -643,19 +643,25 @@ def main():
                   "tensor_achieved_executed": 2 * executed / t_dom / 1e12,
                   "tensor_frac_executed": 2 * executed / t_dom / 1e12 / bf16_peak}
         # the ring FFTs (one launch per FFT-length class and direction; a "launch" below is the
-        # whole direction, all its class launches): HBM-bound
+        # whole direction, all its class launches) and the tile preps: HBM-bound
         traffic = load_traffic()
         fft_bytes = hbm_bytes_ring_fft(B, mmax, g.npairs, npix)
+        hbm_src = "MEASURED_PEAKS.json hbm_gbs, of measured" if peaks else "fallback 6650 GB/s, of fallback"
         stage_roof = {"tensor_legendre": tensor}
-        for key, kern in (("ring_synthesis", "ring_synthesis_kernel<float>"),
-                          ("ring_analysis", "ring_analysis_kernel<float>")):
+        for key, kern in (("ring_synthesis", "ring_pair_synthesis_kernel + ring_synthesis_kernel<float>"),
+                          ("ring_analysis", "ring_pair_analysis_kernel + ring_analysis_kernel<float>")):
             ach = fft_bytes / (stages[key] * 1e-3) / 1e9
             stage_roof[key] = {"bound": "hbm", "kernel": kern + " (all FFT-length classes of one direction)",
                                "achieved": ach, "peak": hbm_peak, "unit": "GB/s", "frac": ach / hbm_peak,
-                               "traffic": traffic.get(f"{key}_nside{nside}_maps{B}"),
-                               "peak_source": ("MEASURED_PEAKS.json hbm_gbs, of measured" if peaks
-                                               else "fallback 6650 GB/s, of fallback"),
+                               "traffic": traffic.get(f"{key}_nside{nside}_maps{B}"), "peak_source": hbm_src,
                                "bytes_per_launch": fft_bytes, "ms": stages[key]}
+        # the preps read their operand once and write the hi/lo tiles, which hold as many bytes
+        for key, kern, nbytes in (("prep_alm", "prep_alm_tiles_kernel", 2 * 8 * B * nalm),
+                                  ("prep_f", "prep_f_tiles_kernel", 2 * hbm_bytes_ring_fft(B, mmax, g.npairs, 0))):
+            ach = nbytes / (stages[key] * 1e-3) / 1e9
+            stage_roof[key] = {"bound": "hbm", "kernel": kern, "achieved": ach, "peak": hbm_peak, "unit": "GB/s",
+                               "frac": ach / hbm_peak, "traffic": traffic.get(f"{key}_nside{nside}_maps{B}"),
+                               "peak_source": hbm_src, "bytes_per_launch": nbytes, "ms": stages[key]}
         tensor["ms"] = stages["tensor_synthesis"] + stages["tensor_analysis"]
         dom = max(stage_roof, key=lambda k: stage_roof[k]["ms"])
         roof = dict(stage_roof[dom])

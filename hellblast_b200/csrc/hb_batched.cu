@@ -454,9 +454,18 @@ constexpr int SYN_GROUPS = 3;
 constexpr int SYN_PW = 4 * SYN_GROUPS;
 constexpr int SYN_THREADS = 32 * (SYN_PW + 2);
 template <int N> constexpr int ana_stages() { return N >= 128 ? 3 : 4; }
+// Dynamic unit queue.  The CTAs draw units from a per-launch global counter (atomicAdd) in list
+// order, so a CTA that is done early takes the next unit instead of waiting out a fixed share.
+// The loader's thread draws each of its CTA's units and publishes it in a shared-memory ring of
+// UQ slots; every role (producer warps, MMA thread, loader) walks the ring in the same order.
+// Slot i % UQ has two barriers: uq_full (one arrival: published) and uq_empty (one arrival per
+// consumer: producer warp or MMA thread, read), so the drawer runs at most UQ units ahead of the
+// slowest role; unit -1 ends every role's walk.
+constexpr int UQ = 8;
 // stages, then per producer warp 128 coefficients (float2) and 64 inverse scales, then barriers
+// and the unit ring
 template <int ST, int N, int PW = 8> constexpr int tc_smem() {
-    return ST * (A_STAGE + tc_b_stage<N>()) + PW * (128 * 8 + 64 * 4) + 128;
+    return ST * (A_STAGE + tc_b_stage<N>()) + PW * (128 * 8 + 64 * 4) + 320;
 }
 
 struct TcSmem {
@@ -464,6 +473,8 @@ struct TcSmem {
     float *inv;    // this producer warp's inverse batch scales 1 / (ls s_b) of the unit's m, b < 64
     uint64_t *full, *empty, *accum, *tfree, *drain;
     uint32_t *tmem_slot;
+    uint64_t *uq_full, *uq_empty;  // unit ring barriers, UQ each
+    int *uq;                       // unit ring slots
 };
 template <int ST, int N, int PW = 8>
 __device__ __forceinline__ TcSmem tc_smem_layout(uint8_t *smem, int warp) {
@@ -479,11 +490,15 @@ __device__ __forceinline__ TcSmem tc_smem_layout(uint8_t *smem, int warp) {
     L.tfree = L.accum + 1;
     L.drain = L.tfree + 1;
     L.tmem_slot = reinterpret_cast<uint32_t *>(L.drain + 1);
+    L.uq_full = L.drain + 2;  // after the tensor-memory slot (8 bytes)
+    L.uq_empty = L.uq_full + UQ;
+    L.uq = reinterpret_cast<int *>(L.uq_empty + UQ);
+    static_assert(8 * (2 * 4 + 3) + 8 + 16 * UQ + 4 * UQ <= 320, "barrier and ring area (up to 4 stages)");
     return L;
 }
 
 template <int ST>
-__device__ __forceinline__ void tc_init_barriers(const TcSmem &L, int full_count, int tfree_count = TC_PRODUCERS) {
+__device__ __forceinline__ void tc_init_barriers(const TcSmem &L, int full_count, int tfree_count, int uq_consumers) {
     for (int s = 0; s < ST; ++s) {
         tc::mbar_init(&L.full[s], full_count);
         tc::mbar_init(&L.empty[s], 1);
@@ -491,7 +506,35 @@ __device__ __forceinline__ void tc_init_barriers(const TcSmem &L, int full_count
     tc::mbar_init(L.accum, 1);
     tc::mbar_init(L.tfree, tfree_count);
     tc::mbar_init(L.drain, 1);
+    for (int i = 0; i < UQ; ++i) {
+        tc::mbar_init(&L.uq_full[i], 1);
+        tc::mbar_init(&L.uq_empty[i], uq_consumers);
+    }
     tc::fence_mbar_init();
+}
+
+// the drawer (the loader's thread): the CTA's ui-th unit from the global counter into ring slot
+// ui % UQ, -1 when the list is exhausted; -2 when a role did not release the slot in time
+__device__ __forceinline__ int uq_publish(const TcSmem &L, int ui, int *ctr, int nunits, uint64_t ns) {
+    const int slot = ui % UQ;
+    if (ui >= UQ && !tc::mbar_wait(&L.uq_empty[slot], ((ui / UQ) - 1) & 1, ns)) return -2;
+    int u = atomicAdd(ctr, 1);
+    if (u >= nunits) u = -1;
+    L.uq[slot] = u;
+    tc::mbar_arrive(&L.uq_full[slot]);  // release: the slot's value is visible to the waiters
+    return u;
+}
+// a consumer's ui-th unit: lane 0 waits, reads the slot and releases it, the warp takes lane 0's
+// value (the MMA thread calls this as lane 0 of its warp alone); -2 when nothing was published
+// in time
+__device__ __forceinline__ int uq_take(const TcSmem &L, int ui, uint64_t ns, bool whole_warp) {
+    const int slot = ui % UQ;
+    int u = -2;
+    if ((threadIdx.x & 31) == 0 && tc::mbar_wait(&L.uq_full[slot], (ui / UQ) & 1, ns)) {
+        u = *reinterpret_cast<volatile int *>(&L.uq[slot]);
+        tc::mbar_arrive(&L.uq_empty[slot]);
+    }
+    return whole_warp ? __shfl_sync(0xffffffffu, u, 0) : u;
 }
 
 // the epilogue's inverse batch scales 1 / (ls s_b) of one m into this warp's table (maps b < nmaps)
@@ -586,7 +629,7 @@ __device__ __forceinline__ void gen_chunk_syn(Rec &R, const float2 *cf, uint8_t 
 template <int N, bool BF16, int S>
 __global__ void __launch_bounds__(SYN_THREADS, 1)
     synth_tc_kernel(const TcGroup *__restrict__ groups, const int4 *__restrict__ units, int nunits, int *err,
-                    TcCtl ctl) {
+                    int *qctr, TcCtl ctl) {
     constexpr int ST = SYN_GROUPS;
     constexpr int B_STAGE = tc_b_stage<N>();
     constexpr int STAGE = A_STAGE + B_STAGE;
@@ -603,7 +646,7 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const TcSmem L = tc_smem_layout<ST, N, SYN_PW>(smem, warp);
 
-    if (threadIdx.x == 0) tc_init_barriers<ST>(L, 128 + 1, 32 * SYN_PW);
+    if (threadIdx.x == 0) tc_init_barriers<ST>(L, 128 + 1, 32 * SYN_PW, SYN_PW + 1);
     if (warp == SYN_PW) {
         tc::tmem_alloc(L.tmem_slot, TCOLS);
         tc::tmem_relinquish();
@@ -620,8 +663,14 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
         const int r = ((warp & 3) << 5) | lane;  // row = pair within the block
         uint8_t *A = smem + wg * STAGE;
         uint32_t gc = 0;  // chunks this group has filled (uses of its stage)
-        int ui = 0;
-        for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++ui) {
+        for (int ui = 0; ok; ++ui) {
+            const int u = uq_take(L, ui, ctl.wait_ns, true);
+            if (u == -2) {
+                if (lane == 0) set_err(err, 6);
+                ok = false;
+                break;
+            }
+            if (u < 0) break;
             const int4 U = units[u];
             const TcGroup &G = groups[U.x];
             const int m = U.y, lmax = G.lmax;
@@ -704,8 +753,14 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
         // ---------------- MMA issuer
         if (lane == 0) {
             uint32_t fbits = 0;  // bit g: parity of stage g's next fill
-            int ui = 0;
-            for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++ui) {
+            for (int ui = 0; ok; ++ui) {
+                const int u = uq_take(L, ui, ctl.wait_ns, false);
+                if (u == -2) {
+                    set_err(err, 7);
+                    ok = false;
+                    break;
+                }
+                if (u < 0) break;
                 const int4 U = units[u];
                 const int nch = (groups[U.x].lmax - U.y + 64) / 64, hb0 = U.w / 2, nhb = (nch + 1) / 2;
                 if (ui > 0 && !tc::mbar_wait(L.tfree, (ui - 1) & 1, ctl.wait_ns)) {
@@ -748,7 +803,14 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
         if (lane == 0) {
             uint32_t ebits = 0, used = 0;  // bit g: parity of stage g's next drain / stage g used
             bool withheld = false;
-            for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+            for (int ui = 0; ok; ++ui) {
+                const int u = uq_publish(L, ui, qctr, nunits, ctl.wait_ns);
+                if (u == -2) {
+                    set_err(err, 8);
+                    ok = false;
+                    break;
+                }
+                if (u < 0) break;
                 const int4 U = units[u];
                 const TcGroup &G = groups[U.x];
                 const int m = U.y;
@@ -807,7 +869,7 @@ __device__ __forceinline__ void gen_chunk_ana(Rec &R, const float2 *cf, uint8_t 
 template <int N, bool BF16, int S>
 __global__ void __launch_bounds__(TC_THREADS, 1)
     anal_tc_kernel(const TcGroup *__restrict__ groups, const int4 *__restrict__ units, int nunits, float2 *alm_out,
-                   int *err, const float *__restrict__ fl, TcCtl ctl) {
+                   int *err, int *qctr, const float *__restrict__ fl, TcCtl ctl) {
     constexpr int ST = ana_stages<N>();
     constexpr int B_STAGE = tc_b_stage<N>();
     constexpr int STAGE = A_STAGE + B_STAGE;
@@ -820,7 +882,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const TcSmem L = tc_smem_layout<ST, N>(smem, warp);
 
-    if (threadIdx.x == 0) tc_init_barriers<ST>(L, 64 + 1);
+    if (threadIdx.x == 0) tc_init_barriers<ST>(L, 64 + 1, TC_PRODUCERS, 8 + 1);
     if (warp == 8) {
         tc::tmem_alloc(L.tmem_slot, TCOLS);
         tc::tmem_relinquish();
@@ -839,8 +901,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         const int quarter = warp & 3, half = warp >> 2;
         const int owner = half ? ((warp - 5) & 3) : quarter;
         uint32_t it = 0;
-        int ui = 0;
-        for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++ui) {
+        for (int ui = 0; ok; ++ui) {
+            const int u = uq_take(L, ui, ctl.wait_ns, true);
+            if (u == -2) {
+                if (lane == 0) set_err(err, 16);
+                ok = false;
+                break;
+            }
+            if (u < 0) break;
             const int4 U = units[u];
             const TcGroup &G = groups[U.x];
             const int m = U.y, jb = U.z, lmax = G.lmax;
@@ -930,8 +998,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         // ---------------- MMA issuer
         if (lane == 0) {
             uint32_t it = 0;
-            int ui = 0;
-            for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x, ++ui) {
+            for (int ui = 0; ok; ++ui) {
+                const int u = uq_take(L, ui, ctl.wait_ns, false);
+                if (u == -2) {
+                    set_err(err, 17);
+                    ok = false;
+                    break;
+                }
+                if (u < 0) break;
                 const int npc = (int)groups[units[u].x].npc, c0 = units[u].w;
                 if (ui > 0 && !tc::mbar_wait(L.tfree, (ui - 1) & 1, ctl.wait_ns)) {
                     set_err(err, 13);
@@ -964,7 +1038,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
         // ---------------- loader of the pre-split E/O tiles
         if (lane == 0) {
             uint32_t it = 0;
-            for (int u = blockIdx.x; u < nunits && ok; u += gridDim.x) {
+            for (int ui = 0; ok; ++ui) {
+                const int u = uq_publish(L, ui, qctr, nunits, ctl.wait_ns);
+                if (u == -2) {
+                    set_err(err, 18);
+                    ok = false;
+                    break;
+                }
+                if (u < 0) break;
                 const int4 U = units[u];
                 const TcGroup &G = groups[U.x];
                 const int m = U.y;
@@ -1051,8 +1132,9 @@ static int launch_syn(hb_batched_plan *bp, cudaStream_t st) {
     constexpr int S = nsets<N>();
     HB_CUDA_TRY(cudaFuncSetAttribute(synth_tc_kernel<N, BF16, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     const int grid = std::min(bp->n_syn, sm_count());
+    HB_CUDA_TRY(cudaMemsetAsync(bp->err + 16, 0, sizeof(int), st));  // unit queue counter
     synth_tc_kernel<N, BF16, S><<<grid, SYN_THREADS, smem, st>>>(bp->dgroups, bp->syn_units, bp->n_syn, bp->err,
-                                                                 TcCtl{bp->wait_ns, bp->inject});
+                                                                 bp->err + 16, TcCtl{bp->wait_ns, bp->inject});
     HB_CHECK_LAUNCH();
     return HB_OK;
 }
@@ -1062,13 +1144,13 @@ static int launch_ana(hb_batched_plan *bp, float2 *alm_out, const float *fl, cud
     constexpr int S = nsets<N>();
     HB_CUDA_TRY(cudaFuncSetAttribute(anal_tc_kernel<N, BF16, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     const int grid = std::min(bp->n_ana, sm_count());
+    HB_CUDA_TRY(cudaMemsetAsync(bp->err + 17, 0, sizeof(int), st));  // unit queue counter
     anal_tc_kernel<N, BF16, S><<<grid, TC_THREADS, smem, st>>>(bp->dgroups, bp->ana_units, bp->n_ana, alm_out,
-                                                                 bp->err, fl, TcCtl{bp->wait_ns, 0});
+                                                                 bp->err, bp->err + 17, fl, TcCtl{bp->wait_ns, 0});
     HB_CHECK_LAUNCH();
     return HB_OK;
 }
-// prep launch: persistent CTAs (one or two per SM), two slice buffers when they fit in shared
-// memory, else one
+// prep launches: persistent CTAs over the (order or order block, map quad) items, 3 to 4 per SM
 template <int N, bool BF16>
 static int launch_prep_alm(hb_batched_plan *bp, int gi, const float2 *alm, int64_t stride, cudaStream_t st) {
     const TcGroup &G = bp->hgroups[gi];

@@ -53,7 +53,8 @@ def _alm(lmax, nmaps, scale=1.0, seed=2):
     return one.expand(nmaps, -1).contiguous()
 
 
-def run(case: str, nside: int, lmax: int, nmaps: int, reps: int, warmup: int, wide: bool = False) -> dict:
+def run(case: str, nside: int, lmax: int, nmaps: int, reps: int, warmup: int, wide: bool = False,
+        bf16: bool = False) -> dict:
     dev = torch.device("cuda", torch.cuda.current_device())
     st = torch.cuda.current_stream(dev)
     out = {"case": case, "nside": nside, "lmax": lmax, "nmaps": nmaps}
@@ -75,7 +76,7 @@ def run(case: str, nside: int, lmax: int, nmaps: int, reps: int, warmup: int, wi
         ms = _time(lambda: ops.alm2cl(a, None, lmax, lmax), reps, warmup, st)
         out["bytes_read"] = a.numel() * a.element_size()
     elif case == "batched":
-        bp = batched.plan(nside, lmax, nmaps, wide=wide)
+        bp = batched.plan(nside, lmax, nmaps, wide=wide, bf16=bf16)
         a = _alm(lmax, nmaps).reshape(-1)
         mp = torch.empty(bp.total_pix, dtype=torch.float32, device=dev)
         r = torch.empty_like(a)
@@ -123,12 +124,13 @@ def main(argv=None):
     p.add_argument("--reps", type=int, default=3)
     p.add_argument("--warmup", type=int, default=1)
     p.add_argument("--wide", action="store_true", help="batched: 64-map groups (MMA N = 128)")
+    p.add_argument("--bf16", action="store_true", help="batched: BF16 hi+lo split (default IEEE half)")
     a = p.parse_args(argv)
     if not torch.cuda.is_available():
         raise SystemExit("kernel_cases needs a CUDA device (there is no CPU path)")
     L.lib()
     lmax = 2 * a.nside - 1 if a.lmax is None else a.lmax
-    print(json.dumps(run(a.case, a.nside, lmax, a.nmaps, a.reps, a.warmup, a.wide)), flush=True)
+    print(json.dumps(run(a.case, a.nside, lmax, a.nmaps, a.reps, a.warmup, a.wide, a.bf16)), flush=True)
 
 
 if __name__ == "__main__":
