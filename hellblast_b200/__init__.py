@@ -29,9 +29,29 @@ map2alm = map2alm_gpu
 alm2map = alm2map_gpu
 anafast = anafast_ring
 
+
+def clear_caches() -> None:
+    """Drop the cached geometries, transform plans and batched plans.  Their device memory
+    (recursion checkpoints, tile and ring buffers: tens of GB at nside >= 2048) is freed as soon
+    as no caller still holds the objects; the torch allocator's unused blocks are released too."""
+    import gc
+
+    import torch
+
+    from . import geometry as _geometry
+
+    with batched._lock:
+        batched._cache.clear()
+    with _geometry._lock:
+        _geometry._cache.clear()
+    gc.collect()
+    if torch.cuda.is_available():
+        torch.cuda.empty_cache()
+
+
 __all__ = [
     "map2alm_gpu", "alm2map_gpu", "anafast_ring", "map2alm", "alm2map", "anafast",
     "almxfl", "alm2cl", "synalm", "alm_index", "alm_size", "getlmax", "healpy_to_ref", "ref_to_healpy",
     "HealpixRingTables", "map2alm_spin_gpu", "eb_from_qu_gpu", "qu_from_eb_gpu", "hp_compat", "autograd",
-    "batched", "smoothing", "synfast", "distributed", "pixelfunc", "io_fits", "rotate",
+    "batched", "smoothing", "synfast", "distributed", "pixelfunc", "io_fits", "rotate", "clear_caches",
 ]

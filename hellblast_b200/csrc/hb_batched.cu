@@ -41,6 +41,7 @@ struct TcGroup {
     const float4 *ck;        // plan checkpoints
     const int64_t *blk_ofs;
     const float4 *ckh;       // checkpoints at l0 + 128 of every block (same indexing as ck)
+    const float4 *ckq1, *ckq3;  // ... at l0 + 64 and l0 + 192 (analysis l-quarters)
     const float2 *coef;      // recursion coefficients (A_l, B_l): [(blk_ofs[m] + b) * 256 + i], l = m + 256 b + i
     // synthesis
     const uint4 *alm_tiles;  // [chunk][4][N x 32] bf16, chunk = tile_ofs[m] + c
@@ -98,13 +99,13 @@ __device__ __forceinline__ float block_pow2_scale(float vmax) {
 // (maps 4j .. 4j+3) of one k8 group are one 128-byte segment, so both kernels work on quads of
 // maps and let 4 lanes write one segment's interleaved rows in the same instruction (scattered
 // 16-byte stores from separate instructions cost one L2 request each and ran at half the rate).
-template <bool BF16>
+template <bool BF16, int KC = 32>  // KC: K positions per chunk (32: synthesis, 16: analysis)
 __device__ __forceinline__ void store_rows8(uint4 *chunk, int N, int qh, int n, int g, const float (&v)[8]) {
     uint4 hi, lo;
     tc::split8<BF16>(v, hi, lo);
-    const int64_t e = (int64_t)(2 * qh) * N * 32 + (n & 7) * 8 + (n >> 3) * 256 + g * 64;  // 16-bit elements
+    const int64_t e = (int64_t)(2 * qh) * N * KC + (n & 7) * 8 + (n >> 3) * (8 * KC) + g * 64;  // 16-bit elements
     chunk[e / 8] = hi;
-    chunk[(e + (int64_t)N * 32) / 8] = lo;
+    chunk[(e + (int64_t)N * KC) / 8] = lo;
 }
 
 // alm [map][nalm] complex64 -> per (m, 64-l chunk) the synthesis B tiles
@@ -209,7 +210,7 @@ __global__ void __launch_bounds__(PA_THREADS, 4) prep_alm_tiles_kernel(const TcG
 }
 
 // F [map][m/8][pair][m%8][north, south] (the m-blocked F the batched ring analysis writes, see
-// fg_off) -> per (m, 32-pair chunk) the analysis B tiles [q][h][N x 32 pairs] (E = F_N + F_S
+// fg_off) -> per (m, 16-pair chunk) the analysis B tiles [q][h][N x 16 pairs] (E = F_N + F_S
 // for q = 0, O = F_N - F_S for q = 1).  Work item = (block of 8 orders, quad of 4 maps): the 8
 // orders of one pair and map are one 128-byte line of F, and the 4 maps' rows of one
 // (m, chunk, k8 group, q, h) are one 128-byte segment of the tile.  F16: a first sweep over the
@@ -300,9 +301,9 @@ __global__ void __launch_bounds__(PF_THREADS, 3) prep_f_tiles_kernel(const TcGro
             tc::cp_async_wait<1>();  // all groups but the one just committed: stage stg is in
             __syncthreads();
             const int p0 = stg * PF_PAIRS + 8 * g8;
-            if (m <= G.mmax && p0 < npad) {
-                const int c = p0 >> 5, g = (p0 >> 3) & 3, b = b0 + bl;
-                uint4 *chunk = const_cast<uint4 *>(G.g_tiles) + ((int64_t)m * npc + c) * (16 * N);
+            if (m <= G.mmax && p0 < npad) {  // 16-pair chunks (the analysis kernel's stages)
+                const int c = p0 >> 4, g = (p0 >> 3) & 1, b = b0 + bl;
+                uint4 *chunk = const_cast<uint4 *>(G.g_tiles) + ((int64_t)m * 2 * npc + c) * (8 * N);
                 float er[8], ei[8], orr[8], oi[8];
 #pragma unroll
                 for (int i = 0; i < 8; ++i) {
@@ -312,10 +313,10 @@ __global__ void __launch_bounds__(PF_THREADS, 3) prep_f_tiles_kernel(const TcGro
                     orr[i] = (f.x - f.z) * sc;
                     oi[i] = (f.y - f.w) * sc;
                 }
-                store_rows8<BF16>(chunk, N, 0, 2 * b, g, er);
-                store_rows8<BF16>(chunk, N, 0, 2 * b + 1, g, ei);
-                store_rows8<BF16>(chunk, N, 1, 2 * b, g, orr);
-                store_rows8<BF16>(chunk, N, 1, 2 * b + 1, g, oi);
+                store_rows8<BF16, 16>(chunk, N, 0, 2 * b, g, er);
+                store_rows8<BF16, 16>(chunk, N, 0, 2 * b + 1, g, ei);
+                store_rows8<BF16, 16>(chunk, N, 1, 2 * b, g, orr);
+                store_rows8<BF16, 16>(chunk, N, 1, 2 * b + 1, g, oi);
             }
             __syncthreads();  // every thread is done with this stage's buffer before it is refilled
         }
@@ -446,14 +447,19 @@ __global__ void __launch_bounds__(128) skip_table_kernel(GeomDev g, int lmax, co
 // bulk copies.  Several producer warps per SM sub-partition hide the recursion's dependency
 // latency.  The recursion restarts from the plan's FP64 checkpoints at every 128 l (block
 // starts and the mid-block table), which is what lets several warps share one row's l range.
-constexpr int TC_THREADS = 320;
-constexpr int TC_PRODUCERS = 256;
 template <int N> constexpr int tc_b_stage() { return 4 * N * 64; }  // [q][h][N x 32] 16-bit
 // synthesis: SYN_GROUPS groups of four producer warps, group g owning stage g
 constexpr int SYN_GROUPS = 3;
 constexpr int SYN_PW = 4 * SYN_GROUPS;
 constexpr int SYN_THREADS = 32 * (SYN_PW + 2);
-template <int N> constexpr int ana_stages() { return N >= 128 ? 3 : 4; }
+// analysis: ANA_ST stages of 16 ring pairs (one MMA K-step per parity), two producer warps per
+// stage, each thread one (pair, l-quarter) of the unit's 256-l block
+constexpr int ANA_A_TILE = 4096;               // 128 rows x 16 K x bf16
+constexpr int ANA_A_STAGE = 4 * ANA_A_TILE;    // [parity][hi/lo]
+template <int N> constexpr int ana_b_stage() { return 4 * N * 32; }  // [q][h][N x 16] 16-bit
+constexpr int ANA_ST = 6;
+constexpr int ANA_PW = 2 * ANA_ST;
+constexpr int ANA_THREADS = 32 * (ANA_PW + 2);
 // Dynamic unit queue.  The CTAs draw units from a per-launch global counter (atomicAdd) in list
 // order, so a CTA that is done early takes the next unit instead of waiting out a fixed share.
 // The loader's thread draws each of its CTA's units and publishes it in a shared-memory ring of
@@ -464,8 +470,8 @@ template <int N> constexpr int ana_stages() { return N >= 128 ? 3 : 4; }
 constexpr int UQ = 8;
 // stages, then per producer warp 128 coefficients (float2) and 64 inverse scales, then barriers
 // and the unit ring
-template <int ST, int N, int PW = 8> constexpr int tc_smem() {
-    return ST * (A_STAGE + tc_b_stage<N>()) + PW * (128 * 8 + 64 * 4) + 320;
+template <int ST, int N, int PW, int STAGE = A_STAGE + tc_b_stage<N>()> constexpr int tc_smem() {
+    return ST * STAGE + PW * (128 * 8 + 64 * 4) + 320;
 }
 
 struct TcSmem {
@@ -476,9 +482,8 @@ struct TcSmem {
     uint64_t *uq_full, *uq_empty;  // unit ring barriers, UQ each
     int *uq;                       // unit ring slots
 };
-template <int ST, int N, int PW = 8>
+template <int ST, int N, int PW, int STAGE = A_STAGE + tc_b_stage<N>()>
 __device__ __forceinline__ TcSmem tc_smem_layout(uint8_t *smem, int warp) {
-    constexpr int STAGE = A_STAGE + tc_b_stage<N>();
     const int pw = warp < PW ? warp : 0;
     TcSmem L;
     L.coef = reinterpret_cast<float2 *>(smem + ST * STAGE) + pw * 128;
@@ -493,7 +498,7 @@ __device__ __forceinline__ TcSmem tc_smem_layout(uint8_t *smem, int warp) {
     L.uq_full = L.drain + 2;  // after the tensor-memory slot (8 bytes)
     L.uq_empty = L.uq_full + UQ;
     L.uq = reinterpret_cast<int *>(L.uq_empty + UQ);
-    static_assert(8 * (2 * 4 + 3) + 8 + 16 * UQ + 4 * UQ <= 320, "barrier and ring area (up to 4 stages)");
+    static_assert(8 * (2 * ST + 3) + 8 + 16 * UQ + 4 * UQ <= 320, "barrier and ring area");
     return L;
 }
 
@@ -543,19 +548,20 @@ __device__ __forceinline__ void load_inv_scales(float *inv, const float *scl, in
     __syncwarp();
 }
 
-// write 8 even + 8 odd split values of one A-tile row group: A + {0,1,2,3} * A_TILE + off
-template <bool BF16>
+// write 8 even + 8 odd split values of one A-tile row group: A + {0,1,2,3} * AT + off
+template <bool BF16, int AT = A_TILE>
 __device__ __forceinline__ void store_split(uint8_t *A, int off, const float (&ev)[8], const float (&od)[8]) {
     uint4 hi, lo;
     tc::split8<BF16>(ev, hi, lo);
-    *reinterpret_cast<uint4 *>(A + 0 * A_TILE + off) = hi;
-    *reinterpret_cast<uint4 *>(A + 1 * A_TILE + off) = lo;
+    *reinterpret_cast<uint4 *>(A + 0 * AT + off) = hi;
+    *reinterpret_cast<uint4 *>(A + 1 * AT + off) = lo;
     tc::split8<BF16>(od, hi, lo);
-    *reinterpret_cast<uint4 *>(A + 2 * A_TILE + off) = hi;
-    *reinterpret_cast<uint4 *>(A + 3 * A_TILE + off) = lo;
+    *reinterpret_cast<uint4 *>(A + 2 * AT + off) = hi;
+    *reinterpret_cast<uint4 *>(A + 3 * AT + off) = lo;
 }
 
-// The MMAs of one stage (2 parities x 2 K-steps x 3 split passes).  The hi*hi products go to
+// The MMAs of one stage (2 parities x KS K-steps x 3 split passes; KS = 2: 32 K per stage,
+// tiles of 128 rows x 32 K; KS = 1: 16 K).  The hi*hi products go to
 // the "hi" set of a set pair, the two cross products (about 2^-11 smaller) to its "lo" set: the
 // tensor core's FP32 accumulation loses about one ulp of the accumulator per MMA, so keeping the
 // large products' set free of the cross products cuts the steps that round the result by 3x.
@@ -563,22 +569,25 @@ __device__ __forceinline__ void store_split(uint8_t *A, int off, const float (&e
 // batch tiles (hi | lo), which lie back to back in shared memory, is one MMA of width 2N into
 // (hi | lo); A_lo times B_hi is a second one into lo.  Live chunk i of a unit uses set pair
 // j = i mod (S/2); `first` (the first S/2 live chunks) starts each pair afresh.
-template <int N>
+template <int N, int KS = 2>
 __device__ __forceinline__ void issue_stage(uint32_t tmem, uint32_t a0, int pair, bool first, uint32_t idesc_n,
                                             uint32_t idesc_2n) {
     // one cta_group::1 MMA is at most 256 wide and N a multiple of 16; the 2N-wide MMA reads the
-    // lo batch tile as B rows N .. 2N-1, so it must follow the hi tile directly (N * 64 bytes)
+    // lo batch tile as B rows N .. 2N-1, so it must follow the hi tile directly (N * 32 KS bytes)
     static_assert(2 * N <= 256 && N % 16 == 0, "the hi x (hi | lo) MMA needs 2N <= 256, N % 16 == 0");
-    static_assert(tc_b_stage<N>() == 4 * N * 64, "batch stage = [parity][hi | lo][N x 32], tiles back to back");
-    const uint32_t b0 = a0 + A_STAGE;
+    static_assert(KS == 1 || KS == 2, "16 or 32 K per stage");
+    // core matrices (8 rows x 16 bytes): 128 bytes apart along K, 256 KS bytes apart along the rows
+    constexpr int AT = 4096 * KS, BT = N * 32 * KS, SBO = 256 * KS;
+    static_assert(KS != 2 || (AT == A_TILE && 4 * BT == tc_b_stage<N>()), "synthesis tile layout");
+    const uint32_t b0 = a0 + 4 * AT;
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
         const uint32_t d = tmem + pair * 4 * N + q * 2 * N;
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const uint64_t ah = tc::sdesc(a0 + (q * 2 + 0) * A_TILE + k * 256, 128, 512);
-            const uint64_t al = tc::sdesc(a0 + (q * 2 + 1) * A_TILE + k * 256, 128, 512);
-            const uint64_t bh = tc::sdesc(b0 + (q * 2 + 0) * (N * 64) + k * 256, 128, 512);
+        for (int k = 0; k < KS; ++k) {
+            const uint64_t ah = tc::sdesc(a0 + (q * 2 + 0) * AT + k * 256, 128, SBO);
+            const uint64_t al = tc::sdesc(a0 + (q * 2 + 1) * AT + k * 256, 128, SBO);
+            const uint64_t bh = tc::sdesc(b0 + (q * 2 + 0) * BT + k * 256, 128, SBO);
             const uint32_t acc = (!first || k > 0) ? 1u : 0u;
             tc::mma_bf16(d, ah, bh, idesc_2n, acc);  // B rows N .. 2N-1: the lo tile
             tc::mma_bf16(d + N, al, bh, idesc_n, 1u);
@@ -853,37 +862,43 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
 }
 
 // ------------------------------------------------------------------------------------ analysis
-// one analysis chunk of one pair: 128 l in eight groups of 8 even + 8 odd values
+// one analysis chunk of one (pair, l-quarter): 64 l in four groups of 8 even + 8 odd values,
+// row groups of 8 rows 256 bytes apart (16-K tiles)
 template <bool CHECKED, bool BF16>
 __device__ __forceinline__ void gen_chunk_ana(Rec &R, const float2 *cf, uint8_t *A, int off0) {
 #pragma unroll 2
-    for (int grp = 0; grp < 8; ++grp) {
+    for (int grp = 0; grp < 4; ++grp) {
         float ev[8], od[8];
         gen16<CHECKED>(R, cf + 16 * grp, ev, od);
-        store_split<BF16>(A, off0 + grp * 512, ev, od);
+        store_split<BF16, ANA_A_TILE>(A, off0 + grp * 256, ev, od);
     }
 }
-// Chunk c (32 ring pairs) of a unit goes to stage c' % ST (c' = running chunk count); two warps
-// fill it, one the rows of l0 .. l0+127, the other those of l0+128 .. l0+255 (restarting from the
-// mid-block checkpoint).
+// Unit = (m, 256-l block); its chunks of 16 ring pairs go to stage c' % ANA_ST (c' = running
+// chunk count).  Warps 2s and 2s + 1 fill stage s (on different SM sub-partitions): thread
+// (warp w, lane) runs the recursion of pair 16 c + lane % 16 over the l-quarter
+// q = 2 (w % 2) + lane / 16 of the block, the 64 l from l0 + 64 q, restarting from the plan's
+// checkpoint there (block start, l0 + 64, the mid-block table, l0 + 192), and writes A-tile rows
+// 32 q .. 32 q + 31 of both parities.  Twelve producer warps fill six stages at once; each stage
+// is one MMA K-step per parity.
 template <int N, bool BF16, int S>
-__global__ void __launch_bounds__(TC_THREADS, 1)
+__global__ void __launch_bounds__(ANA_THREADS, 1)
     anal_tc_kernel(const TcGroup *__restrict__ groups, const int4 *__restrict__ units, int nunits, float2 *alm_out,
                    int *err, int *qctr, const float *__restrict__ fl, TcCtl ctl) {
-    constexpr int ST = ana_stages<N>();
-    constexpr int B_STAGE = tc_b_stage<N>();
-    constexpr int STAGE = A_STAGE + B_STAGE;
+    constexpr int ST = ANA_ST;
+    constexpr int B_STAGE = ana_b_stage<N>();
+    constexpr int STAGE = ANA_A_STAGE + B_STAGE;
     constexpr uint32_t IDESC = tc::idesc_f16kind(128, N, 1, 0, BF16);
     constexpr uint32_t IDESC2 = tc::idesc_f16kind(128, 2 * N, 1, 0, BF16);
     constexpr float LS = BF16 ? 1.0f : 256.0f;
     constexpr int TCOLS = (2 * N * S < 32) ? 32 : 2 * N * S;  // S accumulator sets, see synth_tc_kernel
     static_assert(2 * N * S <= 512, "TMEM holds 512 columns");
+    static_assert(S >= 2 && S % 2 == 0, "accumulator sets come in (hi, cross) pairs");
     extern __shared__ __align__(1024) uint8_t smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const TcSmem L = tc_smem_layout<ST, N>(smem, warp);
+    const TcSmem L = tc_smem_layout<ST, N, ANA_PW, STAGE>(smem, warp);
 
-    if (threadIdx.x == 0) tc_init_barriers<ST>(L, 64 + 1, TC_PRODUCERS, 8 + 1);
-    if (warp == 8) {
+    if (threadIdx.x == 0) tc_init_barriers<ST>(L, 64 + 1, 32 * ANA_PW, ANA_PW + 1);
+    if (warp == ANA_PW) {
         tc::tmem_alloc(L.tmem_slot, TCOLS);
         tc::tmem_relinquish();
     }
@@ -893,13 +908,12 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     const uint32_t tmem = *L.tmem_slot;
     bool ok = true;
 
-    if (warp < 8) {
+    if (warp < ANA_PW) {
         // ---------------- producers + epilogue
-        // warp w < 4 fills the first l half of stage w, warp w >= 4 the second half of stage
-        // (w - 5) mod 4: the two halves of one stage run on different SM sub-partitions, and with
-        // three stages the six busy warps cover all four sub-partitions
-        const int quarter = warp & 3, half = warp >> 2;
-        const int owner = half ? ((warp - 5) & 3) : quarter;
+        const int owner = warp >> 1;                      // stage this warp fills
+        const int qt = 2 * (warp & 1) + (lane >> 4);      // l-quarter of this thread
+        const int pl = lane & 15;                         // pair within the chunk
+        const int quarter = warp & 3, eg = warp >> 2;     // epilogue: TMEM lane quarter, column group
         uint32_t it = 0;
         for (int ui = 0; ok; ++ui) {
             const int u = uq_take(L, ui, ctl.wait_ns, true);
@@ -913,27 +927,28 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             const TcGroup &G = groups[U.x];
             const int m = U.y, jb = U.z, lmax = G.lmax;
             const int l0 = m + 256 * jb;
-            const bool active = l0 + 128 * half <= lmax;  // this half of the block has rows <= lmax
+            const bool active = l0 + 64 * qt <= lmax;  // this quarter of the block has rows <= lmax
             const int64_t np = G.g.npairs;
-            const int npc = (int)G.npc;
+            const int nck = 2 * (int)G.npc, c0 = 2 * U.w;  // 16-pair chunks (skip counts are in 32-pair chunks)
             const int64_t blk = G.blk_ofs[m] + jb;
-            const float4 *ckt = half ? G.ckh : G.ck;
+            const float4 *ckt = qt == 0 ? G.ck : qt == 1 ? G.ckq1 : qt == 2 ? G.ckh : G.ckq3;
             __syncwarp();
 #pragma unroll
-            for (int i = 0; i < 4; ++i) L.coef[lane + 32 * i] = G.coef[blk * 256 + half * 128 + lane + 32 * i];
+            for (int i = 0; i < 4; ++i)  // the coefficients of this warp's two quarters
+                L.coef[lane + 32 * i] = G.coef[blk * 256 + (warp & 1) * 128 + lane + 32 * i];
             __syncwarp();
             // this warp's next chunk (c + ST) has its checkpoint and x fetched one chunk ahead
             float4 knext = make_float4(0.f, 0.f, 0.f, 0.f);
             float xhn = 0.f, xln = 0.f;
             auto fetch = [&](int cc) {
-                const int64_t pp = (int64_t)cc * 32 + lane;
-                const bool lv = active && cc < npc && pp < np;
+                const int64_t pp = (int64_t)cc * 16 + pl;
+                const bool lv = active && cc < nck && pp < np;
                 knext = lv ? ckt[blk * np + pp] : make_float4(0.f, 0.f, 0.f, 0.f);
                 xhn = lv ? G.g.pair_xhi[pp] : 0.f;
                 xln = lv ? G.g.pair_xlo[pp] : 0.f;
             };
             bool first = true;
-            for (int c = U.w; c < npc; ++c, ++it) {
+            for (int c = c0; c < nck; ++c, ++it) {
                 const int s = it % ST;
                 if (s != owner) continue;
                 if (first) fetch(c);
@@ -950,18 +965,20 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     break;
                 }
                 uint8_t *A = smem + s * STAGE;
-                // MN-major: 8 consecutive rows (l of one parity) of pair `lane`
-                const int off0 = (lane & 7) * 16 + (lane >> 3) * 128 + half * 8 * 512;
+                // MN-major 16-K tile: 8 consecutive rows (l of one parity) of pair pl at
+                // (pl % 8) 16 + (pl / 8) 128, row groups 256 bytes apart; rows 32 qt ..
+                const int off0 = (pl & 7) * 16 + (pl >> 3) * 128 + qt * 4 * 256;
+                const float2 *cf = L.coef + (lane >> 4) * 64;
                 if (fast)
-                    gen_chunk_ana<false, BF16>(R, L.coef, A, off0);
+                    gen_chunk_ana<false, BF16>(R, cf, A, off0);
                 else
-                    gen_chunk_ana<true, BF16>(R, L.coef, A, off0);
+                    gen_chunk_ana<true, BF16>(R, cf, A, off0);
                 tc::fence_proxy_async_smem();
                 tc::mbar_arrive(&L.full[s]);
             }
             if (!ok) break;
             // epilogue: lane quarter warp % 4 = rows 32w'..32w'+31 (l = l0 + 2 row + parity),
-            // column blocks j with j % 2 == half; the scales are fetched while the MMAs drain
+            // column blocks j with j % 3 == warp / 4; the scales are fetched while the MMAs drain
             load_inv_scales(L.inv, G.dscale + (int64_t)m * (N / 2), G.nmaps, N / 2, LS);
             if (!warp_wait(L.accum, ui & 1, ctl.wait_ns)) {
                 if (lane == 0) set_err(err, 12);
@@ -972,11 +989,11 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             const int row = quarter * 32 + lane;
             const int le = l0 + 2 * row;
             const uint32_t taddr = tmem + ((uint32_t)(quarter * 32) << 16);
-            const int nsets = 2 * (npc - U.w) < S ? 2 * (npc - U.w) : S;
+            const int nsets = 2 * (nck - c0) < S ? 2 * (nck - c0) : S;
             // optional per-l filter (almxfl fused into the store)
             const float fl0 = fl && le <= lmax ? fl[le] : 1.f, fl1 = fl && le + 1 <= lmax ? fl[le + 1] : 1.f;
 #pragma unroll 1
-            for (int j = half; j < N / 16; j += 2) {
+            for (int j = eg; j < N / 16; j += 3) {
                 float de[16], dd[16];
                 load_sets<N>(taddr, j, nsets, de, dd);
 #pragma unroll
@@ -994,7 +1011,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
             tc::fence_before();
             tc::mbar_arrive(L.tfree);
         }
-    } else if (warp == 8) {
+    } else if (warp == ANA_PW) {
         // ---------------- MMA issuer
         if (lane == 0) {
             uint32_t it = 0;
@@ -1006,14 +1023,14 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                     break;
                 }
                 if (u < 0) break;
-                const int npc = (int)groups[units[u].x].npc, c0 = units[u].w;
+                const int nck = 2 * (int)groups[units[u].x].npc, c0 = 2 * units[u].w;
                 if (ui > 0 && !tc::mbar_wait(L.tfree, (ui - 1) & 1, ctl.wait_ns)) {
                     set_err(err, 13);
                     ok = false;
                     break;
                 }
                 tc::fence_after();
-                for (int c = c0; c < npc; ++c, ++it) {
+                for (int c = c0; c < nck; ++c, ++it) {
                     const int s = it % ST;
                     if (!tc::mbar_wait(&L.full[s], (it / ST) & 1, ctl.wait_ns)) {
                         set_err(err, 14);
@@ -1021,8 +1038,8 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         break;
                     }
                     tc::fence_after();
-                    issue_stage<N>(tmem, tc::smem_u32(smem + s * STAGE), (c - c0) % (S / 2), c - c0 < S / 2,
-                                   IDESC, IDESC2);
+                    issue_stage<N, 1>(tmem, tc::smem_u32(smem + s * STAGE), (c - c0) % (S / 2), c - c0 < S / 2,
+                                      IDESC, IDESC2);
                     tc::mma_commit(&L.empty[s]);
                 }
                 if (!ok) break;
@@ -1049,9 +1066,9 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                 const int4 U = units[u];
                 const TcGroup &G = groups[U.x];
                 const int m = U.y;
-                const int npc = (int)G.npc;
-                const uint4 *src = G.g_tiles + (int64_t)m * npc * (16 * N);
-                for (int c = U.w; c < npc; ++c, ++it) {
+                const int nck = 2 * (int)G.npc, c0 = 2 * U.w;
+                const uint4 *src = G.g_tiles + (int64_t)m * nck * (B_STAGE / 16);
+                for (int c = c0; c < nck; ++c, ++it) {
                     const int s = it % ST;
                     if (it >= ST && !tc::mbar_wait(&L.empty[s], ((it / ST) + 1) & 1, ctl.wait_ns)) {
                         set_err(err, 15);
@@ -1059,7 +1076,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
                         break;
                     }
                     tc::mbar_arrive_expect_tx(&L.full[s], B_STAGE);
-                    tc::bulk_g2s(smem + s * STAGE + A_STAGE, src + (int64_t)c * (16 * N), B_STAGE, &L.full[s]);
+                    tc::bulk_g2s(smem + s * STAGE + ANA_A_STAGE, src + (int64_t)c * (B_STAGE / 16), B_STAGE, &L.full[s]);
                 }
             }
         }
@@ -1067,7 +1084,7 @@ __global__ void __launch_bounds__(TC_THREADS, 1)
     }
     tc::fence_before();
     __syncthreads();
-    if (warp == 8) {
+    if (warp == ANA_PW) {
         tc::fence_after();
         tc::tmem_dealloc(tmem, TCOLS);
     }
@@ -1091,6 +1108,7 @@ struct hb_batched_plan {
         int64_t *tile_ofs;            // device [mmax+1] alm chunk offsets
         float2 *coef;                 // recursion coefficient table (coef_table_kernel)
         float4 *ckh;                  // mid-block recursion checkpoints (launch_ck_mid)
+        float4 *ckq1, *ckq3;          // quarter-block checkpoints (l0 + 64, l0 + 192)
     };
     std::vector<PlanPart> parts;
     std::vector<TcGroup> hgroups;
@@ -1140,12 +1158,12 @@ static int launch_syn(hb_batched_plan *bp, cudaStream_t st) {
 }
 template <int N, bool BF16>
 static int launch_ana(hb_batched_plan *bp, float2 *alm_out, const float *fl, cudaStream_t st) {
-    const int smem = tc_smem<ana_stages<N>(), N>();
+    const int smem = tc_smem<ANA_ST, N, ANA_PW, ANA_A_STAGE + ana_b_stage<N>()>();
     constexpr int S = nsets<N>();
     HB_CUDA_TRY(cudaFuncSetAttribute(anal_tc_kernel<N, BF16, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     const int grid = std::min(bp->n_ana, sm_count());
     HB_CUDA_TRY(cudaMemsetAsync(bp->err + 17, 0, sizeof(int), st));  // unit queue counter
-    anal_tc_kernel<N, BF16, S><<<grid, TC_THREADS, smem, st>>>(bp->dgroups, bp->ana_units, bp->n_ana, alm_out,
+    anal_tc_kernel<N, BF16, S><<<grid, ANA_THREADS, smem, st>>>(bp->dgroups, bp->ana_units, bp->n_ana, alm_out,
                                                                  bp->err, bp->err + 17, fl, TcCtl{bp->wait_ns, 0});
     HB_CHECK_LAUNCH();
     return HB_OK;
@@ -1199,7 +1217,7 @@ int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int np
     // sizes and layout of the single allocation
     size_t total = 0;
     auto carve = [&](size_t b) { size_t o = total; total += (b + 255) & ~(size_t)255; return o; };
-    struct Off { size_t gf, tofs, tiles_a, tiles_g, scales, coef, ckh; };
+    struct Off { size_t gf, tofs, tiles_a, tiles_g, scales, coef, ckh, ckq1, ckq3; };
     std::vector<Off> offs(nplans);
     std::vector<std::vector<int64_t>> tile_ofs(nplans);
     std::vector<int64_t> chunks_a(nplans);
@@ -1222,6 +1240,8 @@ int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int np
         for (int m = 0; m <= p->mmax; ++m) nblocks += (p->lmax - m) / 256 + 1;
         offs[i].coef = carve((size_t)nblocks * 256 * sizeof(float2));
         offs[i].ckh = carve((size_t)nblocks * np * sizeof(float4));
+        offs[i].ckq1 = carve((size_t)nblocks * np * sizeof(float4));
+        offs[i].ckq3 = carve((size_t)nblocks * np * sizeof(float4));
         hb_batched_plan::PlanPart part;
         part.p = p;
         part.nmaps = nmaps[i];
@@ -1285,6 +1305,8 @@ int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int np
         part.tile_ofs = (int64_t *)(base + offs[i].tofs);
         part.coef = (float2 *)(base + offs[i].coef);
         part.ckh = (float4 *)(base + offs[i].ckh);
+        part.ckq1 = (float4 *)(base + offs[i].ckq1);
+        part.ckq3 = (float4 *)(base + offs[i].ckq3);
     }
     {
         int gi = 0;
@@ -1297,6 +1319,8 @@ int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int np
                 G.alm_tile_ofs = bp->parts[i].tile_ofs;
                 G.coef = bp->parts[i].coef;
                 G.ckh = bp->parts[i].ckh;
+                G.ckq1 = bp->parts[i].ckq1;
+                G.ckq3 = bp->parts[i].ckq3;
                 G.Gm = bp->parts[i].GF + (int64_t)GM * k * bp->parts[i].gf_stride;
                 G.gm_stride = bp->parts[i].gf_stride;
                 G.g_tiles = (const uint4 *)(base + offs[i].tiles_g) +
@@ -1321,7 +1345,7 @@ int hb_batched_plan_create(const hb_plan *const *plans, const int *nmaps, int np
     for (int i = 0; i < nplans && rc == HB_OK; ++i) {
         const hb_plan *p = plans[i];
         coef_table_kernel<<<p->mmax + 1, 256>>>(p->lmax, p->blk_ofs, bp->parts[i].coef);
-        if (cudaGetLastError() != cudaSuccess || launch_ck_mid(p, bp->parts[i].ckh) != HB_OK ||
+        if (cudaGetLastError() != cudaSuccess || launch_ck_mid(p, bp->parts[i].ckh, bp->parts[i].ckq1, bp->parts[i].ckq3) != HB_OK ||
             cudaDeviceSynchronize() != cudaSuccess) {
             rc = fail(HB_ERR_CUDA, "hb_batched_plan_create: coefficient table");
             break;

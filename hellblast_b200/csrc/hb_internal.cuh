@@ -153,9 +153,9 @@ struct hb_plan {
 
 namespace hb {
 // kernels' host launchers (implemented in the .cu files)
-// the plan's scalar recursion states at l0 + 128 of every 256-l block (same indexing as ck);
-// default stream, asynchronous
-int launch_ck_mid(const hb_plan *p, float4 *ck_mid);
+// the plan's scalar recursion states at l0 + 128 of every 256-l block (same indexing as ck), and
+// optionally at l0 + 64 and l0 + 192; default stream, asynchronous
+int launch_ck_mid(const hb_plan *p, float4 *ck_mid, float4 *ck_q1 = nullptr, float4 *ck_q3 = nullptr);
 // F(m, ring pair) workspaces: m-major [m][pair][north, south], or with mblk (the batched FP32
 // analysis) blocked by 8 orders, [m/8][pair][m%8][north, south], so that one ring pair's
 // consecutive orders share 128-byte lines; rows = orders padded to a multiple of 8

@@ -45,8 +45,13 @@ constexpr int CK_NT = 128;
 
 // ck (may be null): states at the block starts; ck_mid (may be null): states at l0 + R/2 of every
 // block that reaches that far, same indexing.
+// states at the start of every CKR-l block (ck), and optionally at its quarter points
+// l0 + CKR/4 (ck_q1), l0 + CKR/2 (ck_mid) and l0 + 3 CKR/4 (ck_q3), same indexing; a state past
+// lmax is not written
 __global__ void __launch_bounds__(CK_NT) ck_scalar_kernel(GeomDev g, int lmax, const int64_t *__restrict__ blk_ofs,
-                                                          float4 *__restrict__ ck, float4 *__restrict__ ck_mid) {
+                                                          float4 *__restrict__ ck, float4 *__restrict__ ck_mid,
+                                                          float4 *__restrict__ ck_q1 = nullptr,
+                                                          float4 *__restrict__ ck_q3 = nullptr) {
     const int m = blockIdx.x;
     const int64_t p = (int64_t)blockIdx.y * CK_NT + threadIdx.x;
     __shared__ double2 cf[CKR];
@@ -77,6 +82,8 @@ __global__ void __launch_bounds__(CK_NT) ck_scalar_kernel(GeomDev g, int lmax, c
         const int n = min(CKR, lmax - l0 + 1);
         for (int i = 0; i < n; ++i) {
             if (i == CKR / 2 && live && ck_mid) ck_mid[oj] = to_f32_state(l1, l2, e);
+            if (i == CKR / 4 && live && ck_q1) ck_q1[oj] = to_f32_state(l1, l2, e);
+            if (i == 3 * CKR / 4 && live && ck_q3) ck_q3[oj] = to_f32_state(l1, l2, e);
             double v = cf[i].x * x * l1 + cf[i].y * l2;
             l2 = l1;
             l1 = v;
@@ -145,10 +152,10 @@ __global__ void __launch_bounds__(CK_NT) ck_spin_kernel(GeomDev g, int lmax, con
     }
 }
 
-int launch_ck_mid(const hb_plan *p, float4 *ck_mid) {
+int launch_ck_mid(const hb_plan *p, float4 *ck_mid, float4 *ck_q1, float4 *ck_q3) {
     const int64_t np = p->g->d.npairs;
     dim3 grid((unsigned)(p->mmax + 1), (unsigned)((np + CK_NT - 1) / CK_NT));
-    ck_scalar_kernel<<<grid, CK_NT>>>(p->g->d, p->lmax, p->blk_ofs, nullptr, ck_mid);
+    ck_scalar_kernel<<<grid, CK_NT>>>(p->g->d, p->lmax, p->blk_ofs, nullptr, ck_mid, ck_q1, ck_q3);
     HB_CUDA_TRY(cudaGetLastError());
     return HB_OK;
 }

@@ -121,3 +121,12 @@ def test_autotune_cache_round_trip(tmp_path, monkeypatch):
     assert batched._cache_load()[batched._cache_key(key)] == res
     batched._cache_store((1, 2, 3, "x"), {"bf16": True, "wide": False, "candidates": []})
     assert len(batched._cache_load()) == 2
+
+
+def test_clear_caches_empties_plan_caches():
+    import hellblast_b200 as hb
+    from hellblast_b200 import batched, geometry
+    geometry._cache[("probe",)] = object()
+    batched._cache[("probe",)] = object()
+    hb.clear_caches()
+    assert not geometry._cache and not batched._cache
