@@ -175,10 +175,11 @@ static int finish_geom(HostGeom &h, int64_t nside, const std::vector<double> &xn
     // HB_NO_PAIR_PACK_BLU the Bluestein pairs)
     const bool pack = std::getenv("HB_NO_PAIR_PACK") == nullptr;
     const bool pack_blu = std::getenv("HB_NO_PAIR_PACK_BLU") == nullptr;
+    const bool quad_ok = std::getenv("HB_NO_QUAD_SPLIT") == nullptr;  // HB_NO_QUAD_SPLIT: whole-ring Bluestein
     std::vector<std::pair<int32_t, int32_t>> pk, rest;
     std::vector<int64_t> pkb_ofs(np, -1);
     std::map<int, int64_t> bt_of_n;  // ring length -> offset of its chirp spectrum
-    std::vector<int32_t> bt_n, bt_logL;
+    std::vector<int32_t> bt_n, bt_rn, bt_logL;  // chirp length, ring length, log2 chirp transform length
     std::vector<int64_t> bt_ofs;
     int64_t bt_total = 0;
     int pk_max_log = 0;
@@ -188,17 +189,19 @@ static int finish_geom(HostGeom &h, int64_t nside, const std::vector<double> &xn
         bool blu = false;
         if (pack && pk_pair_ok(h.nphi[rn], rs >= 0 ? h.nphi[rs] : -1, h.phi0_pi[rn], rs >= 0 ? h.phi0_pi[rs] : 0.0, &lg,
                                &blu) && (pack_blu || !blu)) {
-            pk.push_back({lg | (blu ? 256 : 0), p});
-            pk_max_log = std::max(pk_max_log, lg);
+            const int lq = (blu && quad_ok) ? pk_quad_log(h.nphi[rn], lg) : 0;  // quad split: 4 x length n/4
+            const int lc = lq ? lq : lg;                                          // chirp transform length
+            pk.push_back({lc | (blu ? 256 : 0) | (lq ? 512 : 0), p});
+            pk_max_log = std::max(pk_max_log, lc);
             if (blu) {
                 auto it = bt_of_n.find(h.nphi[rn]);
                 if (it == bt_of_n.end()) {
                     it = bt_of_n.emplace(h.nphi[rn], bt_total).first;
-                    bt_n.push_back(h.nphi[rn]);
-                    bt_logL.push_back(lg);
+                    bt_n.push_back(lq ? h.nphi[rn] / 4 : h.nphi[rn]);
+                    bt_rn.push_back(h.nphi[rn]);
+                    bt_logL.push_back(lc);
                     bt_ofs.push_back(bt_total);
-                    // chirp spectrum (L), chirp (L/2), phase block; offsets stay even (16-byte aligned)
-                    bt_total += ((int64_t(3) << lg) / 2 + pk_phase_entries(lg) + 1) & ~int64_t(1);
+                    bt_total += pk_bt_entries(lc, lq != 0);  // chirp spectrum, chirp, phase block
                 }
                 pkb_ofs[p] = it->second;
             }
@@ -243,7 +246,8 @@ static int finish_geom(HostGeom &h, int64_t nside, const std::vector<double> &xn
            o_t64 = carve(16 * ((size_t)1 << (log_tw - 1))), o_t32 = carve(8 * ((size_t)1 << (log_tw - 1))),
            o_cp = carve(4 * (size_t)np), o_pk = carve(4 * (size_t)np), o_rest = carve(4 * (size_t)np),
            o_pkbo = carve(8 * (size_t)np), o_bt = carve(8 * (size_t)(bt_total + 1)),
-           o_btn = carve(4 * (bt_n.size() + 1)), o_btl = carve(4 * (bt_n.size() + 1)), o_bto = carve(8 * (bt_n.size() + 1));
+           o_btn = carve(4 * (bt_n.size() + 1)), o_btl = carve(4 * (bt_n.size() + 1)), o_bto = carve(8 * (bt_n.size() + 1)),
+           o_btr = carve(4 * (bt_n.size() + 1));
     int64_t tw_ofs[PK_MAX_LOG + 1] = {}, tw_total = 0;  // pair-packed table blocks per length class
     for (int lg = PK_MIN_LOG; lg <= PK_MAX_LOG; ++lg) {
         tw_ofs[lg] = tw_total;
@@ -296,7 +300,8 @@ static int finish_geom(HostGeom &h, int64_t nside, const std::vector<double> &xn
         {d.log2spin, spin.data(), 8 * (size_t)(HB_MAX_L + 1)}, {d.cls_pairs, cls_pairs.data(), 4 * (size_t)np},
         {d.pk_pairs, pk_pairs.data(), 4 * (size_t)np}, {d.rest_pairs, rest_pairs.data(), 4 * (size_t)np},
         {d.pkb_bt_ofs, pkb_ofs.data(), 8 * (size_t)np}, {base + o_btn, bt_n.data(), 4 * bt_n.size()},
-        {base + o_btl, bt_logL.data(), 4 * bt_n.size()}, {base + o_bto, bt_ofs.data(), 8 * bt_n.size()}};
+        {base + o_btl, bt_logL.data(), 4 * bt_n.size()}, {base + o_bto, bt_ofs.data(), 8 * bt_n.size()},
+        {base + o_btr, bt_rn.data(), 4 * bt_n.size()}};
     for (auto &u : ups) {
         if (cudaMemcpy(u.dst, u.src, u.n, cudaMemcpyHostToDevice) != cudaSuccess) {
             cudaGetLastError();
@@ -310,8 +315,8 @@ static int finish_geom(HostGeom &h, int64_t nside, const std::vector<double> &xn
         rc = build_pk_chirp_tables(d, (int)bt_n.size(), (const int32_t *)(base + o_btn), (const int32_t *)(base + o_btl),
                                    (const int64_t *)(base + o_bto), pk_max_log, d.pkb_bt, 0);
     if (rc == HB_OK)
-        rc = build_pk_tables(d, (int)bt_n.size(), (const int32_t *)(base + o_btn), (const int32_t *)(base + o_btl),
-                             (const int64_t *)(base + o_bto), 0);
+        rc = build_pk_tables(d, (int)bt_n.size(), (const int32_t *)(base + o_btn), (const int32_t *)(base + o_btr),
+                             (const int32_t *)(base + o_btl), (const int64_t *)(base + o_bto), 0);
     if (rc == HB_OK && cudaStreamSynchronize(0) != cudaSuccess) rc = fail(HB_ERR_CUDA, "hb_geom: table build failed");
     if (rc != HB_OK) {
         cudaFree(base);

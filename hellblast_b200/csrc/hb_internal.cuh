@@ -109,14 +109,14 @@ struct GeomDev {
     int64_t cls_first[33];
     int max_nphi;
     // FP32 ring FFTs: pairs taken by the pair-packed kernels (hb_ringpack.cu), grouped by
-    // class key log2 L | (Bluestein << 8), and the remaining pairs in convolution-length
-    // classes as above
+    // class key log2 L | (Bluestein << 8) | (quad split << 9) (quad split: L is the quarter-length
+    // sub-transform's), and the remaining pairs in convolution-length classes as above
     int32_t *pk_pairs;     // [npairs]
     int pk_n_cls;
     int pk_logn[16];
     int64_t pk_first[17];
     // pair-packed Bluestein tables per distinct n: chirp spectrum (L), chirp (L/2), then the
-    // phase block of the CTA table (pk_phase_entries)
+    // phase block of the CTA table (pk_bt_entries; quad split: the chirp of length n/4)
     float2 *pkb_bt;
     int64_t *pkb_bt_ofs;   // [npairs] offset of the pair's table in pkb_bt (-1: not Bluestein)
     // per transform length 2^k, k in [PK_MIN_LOG, PK_MAX_LOG]: the pair-packed kernels' shared
@@ -192,18 +192,25 @@ int launch_spin_synthesis(const GeomDev &g, int precision, int nmaps, int lmax, 
 int build_fft_tables(GeomDev &g, cudaStream_t st);
 // pair-packed FP32 ring FFTs (hb_ringpack.cu) over the geometry's pk_* pairs
 bool pk_pair_ok(int nphiN, int nphiS, double phi0N_pi, double phi0S_pi, int *logL, bool *blu);
+// log2 of the quarter-length sub-transform when a Bluestein pair of ring length n and whole-ring
+// Bluestein length 2^logL runs split in four (hb_ringpack.cu), else 0
+int pk_quad_log(int n, int logL);
 // chirp spectra of the pair-packed Bluestein pairs: count tables, table e of length 2^logL[e]
-// for ring length ns[e] at out + ofs[e] (device arrays); FP64 computed, FP32 stored
+// for chirp length ns[e] (the ring length, or a quarter of it for a quad-split ring) at
+// out + ofs[e] (device arrays); FP64 computed, FP32 stored
 int build_pk_chirp_tables(const GeomDev &g, int count, const int32_t *ns, const int32_t *logL, const int64_t *ofs,
                           int max_logL, float2 *out, cudaStream_t st);
 // the pair-packed kernels' table blocks: entries of the block for transform length 2^logL
 // (twiddles and phases) and of its phase part (one per Bluestein ring length)
 int64_t pk_tab_entries(int logL);
 int64_t pk_phase_entries(int logL);
+// entries of one Bluestein pair's table (chirp spectrum, chirp, phase block) for chirp length
+// 2^logL, quad-split or not
+int64_t pk_bt_entries(int logL, bool quad);
 // fills g.pk_tw (every length class) and the phase part of each Bluestein table (count tables as
-// for build_pk_chirp_tables, phase block at ofs[e] + 3 L / 2)
-int build_pk_tables(const GeomDev &g, int count, const int32_t *ns, const int32_t *logL, const int64_t *ofs,
-                    cudaStream_t st);
+// for build_pk_chirp_tables, ring lengths rn[e], phase block at ofs[e] + 3 L / 2)
+int build_pk_tables(const GeomDev &g, int count, const int32_t *ns, const int32_t *rn, const int32_t *logL,
+                    const int64_t *ofs, cudaStream_t st);
 int launch_pk_synthesis(const GeomDev &g, int nmaps, const float2 *Gm, int mmax, float *maps, int64_t map_stride,
                         const double *w, bool apply_w, bool mdouble, int flags, cudaStream_t st);
 int launch_pk_analysis(const GeomDev &g, int nmaps, const float *maps, int64_t map_stride, const double *w,

@@ -161,7 +161,7 @@ __device__ __forceinline__ void pk_twiddle(float2 *v, int e, int j, const PkTab 
 // points from L/2 on are zero and are not read.  HOUT (last pass only): output points from L/2
 // on are neither computed nor written.
 template <int LOGL, int P, bool INV, bool HIN, bool HOUT, class Ld, class St>
-__device__ __forceinline__ void pk_pass(const PkTab &T, Ld &&ld, St &&st) {
+__device__ __forceinline__ void pk_pass(const PkTab &T, int tid, Ld &&ld, St &&st) {
     using C = PkCfg<LOGL>;
     constexpr int L = C::L, NT = C::NT, R = PkPass<LOGL, P>::R, NS = PkPass<LOGL, P>::NS, G = 16 / R;
     static_assert(!HIN || (P == 0 && R == 16), "half input: the first pass, radix 16");
@@ -169,11 +169,11 @@ __device__ __forceinline__ void pk_pass(const PkTab &T, Ld &&ld, St &&st) {
     static_assert((L / R) % 16 == 0 && NT % 16 == 0 && (NS == 1 || NS % 16 == 0) && (NS > 1 || R == 16),
                   "padded offsets are base plus constants");
     constexpr int LS = L / R + L / R / 16, US = NT + NT / 16, QS = NS == 1 ? 1 : NS + NS / 16;
-    const int tp = pk_pad(threadIdx.x);
+    const int tp = pk_pad(tid);
     float2 x[16];
 #pragma unroll
     for (int u = 0; u < G; ++u) {
-        const int b = threadIdx.x + u * NT, bp = tp + u * US;
+        const int b = tid + u * NT, bp = tp + u * US;
 #pragma unroll
         for (int t = 0; t < R; ++t)
             if (!HIN || t < R / 2) x[u * R + t] = ld(b + t * (L / R), bp + t * LS);
@@ -181,7 +181,7 @@ __device__ __forceinline__ void pk_pass(const PkTab &T, Ld &&ld, St &&st) {
     __syncthreads();
 #pragma unroll
     for (int u = 0; u < G; ++u) {
-        const int b = threadIdx.x + u * NT;
+        const int b = tid + u * NT;
         const int j = b & (NS - 1);
         float2 *v = x + u * R;
         if constexpr (NS > 1) pk_twiddle<R, INV>(v, j * (L / (NS * R)), j, T);
@@ -198,22 +198,23 @@ __device__ __forceinline__ void pk_pass(const PkTab &T, Ld &&ld, St &&st) {
 }
 
 // passes P .. NPASS-1; pass 0 reads through ld0 (HIN: half input), the last pass writes through
-// stl (HOUT: half output), the others go through the shared buffer
+// stl (HOUT: half output), the others go through the shared buffer.  tid: the thread's index
+// among the L/16 threads of this transform (every thread of the CTA reaches the barriers)
 template <int LOGL, bool INV, bool HIN, bool HOUT, int P = 0, class Ld0, class StL>
-__device__ __forceinline__ void pk_run(float2 *buf, const PkTab &T, Ld0 &&ld0, StL &&stl) {
+__device__ __forceinline__ void pk_run(float2 *buf, const PkTab &T, int tid, Ld0 &&ld0, StL &&stl) {
     constexpr int NP = PkCfg<LOGL>::NPASS;
     static_assert(NP >= 3, "pair-packed lengths have at least three passes");
     auto lds = [&](int, int ip) -> float2 { return buf[ip]; };
     auto sts = [&](int, int ip, float2 v) { buf[ip] = v; };
     if constexpr (P == NP - 1) {
-        pk_pass<LOGL, P, INV, false, HOUT>(T, lds, stl);
+        pk_pass<LOGL, P, INV, false, HOUT>(T, tid, lds, stl);
     } else {
         if constexpr (P == 0)
-            pk_pass<LOGL, P, INV, HIN, false>(T, ld0, sts);
+            pk_pass<LOGL, P, INV, HIN, false>(T, tid, ld0, sts);
         else
-            pk_pass<LOGL, P, INV, false, false>(T, lds, sts);
+            pk_pass<LOGL, P, INV, false, false>(T, tid, lds, sts);
         __syncthreads();
-        pk_run<LOGL, INV, HIN, HOUT, P + 1>(buf, T, ld0, stl);
+        pk_run<LOGL, INV, HIN, HOUT, P + 1>(buf, T, tid, ld0, stl);
     }
 }
 
@@ -240,45 +241,17 @@ struct PkMod {
     }
 };
 
-// ------------------------------------------------------------------------------ synthesis
-// G[map][m][pair][side] (FP32 complex; one float4 = (north, south) per (m, pair)) -> the two
-// rings of each pair.  c_m = 1 for m = 0 and `dbl` (2: real-field synthesis, 1: adjoint of the
-// weighted analysis) for m > 0; apply_w multiplies ring r by scale 2 pi w_r / n (no 2 pi with
-// HB_F_NO2PI).  BLU: n is not a power of two and L is its Bluestein length.
-template <int LOGL, bool BLU>
-__global__ void __launch_bounds__(PkCfg<LOGL>::NT, PkCfg<LOGL>::MINB)
-    ring_pair_synthesis_kernel(GeomDev g, const int32_t *__restrict__ pairs, const float4 *__restrict__ Gm,
-                               int64_t gm_stride4, int mmax, float *__restrict__ maps, int64_t map_stride,
-                               const double *__restrict__ w, int apply_w, int mdouble, int flags) {
-    using C = PkCfg<LOGL>;
-    constexpr int L = C::L, NT = C::NT;
-    extern __shared__ __align__(16) float2 pk_smem[];
-    float2 *buf = pk_smem;
-    const int pair = pairs[BLU ? blockIdx.y : blockIdx.x], bm = BLU ? blockIdx.x : blockIdx.y;
-    const int rN = g.pair_ring[2 * pair], rS = g.pair_ring[2 * pair + 1];
-    const int n = BLU ? g.nphi[rN] : L;
-    // Bluestein tables: chirp spectrum bt[0, L), chirp ch[t] = exp(-i pi t^2 / n) for t < n, then
-    // the ring's phase block
-    const float2 *bt = BLU ? g.pkb_bt + g.pkb_bt_ofs[pair] : nullptr, *ch = BLU ? bt + L : nullptr;
-    const PkTab T = pk_tables<LOGL>(pk_smem + C::BUF, g.pk_tw + g.pk_tw_ofs[LOGL], BLU ? bt + L + L / 2 : nullptr);
-    const int s = (flags & HB_F_NOPHASE) ? 0 : pk_shift(g.phi0_pi[rN], n);
-    const int64_t np = g.npairs;
-    const float4 *gin = Gm + bm * gm_stride4 + pair;  // (m, pair) entry at gin[m * np]
-    const float dbl = mdouble ? 2.f : 1.f, chalf = 0.5f * dbl;
+// The spectrum Z of z = f_N + i f_S from the two rings' coefficients G(m) (ld(m): the float4
+// (north, south) of order m <= mmax): alias fold by m mod n, the phi0 phase exp(i pi s k / n) and
+// (-1)^(s j) over the aliases m = k + j n; put(k, Z_k) for every k < n (CTA-strided loops of NT
+// threads).  c_m = 1 for m = 0, dbl for m > 0.  P2: n is a power of two.
+template <int NT, bool P2, class Ld, class Put>
+__device__ __forceinline__ void pk_fold(int n, int s, int mmax, float dbl, const PkTab &T, Ld &&ld, Put &&put) {
+    const float chalf = 0.5f * dbl;
     const float sg = (s & 1) ? -1.f : 1.f;
-    const bool hasS = rS >= 0;
     const PkMod mod2n{2 * n, 1.f / (float)(2 * n)};
     // phase-table index of exp(i pi s k / n): (s k) mod 2n (s k < 2^31: s < 2n <= 2^15, k <= n)
-    auto pidx = [&](int k) -> int { return BLU ? mod2n(s * k) : ((s * k) & (2 * n - 1)); };
-    __syncthreads();  // tables
-    // spectrum point k of z: stored as is (direct) or as conj(Z[k]) c_k (Bluestein)
-    auto put = [&](int k, float2 z) { buf[pk_pad(k)] = BLU ? cmul(cconj(z), __ldg(ch + k)) : z; };
-    // an unpaired ring's south slot is not read as data: zeros keep the imaginary half finite
-    auto ld = [&](int m) -> float4 {
-        float4 v = __ldg(gin + (int64_t)m * np);
-        if (!hasS) v.z = v.w = 0.f;
-        return v;
-    };
+    auto pidx = [&](int k) -> int { return P2 ? ((s * k) & (2 * n - 1)) : mod2n(s * k); };
     // class sums S(k) = sum_j (-1)^(s j) c_m / 2 G(k + j n), north and south
     auto csum = [&](int k, float2 &a, float2 &c) {
         a = make_float2(0.f, 0.f);
@@ -334,6 +307,44 @@ __global__ void __launch_bounds__(PkCfg<LOGL>::NT, PkCfg<LOGL>::MINB)
         const float2 ph = T.ph(pidx(n / 2));
         put(n / 2, make_float2(2.f * (ph.x * hN.x - ph.y * hN.y), 2.f * (ph.x * hS.x - ph.y * hS.y)));
     }
+}
+
+// ------------------------------------------------------------------------------ synthesis
+// G[map][m][pair][side] (FP32 complex; one float4 = (north, south) per (m, pair)) -> the two
+// rings of each pair.  c_m = 1 for m = 0 and `dbl` (2: real-field synthesis, 1: adjoint of the
+// weighted analysis) for m > 0; apply_w multiplies ring r by scale 2 pi w_r / n (no 2 pi with
+// HB_F_NO2PI).  BLU: n is not a power of two and L is its Bluestein length.
+template <int LOGL, bool BLU>
+__global__ void __launch_bounds__(PkCfg<LOGL>::NT, PkCfg<LOGL>::MINB)
+    ring_pair_synthesis_kernel(GeomDev g, const int32_t *__restrict__ pairs, const float4 *__restrict__ Gm,
+                               int64_t gm_stride4, int mmax, float *__restrict__ maps, int64_t map_stride,
+                               const double *__restrict__ w, int apply_w, int mdouble, int flags) {
+    using C = PkCfg<LOGL>;
+    constexpr int L = C::L, NT = C::NT;
+    extern __shared__ __align__(16) float2 pk_smem[];
+    float2 *buf = pk_smem;
+    const int pair = pairs[BLU ? blockIdx.y : blockIdx.x], bm = BLU ? blockIdx.x : blockIdx.y;
+    const int rN = g.pair_ring[2 * pair], rS = g.pair_ring[2 * pair + 1];
+    const int n = BLU ? g.nphi[rN] : L;
+    // Bluestein tables: chirp spectrum bt[0, L), chirp ch[t] = exp(-i pi t^2 / n) for t < n, then
+    // the ring's phase block
+    const float2 *bt = BLU ? g.pkb_bt + g.pkb_bt_ofs[pair] : nullptr, *ch = BLU ? bt + L : nullptr;
+    const PkTab T = pk_tables<LOGL>(pk_smem + C::BUF, g.pk_tw + g.pk_tw_ofs[LOGL], BLU ? bt + L + L / 2 : nullptr);
+    const int s = (flags & HB_F_NOPHASE) ? 0 : pk_shift(g.phi0_pi[rN], n);
+    const int64_t np = g.npairs;
+    const float4 *gin = Gm + bm * gm_stride4 + pair;  // (m, pair) entry at gin[m * np]
+    const float dbl = mdouble ? 2.f : 1.f;
+    const bool hasS = rS >= 0;
+    __syncthreads();  // tables
+    // spectrum point k of z: stored as is (direct) or as conj(Z[k]) c_k (Bluestein)
+    auto put = [&](int k, float2 z) { buf[pk_pad(k)] = BLU ? cmul(cconj(z), __ldg(ch + k)) : z; };
+    // an unpaired ring's south slot is not read as data: zeros keep the imaginary half finite
+    auto ld = [&](int m) -> float4 {
+        float4 v = __ldg(gin + (int64_t)m * np);
+        if (!hasS) v.z = v.w = 0.f;
+        return v;
+    };
+    pk_fold<NT, !BLU>(n, s, mmax, dbl, T, ld, put);
     if (BLU)  // zero padding of the convolution (the first pass reads points below L/2 only)
         for (int k = n + threadIdx.x; k < L / 2; k += NT) buf[pk_pad(k)] = make_float2(0.f, 0.f);
     __syncthreads();
@@ -344,24 +355,61 @@ __global__ void __launch_bounds__(PkCfg<LOGL>::NT, PkCfg<LOGL>::MINB)
     float *fS = hasS ? maps + bm * map_stride + g.ofs[rS] : nullptr;
     auto lds = [&](int, int ip) -> float2 { return buf[ip]; };
     if constexpr (!BLU) {
-        pk_run<LOGL, true, false, false>(buf, T, lds, [&](int i, int, float2 v) {
+        pk_run<LOGL, true, false, false>(buf, T, threadIdx.x, lds, [&](int i, int, float2 v) {
             fN[i] = v.x * psN;
             if (fS) fS[i] = v.y * psS;
         });
     } else {
         // forward FFT_L (input zero from L/2 on), times the chirp spectrum
-        pk_run<LOGL, false, true, false>(buf, T, lds, [&](int, int ip, float2 v) { buf[ip] = v; });
+        pk_run<LOGL, false, true, false>(buf, T, threadIdx.x, lds, [&](int, int ip, float2 v) { buf[ip] = v; });
         __syncthreads();
         for (int i = threadIdx.x; i < L; i += NT) buf[pk_pad(i)] = cmul(buf[pk_pad(i)], __ldg(bt + i));
         __syncthreads();
         // inverse FFT_L, points below L/2 only; times the chirp, conjugated, to the two rings
-        pk_run<LOGL, true, false, true>(buf, T, lds, [&](int i, int, float2 v) {
+        pk_run<LOGL, true, false, true>(buf, T, threadIdx.x, lds, [&](int i, int, float2 v) {
             if (i < n) {
                 const float2 z = cconj(cmul(__ldg(ch + i), v));
                 fN[i] = z.x * psN;
                 if (fS) fS[i] = z.y * psS;
             }
         });
+    }
+}
+
+// The orders of the two rings from the spectrum Z of z = f_N + i f_S (Zf(k), k < n):
+// D_N = (Z[k] + conj Z[n-k]) / 2 and D_S = (Z[k] - conj Z[n-k]) / (2 i), times exp(-i pi s k / n)
+// and the ring scales scN / scS, stored through at(m) for every m <= mlim of residue class k
+// ((-1)^(s j) over the aliases m = k + j n) and, conjugated, of class n - k; c_m = 2 for m > 0
+// with mdouble; the orders mlim < m <= mmax are zero.  CTA-strided loops of NT threads; P2: n is
+// a power of two.
+template <int NT, bool P2, class Zfn, class At>
+__device__ __forceinline__ void pk_emit(int n, int s, int mmax, int mlim, bool mdouble, float scN, float scS,
+                                        const PkTab &T, Zfn &&Zf, At &&at) {
+    const PkMod mod2n{2 * n, 1.f / (float)(2 * n)};
+    auto pidx = [&](int k) -> int { return P2 ? ((s * k) & (2 * n - 1)) : mod2n(s * k); };
+    // HB_F_NOFOLD: the orders the ring does not resolve (m >= n) are zero, not left unwritten
+    for (int m = mlim + 1 + threadIdx.x; m <= mmax; m += NT) at(m) = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int k = threadIdx.x; k <= n / 2; k += NT) {
+        const float2 zk = Zf(k), zc = k == 0 ? zk : Zf(n - k);
+        // D_N = (Z[k] + conj Z[n-k]) / 2, D_S = (Z[k] - conj Z[n-k]) / (2 i)
+        const float2 dN = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y - zc.y));
+        const float2 dS = make_float2(0.5f * (zk.y + zc.y), -0.5f * (zk.x - zc.x));
+        const float2 ph = cconj(T.ph(pidx(k)));
+        const float2 yN = cscale(cmul(ph, dN), scN), yS = cscale(cmul(ph, dS), scS);
+        float sj = 1.f;
+        for (int m = k; m <= mlim; m += n) {  // class k: (-1)^(s j) Y
+            const float c = (mdouble && m > 0) ? 2.f * sj : sj;
+            at(m) = make_float4(c * yN.x, c * yN.y, c * yS.x, c * yS.y);
+            if (s & 1) sj = -sj;
+        }
+        if (k > 0 && 2 * k < n) {  // class n - k: (-1)^(s (j + 1)) conj Y
+            sj = (s & 1) ? -1.f : 1.f;
+            for (int m = n - k; m <= mlim; m += n) {
+                const float c = mdouble ? 2.f * sj : sj;
+                at(m) = make_float4(c * yN.x, -c * yN.y, c * yS.x, -c * yS.y);
+                if (s & 1) sj = -sj;
+            }
+        }
     }
 }
 
@@ -392,23 +440,21 @@ __global__ void __launch_bounds__(PkCfg<LOGL>::NT, PkCfg<LOGL>::MINB)
     const int64_t np = g.npairs;
     const float *fN = maps + bm * map_stride + g.ofs[rN];
     const float *fS = rS >= 0 ? maps + bm * map_stride + g.ofs[rS] : nullptr;
-    const PkMod mod2n{2 * n, 1.f / (float)(2 * n)};
-    auto pidx = [&](int k) -> int { return BLU ? mod2n(s * k) : ((s * k) & (2 * n - 1)); };
     auto sts = [&](int, int ip, float2 v) { buf[ip] = v; };
     auto ring = [&](int i, int = 0) -> float2 { return make_float2(__ldg(fN + i), fS ? __ldg(fS + i) : 0.f); };
     __syncthreads();  // tables
     if constexpr (!BLU) {
-        pk_run<LOGL, false, false, false>(buf, T, ring, sts);
+        pk_run<LOGL, false, false, false>(buf, T, threadIdx.x, ring, sts);
     } else {
         // forward FFT_L of the chirped ring (zero from n on; read below L/2 only), times the chirp
         // spectrum; inverse FFT_L, points below L/2 only
         auto lds = [&](int, int ip) -> float2 { return buf[ip]; };
         auto ld0 = [&](int i, int) -> float2 { return i < n ? cmul(ring(i), __ldg(ch + i)) : make_float2(0.f, 0.f); };
-        pk_run<LOGL, false, true, false>(buf, T, ld0, sts);
+        pk_run<LOGL, false, true, false>(buf, T, threadIdx.x, ld0, sts);
         __syncthreads();
         for (int i = threadIdx.x; i < L; i += NT) buf[pk_pad(i)] = cmul(buf[pk_pad(i)], __ldg(bt + i));
         __syncthreads();
-        pk_run<LOGL, true, false, true>(buf, T, lds, sts);
+        pk_run<LOGL, true, false, true>(buf, T, threadIdx.x, lds, sts);
     }
     __syncthreads();
     auto Zf = [&](int k) -> float2 { return BLU ? cmul(__ldg(ch + k), buf[pk_pad(k)]) : buf[pk_pad(k)]; };
@@ -418,30 +464,199 @@ __global__ void __launch_bounds__(PkCfg<LOGL>::NT, PkCfg<LOGL>::MINB)
     const int mlim = (flags & HB_F_NOFOLD) ? min(mmax, n - 1) : mmax;
     float4 *out = Fm + bm * fm_stride4;
     auto at = [&](int m) -> float4 & { return out[fg_off(m, pair, np, mblk != 0)]; };
-    // HB_F_NOFOLD: the orders the ring does not resolve (m >= n) are zero, not left unwritten
-    for (int m = mlim + 1 + threadIdx.x; m <= mmax; m += NT) at(m) = make_float4(0.f, 0.f, 0.f, 0.f);
-    for (int k = threadIdx.x; k <= n / 2; k += NT) {
-        const float2 zk = Zf(k), zc = k == 0 ? zk : Zf(n - k);
-        // D_N = (Z[k] + conj Z[n-k]) / 2, D_S = (Z[k] - conj Z[n-k]) / (2 i)
-        const float2 dN = make_float2(0.5f * (zk.x + zc.x), 0.5f * (zk.y - zc.y));
-        const float2 dS = make_float2(0.5f * (zk.y + zc.y), -0.5f * (zk.x - zc.x));
-        const float2 ph = cconj(T.ph(pidx(k)));
-        const float2 yN = cscale(cmul(ph, dN), scN), yS = cscale(cmul(ph, dS), scS);
-        float sj = 1.f;
-        for (int m = k; m <= mlim; m += n) {  // class k: (-1)^(s j) Y
-            const float c = (mdouble && m > 0) ? 2.f * sj : sj;
-            at(m) = make_float4(c * yN.x, c * yN.y, c * yS.x, c * yS.y);
-            if (s & 1) sj = -sj;
-        }
-        if (k > 0 && 2 * k < n) {  // class n - k: (-1)^(s (j + 1)) conj Y
-            sj = (s & 1) ? -1.f : 1.f;
-            for (int m = n - k; m <= mlim; m += n) {
-                const float c = mdouble ? 2.f * sj : sj;
-                at(m) = make_float4(c * yN.x, -c * yN.y, c * yS.x, -c * yS.y);
-                if (s & 1) sj = -sj;
-            }
+    pk_emit<NT, !BLU>(n, s, mmax, mlim, mdouble != 0, scN, scS, T, Zf, at);
+}
+
+// ------------------------------------------------------------------------ quad-split Bluestein
+// Ring length n = 4 q (HEALPix polar rings: n = 4 i) that is not a power of two and whose
+// Bluestein length for the whole ring would be 2^13 or 2^14: radix-4 Cooley-Tukey turns the
+// length-n DFT into four length-q DFTs, and each of those runs as a Bluestein convolution of
+// length LQ = 2^LOGQ >= 2q - 1 (a quarter of the whole ring's L), all four side by side in one
+// CTA: four groups of LQ/16 threads, one sub-buffer each.  With Y = conj Z (synthesis, the
+// inverse DFT as conj(DFT(conj Z))) and W_n = exp(-2 pi i / n):
+//   synthesis (decimation of the output): y_{4a+b} = sum_r W_q^(a r) V^b_r,
+//     V^b_r = W_n^(b r) sum_t Y_(r+qt) (-i)^(b t);
+//   analysis (decimation of the input): U^b = DFT_q(z_(4a+b)),
+//     Z_(k+qt) = sum_b (-i)^(b t) W_n^(b k) U^b_k.
+// Each length-LQ transform takes 3 passes (LOGQ = 11, 12) where the whole ring's takes 4, and the
+// chirp spectrum (LQ entries) fits in shared memory beside the buffers, so its product rides in
+// the forward transform's last pass.  The radix-4 steps are one extra exchange through the
+// shared buffer each (natural order <-> the four sub-buffers).  Per-ring table (pkb_bt): the
+// length-q chirp spectrum (LQ), the length-q chirp c_t = exp(-i pi t^2 / q) (t < LQ/2, zero from
+// q on), then the phase block of n with 4 LQ / 64 coarse entries (2n <= 4 LQ).
+template <int LOGQ> struct QkCfg {
+    using S = PkCfg<LOGQ>;
+    static constexpr int LQ = S::L, NTQ = S::NT, NT = 4 * NTQ;
+    static constexpr int SBUF = S::BUF, BUF = 4 * SBUF;  // four sub-buffers
+    static constexpr int PHC = 4 * LQ / 64;              // coarse phases exp(i pi 64 c / n), 2n <= 4 LQ
+    static constexpr int TAB = S::TWB + 64 + PHC;        // twiddles of LQ, then the phases of n
+    static constexpr int SMEM = (BUF + TAB + LQ) * (int)sizeof(float2);  // + the chirp spectrum
+    static constexpr int MINB = 65536 / (NT * 64) > 0 ? 65536 / (NT * 64) : 1;  // <= 64 registers
+    static constexpr int RPT = (LQ / 2) / NT;            // radix-4 steps: residues r < LQ/2 per thread
+    static_assert(NT <= 1024 && RPT * NT == LQ / 2, "one CTA of four sub-transforms");
+    static_assert(LQ / 2 + (LQ - 1) / 16 < SBUF, "upper half-buffers hold q <= LQ/2 spectrum points each");
+};
+
+// the CTA's tables: twiddles of LQ (gtw), the phase block of n (gph), the chirp spectrum (gbt)
+template <int LOGQ>
+__device__ __forceinline__ PkTab qk_tables(float2 *base, const float2 *__restrict__ gtw,
+                                           const float2 *__restrict__ gph, const float2 *__restrict__ gbt) {
+    using C = QkCfg<LOGQ>;
+    using S = PkCfg<LOGQ>;
+    float2 *tw1 = base, *tw4 = tw1 + S::TWP, *tws = tw4 + S::TWP, *phf = tws + S::TWS, *phc = phf + 64;
+    for (int i = threadIdx.x; i < C::TAB + C::LQ; i += C::NT)
+        base[i] = pk_ld(i < S::TWB ? gtw + i : (i < C::TAB ? gph + (i - S::TWB) : gbt + (i - C::TAB)));
+    return {tw1, tw4, tws, phf, phc};
+}
+
+// Slot of natural-order spectrum point k = j + q t (j < q, t < 4): the upper half of sub-buffer t,
+// which the sub-transforms leave free (their inputs and outputs lie below LQ/2), so the radix-4
+// steps read one half and write the other without a barrier in between
+template <int LOGQ> __device__ __forceinline__ int qk_slot(int k, int q) {
+    using C = QkCfg<LOGQ>;
+    const int t = (k >= q) + (k >= 2 * q) + (k >= 3 * q);
+    return t * C::SBUF + pk_pad(C::LQ / 2 + k - t * q);
+}
+
+// W_n^(b r) for b = 1, 2, 3 (b r < 3n/4): w1 = conj exp(i pi 2r / n), w2 = w1^2, w3 = w1 w2
+__device__ __forceinline__ void qk_twiddles(const PkTab &T, int r, float2 &w1, float2 &w2, float2 &w3) {
+    w1 = cconj(T.ph(2 * r));
+    w2 = cmul(w1, w1);
+    w3 = cmul(w1, w2);
+}
+
+template <int LOGQ>
+__global__ void __launch_bounds__(QkCfg<LOGQ>::NT, QkCfg<LOGQ>::MINB)
+    ring_quad_synthesis_kernel(GeomDev g, const int32_t *__restrict__ pairs, const float4 *__restrict__ Gm,
+                               int64_t gm_stride4, int mmax, float *__restrict__ maps, int64_t map_stride,
+                               const double *__restrict__ w, int apply_w, int mdouble, int flags) {
+    using C = QkCfg<LOGQ>;
+    constexpr int LQ = C::LQ, NTQ = C::NTQ, NT = C::NT, SB = C::SBUF;
+    extern __shared__ __align__(16) float2 pk_smem[];
+    float2 *buf = pk_smem;
+    const float2 *spec = pk_smem + C::BUF + C::TAB;
+    const int pair = pairs[blockIdx.y], bm = blockIdx.x;  // (map, pair): the maps of a pair share its tables
+    const int rN = g.pair_ring[2 * pair], rS = g.pair_ring[2 * pair + 1];
+    const int n = g.nphi[rN], q = n >> 2;
+    const float2 *bt = g.pkb_bt + g.pkb_bt_ofs[pair], *ch = bt + LQ;
+    const PkTab T = qk_tables<LOGQ>(pk_smem + C::BUF, g.pk_tw + g.pk_tw_ofs[LOGQ], bt + LQ + LQ / 2, bt);
+    const int s = (flags & HB_F_NOPHASE) ? 0 : pk_shift(g.phi0_pi[rN], n);
+    const int64_t np = g.npairs;
+    const float4 *gin = Gm + bm * gm_stride4 + pair;
+    const bool hasS = rS >= 0;
+    __syncthreads();  // tables
+    auto ld = [&](int m) -> float4 {
+        float4 v = __ldg(gin + (int64_t)m * np);
+        if (!hasS) v.z = v.w = 0.f;
+        return v;
+    };
+    // conj Z, point k at qk_slot(k)
+    pk_fold<NT, false>(n, s, mmax, mdouble ? 2.f : 1.f, T, ld,
+                       [&](int k, float2 z) { buf[qk_slot<LOGQ>(k, q)] = cconj(z); });
+    __syncthreads();
+    // radix-4 step: V^b_r c_r into sub-buffer b at r (zero for q <= r < LQ/2)
+#pragma unroll
+    for (int u = 0; u < C::RPT; ++u) {
+        const int r = threadIdx.x + u * NT, rp = pk_pad(r);
+        if (r < q) {
+            const int zp = pk_pad(LQ / 2 + r);
+            float2 x0 = buf[zp], x1 = buf[SB + zp], x2 = buf[2 * SB + zp], x3 = buf[3 * SB + zp];
+            dft4<false>(x0, x1, x2, x3);
+            float2 w1, w2, w3;
+            qk_twiddles(T, r, w1, w2, w3);
+            const float2 c = __ldg(ch + r);
+            buf[rp] = cmul(x0, c);
+            buf[SB + rp] = cmul(x1, cmul(w1, c));
+            buf[2 * SB + rp] = cmul(x2, cmul(w2, c));
+            buf[3 * SB + rp] = cmul(x3, cmul(w3, c));
+        } else {
+            buf[rp] = buf[SB + rp] = buf[2 * SB + rp] = buf[3 * SB + rp] = make_float2(0.f, 0.f);
         }
     }
+    __syncthreads();
+    const int grp = threadIdx.x / NTQ, tq = threadIdx.x % NTQ;
+    float2 *sb = buf + grp * SB;
+    auto lds = [&](int, int ip) -> float2 { return sb[ip]; };
+    // forward FFT_LQ (input zero from LQ/2 on), times the chirp spectrum in its last pass
+    pk_run<LOGQ, false, true, false>(sb, T, tq, lds, [&](int k, int ip, float2 v) { sb[ip] = cmul(v, spec[k]); });
+    __syncthreads();
+    const double sc2 = (flags & HB_F_NO2PI) ? 1.0 : 6.283185307179586476925286766559;
+    const float psN = apply_w ? (float)(sc2 * w[rN] / (double)n) : 1.f;
+    const float psS = (apply_w && hasS) ? (float)(sc2 * w[rS] / (double)n) : 1.f;
+    float *fN = maps + bm * map_stride + g.ofs[rN] + grp;
+    float *fS = hasS ? maps + bm * map_stride + g.ofs[rS] + grp : nullptr;
+    // inverse FFT_LQ, points below LQ/2; output a of sub-transform b is pixel 4a + b
+    pk_run<LOGQ, true, false, true>(sb, T, tq, lds, [&](int a, int, float2 v) {
+        if (a < q) {
+            const float2 z = cconj(cmul(__ldg(ch + a), v));
+            fN[4 * a] = z.x * psN;
+            if (fS) fS[4 * a] = z.y * psS;
+        }
+    });
+}
+
+template <int LOGQ>
+__global__ void __launch_bounds__(QkCfg<LOGQ>::NT, QkCfg<LOGQ>::MINB)
+    ring_quad_analysis_kernel(GeomDev g, const int32_t *__restrict__ pairs, const float *__restrict__ maps,
+                              int64_t map_stride, const double *__restrict__ w, float4 *__restrict__ Fm,
+                              int64_t fm_stride4, int mmax, int flags, int unit_w, int mdouble, int mblk) {
+    using C = QkCfg<LOGQ>;
+    constexpr int LQ = C::LQ, NTQ = C::NTQ, NT = C::NT, SB = C::SBUF;
+    extern __shared__ __align__(16) float2 pk_smem[];
+    float2 *buf = pk_smem;
+    const float2 *spec = pk_smem + C::BUF + C::TAB;
+    const int pair = pairs[mblk ? blockIdx.y : blockIdx.x], bm = mblk ? blockIdx.x : blockIdx.y;
+    const int rN = g.pair_ring[2 * pair], rS = g.pair_ring[2 * pair + 1];
+    const int n = g.nphi[rN], q = n >> 2;
+    const float2 *bt = g.pkb_bt + g.pkb_bt_ofs[pair], *ch = bt + LQ;
+    const PkTab T = qk_tables<LOGQ>(pk_smem + C::BUF, g.pk_tw + g.pk_tw_ofs[LOGQ], bt + LQ + LQ / 2, bt);
+    const int s = (flags & HB_F_NOPHASE) ? 0 : pk_shift(g.phi0_pi[rN], n);
+    const int64_t np = g.npairs;
+    const int grp = threadIdx.x / NTQ, tq = threadIdx.x % NTQ;
+    const float *fN = maps + bm * map_stride + g.ofs[rN] + grp;
+    const float *fS = rS >= 0 ? maps + bm * map_stride + g.ofs[rS] + grp : nullptr;
+    float2 *sb = buf + grp * SB;
+    auto lds = [&](int, int ip) -> float2 { return sb[ip]; };
+    auto sts = [&](int, int ip, float2 v) { sb[ip] = v; };
+    __syncthreads();  // tables
+    // sub-sequence b = grp: samples 4a + b times the chirp c_a (a < q; zero from q to LQ/2);
+    // forward FFT_LQ times the chirp spectrum, inverse FFT_LQ (points below LQ/2)
+    auto ld0 = [&](int a, int) -> float2 {
+        return a < q ? cmul(make_float2(__ldg(fN + 4 * a), fS ? __ldg(fS + 4 * a) : 0.f), __ldg(ch + a))
+                     : make_float2(0.f, 0.f);
+    };
+    pk_run<LOGQ, false, true, false>(sb, T, tq, ld0, [&](int k, int ip, float2 v) { sb[ip] = cmul(v, spec[k]); });
+    __syncthreads();
+    pk_run<LOGQ, true, false, true>(sb, T, tq, lds, sts);
+    __syncthreads();
+    // radix-4 step: U^b_k = c_k (sub-buffer b at k); Z_(k+qt) = sum_b (-i)^(b t) W_n^(b k) U^b_k
+    // to qk_slot(k + q t)
+#pragma unroll
+    for (int u = 0; u < C::RPT; ++u) {
+        const int k = threadIdx.x + u * NT;
+        if (k < q) {
+            const int kp = pk_pad(k), zp = pk_pad(LQ / 2 + k);
+            float2 w1, w2, w3;
+            qk_twiddles(T, k, w1, w2, w3);
+            const float2 c = __ldg(ch + k);
+            float2 x0 = cmul(buf[kp], c), x1 = cmul(buf[SB + kp], cmul(w1, c));
+            float2 x2 = cmul(buf[2 * SB + kp], cmul(w2, c)), x3 = cmul(buf[3 * SB + kp], cmul(w3, c));
+            dft4<false>(x0, x1, x2, x3);
+            buf[zp] = x0;
+            buf[SB + zp] = x1;
+            buf[2 * SB + zp] = x2;
+            buf[3 * SB + zp] = x3;
+        }
+    }
+    __syncthreads();
+    const double sc2 = (flags & HB_F_NO2PI) ? 1.0 : 6.283185307179586476925286766559;
+    const float scN = unit_w ? 1.f : (float)(sc2 * w[rN] / (double)n);
+    const float scS = rS < 0 ? 0.f : (unit_w ? 1.f : (float)(sc2 * w[rS] / (double)n));
+    const int mlim = (flags & HB_F_NOFOLD) ? min(mmax, n - 1) : mmax;
+    float4 *out = Fm + bm * fm_stride4;
+    auto at = [&](int m) -> float4 & { return out[fg_off(m, pair, np, mblk != 0)]; };
+    pk_emit<NT, false>(n, s, mmax, mlim, mdouble != 0, scN, scS, T, [&](int k) { return buf[qk_slot<LOGQ>(k, q)]; },
+                       at);
 }
 
 // ------------------------------------------------------------------------------ host side
@@ -464,6 +679,15 @@ bool pk_pair_ok(int nphiN, int nphiS, double phi0N, double phi0S, int *logL, boo
     *logL = lg;
     *blu = !p2;
     return true;
+}
+
+// log2 of the sub-transform length LQ when a Bluestein pair of ring length n (whole-ring length
+// 2^logL) runs as four quarter-length convolutions (see the quad-split kernels), else 0: n a
+// multiple of 4 and 2^logL = 2^13 or 2^14, where the quarter length saves a pass
+int pk_quad_log(int n, int logL) {
+    if ((n & 3) || (n & (n - 1)) == 0 || (logL != 13 && logL != 14)) return 0;
+    const int lq = pk_log2(2 * (int64_t)(n / 4) - 1);
+    return (lq == logL - 2) ? lq : 0;
 }
 
 template <int LOGL, bool BLU> static int pk_prepare() {
@@ -536,6 +760,62 @@ static int pk_ana_one(const GeomDev &g, const int32_t *pairs, int64_t cnt, const
     return HB_OK;
 }
 
+template <int LOGQ> static int qk_prepare() {
+    static bool done = false;
+    if (!done) {
+        HB_CUDA_TRY(cudaFuncSetAttribute(ring_quad_synthesis_kernel<LOGQ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         QkCfg<LOGQ>::SMEM));
+        HB_CUDA_TRY(cudaFuncSetAttribute(ring_quad_analysis_kernel<LOGQ>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         QkCfg<LOGQ>::SMEM));
+        done = true;
+    }
+    return HB_OK;
+}
+
+// quad-split pairs: (map, pair) grid for the synthesis and the m-blocked analysis, as the
+// Bluestein pairs above
+template <int LOGQ>
+static int qk_syn_one(const GeomDev &g, const int32_t *pairs, int64_t cnt, const PkSynArgs &a, cudaStream_t st) {
+    int rc = qk_prepare<LOGQ>();
+    dim3 grid;
+    if (!rc) rc = pk_grid<true>(cnt, a.nmaps, &grid);
+    if (rc) return rc;
+    const int64_t gm4 = (int64_t)(a.mmax + 1) * g.npairs;
+    ring_quad_synthesis_kernel<LOGQ><<<grid, QkCfg<LOGQ>::NT, QkCfg<LOGQ>::SMEM, st>>>(
+        g, pairs, reinterpret_cast<const float4 *>(a.Gm), gm4, a.mmax, a.maps, a.map_stride, a.w, a.apply_w ? 1 : 0,
+        a.mdouble ? 1 : 0, a.flags);
+    HB_CHECK_LAUNCH();
+    return HB_OK;
+}
+
+template <int LOGQ>
+static int qk_ana_one(const GeomDev &g, const int32_t *pairs, int64_t cnt, const PkAnaArgs &a, cudaStream_t st) {
+    int rc = qk_prepare<LOGQ>();
+    dim3 grid;
+    if (!rc) rc = a.mblk ? pk_grid<true>(cnt, a.nmaps, &grid) : pk_grid<false>(cnt, a.nmaps, &grid);
+    if (rc) return rc;
+    const int64_t fm4 = fg_rows(a.mmax, a.mblk) * g.npairs;
+    ring_quad_analysis_kernel<LOGQ><<<grid, QkCfg<LOGQ>::NT, QkCfg<LOGQ>::SMEM, st>>>(
+        g, pairs, a.maps, a.map_stride, a.w, reinterpret_cast<float4 *>(a.Fm), fm4, a.mmax, a.flags, a.unit_w ? 1 : 0,
+        a.mdouble ? 1 : 0, a.mblk ? 1 : 0);
+    HB_CHECK_LAUNCH();
+    return HB_OK;
+}
+
+template <class A>
+static int qk_dispatch(const GeomDev &g, int logQ, const int32_t *pp, int64_t cnt, const A &a, cudaStream_t st) {
+    constexpr bool SYN = std::is_same<A, PkSynArgs>::value;
+    switch (logQ) {
+#define HB_QK_CASE(LG) \
+    case LG:           \
+        if constexpr (SYN) return qk_syn_one<LG>(g, pp, cnt, a, st); else return qk_ana_one<LG>(g, pp, cnt, a, st);
+        HB_QK_CASE(11) HB_QK_CASE(12)
+#undef HB_QK_CASE
+        default:
+            return fail(HB_ERR_UNSUPPORTED, "pair-packed ring FFT: unsupported quad-split length class");
+    }
+}
+
 template <bool BLU, class A>
 static int pk_dispatch(const GeomDev &g, int logL, const int32_t *pp, int64_t cnt, const A &a, cudaStream_t st) {
     constexpr bool SYN = std::is_same<A, PkSynArgs>::value;
@@ -555,9 +835,10 @@ template <class A> static int pk_all(const GeomDev &g, const A &a, cudaStream_t 
         const int64_t first = g.pk_first[c], cnt = g.pk_first[c + 1] - first;
         if (cnt <= 0) continue;
         const int lg = g.pk_logn[c] & 0xff;
-        const bool blu = (g.pk_logn[c] >> 8) & 1;
-        int rc = blu ? pk_dispatch<true>(g, lg, g.pk_pairs + first, cnt, a, st)
-                     : pk_dispatch<false>(g, lg, g.pk_pairs + first, cnt, a, st);
+        const bool blu = (g.pk_logn[c] >> 8) & 1, quad = (g.pk_logn[c] >> 9) & 1;
+        int rc = quad  ? qk_dispatch(g, lg, g.pk_pairs + first, cnt, a, st)
+                 : blu ? pk_dispatch<true>(g, lg, g.pk_pairs + first, cnt, a, st)
+                       : pk_dispatch<false>(g, lg, g.pk_pairs + first, cnt, a, st);
         if (rc) return rc;
     }
     return HB_OK;
@@ -587,29 +868,38 @@ int64_t pk_tab_entries(int logL) {
     }
 }
 int64_t pk_phase_entries(int logL) { return 64 + 2 * (int64_t(1) << logL) / 64; }
+// entries of a Bluestein pair's table in pkb_bt: chirp spectrum (L), chirp (L/2), phase block;
+// even, so that every table starts 16-byte aligned
+int64_t pk_bt_entries(int logL, bool quad) {
+    const int64_t L = int64_t(1) << logL;
+    return (3 * L / 2 + 64 + (quad ? 4 : 2) * L / 64 + 1) & ~int64_t(1);
+}
 
 template <int LOGL> __global__ void __launch_bounds__(256) pk_twtab_kernel(float2 *out) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < PkCfg<LOGL>::TAB; i += gridDim.x * blockDim.x)
         out[i] = pk_table_entry<LOGL>(i, PkCfg<LOGL>::L);
 }
-// one CTA per Bluestein table: its ring's phase block at ofs[e] + 3 L / 2
-__global__ void __launch_bounds__(256) pk_phtab_kernel(const int32_t *__restrict__ ns, const int32_t *__restrict__ logLs,
+// one CTA per Bluestein table: the phase block of its ring length rn[e] at ofs[e] + 3 L / 2 (L the
+// chirp's transform length); 2 L / 64 coarse entries, 4 L / 64 for a quad-split ring
+// (rn[e] = 4 ns[e], 2 rn <= 4 L)
+__global__ void __launch_bounds__(256) pk_phtab_kernel(const int32_t *__restrict__ ns, const int32_t *__restrict__ rn,
+                                                       const int32_t *__restrict__ logLs,
                                                        const int64_t *__restrict__ ofs, float2 *out) {
-    const int e = blockIdx.x, n = ns[e], L = 1 << logLs[e];
-    const int cnt = 64 + 2 * L / 64;
+    const int e = blockIdx.x, n = rn[e], L = 1 << logLs[e];
+    const int cnt = 64 + (n != ns[e] ? 4 : 2) * L / 64;
     float2 *dst = out + ofs[e] + 3 * (int64_t)L / 2;
     for (int i = threadIdx.x; i < cnt; i += blockDim.x) dst[i] = pk_phase_entry(i, n);
 }
 
-int build_pk_tables(const GeomDev &g, int count, const int32_t *ns, const int32_t *logL, const int64_t *ofs,
-                    cudaStream_t st) {
+int build_pk_tables(const GeomDev &g, int count, const int32_t *ns, const int32_t *rn, const int32_t *logL,
+                    const int64_t *ofs, cudaStream_t st) {
 #define HB_PK_TW(LG)                                                                                   \
     pk_twtab_kernel<LG><<<(PkCfg<LG>::TAB + 255) / 256, 256, 0, st>>>(g.pk_tw + g.pk_tw_ofs[LG]); \
     HB_CHECK_LAUNCH();
     HB_PK_TW(9) HB_PK_TW(10) HB_PK_TW(11) HB_PK_TW(12) HB_PK_TW(13) HB_PK_TW(14)
 #undef HB_PK_TW
     if (count > 0) {
-        pk_phtab_kernel<<<count, 256, 0, st>>>(ns, logL, ofs, g.pkb_bt);
+        pk_phtab_kernel<<<count, 256, 0, st>>>(ns, rn, logL, ofs, g.pkb_bt);
         HB_CHECK_LAUNCH();
     }
     return HB_OK;

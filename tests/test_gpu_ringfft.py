@@ -2,12 +2,14 @@
 C ABI) against the oracle's numpy ring FFTs (sht_raw.py:38-43 and isht.py:16-24 of the
 reference, with the phi0 phase and alias fold).
 
-On HEALPix grids from nside 128 up the equatorial belt and the polar rings whose index is a power
-of two run on the pair-packed kernels (one complex FFT per ring pair), the other rings on the
-general ring kernels; these cases cover both conventions of phi0 (HEALPix: s = 0 or 1 in
-phi0 = s pi / nphi; the reference's: s = 1 or 2), the unpaired equator ring, the flags, and the
-three alias regimes (mmax < nphi/2, nphi/2 <= mmax < nphi, mmax >= nphi).  Tolerance: 1e-5
-relative (L2), FP32.
+On HEALPix grids the equatorial belt and the polar rings from ring index 64 on run on the
+pair-packed kernels (one complex FFT per ring pair; Bluestein for the polar rings, whose nphi = 4i
+is not a power of two), the smaller polar rings on the general ring kernels.  The polar rings
+with 2048 < nphi < 8192 (nside >= 513) run split in four quarter-length Bluestein transforms
+(ring_quad_*_kernel); the nside 1024 and 2048 cases cover both of those classes.  The cases cover
+both conventions of phi0 (HEALPix: s = 0 or 1 in phi0 = s pi / nphi; the reference's: s = 1 or
+2), the unpaired equator ring, the flags, and the three alias regimes (mmax < nphi/2,
+nphi/2 <= mmax < nphi, mmax >= nphi).  Tolerance: 1e-5 relative (L2), FP32.
 """
 import ctypes
 
@@ -41,7 +43,12 @@ def _pairs(g):
 
 
 CASES = [(128, "healpix", 200, 0), (256, "healpix", 767, 0), (256, "reference", 767, 0), (256, "healpix", 1500, 0),
-         (256, "healpix", 767, 1), (256, "reference", 300, 2), (256, "healpix", 1100, 3)]
+         (256, "healpix", 767, 1), (256, "reference", 300, 2), (256, "healpix", 1100, 3),
+         (1024, "healpix", 2047, 0), (2048, "healpix", 4095, 0), (2048, "reference", 4095, 2)]
+
+
+def _nmaps(nside):
+    return 2 if nside <= 256 else 1
 
 
 @pytest.mark.parametrize("nside,phi0,lmax,flags", CASES)
@@ -51,7 +58,7 @@ def test_ring_analysis_fp32_vs_oracle(hb, oracle, nside, phi0, lmax, flags):
     g = G.healpix(nside, phi0=phi0)
     p = G.plan(g, lmax, precision=64)
     go = oracle.ring_tables(nside, phi0=phi0)
-    nmaps = 2
+    nmaps = _nmaps(nside)
     rng = np.random.default_rng(nside + lmax + flags)
     maps = rng.standard_normal((nmaps, g.npix)).astype(np.float32)
     F = torch.empty(nmaps, lmax + 1, g.npairs, 2, dtype=torch.complex64, device="cuda")
@@ -77,7 +84,7 @@ def test_ring_synthesis_fp32_vs_oracle(hb, oracle, nside, phi0, lmax, flags):
     g = G.healpix(nside, phi0=phi0)
     p = G.plan(g, lmax, precision=64)
     go = oracle.ring_tables(nside, phi0=phi0)
-    nmaps = 2
+    nmaps = _nmaps(nside)
     rng = np.random.default_rng(3 * nside + lmax + flags)
     Gm = (rng.standard_normal((nmaps, lmax + 1, g.npairs, 2)) + 1j * rng.standard_normal((nmaps, lmax + 1, g.npairs, 2)))
     Gm = Gm.astype(np.complex64)
