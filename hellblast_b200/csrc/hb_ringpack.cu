@@ -60,6 +60,7 @@
 
 #include "hb_internal.cuh"
 #include "hb_fftcore.cuh"
+#include "hb_tc.cuh"
 
 namespace hb {
 
@@ -241,6 +242,20 @@ struct PkMod {
     }
 };
 
+// Spectrum points k and n - k of z = f_N + i f_S from the class sums S(k), S(n - k) of the north
+// and south rings (ph = exp(i pi s k / n), sg = (-1)^s):
+// X(k) = ph (S(k) + sg conj S(n-k)), X(n-k) = conj(ph) (sg S(n-k) + conj S(k)), put as X_N + i X_S
+template <class Put>
+__device__ __forceinline__ void pk_put_pair(int k, int n, float sg, float2 ph, float2 SkN, float2 SkS, float2 SmN,
+                                            float2 SmS, Put &&put) {
+    const float2 xkN = cmul(ph, make_float2(SkN.x + sg * SmN.x, SkN.y - sg * SmN.y));
+    const float2 xkS = cmul(ph, make_float2(SkS.x + sg * SmS.x, SkS.y - sg * SmS.y));
+    const float2 xcN = cmul(cconj(ph), make_float2(sg * SmN.x + SkN.x, sg * SmN.y - SkN.y));
+    const float2 xcS = cmul(cconj(ph), make_float2(sg * SmS.x + SkS.x, sg * SmS.y - SkS.y));
+    put(k, make_float2(xkN.x - xkS.y, xkN.y + xkS.x));
+    put(n - k, make_float2(xcN.x - xcS.y, xcN.y + xcS.x));
+}
+
 // The spectrum Z of z = f_N + i f_S from the two rings' coefficients G(m) (ld(m): the float4
 // (north, south) of order m <= mmax): alias fold by m mod n, the phi0 phase exp(i pi s k / n) and
 // (-1)^(s j) over the aliases m = k + j n; put(k, Z_k) for every k < n (CTA-strided loops of NT
@@ -267,14 +282,7 @@ __device__ __forceinline__ void pk_fold(int n, int s, int mmax, float dbl, const
         c = cscale(c, chalf);
     };
     auto put_pair = [&](int k, float2 SkN, float2 SkS, float2 SmN, float2 SmS) {
-        const float2 ph = T.ph(pidx(k));
-        // X(k) = ph (S(k) + (-1)^s conj S(n-k)), X(n-k) = conj(ph) ((-1)^s S(n-k) + conj S(k))
-        const float2 xkN = cmul(ph, make_float2(SkN.x + sg * SmN.x, SkN.y - sg * SmN.y));
-        const float2 xkS = cmul(ph, make_float2(SkS.x + sg * SmS.x, SkS.y - sg * SmS.y));
-        const float2 xcN = cmul(cconj(ph), make_float2(sg * SmN.x + SkN.x, sg * SmN.y - SkN.y));
-        const float2 xcS = cmul(cconj(ph), make_float2(sg * SmS.x + SkS.x, sg * SmS.y - SkS.y));
-        put(k, make_float2(xkN.x - xkS.y, xkN.y + xkS.x));  // X_N + i X_S
-        put(n - k, make_float2(xcN.x - xcS.y, xcN.y + xcS.x));
+        pk_put_pair(k, n, sg, T.ph(pidx(k)), SkN, SkS, SmN, SmS, put);
     };
     if (mmax < n) {  // at most one harmonic per residue class (the equatorial belt when mmax < 4 nside)
 #pragma unroll 4
@@ -490,22 +498,32 @@ template <int LOGQ> struct QkCfg {
     static constexpr int SBUF = S::BUF, BUF = 4 * SBUF;  // four sub-buffers
     static constexpr int PHC = 4 * LQ / 64;              // coarse phases exp(i pi 64 c / n), 2n <= 4 LQ
     static constexpr int TAB = S::TWB + 64 + PHC;        // twiddles of LQ, then the phases of n
-    static constexpr int SMEM = (BUF + TAB + LQ) * (int)sizeof(float2);  // + the chirp spectrum
+    static constexpr int ALL = TAB + 3 * LQ / 2;         // + the chirp spectrum (LQ) and the chirp (LQ/2)
+    static constexpr int SMEM = (BUF + ALL) * (int)sizeof(float2);
+    static constexpr int KPT = LQ / NT;                  // spectrum bins k < n/2 < LQ per thread (fold)
     static constexpr int MINB = 65536 / (NT * 64) > 0 ? 65536 / (NT * 64) : 1;  // <= 64 registers
     static constexpr int RPT = (LQ / 2) / NT;            // radix-4 steps: residues r < LQ/2 per thread
     static_assert(NT <= 1024 && RPT * NT == LQ / 2, "one CTA of four sub-transforms");
     static_assert(LQ / 2 + (LQ - 1) / 16 < SBUF, "upper half-buffers hold q <= LQ/2 spectrum points each");
+    static_assert(BUF % 2 == 0 && S::TWB % 2 == 0 && TAB % 2 == 0 && KPT * NT == LQ,
+                  "16-byte cp.async chunks never straddle two table parts");
 };
 
-// the CTA's tables: twiddles of LQ (gtw), the phase block of n (gph), the chirp spectrum (gbt)
+// the CTA's tables, copied asynchronously (16-byte cp.async, one commit group; the caller waits):
+// twiddles of LQ (gtw), the phase block of n (gph), then the chirp spectrum and the chirp (gbt,
+// 3 LQ / 2 entries back to back).  Every part has an even entry count and starts 16-byte aligned
+// in global memory (even table offsets) and in shared memory (BUF, TWB and TAB are even).
 template <int LOGQ>
-__device__ __forceinline__ PkTab qk_tables(float2 *base, const float2 *__restrict__ gtw,
-                                           const float2 *__restrict__ gph, const float2 *__restrict__ gbt) {
+__device__ __forceinline__ PkTab qk_tables_async(float2 *base, const float2 *__restrict__ gtw,
+                                                 const float2 *__restrict__ gph, const float2 *__restrict__ gbt) {
     using C = QkCfg<LOGQ>;
     using S = PkCfg<LOGQ>;
+    for (int c = threadIdx.x; c < C::ALL / 2; c += C::NT) {
+        const int i = 2 * c;
+        tc::cp_async16(base + i, i < S::TWB ? gtw + i : (i < C::TAB ? gph + (i - S::TWB) : gbt + (i - C::TAB)));
+    }
+    tc::cp_async_commit();
     float2 *tw1 = base, *tw4 = tw1 + S::TWP, *tws = tw4 + S::TWP, *phf = tws + S::TWS, *phc = phf + 64;
-    for (int i = threadIdx.x; i < C::TAB + C::LQ; i += C::NT)
-        base[i] = pk_ld(i < S::TWB ? gtw + i : (i < C::TAB ? gph + (i - S::TWB) : gbt + (i - C::TAB)));
     return {tw1, tw4, tws, phf, phc};
 }
 
@@ -534,25 +552,63 @@ __global__ void __launch_bounds__(QkCfg<LOGQ>::NT, QkCfg<LOGQ>::MINB)
     constexpr int LQ = C::LQ, NTQ = C::NTQ, NT = C::NT, SB = C::SBUF;
     extern __shared__ __align__(16) float2 pk_smem[];
     float2 *buf = pk_smem;
-    const float2 *spec = pk_smem + C::BUF + C::TAB;
+    const float2 *spec = pk_smem + C::BUF + C::TAB, *chs = spec + LQ;  // chirp spectrum, chirp
     const int pair = pairs[blockIdx.y], bm = blockIdx.x;  // (map, pair): the maps of a pair share its tables
     const int rN = g.pair_ring[2 * pair], rS = g.pair_ring[2 * pair + 1];
     const int n = g.nphi[rN], q = n >> 2;
-    const float2 *bt = g.pkb_bt + g.pkb_bt_ofs[pair], *ch = bt + LQ;
-    const PkTab T = qk_tables<LOGQ>(pk_smem + C::BUF, g.pk_tw + g.pk_tw_ofs[LOGQ], bt + LQ + LQ / 2, bt);
+    const float2 *bt = g.pkb_bt + g.pkb_bt_ofs[pair];
+    const PkTab T = qk_tables_async<LOGQ>(pk_smem + C::BUF, g.pk_tw + g.pk_tw_ofs[LOGQ], bt + LQ + LQ / 2, bt);
     const int s = (flags & HB_F_NOPHASE) ? 0 : pk_shift(g.phi0_pi[rN], n);
     const int64_t np = g.npairs;
     const float4 *gin = Gm + bm * gm_stride4 + pair;
     const bool hasS = rS >= 0;
-    __syncthreads();  // tables
     auto ld = [&](int m) -> float4 {
         float4 v = __ldg(gin + (int64_t)m * np);
         if (!hasS) v.z = v.w = 0.f;
         return v;
     };
-    // conj Z, point k at qk_slot(k)
-    pk_fold<NT, false>(n, s, mmax, mdouble ? 2.f : 1.f, T, ld,
-                       [&](int k, float2 z) { buf[qk_slot<LOGQ>(k, q)] = cconj(z); });
+    auto put = [&](int k, float2 z) { buf[qk_slot<LOGQ>(k, q)] = cconj(z); };  // conj Z, point k at qk_slot(k)
+    const float dbl = mdouble ? 2.f : 1.f;
+    if (mmax < n) {
+        // at most one order per residue class: this thread's orders are loaded while the tables
+        // arrive.  Bins k = tid + 1 + j NT < n/2 take G(k) and G(n - k); the last thread's last
+        // slot (k = LQ > n/2) carries bins 0 and n/2 instead: G(0) and G(n/2).
+        const float4 z4 = make_float4(0.f, 0.f, 0.f, 0.f);
+        const bool last = threadIdx.x == NT - 1;
+        float4 ga[C::KPT], gc[C::KPT];
+#pragma unroll
+        for (int j = 0; j < C::KPT; ++j) {
+            const int k = threadIdx.x + 1 + j * NT;
+            const bool in = k < n / 2;
+            ga[j] = (in && k <= mmax) ? ld(k) : z4;
+            gc[j] = (in && n - k <= mmax) ? ld(n - k) : z4;
+        }
+        if (last) {
+            ga[C::KPT - 1] = ld(0);
+            gc[C::KPT - 1] = n / 2 <= mmax ? ld(n / 2) : z4;
+        }
+        tc::cp_async_wait<0>();
+        __syncthreads();  // tables
+        const float chalf = 0.5f * dbl, sg = (s & 1) ? -1.f : 1.f;
+        const PkMod mod2n{2 * n, 1.f / (float)(2 * n)};
+#pragma unroll
+        for (int j = 0; j < C::KPT; ++j) {
+            const int k = threadIdx.x + 1 + j * NT;
+            if (k < n / 2)
+                pk_put_pair(k, n, sg, T.ph(mod2n(s * k)), cscale(f4lo(ga[j]), chalf), cscale(f4hi(ga[j]), chalf),
+                            cscale(f4lo(gc[j]), chalf), cscale(f4hi(gc[j]), chalf), put);
+        }
+        if (last) {  // bin 0: Re G(0) (c_0 = 1); bin n/2: c Re(G(n/2) exp(i pi s / 2))
+            const float4 v0 = ga[C::KPT - 1], vh = gc[C::KPT - 1];
+            put(0, make_float2(v0.x, v0.z));
+            const float2 ph = T.ph(mod2n(s * (n / 2)));
+            put(n / 2, make_float2(dbl * (ph.x * vh.x - ph.y * vh.y), dbl * (ph.x * vh.z - ph.y * vh.w)));
+        }
+    } else {
+        tc::cp_async_wait<0>();
+        __syncthreads();  // tables
+        pk_fold<NT, false>(n, s, mmax, dbl, T, ld, put);
+    }
     __syncthreads();
     // radix-4 step: V^b_r c_r into sub-buffer b at r (zero for q <= r < LQ/2)
 #pragma unroll
@@ -564,7 +620,7 @@ __global__ void __launch_bounds__(QkCfg<LOGQ>::NT, QkCfg<LOGQ>::MINB)
             dft4<false>(x0, x1, x2, x3);
             float2 w1, w2, w3;
             qk_twiddles(T, r, w1, w2, w3);
-            const float2 c = __ldg(ch + r);
+            const float2 c = chs[r];
             buf[rp] = cmul(x0, c);
             buf[SB + rp] = cmul(x1, cmul(w1, c));
             buf[2 * SB + rp] = cmul(x2, cmul(w2, c));
@@ -583,16 +639,30 @@ __global__ void __launch_bounds__(QkCfg<LOGQ>::NT, QkCfg<LOGQ>::MINB)
     const double sc2 = (flags & HB_F_NO2PI) ? 1.0 : 6.283185307179586476925286766559;
     const float psN = apply_w ? (float)(sc2 * w[rN] / (double)n) : 1.f;
     const float psS = (apply_w && hasS) ? (float)(sc2 * w[rS] / (double)n) : 1.f;
-    float *fN = maps + bm * map_stride + g.ofs[rN] + grp;
-    float *fS = hasS ? maps + bm * map_stride + g.ofs[rS] + grp : nullptr;
-    // inverse FFT_LQ, points below LQ/2; output a of sub-transform b is pixel 4a + b
-    pk_run<LOGQ, true, false, true>(sb, T, tq, lds, [&](int a, int, float2 v) {
-        if (a < q) {
-            const float2 z = cconj(cmul(__ldg(ch + a), v));
-            fN[4 * a] = z.x * psN;
-            if (fS) fS[4 * a] = z.y * psS;
+    float *fN = maps + bm * map_stride + g.ofs[rN];
+    float *fS = hasS ? maps + bm * map_stride + g.ofs[rS] : nullptr;
+    // inverse FFT_LQ, points below LQ/2, into the sub-buffers
+    pk_run<LOGQ, true, false, true>(sb, T, tq, lds, [&](int, int ip, float2 v) { sb[ip] = v; });
+    __syncthreads();
+    // output a of sub-transform b, conj(c_a v), is pixel 4a + b: one thread writes pixels
+    // 4a .. 4a+3 of both rings (16-byte stores where the rings start 16-byte aligned)
+    const bool vec = ((reinterpret_cast<uintptr_t>(fN) | reinterpret_cast<uintptr_t>(fS)) & 15) == 0;
+    for (int a = threadIdx.x; a < q; a += NT) {
+        const float2 c = chs[a];
+        const int ap = pk_pad(a);
+        float2 z[4];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) z[b] = cconj(cmul(c, buf[b * SB + ap]));
+        const float4 oN = make_float4(z[0].x * psN, z[1].x * psN, z[2].x * psN, z[3].x * psN);
+        const float4 oS = make_float4(z[0].y * psS, z[1].y * psS, z[2].y * psS, z[3].y * psS);
+        if (vec) {
+            *reinterpret_cast<float4 *>(fN + 4 * a) = oN;
+            if (fS) *reinterpret_cast<float4 *>(fS + 4 * a) = oS;
+        } else {
+            fN[4 * a] = oN.x; fN[4 * a + 1] = oN.y; fN[4 * a + 2] = oN.z; fN[4 * a + 3] = oN.w;
+            if (fS) { fS[4 * a] = oS.x; fS[4 * a + 1] = oS.y; fS[4 * a + 2] = oS.z; fS[4 * a + 3] = oS.w; }
         }
-    });
+    }
 }
 
 template <int LOGQ>
@@ -604,28 +674,47 @@ __global__ void __launch_bounds__(QkCfg<LOGQ>::NT, QkCfg<LOGQ>::MINB)
     constexpr int LQ = C::LQ, NTQ = C::NTQ, NT = C::NT, SB = C::SBUF;
     extern __shared__ __align__(16) float2 pk_smem[];
     float2 *buf = pk_smem;
-    const float2 *spec = pk_smem + C::BUF + C::TAB;
+    const float2 *spec = pk_smem + C::BUF + C::TAB, *chs = spec + LQ;  // chirp spectrum, chirp
     const int pair = pairs[mblk ? blockIdx.y : blockIdx.x], bm = mblk ? blockIdx.x : blockIdx.y;
     const int rN = g.pair_ring[2 * pair], rS = g.pair_ring[2 * pair + 1];
     const int n = g.nphi[rN], q = n >> 2;
     const float2 *bt = g.pkb_bt + g.pkb_bt_ofs[pair], *ch = bt + LQ;
-    const PkTab T = qk_tables<LOGQ>(pk_smem + C::BUF, g.pk_tw + g.pk_tw_ofs[LOGQ], bt + LQ + LQ / 2, bt);
+    const PkTab T = qk_tables_async<LOGQ>(pk_smem + C::BUF, g.pk_tw + g.pk_tw_ofs[LOGQ], bt + LQ + LQ / 2, bt);
     const int s = (flags & HB_F_NOPHASE) ? 0 : pk_shift(g.phi0_pi[rN], n);
     const int64_t np = g.npairs;
     const int grp = threadIdx.x / NTQ, tq = threadIdx.x % NTQ;
-    const float *fN = maps + bm * map_stride + g.ofs[rN] + grp;
-    const float *fS = rS >= 0 ? maps + bm * map_stride + g.ofs[rS] + grp : nullptr;
+    const float *fN = maps + bm * map_stride + g.ofs[rN];
+    const float *fS = rS >= 0 ? maps + bm * map_stride + g.ofs[rS] : nullptr;
     float2 *sb = buf + grp * SB;
     auto lds = [&](int, int ip) -> float2 { return sb[ip]; };
     auto sts = [&](int, int ip, float2 v) { sb[ip] = v; };
-    __syncthreads();  // tables
-    // sub-sequence b = grp: samples 4a + b times the chirp c_a (a < q; zero from q to LQ/2);
-    // forward FFT_LQ times the chirp spectrum, inverse FFT_LQ (points below LQ/2)
-    auto ld0 = [&](int a, int) -> float2 {
-        return a < q ? cmul(make_float2(__ldg(fN + 4 * a), fS ? __ldg(fS + 4 * a) : 0.f), __ldg(ch + a))
-                     : make_float2(0.f, 0.f);
+    // sub-sequence b: samples 4a + b times the chirp c_a into sub-buffer b at a (a < q; zero from q
+    // to LQ/2).  One thread reads pixels 4a .. 4a+3 of both rings (16-byte loads where the rings
+    // start 16-byte aligned) and the chirp from global memory, while the tables arrive.
+    const bool vec = ((reinterpret_cast<uintptr_t>(fN) | reinterpret_cast<uintptr_t>(fS)) & 15) == 0;
+    auto ld4 = [&](const float *f, int a) -> float4 {
+        if (!f) return make_float4(0.f, 0.f, 0.f, 0.f);
+        if (vec) return __ldg(reinterpret_cast<const float4 *>(f + 4 * a));
+        return make_float4(__ldg(f + 4 * a), __ldg(f + 4 * a + 1), __ldg(f + 4 * a + 2), __ldg(f + 4 * a + 3));
     };
-    pk_run<LOGQ, false, true, false>(sb, T, tq, ld0, [&](int k, int ip, float2 v) { sb[ip] = cmul(v, spec[k]); });
+#pragma unroll
+    for (int u = 0; u < C::RPT; ++u) {
+        const int a = threadIdx.x + u * NT, ap = pk_pad(a);
+        if (a < q) {
+            const float4 xN = ld4(fN, a), xS = ld4(fS, a);
+            const float2 c = __ldg(ch + a);
+            buf[ap] = cmul(make_float2(xN.x, xS.x), c);
+            buf[SB + ap] = cmul(make_float2(xN.y, xS.y), c);
+            buf[2 * SB + ap] = cmul(make_float2(xN.z, xS.z), c);
+            buf[3 * SB + ap] = cmul(make_float2(xN.w, xS.w), c);
+        } else {
+            buf[ap] = buf[SB + ap] = buf[2 * SB + ap] = buf[3 * SB + ap] = make_float2(0.f, 0.f);
+        }
+    }
+    tc::cp_async_wait<0>();
+    __syncthreads();  // samples and tables
+    // forward FFT_LQ times the chirp spectrum, inverse FFT_LQ (points below LQ/2)
+    pk_run<LOGQ, false, true, false>(sb, T, tq, lds, [&](int k, int ip, float2 v) { sb[ip] = cmul(v, spec[k]); });
     __syncthreads();
     pk_run<LOGQ, true, false, true>(sb, T, tq, lds, sts);
     __syncthreads();
@@ -638,7 +727,7 @@ __global__ void __launch_bounds__(QkCfg<LOGQ>::NT, QkCfg<LOGQ>::MINB)
             const int kp = pk_pad(k), zp = pk_pad(LQ / 2 + k);
             float2 w1, w2, w3;
             qk_twiddles(T, k, w1, w2, w3);
-            const float2 c = __ldg(ch + k);
+            const float2 c = chs[k];
             float2 x0 = cmul(buf[kp], c), x1 = cmul(buf[SB + kp], cmul(w1, c));
             float2 x2 = cmul(buf[2 * SB + kp], cmul(w2, c)), x3 = cmul(buf[3 * SB + kp], cmul(w3, c));
             dft4<false>(x0, x1, x2, x3);

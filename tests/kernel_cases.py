@@ -9,6 +9,8 @@ CASE is one of
   plain        FP32 alm2map + map2alm per map (leg_*_kernel, ring_*_kernel)
   spin         FP32 spin-2 alm2map + map2alm (spin_*_kernel)
   alm2cl       hb_alm2cl on B alm vectors (alm_ops.py:19-32)
+  ring         FP32 ring synthesis + ring analysis alone (hb_ring_synthesis / hb_ring_analysis;
+               ring_pair_*, ring_quad_* and ring_*_kernel<float>) on B maps of Gaussian G(m)
   batched      batched split-precision alm2map + map2alm (synth_tc/anal_tc + ring FFTs)
   diff         the differentiable T/Q/U power-spectrum loss: forward, and forward + backward
                through the adjoint kernels; prints both times and their ratio
@@ -75,6 +77,20 @@ def run(case: str, nside: int, lmax: int, nmaps: int, reps: int, warmup: int, wi
         a = _alm(lmax, nmaps)
         ms = _time(lambda: ops.alm2cl(a, None, lmax, lmax), reps, warmup, st)
         out["bytes_read"] = a.numel() * a.element_size()
+    elif case == "ring":
+        g = G.healpix(nside)
+        p = G.plan(g, lmax, precision=64)
+        torch.manual_seed(2)
+        Gm = torch.randn(nmaps, lmax + 1, g.npairs, 2, dtype=torch.complex64, device=dev)
+        Gm[:, :, g.npairs - 1, 1] = 0  # the unpaired equator's south slot is not data
+        mp = torch.empty(nmaps, g.npix, dtype=torch.float32, device=dev)
+        F = torch.empty_like(Gm)
+        sp = st.cuda_stream
+
+        def fn():
+            L.call("hb_ring_synthesis", p.handle, 32, nmaps, Gm.data_ptr(), mp.data_ptr(), 0, sp)
+            L.call("hb_ring_analysis", p.handle, 32, nmaps, mp.data_ptr(), None, F.data_ptr(), 0, sp)
+        ms = _time(fn, reps, warmup, st)
     elif case == "batched":
         bp = batched.plan(nside, lmax, nmaps, wide=wide, bf16=bf16)
         a = _alm(lmax, nmaps).reshape(-1)
@@ -117,7 +133,7 @@ def run(case: str, nside: int, lmax: int, nmaps: int, reps: int, warmup: int, wi
 
 def main(argv=None):
     p = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
-    p.add_argument("case", choices=["ring_tables", "plain", "spin", "alm2cl", "batched", "diff"])
+    p.add_argument("case", choices=["ring_tables", "plain", "spin", "alm2cl", "ring", "batched", "diff"])
     p.add_argument("--nside", type=int, default=1024)
     p.add_argument("--lmax", type=int, default=None)
     p.add_argument("--nmaps", type=int, default=1)
