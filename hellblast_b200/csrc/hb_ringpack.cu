@@ -245,15 +245,39 @@ struct PkMod {
 // Spectrum points k and n - k of z = f_N + i f_S from the class sums S(k), S(n - k) of the north
 // and south rings (ph = exp(i pi s k / n), sg = (-1)^s):
 // X(k) = ph (S(k) + sg conj S(n-k)), X(n-k) = conj(ph) (sg S(n-k) + conj S(k)), put as X_N + i X_S
-template <class Put>
-__device__ __forceinline__ void pk_put_pair(int k, int n, float sg, float2 ph, float2 SkN, float2 SkS, float2 SmN,
-                                            float2 SmS, Put &&put) {
+__device__ __forceinline__ void pk_pair_values(float sg, float2 ph, float2 SkN, float2 SkS, float2 SmN, float2 SmS,
+                                               float2 &xk, float2 &xnk) {
     const float2 xkN = cmul(ph, make_float2(SkN.x + sg * SmN.x, SkN.y - sg * SmN.y));
     const float2 xkS = cmul(ph, make_float2(SkS.x + sg * SmS.x, SkS.y - sg * SmS.y));
     const float2 xcN = cmul(cconj(ph), make_float2(sg * SmN.x + SkN.x, sg * SmN.y - SkN.y));
     const float2 xcS = cmul(cconj(ph), make_float2(sg * SmS.x + SkS.x, sg * SmS.y - SkS.y));
-    put(k, make_float2(xkN.x - xkS.y, xkN.y + xkS.x));
-    put(n - k, make_float2(xcN.x - xcS.y, xcN.y + xcS.x));
+    xk = make_float2(xkN.x - xkS.y, xkN.y + xkS.x);
+    xnk = make_float2(xcN.x - xcS.y, xcN.y + xcS.x);
+}
+template <class Put>
+__device__ __forceinline__ void pk_put_pair(int k, int n, float sg, float2 ph, float2 SkN, float2 SkS, float2 SmN,
+                                            float2 SmS, Put &&put) {
+    float2 xk, xnk;
+    pk_pair_values(sg, ph, SkN, SkS, SmN, SmS, xk, xnk);
+    put(k, xk);
+    put(n - k, xnk);
+}
+
+// class sums S(k) = sum_j (-1)^(s j) chalf G(k + j n) over the orders m = k + j n <= mmax, north (a)
+// and south (c)
+template <class Ld>
+__device__ __forceinline__ void pk_csum(int k, int n, int s, int mmax, float chalf, Ld &&ld, float2 &a, float2 &c) {
+    a = make_float2(0.f, 0.f);
+    c = a;
+    float sj = 1.f;
+    for (int m = k; m <= mmax; m += n) {
+        const float4 v = ld(m);
+        a.x += sj * v.x; a.y += sj * v.y;
+        c.x += sj * v.z; c.y += sj * v.w;
+        if (s & 1) sj = -sj;
+    }
+    a = cscale(a, chalf);
+    c = cscale(c, chalf);
 }
 
 // The spectrum Z of z = f_N + i f_S from the two rings' coefficients G(m) (ld(m): the float4
@@ -267,20 +291,7 @@ __device__ __forceinline__ void pk_fold(int n, int s, int mmax, float dbl, const
     const PkMod mod2n{2 * n, 1.f / (float)(2 * n)};
     // phase-table index of exp(i pi s k / n): (s k) mod 2n (s k < 2^31: s < 2n <= 2^15, k <= n)
     auto pidx = [&](int k) -> int { return P2 ? ((s * k) & (2 * n - 1)) : mod2n(s * k); };
-    // class sums S(k) = sum_j (-1)^(s j) c_m / 2 G(k + j n), north and south
-    auto csum = [&](int k, float2 &a, float2 &c) {
-        a = make_float2(0.f, 0.f);
-        c = a;
-        float sj = 1.f;
-        for (int m = k; m <= mmax; m += n) {
-            const float4 v = ld(m);
-            a.x += sj * v.x; a.y += sj * v.y;
-            c.x += sj * v.z; c.y += sj * v.w;
-            if (s & 1) sj = -sj;
-        }
-        a = cscale(a, chalf);
-        c = cscale(c, chalf);
-    };
+    auto csum = [&](int k, float2 &a, float2 &c) { pk_csum(k, n, s, mmax, chalf, ld, a, c); };
     auto put_pair = [&](int k, float2 SkN, float2 SkS, float2 SmN, float2 SmS) {
         pk_put_pair(k, n, sg, T.ph(pidx(k)), SkN, SkS, SmN, SmS, put);
     };
