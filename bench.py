@@ -648,8 +648,10 @@ def main():
         fft_bytes = hbm_bytes_ring_fft(B, mmax, g.npairs, npix)
         hbm_src = "MEASURED_PEAKS.json hbm_gbs, of measured" if peaks else "fallback 6650 GB/s, of fallback"
         stage_roof = {"tensor_legendre": tensor}
-        for key, kern in (("ring_synthesis", "ring_pair_synthesis_kernel + ring_synthesis_kernel<float>"),
-                          ("ring_analysis", "ring_pair_analysis_kernel + ring_analysis_kernel<float>")):
+        for key, kern in (("ring_synthesis", "ring_quad_synthesis_kernel + ring_pair_synthesis_kernel + "
+                                             "ring_synthesis_kernel<float>"),
+                          ("ring_analysis", "ring_quad_analysis_kernel + ring_pair_analysis_kernel + "
+                                            "ring_analysis_kernel<float>")):
             ach = fft_bytes / (stages[key] * 1e-3) / 1e9
             stage_roof[key] = {"bound": "hbm", "kernel": kern + " (all FFT-length classes of one direction)",
                                "achieved": ach, "peak": hbm_peak, "unit": "GB/s", "frac": ach / hbm_peak,
