@@ -9,7 +9,8 @@
 // [512, 16384].  On a HEALPix grid that is the whole equatorial belt (n = 4 nside, s = 0 or 1
 // alternating; with the reference's phi0 convention s = 1 or 2) and every polar ring from
 // ring index 64 on (n = 4i, s = 1).  Everything else (the smallest polar rings, generic grids,
-// FP64) runs in hb_fft.cu.
+// FP64) runs in hb_fft.cu.  Bluestein rings with n = 4q and L = 2^13 or 2^14 (polar rings 513 to
+// 2047) run split in four quarter-length transforms (ring_quad_*_kernel, below).
 //
 // Bluestein (n not a power of two): the length-n DFT X_j = c_j sum_k (x_k c_k) b_{j-k},
 // c_t = exp(-i pi t^2 / n), b_t = conj c_t, is a circular convolution of length L >= 2n - 1:
