@@ -192,7 +192,7 @@ __global__ void __launch_bounds__(PA_THREADS, 4) prep_alm_tiles_kernel(const TcG
             const int i0 = stg * PA_L + 16 * gl;  // l - m of this k8 group's first value
             if (i0 < nch * 64) {
                 const int c = i0 >> 6, g = (i0 >> 4) & 3;
-                uint4 *chunk = base + (int64_t)c * (16 * N);
+                uint4 *chunk = base + (int64_t)c * (16 * N) + (g >> 1) * (8 * N);  // K-step half g / 2
                 float re[8], im[8];
 #pragma unroll
                 for (int k = 0; k < 8; ++k) {
@@ -200,8 +200,8 @@ __global__ void __launch_bounds__(PA_THREADS, 4) prep_alm_tiles_kernel(const TcG
                     re[k] = v.x * sc;
                     im[k] = v.y * sc;
                 }
-                store_rows8<BF16>(chunk, N, q, 2 * b, g, re);
-                store_rows8<BF16>(chunk, N, q, 2 * b + 1, g, im);
+                store_rows8<BF16, 16>(chunk, N, q, 2 * b, g & 1, re);
+                store_rows8<BF16, 16>(chunk, N, q, 2 * b + 1, g & 1, im);
             }
             __syncthreads();  // every thread is done with this stage's buffer before it is refilled
         }
@@ -619,29 +619,30 @@ __device__ __forceinline__ void load_sets(uint32_t taddr, int j, int nsets, floa
 // ------------------------------------------------------------------------------------ synthesis
 // one synthesis chunk of one row: 64 l in four groups of 8 even + 8 odd values
 template <bool CHECKED, bool BF16>
-__device__ __forceinline__ void gen_chunk_syn(Rec &R, const float2 *cf, uint8_t *A, int off) {
+__device__ __forceinline__ void gen_half_syn(Rec &R, const float2 *cf, uint8_t *A, int off) {
 #pragma unroll
-    for (int grp = 0; grp < 4; ++grp) {
+    for (int grp = 0; grp < 2; ++grp) {
         float ev[8], od[8];
         gen16<CHECKED>(R, cf + 16 * grp, ev, od);
-        store_split<BF16>(A, off + grp * 128, ev, od);
+        store_split<BF16, ANA_A_TILE>(A, off + grp * 128, ev, od);
     }
 }
 
 // Chunk c (64 l) of a unit belongs to half-block hb = c / 2 (128 l).  The unit's live half-blocks
 // hb0, hb0 + 1, ... go round-robin to SYN_GROUPS producer groups of four warps (three producer
-// warps per SM sub-partition hide the recursion's latency); group g fills only stage g, two
-// chunks per half-block, and waits only for the MMAs of its own previous chunk.  The MMA
+// warps per SM sub-partition hide the recursion's latency); group g fills stages 2g (the first 32
+// l of each chunk: one 16-K MMA step per parity) and 2g + 1 (the last 32 l), two chunks per
+// half-block, so its producers fill one half-stage while the MMAs drain the other.  The MMA
 // thread (and the batch-tile loader) take the chunks in rounds: (group 0, 1, 2) for the first
-// chunk of their half-blocks, then for the second, then the next three half-blocks, so each
-// stage is consumed in the order its group fills it.
+// chunk of their half-blocks, then for the second, then the next three half-blocks, each chunk's
+// two half-stages in turn, so every stage is consumed in the order its group fills it.
 template <int N, bool BF16, int S>
 __global__ void __launch_bounds__(SYN_THREADS, 1)
     synth_tc_kernel(const TcGroup *__restrict__ groups, const int4 *__restrict__ units, int nunits, int *err,
                     int *qctr, TcCtl ctl) {
-    constexpr int ST = SYN_GROUPS;
-    constexpr int B_STAGE = tc_b_stage<N>();
-    constexpr int STAGE = A_STAGE + B_STAGE;
+    constexpr int ST = 2 * SYN_GROUPS;
+    constexpr int B_STAGE = ana_b_stage<N>();      // [q][h][N x 16] 16-bit: half a chunk's alm tiles
+    constexpr int STAGE = ANA_A_STAGE + B_STAGE;   // 16-K A tiles [q][h][128 x 16]
     constexpr uint32_t IDESC = tc::idesc_f16kind(128, N, 0, 0, BF16);
     constexpr uint32_t IDESC2 = tc::idesc_f16kind(128, 2 * N, 0, 0, BF16);
     constexpr float LS = BF16 ? 1.0f : 256.0f;  // lambda scale (|lambda| < 2^7 -> < 2^15 in half)
@@ -653,7 +654,7 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
     static_assert(S >= 2 && S % 2 == 0, "accumulator sets come in (hi, cross) pairs");
     extern __shared__ __align__(1024) uint8_t smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const TcSmem L = tc_smem_layout<ST, N, SYN_PW>(smem, warp);
+    const TcSmem L = tc_smem_layout<ST, N, SYN_PW, STAGE>(smem, warp);
 
     if (threadIdx.x == 0) tc_init_barriers<ST>(L, 128 + 1, 32 * SYN_PW, SYN_PW + 1);
     if (warp == SYN_PW) {
@@ -668,10 +669,9 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
 
     if (warp < SYN_PW) {
         // ---------------- producers + epilogue
-        const int wg = warp >> 2;                // producer group = stage
+        const int wg = warp >> 2;                // producer group: stages 2 wg and 2 wg + 1
         const int r = ((warp & 3) << 5) | lane;  // row = pair within the block
-        uint8_t *A = smem + wg * STAGE;
-        uint32_t gc = 0;  // chunks this group has filled (uses of its stage)
+        uint32_t gc = 0;  // chunks this group has filled (uses of each of its two stages)
         for (int ui = 0; ok; ++ui) {
             const int u = uq_take(L, ui, ctl.wait_ns, true);
             if (u == -2) {
@@ -709,20 +709,25 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
                 R.load(kpre, LS);
                 const bool fast = __all_sync(0xffffffffu, R.e == 0);
                 if (hb + SYN_GROUPS < nhb) fetch(hb + SYN_GROUPS);
-                for (int cc = 0; cc < 2 && 2 * hb + cc < nch; ++cc, ++gc) {
-                    if (gc >= 1 && !warp_wait(&L.empty[wg], (gc + 1) & 1, ctl.wait_ns)) {
-                        if (lane == 0) set_err(err, 1);
-                        ok = false;
-                        break;
+                for (int cc = 0; cc < 2 && 2 * hb + cc < nch && ok; ++cc, ++gc) {
+                    const int off = (r & 7) * 16 + (r >> 3) * 256;  // K-major, row groups 256 bytes apart
+#pragma unroll
+                    for (int half = 0; half < 2; ++half) {
+                        const int sg = 2 * wg + half;
+                        if (gc >= 1 && !warp_wait(&L.empty[sg], (gc + 1) & 1, ctl.wait_ns)) {
+                            if (lane == 0) set_err(err, 1);
+                            ok = false;
+                            break;
+                        }
+                        const float2 *cf = L.coef + cc * 64 + half * 32;
+                        uint8_t *A = smem + sg * STAGE;
+                        if (fast)  // one branch per half-chunk: straight-line code over its two row groups
+                            gen_half_syn<false, BF16>(R, cf, A, off);
+                        else
+                            gen_half_syn<true, BF16>(R, cf, A, off);
+                        tc::fence_proxy_async_smem();
+                        tc::mbar_arrive(&L.full[sg]);
                     }
-                    const float2 *cf = L.coef + cc * 64;
-                    const int off = (r & 7) * 16 + (r >> 3) * 512;
-                    if (fast)  // one branch per chunk: straight-line code over its four row groups
-                        gen_chunk_syn<false, BF16>(R, cf, A, off);
-                    else
-                        gen_chunk_syn<true, BF16>(R, cf, A, off);
-                    tc::fence_proxy_async_smem();
-                    tc::mbar_arrive(&L.full[wg]);
                 }
             }
             if (!ok) break;
@@ -761,7 +766,7 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
     } else if (warp == SYN_PW) {
         // ---------------- MMA issuer
         if (lane == 0) {
-            uint32_t fbits = 0;  // bit g: parity of stage g's next fill
+            uint32_t fbits = 0;  // bit s: parity of stage s's next fill
             for (int ui = 0; ok; ++ui) {
                 const int u = uq_take(L, ui, ctl.wait_ns, false);
                 if (u == -2) {
@@ -784,16 +789,21 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
                         for (int g = 0; g < SYN_GROUPS; ++g) {
                             const int hb = h3 + g;
                             if (hb >= nhb || 2 * hb + cc >= nch) continue;
-                            if (!tc::mbar_wait(&L.full[g], (fbits >> g) & 1u, ctl.wait_ns)) {
-                                set_err(err, 4);
-                                ok = false;
-                                break;
+                            for (int half = 0; half < 2; ++half) {
+                                const int sg = 2 * g + half;
+                                if (!tc::mbar_wait(&L.full[sg], (fbits >> sg) & 1u, ctl.wait_ns)) {
+                                    set_err(err, 4);
+                                    ok = false;
+                                    break;
+                                }
+                                fbits ^= 1u << sg;
+                                tc::fence_after();
+                                // the second half accumulates onto the first
+                                issue_stage<N, 1>(tmem, tc::smem_u32(smem + sg * STAGE), k % (S / 2),
+                                                  half == 0 && k < S / 2, IDESC, IDESC2);
+                                tc::mma_commit(&L.empty[sg]);
                             }
-                            fbits ^= 1u << g;
-                            tc::fence_after();
-                            issue_stage<N>(tmem, tc::smem_u32(smem + g * STAGE), k % (S / 2), k < S / 2, IDESC,
-                                           IDESC2);
-                            tc::mma_commit(&L.empty[g]);
+                            if (!ok) break;
                             ++k;
                         }
                     }
@@ -810,7 +820,7 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
     } else {
         // ---------------- loader of the pre-split alm tiles (same order as the MMA thread)
         if (lane == 0) {
-            uint32_t ebits = 0, used = 0;  // bit g: parity of stage g's next drain / stage g used
+            uint32_t ebits = 0, used = 0;  // bit s: parity of stage s's next drain / stage s used
             bool withheld = false;
             for (int ui = 0; ok; ++ui) {
                 const int u = uq_publish(L, ui, qctr, nunits, ctl.wait_ns);
@@ -830,22 +840,26 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
                         for (int g = 0; g < SYN_GROUPS; ++g) {
                             const int hb = h3 + g, c = 2 * hb + cc;
                             if (hb >= nhb || c >= nch) continue;
-                            if (used & (1u << g)) {
-                                if (!tc::mbar_wait(&L.empty[g], (ebits >> g) & 1u, ctl.wait_ns)) {
-                                    set_err(err, 5);
-                                    ok = false;
-                                    break;
+                            for (int half = 0; half < 2; ++half) {  // the chunk's K-step halves, 8N uint4 each
+                                const int sg = 2 * g + half;
+                                if (used & (1u << sg)) {
+                                    if (!tc::mbar_wait(&L.empty[sg], (ebits >> sg) & 1u, ctl.wait_ns)) {
+                                        set_err(err, 5);
+                                        ok = false;
+                                        break;
+                                    }
+                                    ebits ^= 1u << sg;
                                 }
-                                ebits ^= 1u << g;
+                                used |= 1u << sg;
+                                if (ctl.inject == 1 && blockIdx.x == 0 && !withheld) {  // failure-detection test
+                                    withheld = true;
+                                    continue;
+                                }
+                                tc::mbar_arrive_expect_tx(&L.full[sg], B_STAGE);
+                                tc::bulk_g2s(smem + sg * STAGE + ANA_A_STAGE,
+                                             src + (int64_t)c * (16 * N) + half * (8 * N), B_STAGE, &L.full[sg]);
                             }
-                            used |= 1u << g;
-                            if (ctl.inject == 1 && blockIdx.x == 0 && !withheld) {  // failure-detection test
-                                withheld = true;
-                                continue;
-                            }
-                            tc::mbar_arrive_expect_tx(&L.full[g], B_STAGE);
-                            tc::bulk_g2s(smem + g * STAGE + A_STAGE, src + (int64_t)c * (16 * N), B_STAGE,
-                                         &L.full[g]);
+                            if (!ok) break;
                         }
                     }
                 }
@@ -1146,7 +1160,7 @@ template <int N> constexpr int nsets() { return 512 / (2 * N) > 4 ? 4 : 512 / (2
 
 template <int N, bool BF16>
 static int launch_syn(hb_batched_plan *bp, cudaStream_t st) {
-    const int smem = tc_smem<SYN_GROUPS, N, SYN_PW>();
+    const int smem = tc_smem<2 * SYN_GROUPS, N, SYN_PW, ANA_A_STAGE + ana_b_stage<N>()>();
     constexpr int S = nsets<N>();
     HB_CUDA_TRY(cudaFuncSetAttribute(synth_tc_kernel<N, BF16, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     const int grid = std::min(bp->n_syn, sm_count());
