@@ -395,15 +395,17 @@ __global__ void coef_table_kernel(int lmax, const int64_t *__restrict__ blk_ofs,
     for (int64_t i = threadIdx.x; i < nb * 256; i += blockDim.x) coef_scalar(m + (int)i, m, lmax, tab[b0 * 256 + i]);
 }
 
-// Evanescent skip ranges.  Below its turning point the FP32 recursion state of a ring pair carries
-// an exponent e < 0 (|lambda| < 2^-32; its values are gated to exact zeros) and e never decreases
-// with l, so every value before a checkpoint at which all rows have e < 0 is an exact zero:
+// Evanescent skip ranges.  Below its turning point the plan's checkpoint state of a ring pair
+// carries an exponent e < 0 (|lambda| < 2^-32) and e never decreases with l, so every value before
+// a checkpoint at which all rows have e < 0 is below 2^-32 (the tensor-core kernels' recursion,
+// scaled by LS = 256, gates the values below 2^-40 to zeros and keeps the rest):
 //   syn[m * npb + pb] = leading 128-l half-blocks of (m, pair block pb) that end at such a
 //     checkpoint (checkpoint h at l = m + 128 h: h even ck, h odd the mid-block table; the
 //     half-block that reaches past lmax is never skipped);
 //   ana[blk_ofs[m] + jb] = leading 32-pair chunks whose rows all have e < 0 at the end of the
 //     256-l block jb (none when the block reaches past lmax; at least one chunk stays).
-// The kernels skip those chunks entirely (no recursion, no tile, no MMA): same results, less work.
+// The kernels skip those chunks entirely (no recursion, no tile, no MMA): the values they drop are
+// below 2^-32 of the normalised lambda, far under the 1e-5 error bar.
 __global__ void __launch_bounds__(128) skip_table_kernel(GeomDev g, int lmax, const int64_t *__restrict__ blk_ofs,
                                                          const float4 *__restrict__ ck, const float4 *__restrict__ ckh,
                                                          int *__restrict__ syn, int *__restrict__ ana) {
@@ -645,7 +647,11 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
     constexpr int STAGE = ANA_A_STAGE + B_STAGE;   // 16-K A tiles [q][h][128 x 16]
     constexpr uint32_t IDESC = tc::idesc_f16kind(128, N, 0, 0, BF16);
     constexpr uint32_t IDESC2 = tc::idesc_f16kind(128, 2 * N, 0, 0, BF16);
-    constexpr float LS = BF16 ? 1.0f : 256.0f;  // lambda scale (|lambda| < 2^7 -> < 2^15 in half)
+    // lambda scale, a power of two in both formats: |lambda| < 2^7 -> < 2^15 in IEEE half.  It
+    // also sets where a row leaves its gated state (e < 0: |lambda LS| < 2^-32), so 256 moves that
+    // 8 bits of lambda earlier and more chunks take the unchecked path (BF16 analysis measured
+    // 22.1 -> 19.4 ms at nside 2048, 64 maps, against LS = 1)
+    constexpr float LS = 256.0f;
     // S accumulator sets in S/2 (hi*hi, cross products) pairs, the k-th chunk of a unit (in MMA
     // order) using pair k mod S/2 (issue_stage): the tensor core's FP32 accumulation error grows
     // with the number of accumulate steps into one set; the epilogue sums the sets in IEEE FP32.
@@ -903,7 +909,7 @@ __global__ void __launch_bounds__(ANA_THREADS, 1)
     constexpr int STAGE = ANA_A_STAGE + B_STAGE;
     constexpr uint32_t IDESC = tc::idesc_f16kind(128, N, 1, 0, BF16);
     constexpr uint32_t IDESC2 = tc::idesc_f16kind(128, 2 * N, 1, 0, BF16);
-    constexpr float LS = BF16 ? 1.0f : 256.0f;
+    constexpr float LS = 256.0f;  // lambda scale: as in synth_tc_kernel
     constexpr int TCOLS = (2 * N * S < 32) ? 32 : 2 * N * S;  // S accumulator sets, see synth_tc_kernel
     static_assert(2 * N * S <= 512, "TMEM holds 512 columns");
     static_assert(S >= 2 && S % 2 == 0, "accumulator sets come in (hi, cross) pairs");
