@@ -30,8 +30,10 @@
 namespace hb {
 
 constexpr uint64_t HB_TC_WAIT_NS = 2000000000ull;  // 2 s
-constexpr int A_TILE = 8192;       // 128 rows x 32 K x bf16
-constexpr int A_STAGE = 4 * A_TILE;  // [parity][hi/lo]
+// one pipeline stage of either tensor-core kernel: one MMA K-step (16 K) per parity
+constexpr int TC_A_TILE = 4096;                // 128 rows x 16 K x 16-bit
+constexpr int TC_A_STAGE = 4 * TC_A_TILE;      // [parity][hi/lo]
+template <int N> constexpr int tc_b_stage() { return 4 * N * 32; }  // [q][h][N x 16] 16-bit
 
 struct TcGroup {
     GeomDev g;
@@ -95,12 +97,14 @@ __device__ __forceinline__ float block_pow2_scale(float vmax) {
 
 // The prep kernels (prep_alm_tiles_kernel, prep_f_tiles_kernel) turn runs of 8 consecutive K
 // positions into the hi/lo rows of the K-major core matrices (row n = 2 map + re/im; element
-// (n, k) at (n%8)*8 + (n/8)*256 + (k/8)*64 + k%8), written as 16-byte stores.  Rows 8j .. 8j+7
+// (n, k) of a 16-K tile at (n%8)*8 + (n/8)*128 + (k/8)*64 + k%8), written as 16-byte stores.  Rows 8j .. 8j+7
 // (maps 4j .. 4j+3) of one k8 group are one 128-byte segment, so both kernels work on quads of
 // maps and let 4 lanes write one segment's interleaved rows in the same instruction (scattered
 // 16-byte stores from separate instructions cost one L2 request each and ran at half the rate).
-template <bool BF16, int KC = 32>  // KC: K positions per chunk (32: synthesis, 16: analysis)
+// tile set [qh][hi/lo][N rows x 16 K]; g: the k8 group (0 or 1) within the 16 K
+template <bool BF16>
 __device__ __forceinline__ void store_rows8(uint4 *chunk, int N, int qh, int n, int g, const float (&v)[8]) {
+    constexpr int KC = 16;
     uint4 hi, lo;
     tc::split8<BF16>(v, hi, lo);
     const int64_t e = (int64_t)(2 * qh) * N * KC + (n & 7) * 8 + (n >> 3) * (8 * KC) + g * 64;  // 16-bit elements
@@ -109,7 +113,8 @@ __device__ __forceinline__ void store_rows8(uint4 *chunk, int N, int qh, int n, 
 }
 
 // alm [map][nalm] complex64 -> per (m, 64-l chunk) the synthesis B tiles
-// [q][h][N rows x 32 K (l = l0 + 2k + q)], chunks of m covering l = m .. lmax (zero past lmax).
+// [K-step half][q][h][N rows x 16 K] (l = l0 + 32 half + 2k + q), chunks of m covering
+// l = m .. lmax (zero past lmax).
 // Work item = (m, quad of 4 maps): the 4 maps' rows of one (chunk, k8 group, q, h) are one
 // 128-byte segment of the tile.  F16: a first sweep over the item's alm takes the maximum |value|
 // per (m, map) (the power-of-two scale, as block_pow2_scale); BF16 uses scale 1 (a power-of-two
@@ -200,8 +205,8 @@ __global__ void __launch_bounds__(PA_THREADS, 4) prep_alm_tiles_kernel(const TcG
                     re[k] = v.x * sc;
                     im[k] = v.y * sc;
                 }
-                store_rows8<BF16, 16>(chunk, N, q, 2 * b, g & 1, re);
-                store_rows8<BF16, 16>(chunk, N, q, 2 * b + 1, g & 1, im);
+                store_rows8<BF16>(chunk, N, q, 2 * b, g & 1, re);
+                store_rows8<BF16>(chunk, N, q, 2 * b + 1, g & 1, im);
             }
             __syncthreads();  // every thread is done with this stage's buffer before it is refilled
         }
@@ -313,10 +318,10 @@ __global__ void __launch_bounds__(PF_THREADS, 3) prep_f_tiles_kernel(const TcGro
                     orr[i] = (f.x - f.z) * sc;
                     oi[i] = (f.y - f.w) * sc;
                 }
-                store_rows8<BF16, 16>(chunk, N, 0, 2 * b, g, er);
-                store_rows8<BF16, 16>(chunk, N, 0, 2 * b + 1, g, ei);
-                store_rows8<BF16, 16>(chunk, N, 1, 2 * b, g, orr);
-                store_rows8<BF16, 16>(chunk, N, 1, 2 * b + 1, g, oi);
+                store_rows8<BF16>(chunk, N, 0, 2 * b, g, er);
+                store_rows8<BF16>(chunk, N, 0, 2 * b + 1, g, ei);
+                store_rows8<BF16>(chunk, N, 1, 2 * b, g, orr);
+                store_rows8<BF16>(chunk, N, 1, 2 * b + 1, g, oi);
             }
             __syncthreads();  // every thread is done with this stage's buffer before it is refilled
         }
@@ -442,23 +447,20 @@ __global__ void __launch_bounds__(128) skip_table_kernel(GeomDev g, int lmax, co
 }
 
 // ------------------------------------------------------------------------------------ pipeline
-// Both kernels: the producer warps (8 in analysis, 12 in synthesis) generate A tiles (recursion,
-// one ring pair or l row per thread) and run the epilogue (TMEM lane quarter = warp % 4, column
-// blocks split between the warps of one quarter); the next warp allocates TMEM and one of its
-// threads issues the MMAs; one thread of the last warp streams the pre-split batch tiles with
-// bulk copies.  Several producer warps per SM sub-partition hide the recursion's dependency
-// latency.  The recursion restarts from the plan's FP64 checkpoints at every 128 l (block
-// starts and the mid-block table), which is what lets several warps share one row's l range.
-template <int N> constexpr int tc_b_stage() { return 4 * N * 64; }  // [q][h][N x 32] 16-bit
-// synthesis: SYN_GROUPS groups of four producer warps, group g owning stage g
+// Both kernels: twelve producer warps generate A tiles (recursion, one ring pair per thread) and
+// run the epilogue (TMEM lane quarter = warp % 4, column blocks split between the warps of one
+// quarter); the next warp allocates TMEM and one of its threads issues the MMAs; one thread of
+// the last warp streams the pre-split batch tiles with bulk copies.  Several producer warps per
+// SM sub-partition hide the recursion's dependency latency.  The recursion restarts from the
+// plan's FP64 checkpoints (every 128 l in the synthesis: block starts and the mid-block table;
+// every 64 l in the analysis: the quarter tables too), which is what lets several warps share
+// one row's l range.  Stages hold one 16-K MMA step per parity (TC_A_STAGE + tc_b_stage).
+// synthesis: SYN_GROUPS groups of four producer warps, group g owning stages 2g and 2g + 1
 constexpr int SYN_GROUPS = 3;
 constexpr int SYN_PW = 4 * SYN_GROUPS;
 constexpr int SYN_THREADS = 32 * (SYN_PW + 2);
 // analysis: ANA_ST stages of 16 ring pairs (one MMA K-step per parity), two producer warps per
 // stage, each thread one (pair, l-quarter) of the unit's 256-l block
-constexpr int ANA_A_TILE = 4096;               // 128 rows x 16 K x bf16
-constexpr int ANA_A_STAGE = 4 * ANA_A_TILE;    // [parity][hi/lo]
-template <int N> constexpr int ana_b_stage() { return 4 * N * 32; }  // [q][h][N x 16] 16-bit
 constexpr int ANA_ST = 6;
 constexpr int ANA_PW = 2 * ANA_ST;
 constexpr int ANA_THREADS = 32 * (ANA_PW + 2);
@@ -472,7 +474,7 @@ constexpr int ANA_THREADS = 32 * (ANA_PW + 2);
 constexpr int UQ = 8;
 // stages, then per producer warp 128 coefficients (float2) and 64 inverse scales, then barriers
 // and the unit ring
-template <int ST, int N, int PW, int STAGE = A_STAGE + tc_b_stage<N>()> constexpr int tc_smem() {
+template <int ST, int N, int PW, int STAGE = TC_A_STAGE + tc_b_stage<N>()> constexpr int tc_smem() {
     return ST * STAGE + PW * (128 * 8 + 64 * 4) + 320;
 }
 
@@ -484,7 +486,7 @@ struct TcSmem {
     uint64_t *uq_full, *uq_empty;  // unit ring barriers, UQ each
     int *uq;                       // unit ring slots
 };
-template <int ST, int N, int PW, int STAGE = A_STAGE + tc_b_stage<N>()>
+template <int ST, int N, int PW, int STAGE = TC_A_STAGE + tc_b_stage<N>()>
 __device__ __forceinline__ TcSmem tc_smem_layout(uint8_t *smem, int warp) {
     const int pw = warp < PW ? warp : 0;
     TcSmem L;
@@ -551,7 +553,7 @@ __device__ __forceinline__ void load_inv_scales(float *inv, const float *scl, in
 }
 
 // write 8 even + 8 odd split values of one A-tile row group: A + {0,1,2,3} * AT + off
-template <bool BF16, int AT = A_TILE>
+template <bool BF16, int AT = TC_A_TILE>
 __device__ __forceinline__ void store_split(uint8_t *A, int off, const float (&ev)[8], const float (&od)[8]) {
     uint4 hi, lo;
     tc::split8<BF16>(ev, hi, lo);
@@ -562,38 +564,32 @@ __device__ __forceinline__ void store_split(uint8_t *A, int off, const float (&e
     *reinterpret_cast<uint4 *>(A + 3 * AT + off) = lo;
 }
 
-// The MMAs of one stage (2 parities x KS K-steps x 3 split passes; KS = 2: 32 K per stage,
-// tiles of 128 rows x 32 K; KS = 1: 16 K).  The hi*hi products go to
+// The MMAs of one stage (2 parities x 3 split passes, one 16-K step each).  The hi*hi products go to
 // the "hi" set of a set pair, the two cross products (about 2^-11 smaller) to its "lo" set: the
 // tensor core's FP32 accumulation loses about one ulp of the accumulator per MMA, so keeping the
 // large products' set free of the cross products cuts the steps that round the result by 3x.
 // TMEM columns of set pair j, parity q: hi at 4N j + 2N q, lo N further.  A_hi times the
 // batch tiles (hi | lo), which lie back to back in shared memory, is one MMA of width 2N into
-// (hi | lo); A_lo times B_hi is a second one into lo.  Live chunk i of a unit uses set pair
-// j = i mod (S/2); `first` (the first S/2 live chunks) starts each pair afresh.
-template <int N, int KS = 2>
+// (hi | lo); A_lo times B_hi is a second one into lo.  `first` starts the pair afresh (the
+// stage's MMAs overwrite instead of accumulating).
+template <int N>
 __device__ __forceinline__ void issue_stage(uint32_t tmem, uint32_t a0, int pair, bool first, uint32_t idesc_n,
                                             uint32_t idesc_2n) {
     // one cta_group::1 MMA is at most 256 wide and N a multiple of 16; the 2N-wide MMA reads the
-    // lo batch tile as B rows N .. 2N-1, so it must follow the hi tile directly (N * 32 KS bytes)
+    // lo batch tile as B rows N .. 2N-1, so it must follow the hi tile directly (N * 32 bytes)
     static_assert(2 * N <= 256 && N % 16 == 0, "the hi x (hi | lo) MMA needs 2N <= 256, N % 16 == 0");
-    static_assert(KS == 1 || KS == 2, "16 or 32 K per stage");
-    // core matrices (8 rows x 16 bytes): 128 bytes apart along K, 256 KS bytes apart along the rows
-    constexpr int AT = 4096 * KS, BT = N * 32 * KS, SBO = 256 * KS;
-    static_assert(KS != 2 || (AT == A_TILE && 4 * BT == tc_b_stage<N>()), "synthesis tile layout");
+    // core matrices (8 rows x 16 bytes): 128 bytes apart along K, 256 bytes apart along the rows
+    constexpr int AT = TC_A_TILE, BT = N * 32, SBO = 256;
+    static_assert(4 * BT == tc_b_stage<N>(), "B tiles [q][h][N x 16]");
     const uint32_t b0 = a0 + 4 * AT;
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
         const uint32_t d = tmem + pair * 4 * N + q * 2 * N;
-#pragma unroll
-        for (int k = 0; k < KS; ++k) {
-            const uint64_t ah = tc::sdesc(a0 + (q * 2 + 0) * AT + k * 256, 128, SBO);
-            const uint64_t al = tc::sdesc(a0 + (q * 2 + 1) * AT + k * 256, 128, SBO);
-            const uint64_t bh = tc::sdesc(b0 + (q * 2 + 0) * BT + k * 256, 128, SBO);
-            const uint32_t acc = (!first || k > 0) ? 1u : 0u;
-            tc::mma_bf16(d, ah, bh, idesc_2n, acc);  // B rows N .. 2N-1: the lo tile
-            tc::mma_bf16(d + N, al, bh, idesc_n, 1u);
-        }
+        const uint64_t ah = tc::sdesc(a0 + (q * 2 + 0) * AT, 128, SBO);
+        const uint64_t al = tc::sdesc(a0 + (q * 2 + 1) * AT, 128, SBO);
+        const uint64_t bh = tc::sdesc(b0 + (q * 2 + 0) * BT, 128, SBO);
+        tc::mma_bf16(d, ah, bh, idesc_2n, first ? 0u : 1u);  // B rows N .. 2N-1: the lo tile
+        tc::mma_bf16(d + N, al, bh, idesc_n, 1u);
     }
 }
 
@@ -626,7 +622,7 @@ __device__ __forceinline__ void gen_half_syn(Rec &R, const float2 *cf, uint8_t *
     for (int grp = 0; grp < 2; ++grp) {
         float ev[8], od[8];
         gen16<CHECKED>(R, cf + 16 * grp, ev, od);
-        store_split<BF16, ANA_A_TILE>(A, off + grp * 128, ev, od);
+        store_split<BF16, TC_A_TILE>(A, off + grp * 128, ev, od);
     }
 }
 
@@ -643,8 +639,8 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
     synth_tc_kernel(const TcGroup *__restrict__ groups, const int4 *__restrict__ units, int nunits, int *err,
                     int *qctr, TcCtl ctl) {
     constexpr int ST = 2 * SYN_GROUPS;
-    constexpr int B_STAGE = ana_b_stage<N>();      // [q][h][N x 16] 16-bit: half a chunk's alm tiles
-    constexpr int STAGE = ANA_A_STAGE + B_STAGE;   // 16-K A tiles [q][h][128 x 16]
+    constexpr int B_STAGE = tc_b_stage<N>();      // [q][h][N x 16] 16-bit: half a chunk's alm tiles
+    constexpr int STAGE = TC_A_STAGE + B_STAGE;   // 16-K A tiles [q][h][128 x 16]
     constexpr uint32_t IDESC = tc::idesc_f16kind(128, N, 0, 0, BF16);
     constexpr uint32_t IDESC2 = tc::idesc_f16kind(128, 2 * N, 0, 0, BF16);
     // lambda scale, a power of two in both formats: |lambda| < 2^7 -> < 2^15 in IEEE half.  It
@@ -805,7 +801,7 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
                                 fbits ^= 1u << sg;
                                 tc::fence_after();
                                 // the second half accumulates onto the first
-                                issue_stage<N, 1>(tmem, tc::smem_u32(smem + sg * STAGE), k % (S / 2),
+                                issue_stage<N>(tmem, tc::smem_u32(smem + sg * STAGE), k % (S / 2),
                                                   half == 0 && k < S / 2, IDESC, IDESC2);
                                 tc::mma_commit(&L.empty[sg]);
                             }
@@ -862,7 +858,7 @@ __global__ void __launch_bounds__(SYN_THREADS, 1)
                                     continue;
                                 }
                                 tc::mbar_arrive_expect_tx(&L.full[sg], B_STAGE);
-                                tc::bulk_g2s(smem + sg * STAGE + ANA_A_STAGE,
+                                tc::bulk_g2s(smem + sg * STAGE + TC_A_STAGE,
                                              src + (int64_t)c * (16 * N) + half * (8 * N), B_STAGE, &L.full[sg]);
                             }
                             if (!ok) break;
@@ -890,7 +886,7 @@ __device__ __forceinline__ void gen_chunk_ana(Rec &R, const float2 *cf, uint8_t 
     for (int grp = 0; grp < 4; ++grp) {
         float ev[8], od[8];
         gen16<CHECKED>(R, cf + 16 * grp, ev, od);
-        store_split<BF16, ANA_A_TILE>(A, off0 + grp * 256, ev, od);
+        store_split<BF16, TC_A_TILE>(A, off0 + grp * 256, ev, od);
     }
 }
 // Unit = (m, 256-l block); its chunks of 16 ring pairs go to stage c' % ANA_ST (c' = running
@@ -905,8 +901,8 @@ __global__ void __launch_bounds__(ANA_THREADS, 1)
     anal_tc_kernel(const TcGroup *__restrict__ groups, const int4 *__restrict__ units, int nunits, float2 *alm_out,
                    int *err, int *qctr, const float *__restrict__ fl, TcCtl ctl) {
     constexpr int ST = ANA_ST;
-    constexpr int B_STAGE = ana_b_stage<N>();
-    constexpr int STAGE = ANA_A_STAGE + B_STAGE;
+    constexpr int B_STAGE = tc_b_stage<N>();
+    constexpr int STAGE = TC_A_STAGE + B_STAGE;
     constexpr uint32_t IDESC = tc::idesc_f16kind(128, N, 1, 0, BF16);
     constexpr uint32_t IDESC2 = tc::idesc_f16kind(128, 2 * N, 1, 0, BF16);
     constexpr float LS = 256.0f;  // lambda scale: as in synth_tc_kernel
@@ -1058,7 +1054,7 @@ __global__ void __launch_bounds__(ANA_THREADS, 1)
                         break;
                     }
                     tc::fence_after();
-                    issue_stage<N, 1>(tmem, tc::smem_u32(smem + s * STAGE), (c - c0) % (S / 2), c - c0 < S / 2,
+                    issue_stage<N>(tmem, tc::smem_u32(smem + s * STAGE), (c - c0) % (S / 2), c - c0 < S / 2,
                                       IDESC, IDESC2);
                     tc::mma_commit(&L.empty[s]);
                 }
@@ -1096,7 +1092,7 @@ __global__ void __launch_bounds__(ANA_THREADS, 1)
                         break;
                     }
                     tc::mbar_arrive_expect_tx(&L.full[s], B_STAGE);
-                    tc::bulk_g2s(smem + s * STAGE + ANA_A_STAGE, src + (int64_t)c * (B_STAGE / 16), B_STAGE, &L.full[s]);
+                    tc::bulk_g2s(smem + s * STAGE + TC_A_STAGE, src + (int64_t)c * (B_STAGE / 16), B_STAGE, &L.full[s]);
                 }
             }
         }
@@ -1166,7 +1162,7 @@ template <int N> constexpr int nsets() { return 512 / (2 * N) > 4 ? 4 : 512 / (2
 
 template <int N, bool BF16>
 static int launch_syn(hb_batched_plan *bp, cudaStream_t st) {
-    const int smem = tc_smem<2 * SYN_GROUPS, N, SYN_PW, ANA_A_STAGE + ana_b_stage<N>()>();
+    const int smem = tc_smem<2 * SYN_GROUPS, N, SYN_PW, TC_A_STAGE + tc_b_stage<N>()>();
     constexpr int S = nsets<N>();
     HB_CUDA_TRY(cudaFuncSetAttribute(synth_tc_kernel<N, BF16, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     const int grid = std::min(bp->n_syn, sm_count());
@@ -1178,7 +1174,7 @@ static int launch_syn(hb_batched_plan *bp, cudaStream_t st) {
 }
 template <int N, bool BF16>
 static int launch_ana(hb_batched_plan *bp, float2 *alm_out, const float *fl, cudaStream_t st) {
-    const int smem = tc_smem<ANA_ST, N, ANA_PW, ANA_A_STAGE + ana_b_stage<N>()>();
+    const int smem = tc_smem<ANA_ST, N, ANA_PW, TC_A_STAGE + tc_b_stage<N>()>();
     constexpr int S = nsets<N>();
     HB_CUDA_TRY(cudaFuncSetAttribute(anal_tc_kernel<N, BF16, S>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem));
     const int grid = std::min(bp->n_ana, sm_count());
