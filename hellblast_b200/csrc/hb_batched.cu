@@ -46,12 +46,12 @@ struct TcGroup {
     const float4 *ckq1, *ckq3;  // ... at l0 + 64 and l0 + 192 (analysis l-quarters)
     const float2 *coef;      // recursion coefficients (A_l, B_l): [(blk_ofs[m] + b) * 256 + i], l = m + 256 b + i
     // synthesis
-    const uint4 *alm_tiles;  // [chunk][4][N x 32] bf16, chunk = tile_ofs[m] + c
+    const uint4 *alm_tiles;  // [chunk][K-step half][4][N x 16] 16-bit, chunk = tile_ofs[m] + c
     const int64_t *alm_tile_ofs;
     float2 *Gm;              // [map][m][pair][2]
     int64_t gm_stride;
     // analysis
-    const uint4 *g_tiles;    // [m][pc][4][N x 32] 16-bit
+    const uint4 *g_tiles;    // [m][16-pair chunk][4][N x 16] 16-bit
     float *dscale;           // [mmax+1][N/2] power-of-two scale of the batch operand per (m, map column)
     int64_t alm_out_ofs;     // this group's first alm in the caller's output buffer (complex elements)
     int64_t alm_stride;
